@@ -1,0 +1,168 @@
+/* uqc.h - C ABI of the B200 implementation of UQCreator's IPM hot path.
+ *
+ * The hot path is one explicit time step of the intrusive polynomial moment
+ * method: per-cell dual Newton closure, reconstruction at quadrature nodes,
+ * kinetic numerical flux projected onto the moments, explicit Euler update.
+ * Plain pointers and sizes only; every call returns an int status (0 = ok,
+ * negative = error) and never exits the process. uqc_last_error() gives the
+ * message of the last failed call on a handle.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to UQCreator's code/src). The reference calls exit(EXIT_FAILURE) on every
+ * error (closure.cpp:180-192, vectorspace.cpp:166-170, settings.cpp:316-322);
+ * here the same conditions return a status.
+ *
+ * State layouts (per cell, nS states x nT moments):
+ *   UQC_LAYOUT_REF          the reference's Matrix(nS, nT): column-major,
+ *                           element (s, i) at i * nS + s (matrix.cpp:8,107)
+ *   UQC_LAYOUT_STATE_MAJOR  element (s, i) at s * nT + i, the order of the
+ *                           reference's gradient vectors (closure.cpp:245)
+ * Cells are contiguous, nS * nT doubles each, nT = the finest level's size.
+ *
+ * Threading: a handle owns a CUDA stream (the one passed at creation, or its
+ * own). Calls on one handle must be serialised by the caller; distinct
+ * handles may be used concurrently from different threads.
+ */
+#ifndef UQC_H
+#define UQC_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct uqc_solver uqc_solver;
+
+enum uqc_status_code {
+    UQC_OK               = 0,
+    UQC_ERR_ARGUMENT     = -1, /* bad pointer, size or enum value */
+    UQC_ERR_CONFIG       = -2, /* invalid or unsupported TOML configuration */
+    UQC_ERR_CUDA         = -3, /* CUDA runtime error (message has the name) */
+    UQC_ERR_NOT_CONVERGED = -4, /* at least one cell's Newton failed; see uqc_cell_status */
+    UQC_ERR_MEMORY       = -5, /* device allocation failed */
+    UQC_ERR_STATE        = -6, /* call out of order (e.g. step before init) */
+    UQC_ERR_CAPACITY     = -7  /* request exceeds a fixed capacity */
+};
+
+enum uqc_layout { UQC_LAYOUT_REF = 0, UQC_LAYOUT_STATE_MAJOR = 1 };
+
+/* Hessian precision of the Newton closure.
+ * UQC_FP64:  all-FP64 (the reference's arithmetic).
+ * UQC_MIXED: Hessian assembled on tensor cores (BF16 inputs, FP32
+ *            accumulation in TMEM) and factored in FP32; the residual, the
+ *            line-search test and the moment update stay FP64; cells whose FP32
+ *            pivot test fails are refactored in FP64. */
+enum uqc_precision { UQC_FP64 = 0, UQC_MIXED = 1 };
+
+/* Per-cell closure status (uqc_cell_status). */
+enum uqc_cell_code {
+    UQC_CELL_CONVERGED     = 0,
+    UQC_CELL_MAX_ITER      = 1, /* "Newton did not converge" (closure.cpp:191-192) */
+    UQC_CELL_LINE_SEARCH   = 2, /* "too many refinement steps" (closure.cpp:180-183) */
+    UQC_CELL_NOT_PD        = 3, /* posv info > 0 (vectorspace.cpp:166-170) */
+    UQC_CELL_NONFINITE     = 4  /* moments or duals not finite on entry */
+};
+
+typedef struct uqc_info {
+    int n_cells, n_states, n_total, n_quad, n_levels, dim_xi, n_faces, mesh_dim;
+    int n_total_level[16]; /* moments per refinement level */
+    int precision;         /* uqc_precision in use */
+    int newton_mode;       /* 0 reference SolveClosure, 1 guarded, 2 SolveClosureSafe */
+    double t;              /* simulated time */
+    long long steps;       /* time steps taken */
+} uqc_info;
+
+typedef struct uqc_step_info {
+    double t, dt, residual;   /* after the last step (momentsolver.cpp:134,149-152) */
+    int steps;                /* steps taken by this call */
+    int failed_cells;         /* cells whose closure did not converge */
+    long long newton_iterations; /* summed over cells and steps of this call */
+    long long line_search_trials;
+    int active_cells;         /* cells that needed Newton iterations in the last step */
+} uqc_step_info;
+
+/* ---- lifecycle and configuration ------------------------------------ */
+
+/* Creates a solver from a UQCreator TOML input file: Settings(toml)
+ * (settings.h:103, settings.cpp:22-323) + Problem::Create (problem.cpp:18-42) +
+ * Mesh::Create (mesh.cpp:19-32) + Closure::Create (closure.cpp:94-131) +
+ * MomentSolver(settings, mesh, problem) (momentsolver.h:139). cuda_stream may be
+ * NULL (the handle creates its own stream). On error *out is NULL and the
+ * message is copied to err (when err != NULL). */
+int uqc_create_from_file( const char* toml_path, void* cuda_stream, uqc_solver** out, char* err, int err_len );
+/* Same, from TOML text in memory. */
+int uqc_create_from_string( const char* toml_text, void* cuda_stream, uqc_solver** out, char* err, int err_len );
+void uqc_destroy( uqc_solver* h );                        /* ~MomentSolver (momentsolver.cpp:32-35) */
+const char* uqc_last_error( const uqc_solver* h );
+int uqc_get_info( const uqc_solver* h, uqc_info* out );
+int uqc_set_precision( uqc_solver* h, int precision );
+/* Closure::SetMaxIterations (closure.cpp:341) and the epsilon of settings.cpp:314. */
+int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newton_mode );
+
+/* Host copies of the tables of Closure::Closure (closure.cpp:16-84):
+ * phi[k * nT + i] = phiTilde(k, i), phi_wf = phiTildeWf, xi[k * dimXi + l],
+ * w[k]. Any pointer may be NULL. */
+int uqc_get_tables( const uqc_solver* h, double* phi, double* phi_wf, double* xi, double* w );
+/* Host copies of the mesh geometry (Cell/Line/Triangle, cell.h:52-77):
+ * per cell area, max edge, centre (2); per face unit normal (2), scaled
+ * normal (2), neighbour id (ghost id = n_cells), boundary flag. */
+int uqc_get_geometry( const uqc_solver* h, double* area, double* max_edge, double* center, double* unit_normal,
+                      double* scaled_normal, int* neighbor, int* boundary );
+
+/* ---- state ------------------------------------------------------------ */
+
+/* Initial moments and duals on the device: MomentSolver::SetupIC
+ * (momentsolver.cpp:535-563) and SetDuals without restart (:463-485). */
+int uqc_init_state( uqc_solver* h );
+/* Copies caller-owned host state to the device (u, lambda: n_cells * nS * nT
+ * doubles in `layout`; level: n_cells refinement levels or NULL to keep). */
+int uqc_upload_state( uqc_solver* h, const double* u, const double* lambda, const unsigned* level, int layout, double t );
+int uqc_download_state( uqc_solver* h, double* u, double* lambda, unsigned* level, int layout );
+
+/* ---- hot path ----------------------------------------------------------- */
+
+/* Batched Closure::SolveClosure (closure.cpp:133-193) on the resident state:
+ * every cell's duals solved in place for its current refinement level. */
+int uqc_solve_closure( uqc_solver* h, uqc_step_info* info );
+/* Closure status and Newton iterations per cell from the last closure solve. */
+int uqc_cell_status( uqc_solver* h, int* status, int* iterations );
+/* n_steps time steps: the body of MomentSolver::Solve (momentsolver.cpp:79-152)
+ * with ExplicitEuler::Advance (expliciteuler.cpp:8-75). Stops early once
+ * t >= tEnd or residual <= minResidual (the loop condition of :79). */
+int uqc_step( uqc_solver* h, int n_steps, uqc_step_info* info );
+/* MomentSolver::Solve's time loop to the configured tEnd (or t_end > 0). */
+int uqc_run( uqc_solver* h, double t_end, uqc_step_info* info );
+/* Mean and variance per cell and state (MomentSolver::WriteMeanAndVar,
+ * momentsolver.cpp:302-328): out[j * 2 nS + s] = E, out[j * 2 nS + nS + s] = Var. */
+int uqc_mean_var( uqc_solver* h, double* out );
+
+/* Drop-in for Closure::SolveClosure on caller-owned HOST arrays (the call a
+ * GpuClosure adapter makes): n cells of (lambda, u) in `layout`, solved for
+ * n_total[j] moments (NULL = finest). Copies in, solves, copies lambda back.
+ * status[j] gets a uqc_cell_code (may be NULL). */
+int uqc_closure_solve_host( uqc_solver* h, int n, double* lambda, const double* u, const unsigned* n_total, int layout,
+                            int* status );
+/* Same on caller-owned DEVICE arrays in UQC_LAYOUT_STATE_MAJOR, enqueued on
+ * the handle's stream; no host synchronisation. */
+int uqc_closure_solve_device( uqc_solver* h, int n, double* d_lambda, const double* d_u, const unsigned* d_n_total,
+                              int* d_status );
+
+/* ---- introspection ----------------------------------------------------- */
+
+/* Device time (ms) of the kernels of the last uqc_step call, by phase:
+ * [0] closure + reconstruction, [1] flux + update, [2] total. */
+int uqc_last_timing( uqc_solver* h, float* ms3 );
+/* Device pointers of the resident state (for zero-copy callers): u, lambda. */
+int uqc_device_state( uqc_solver* h, double** d_u, double** d_lambda );
+/* Number of kernel launches issued by the last uqc_step / uqc_solve_closure. */
+int uqc_last_launch_count( uqc_solver* h );
+/* CUDA stream of the handle (cudaStream_t). */
+void* uqc_stream( uqc_solver* h );
+
+/* Seeded jittered triangle mesh of the "tri_jitter" workloads (host only):
+ * xy[2 (nx+1)(ny+1)], node_boundary[(nx+1)(ny+1)], tri[3 * 2 nx ny]. */
+int uqc_mesh_tri_jitter( int nx, int ny, double jitter, unsigned long long seed, double* xy, int* node_boundary, int* tri );
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UQC_H */

@@ -1,0 +1,147 @@
+"""CUDA path vs the oracle, through the C ABI (needs a B200).
+
+Tolerances: the plain FP64 GPU form must reproduce the FP64 oracle's mean and
+variance of every state within relative L1 1e-10 (the bound the hot path
+states); duals and moments are compared elementwise at 1e-9 relative (GPU
+exp/pow and reduction order differ from glibc's at the last bits, and Newton
+amplifies them by at most the Hessian's condition number).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from uqcreator_b200 import Solver, workloads as W, LAYOUT_REF, LAYOUT_STATE_MAJOR, UqcError
+
+from ._util import rel_l1
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+TOL_MV = 1e-10
+
+
+def _pair(toml):
+    s = Solver(toml)
+    o = Oracle(toml, W.mesh_for(toml))
+    s.init_state(); o.init_state()
+    return s, o
+
+
+def test_init_state_matches_oracle():
+    for toml in (W.burgers1d(), W.euler2d(nx=12, ny=3), W.shallow_water1d(ncells=200), W.euler2d_3u(nx=4, ny=2)):
+        s, o = _pair(toml)
+        us, ls, vs = s.download_state()
+        uo, lo, vo = o.get_state()
+        np.testing.assert_allclose(us, uo, rtol=1e-13, atol=1e-14)
+        np.testing.assert_allclose(ls, lo, rtol=1e-12, atol=1e-13)
+        np.testing.assert_array_equal(vs, vo)
+
+
+def test_burgers_full_run_matches_reference_solve():
+    """500 cells to T = 0.11 (459 steps): E and Var vs the reference's own
+    MomentSolver::Solve (golden) within relative L1 1e-10."""
+    g = np.load(GOLD / "c1_solve.npz")
+    s = Solver(str(g["toml"]))
+    s.init_state()
+    info = s.run()
+    assert info["steps"] == 459 and info["failed_cells"] == 0
+    mv = s.mean_var()
+    err = rel_l1(mv, g["mean_var"], s.geometry()["area"])
+    assert np.all(err <= TOL_MV), err
+
+
+@pytest.mark.parametrize("case", ["c1", "c2", "c3", "c5"])
+def test_steps_match_golden(case):
+    g = np.load(GOLD / f"{case}_steps.npz")
+    s = Solver(str(g["toml"]))
+    s.init_state()
+    info = s.step(int(g["steps"]))
+    assert info["failed_cells"] == 0
+    assert abs(info["t"] - float(g["t"])) <= 1e-12 * abs(float(g["t"]))
+    u, lam, lev = s.download_state()
+    np.testing.assert_array_equal(lev, g["level"])
+    np.testing.assert_allclose(u, g["u"], rtol=1e-9, atol=1e-11)
+    err = rel_l1(s.mean_var(), g["mean_var"], s.geometry()["area"])
+    assert np.all(err <= TOL_MV), err
+
+
+@pytest.mark.parametrize("mode", ["reference", "guarded", "safe"])
+def test_batched_closure_matches_golden(mode):
+    g = np.load(GOLD / "c2_closure.npz")
+    toml = str(g["toml"]).replace('newton = "guarded"', f'newton = "{mode}"')
+    s = Solver(toml)
+    lam, st = s.closure_solve_host(g["lam0"], g["u"])
+    ok = g[f"status_{mode}"] == 0
+    np.testing.assert_array_equal(st == 0, ok)
+    np.testing.assert_allclose(lam[ok], g[f"lam_{mode}"][ok], rtol=1e-8, atol=1e-9)
+
+
+@pytest.mark.parametrize("toml,steps", [
+    (W.euler2d(nx=30, ny=6), 8),
+    (W.shallow_water1d(ncells=2000), 40),
+    (W.euler2d_3u(nx=10, ny=3), 3),
+    (W.burgers1d(ncells=1000, degree=6, nquad=24, tend=0.05), 60),
+])
+def test_time_steps_match_oracle(toml, steps):
+    s, o = _pair(toml)
+    a = s.step(steps)
+    b = o.step(steps)
+    assert a["failed_cells"] == 0 and b["failures"] == 0
+    assert abs(a["t"] - b["t"]) <= 1e-11 * b["t"]
+    area = o.geometry()["area"]
+    err = rel_l1(s.mean_var(), o.mean_var(), area)
+    assert np.all(err <= TOL_MV), err
+    us, _, vs = s.download_state()
+    uo, _, vo = o.get_state()
+    np.testing.assert_array_equal(vs, vo)
+    np.testing.assert_allclose(us, uo, rtol=1e-8, atol=1e-10)
+
+
+def test_layouts_round_trip_and_host_closure():
+    toml = W.euler2d(nx=6, ny=2)
+    s = Solver(toml)
+    s.init_state()
+    u, lam, lev = s.download_state(LAYOUT_STATE_MAJOR)
+    ur, lr, _ = s.download_state(LAYOUT_REF)
+    np.testing.assert_array_equal(ur.reshape(len(u), -1), u.transpose(0, 2, 1).reshape(len(u), -1))
+    s.upload_state(ur, lr, lev, layout=LAYOUT_REF)
+    u2, lam2, _ = s.download_state()
+    np.testing.assert_array_equal(u2, u)
+    np.testing.assert_array_equal(lam2, lam)
+    # resident closure == host drop-in closure
+    lh, st = s.closure_solve_host(lam, u)
+    s.solve_closure()
+    _, lres, _ = s.download_state()
+    assert np.all(st == 0)
+    np.testing.assert_array_equal(lh, lres)
+
+
+def test_nonfinite_input_reports_status():
+    toml = W.euler2d(nx=6, ny=2)
+    s = Solver(toml)
+    s.init_state()
+    u, lam, lev = s.download_state()
+    u[3, 0, 0] = np.nan
+    lam_out, st = s.closure_solve_host(lam, u)
+    assert st[3] == 4 and np.count_nonzero(st) == 1
+    with pytest.raises(UqcError):
+        s.upload_state(u, lam, lev)
+        s.solve_closure()
+
+
+def test_full_size_euler_step_is_finite_and_deterministic():
+    """200k-cell mesh, one step twice from the same state: identical results."""
+    toml = W.euler2d()
+    s = Solver(toml)
+    s.init_state()
+    u0, l0, v0 = s.download_state()
+    a = s.step(1)
+    u1, l1, _ = s.download_state()
+    s.upload_state(u0, l0, v0)
+    b = s.step(1)
+    u2, l2, _ = s.download_state()
+    assert a["failed_cells"] == 0 and np.isfinite(u1).all()
+    assert a["dt"] == b["dt"] and a["residual"] == b["residual"]
+    np.testing.assert_array_equal(u1, u2)
+    np.testing.assert_array_equal(l1, l2)

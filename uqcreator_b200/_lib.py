@@ -1,0 +1,121 @@
+"""ctypes binding of the C ABI in include/uqc.h (libuqc_b200.so, built in-tree).
+
+There is no CPU fallback: if the extension is missing or a CUDA device is not
+available, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libuqc_b200.so"
+_lib = None
+
+UQC_OK = 0
+ERRORS = {-1: "argument", -2: "config", -3: "cuda", -4: "not converged", -5: "memory", -6: "state", -7: "capacity"}
+LAYOUT_REF, LAYOUT_STATE_MAJOR = 0, 1
+FP64, MIXED = 0, 1
+CELL_CODES = {0: "converged", 1: "max iterations", 2: "line search", 3: "not positive definite", 4: "non-finite"}
+
+# every symbol include/uqc.h declares
+EXPORTS = [
+    "uqc_create_from_file", "uqc_create_from_string", "uqc_destroy", "uqc_last_error", "uqc_get_info",
+    "uqc_set_precision", "uqc_set_newton", "uqc_get_tables", "uqc_get_geometry", "uqc_init_state",
+    "uqc_upload_state", "uqc_download_state", "uqc_solve_closure", "uqc_cell_status", "uqc_step", "uqc_run",
+    "uqc_mean_var", "uqc_closure_solve_host", "uqc_closure_solve_device", "uqc_last_timing", "uqc_device_state",
+    "uqc_last_launch_count", "uqc_stream", "uqc_mesh_tri_jitter",
+]
+
+
+class UqcError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"uqc error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Info(C.Structure):
+    _fields_ = [("n_cells", C.c_int), ("n_states", C.c_int), ("n_total", C.c_int), ("n_quad", C.c_int),
+                ("n_levels", C.c_int), ("dim_xi", C.c_int), ("n_faces", C.c_int), ("mesh_dim", C.c_int),
+                ("n_total_level", C.c_int * 16), ("precision", C.c_int), ("newton_mode", C.c_int),
+                ("t", C.c_double), ("steps", C.c_longlong)]
+
+
+class StepInfo(C.Structure):
+    _fields_ = [("t", C.c_double), ("dt", C.c_double), ("residual", C.c_double), ("steps", C.c_int),
+                ("failed_cells", C.c_int), ("newton_iterations", C.c_longlong), ("line_search_trials", C.c_longlong),
+                ("active_cells", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_up = C.POINTER(C.c_uint)
+_vp = C.c_void_p
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is not built; run `python -m uqcreator_b200.build` "
+                          "(there is no CPU fallback for the hot path)")
+    L = C.CDLL(str(LIB_PATH))
+    sig = {
+        "uqc_create_from_file": ([C.c_char_p, _vp, C.POINTER(_vp), C.c_char_p, C.c_int], C.c_int),
+        "uqc_create_from_string": ([C.c_char_p, _vp, C.POINTER(_vp), C.c_char_p, C.c_int], C.c_int),
+        "uqc_destroy": ([_vp], None),
+        "uqc_last_error": ([_vp], C.c_char_p),
+        "uqc_get_info": ([_vp, C.POINTER(Info)], C.c_int),
+        "uqc_set_precision": ([_vp, C.c_int], C.c_int),
+        "uqc_set_newton": ([_vp, C.c_int, C.c_double, C.c_int], C.c_int),
+        "uqc_get_tables": ([_vp, _dp, _dp, _dp, _dp], C.c_int),
+        "uqc_get_geometry": ([_vp, _dp, _dp, _dp, _dp, _dp, _ip, _ip], C.c_int),
+        "uqc_init_state": ([_vp], C.c_int),
+        "uqc_upload_state": ([_vp, _dp, _dp, _up, C.c_int, C.c_double], C.c_int),
+        "uqc_download_state": ([_vp, _dp, _dp, _up, C.c_int], C.c_int),
+        "uqc_solve_closure": ([_vp, C.POINTER(StepInfo)], C.c_int),
+        "uqc_cell_status": ([_vp, _ip, _ip], C.c_int),
+        "uqc_step": ([_vp, C.c_int, C.POINTER(StepInfo)], C.c_int),
+        "uqc_run": ([_vp, C.c_double, C.POINTER(StepInfo)], C.c_int),
+        "uqc_mean_var": ([_vp, _dp], C.c_int),
+        "uqc_closure_solve_host": ([_vp, C.c_int, _dp, _dp, _up, C.c_int, _ip], C.c_int),
+        "uqc_closure_solve_device": ([_vp, C.c_int, _vp, _vp, _vp, _vp], C.c_int),
+        "uqc_last_timing": ([_vp, C.POINTER(C.c_float)], C.c_int),
+        "uqc_device_state": ([_vp, C.POINTER(_vp), C.POINTER(_vp)], C.c_int),
+        "uqc_last_launch_count": ([_vp], C.c_int),
+        "uqc_stream": ([_vp], _vp),
+        "uqc_mesh_tri_jitter": ([C.c_int, C.c_int, C.c_double, C.c_ulonglong, _dp, _ip, _ip], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def ptr(a, t=_dp):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def check(h, rc: int):
+    if rc != UQC_OK:
+        msg = lib().uqc_last_error(h).decode() if h else ""
+        raise UqcError(rc, msg)
+    return rc
+
+
+def mesh_tri_jitter(nx: int, ny: int, jitter: float, seed: int):
+    """The product's own seeded triangle mesh (host code, no GPU needed)."""
+    nn = (nx + 1) * (ny + 1)
+    xy = np.zeros((nn, 2)); bnd = np.zeros(nn, dtype=np.int32); tri = np.zeros((2 * nx * ny, 3), dtype=np.int32)
+    rc = lib().uqc_mesh_tri_jitter(nx, ny, jitter, seed, ptr(xy), ptr(bnd, _ip), ptr(tri, _ip))
+    if rc != 0:
+        raise UqcError(rc, "mesh")
+    return dict(xy=xy, node_boundary=bnd, tri=tri)

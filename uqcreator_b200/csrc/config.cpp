@@ -1,0 +1,256 @@
+// Reader for UQCreator's TOML input files (the subset they use: [tables],
+// key = string | integer | float | boolean | nested arrays, # comments) and
+// the mapping of its keys onto uqc::Config, following Settings::Init
+// (settings.cpp:22-323) for key names, accepted values and defaults.
+#include <cmath>
+#include <sstream>
+
+#include "host.h"
+
+namespace uqc {
+namespace {
+
+struct Value {
+    enum Kind { STR, INT, FLT, BOOL, ARR } kind = STR;
+    std::string s;
+    long long i = 0;
+    double f    = 0.0;
+    bool b      = false;
+    std::vector<Value> items;
+    double num() const {
+        if( kind == INT ) return double( i );
+        if( kind == FLT ) return f;
+        throw ConfigError( "expected a number" );
+    }
+};
+
+using Table = std::map<std::string, Value>;
+using Doc   = std::map<std::string, Table>;
+
+struct Parser {
+    const char* p;
+    int line;
+    void ws() {
+        while( *p == ' ' || *p == '\t' || *p == '\r' ) ++p;
+    }
+    [[noreturn]] void fail( const std::string& m ) { throw ConfigError( "TOML line " + std::to_string( line ) + ": " + m ); }
+    Value value() {
+        ws();
+        Value v;
+        if( *p == '"' ) {
+            ++p;
+            v.kind = Value::STR;
+            while( *p && *p != '"' ) v.s += *p++;
+            if( *p != '"' ) fail( "unterminated string" );
+            ++p;
+        }
+        else if( *p == '[' ) {
+            ++p;
+            v.kind = Value::ARR;
+            ws();
+            while( *p && *p != ']' ) {
+                v.items.push_back( value() );
+                ws();
+                if( *p == ',' ) ++p;
+                ws();
+            }
+            if( *p != ']' ) fail( "unterminated array" );
+            ++p;
+        }
+        else if( std::string( p, 4 ) == "true" ) {
+            v.kind = Value::BOOL;
+            v.b    = true;
+            p += 4;
+        }
+        else if( std::string( p, 5 ) == "false" ) {
+            v.kind = Value::BOOL;
+            p += 5;
+        }
+        else {
+            std::string tok;
+            while( *p && *p != ',' && *p != ']' && *p != '#' && *p != ' ' && *p != '\t' && *p != '\r' ) tok += *p++;
+            if( tok.empty() ) fail( "missing value" );
+            try {
+                if( tok.find_first_of( ".eEn" ) != std::string::npos ) {
+                    v.kind = Value::FLT;
+                    v.f    = std::stod( tok );
+                }
+                else {
+                    v.kind = Value::INT;
+                    v.i    = std::stoll( tok );
+                }
+            } catch( const std::exception& ) {
+                fail( "bad number '" + tok + "'" );
+            }
+        }
+        return v;
+    }
+};
+
+std::string trim( const std::string& s ) {
+    size_t a = s.find_first_not_of( " \t\r" ), b = s.find_last_not_of( " \t\r" );
+    return a == std::string::npos ? std::string() : s.substr( a, b - a + 1 );
+}
+
+Doc parse_doc( const std::string& text ) {
+    Doc doc;
+    std::istringstream in( text );
+    std::string ln, section;
+    Parser ps{nullptr, 0};
+    while( std::getline( in, ln ) ) {
+        ++ps.line;
+        ps.p = ln.c_str();
+        ps.ws();
+        if( *ps.p == 0 || *ps.p == '#' ) continue;
+        if( *ps.p == '[' ) {
+            size_t e = ln.find( ']' );
+            if( e == std::string::npos ) ps.fail( "bad table header" );
+            section = trim( ln.substr( ln.find( '[' ) + 1, e - ln.find( '[' ) - 1 ) );
+            doc[section];
+            continue;
+        }
+        size_t eq = ln.find( '=' );
+        if( eq == std::string::npos ) ps.fail( "expected key = value" );
+        std::string key = trim( ln.substr( 0, eq ) );
+        ps.p            = ln.c_str() + eq + 1;
+        doc[section][key] = ps.value();
+    }
+    return doc;
+}
+
+const Value* find( const Doc& d, const std::string& t, const std::string& k ) {
+    auto it = d.find( t );
+    if( it == d.end() ) return nullptr;
+    auto jt = it->second.find( k );
+    return jt == it->second.end() ? nullptr : &jt->second;
+}
+
+const Value& need( const Doc& d, const std::string& t, const std::string& k ) {
+    const Value* v = find( d, t, k );
+    if( !v ) throw ConfigError( "[" + t + "] '" + k + "' not set!" );
+    return *v;
+}
+
+std::string str( const Value& v, const std::string& what ) {
+    if( v.kind != Value::STR ) throw ConfigError( what + " must be a string" );
+    return v.s;
+}
+
+}    // namespace
+
+Config parse_config( const std::string& text ) {
+    Doc d = parse_doc( text );
+    Config c;
+    // [general] problem (settings.cpp:34-63)
+    c.problemName = str( need( d, "general", "problem" ), "[general] problem" );
+    if( c.problemName == "Burgers1D" )
+        c.problem = PR_BURGERS;
+    else if( c.problemName == "Euler2D" )
+        c.problem = PR_EULER2D;
+    else if( c.problemName == "ShallowWater1D" )
+        c.problem = PR_SHALLOW_WATER;
+    else
+        throw ConfigError( "[general] 'problem' = '" + c.problemName + "' is not on this hot path (Burgers1D, Euler2D, ShallowWater1D)" );
+    // [mesh] (settings.cpp:95-111, mesh1d.cpp:6-17)
+    c.meshDim = int( need( d, "mesh", "dimension" ).num() );
+    if( const Value* v = find( d, "mesh", "numberOfCells" ) ) c.nCells1d = int( v->num() );
+    if( const Value* v = find( d, "mesh", "a" ) ) c.a = v->num();
+    if( const Value* v = find( d, "mesh", "b" ) ) c.b = v->num();
+    // [problem] (settings.cpp:114-170, euler2d.cpp:10)
+    std::string ts = str( need( d, "problem", "timestepping" ), "[problem] timestepping" );
+    if( ts != "explicitEuler" ) throw ConfigError( "[problem] 'timestepping' is invalid! Please set one of the following types: explicitEuler" );
+    const Value& dist = need( d, "problem", "distribution" );
+    if( dist.kind != Value::ARR || dist.items.size() != 2 || dist.items[0].kind != Value::ARR )
+        throw ConfigError( "[problem] 'distribution' must be [[types],[sigmas]]" );
+    c.dimXi = int( dist.items[0].items.size() );
+    for( size_t l = 0; l < dist.items[0].items.size(); ++l ) {
+        if( str( dist.items[0].items[l], "distribution type" ) != "Legendre" )
+            throw ConfigError( "[problem] 'distribution': only Legendre is on this hot path" );
+        c.sigma.push_back( dist.items[1].items.at( l ).num() );
+    }
+    if( c.dimXi < 1 || c.dimXi > 3 ) throw ConfigError( "[problem] 'distribution': 1 to 3 uncertain dimensions supported" );
+    c.cfl  = need( d, "problem", "CFL" ).num();
+    c.tEnd = need( d, "problem", "tEnd" ).num();
+    if( const Value* v = find( d, "problem", "residual" ) ) c.minResidual = v->num();
+    if( const Value* v = find( d, "problem", "gamma" ) ) c.gamma = v->num();
+    // [moment_system] (settings.cpp:173-314)
+    std::string cl = str( need( d, "moment_system", "closure" ), "[moment_system] closure" );
+    if( cl == "BoundedBarrier" )
+        c.closure = CL_BOUNDED_BARRIER;
+    else if( cl == "Euler2D" )
+        c.closure = CL_EULER2D;
+    else if( cl == "ShallowWater" )
+        c.closure = CL_SHALLOW_WATER;
+    else
+        throw ConfigError( "[moment_system] 'closure' = '" + cl + "' is not on this hot path (BoundedBarrier, Euler2D, ShallowWater)" );
+    const Value& mom = need( d, "moment_system", "moments" );
+    if( mom.kind != Value::ARR || mom.items.size() != 2 ) throw ConfigError( "[moment_system] 'moments' must be [[type],[degrees]]" );
+    std::string degType = str( mom.items[0].items.at( 0 ), "moments type" );
+    if( degType == "maxDegree" )
+        c.maxDegree = true;
+    else if( degType != "totalDegree" )
+        throw ConfigError( "[moment_system] 'moments' is invalid! Please set one of the following types: totalDegree, maxDegree" );
+    for( auto& v : mom.items[1].items ) c.degrees.push_back( int( v.num() ) );
+    if( c.degrees.empty() || c.degrees.size() > 16 ) throw ConfigError( "[moment_system] 'moments': 1 to 16 refinement levels" );
+    const Value& qp = need( d, "moment_system", "quadPoints" );
+    if( qp.kind != Value::ARR || qp.items.size() != 2 ) throw ConfigError( "[moment_system] 'quadPoints' must be [[type],[n per level]]" );
+    if( str( qp.items[0].items.at( 0 ), "quadPoints type" ) == "sparseGrid" )
+        throw ConfigError( "[moment_system] 'quadPoints': sparse grids are not on this hot path" );
+    c.nQuad = int( qp.items[1].items.back().num() );
+    if( const Value* v = find( d, "moment_system", "maxIterations" ) ) c.maxIterations = int( v->num() );
+    if( const Value* v = find( d, "moment_system", "epsilon" ) ) c.epsilon = v->num();
+    // closure / problem consistency (the reference pairs them in Problem::Create)
+    int nS = c.closure == CL_BOUNDED_BARRIER ? 1 : ( c.closure == CL_EULER2D ? 4 : 2 );
+    int nSp = c.problem == PR_BURGERS ? 1 : ( c.problem == PR_EULER2D ? 4 : 2 );
+    if( nS != nSp ) throw ConfigError( "closure '" + cl + "' does not match problem '" + c.problemName + "'" );
+    // [uqc]
+    if( const Value* v = find( d, "uqc", "ic" ) )
+        for( auto& x : v->items ) c.ic.push_back( x.num() );
+    if( const Value* v = find( d, "uqc", "bounds" ) ) {
+        c.bbMinus = v->items.at( 0 ).num();
+        c.bbPlus  = v->items.at( 1 ).num();
+    }
+    if( const Value* v = find( d, "uqc", "mesh" ) ) c.meshKind = str( *v, "[uqc] mesh" );
+    if( const Value* v = find( d, "uqc", "mesh_params" ) ) {
+        c.nx     = int( v->items.at( 0 ).num() );
+        c.ny     = int( v->items.at( 1 ).num() );
+        c.jitter = v->items.at( 2 ).num();
+        c.seed   = uint64_t( v->items.at( 3 ).num() );
+    }
+    if( const Value* v = find( d, "uqc", "precision" ) ) {
+        std::string p = str( *v, "[uqc] precision" );
+        if( p == "fp64" )
+            c.precision = 0;
+        else if( p == "mixed" )
+            c.precision = 1;
+        else
+            throw ConfigError( "[uqc] 'precision' must be fp64 or mixed" );
+    }
+    if( const Value* v = find( d, "uqc", "newton" ) ) {
+        std::string p = str( *v, "[uqc] newton" );
+        if( p == "reference" )
+            c.newtonMode = 0;
+        else if( p == "guarded" )
+            c.newtonMode = 1;
+        else if( p == "safe" )
+            c.newtonMode = 2;
+        else
+            throw ConfigError( "[uqc] 'newton' must be reference, guarded or safe" );
+    }
+    size_t needIc = c.problem == PR_BURGERS ? 4 : ( c.problem == PR_EULER2D ? 5 : 3 );
+    if( c.ic.size() < needIc ) throw ConfigError( "[uqc] 'ic' needs " + std::to_string( needIc ) + " values for " + c.problemName );
+    if( c.meshDim == 1 ) {
+        if( c.nCells1d < 3 || ( std::fabs( c.a ) <= 2.2e-16 && std::fabs( c.b ) <= 2.2e-16 ) )
+            throw ConfigError( "[mesh1d] Invalid mesh parameters!" );
+    }
+    else if( c.meshDim == 2 ) {
+        if( c.meshKind != "tri_jitter" || c.nx < 2 || c.ny < 2 ) throw ConfigError( "[uqc] 2-D runs need mesh = \"tri_jitter\" with mesh_params = [nx, ny, jitter, seed], nx, ny >= 2" );
+    }
+    else
+        throw ConfigError( "[mesh] 'dimension' must be 1 or 2" );
+    if( c.closure == CL_EULER2D && c.meshDim != 2 ) throw ConfigError( "Euler2D needs a 2-D mesh" );
+    if( c.closure != CL_EULER2D && c.meshDim != 1 ) throw ConfigError( c.problemName + " needs a 1-D mesh" );
+    return c;
+}
+
+}    // namespace uqc

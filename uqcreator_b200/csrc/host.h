@@ -1,0 +1,82 @@
+// Host-side core of the B200 IPM solver: configuration (the reference's TOML
+// schema), basis/quadrature tables and meshes. Device code lives in *.cu.
+#pragma once
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace uqc {
+
+struct ConfigError : public std::runtime_error {
+    explicit ConfigError( const std::string& m ) : std::runtime_error( m ) {}
+};
+
+enum ClosureKind { CL_BOUNDED_BARRIER = 0, CL_EULER2D = 1, CL_SHALLOW_WATER = 2 };
+enum ProblemKind { PR_BURGERS = 0, PR_EULER2D = 1, PR_SHALLOW_WATER = 2 };
+
+// Everything the hot path reads from the input file. Keys and defaults follow
+// Settings::Init (settings.cpp:22-323); the [uqc] table carries what the
+// reference hard-codes in its problem classes (initial data, barrier bounds)
+// and this implementation's own options.
+struct Config {
+    // [general]
+    std::string problemName;
+    ProblemKind problem = PR_BURGERS;
+    // [mesh]
+    int meshDim = 1;
+    int nCells1d = 0;
+    double a = 0.0, b = 0.0;
+    // [problem]
+    int dimXi = 1;
+    std::vector<double> sigma;
+    double cfl = 0.0, tEnd = 0.0, minResidual = -1.0, gamma = 1.4;
+    // [moment_system]
+    ClosureKind closure = CL_BOUNDED_BARRIER;
+    bool maxDegree = false;
+    std::vector<int> degrees;    // per refinement level
+    int nQuad = 0;               // Gauss nodes per dimension (last level)
+    int maxIterations = 1000;
+    double epsilon = 5e-5;
+    // [uqc]
+    std::vector<double> ic;
+    double bbMinus = 3.0, bbPlus = 12.0;
+    std::string meshKind = "uniform1d";
+    int nx = 0, ny = 0;
+    double jitter = 0.0;
+    uint64_t seed = 0;
+    int precision = 0;     // uqc_precision
+    int newtonMode = 0;    // 0 reference, 1 guarded, 2 safe
+};
+
+Config parse_config( const std::string& tomlText );
+
+// Basis and quadrature: tensor Gauss-Legendre grid and scaled Legendre basis
+// tables phiTilde / phiTildeWf of Closure::Closure (closure.cpp:16-84).
+struct Tables {
+    int nT = 0, nQ = 0, dimXi = 0, nLevels = 0;
+    std::vector<int> nTLevel;       // moments per refinement level
+    std::vector<int> index;         // nT x dimXi polynomial degrees (settings.cpp:241-265)
+    std::vector<double> xi, w;      // nodes (nQ x dimXi), weights
+    std::vector<double> phi, phiWf; // nQ x nT, row k contiguous
+};
+
+Tables build_tables( const Config& c );
+void gauss_legendre( int n, std::vector<double>& x, std::vector<double>& w );
+
+// Cell geometry in structure-of-arrays form, faces per cell = 2 (1-D) or 3.
+struct Mesh {
+    int nCells = 0, nFaces = 0, dim = 1;
+    std::vector<double> area, maxEdge, center;       // center: 2 per cell
+    std::vector<double> unitN, scaledN;              // 2 per face
+    std::vector<int> nbr;                            // per face; ghost = nCells
+    std::vector<int> boundary;                       // Dirichlet cell flag
+};
+
+Mesh build_mesh_1d( int nCells, double a, double b );
+void tri_jitter_nodes( int nx, int ny, double jitter, uint64_t seed, double* xy, int* bnd, int* tri );
+Mesh build_mesh_tri( int nNodes, const double* xy, const int* bnd, int nTri, const int* tri );
+
+}    // namespace uqc

@@ -1,0 +1,797 @@
+// FP64 kernels of the IPM time step.
+//
+//   k_closure  persistent, work-stealing: one thread group (a warp for small
+//              systems, a whole CTA for n = nS nT > 32) per cell. Runs the
+//              damped Newton of Closure::SolveClosure (closure.cpp:133-193) with
+//              the basis tables staged in shared memory, the Hessian kept in
+//              packed upper-triangular form in shared memory and a right-looking
+//              Cholesky; then, in step mode, the fused epilogue of
+//              MomentSolver::Solve phases [C]-[F] (momentsolver.cpp:99-133):
+//              nodal reconstruction uQ, refinement level, moment
+//              re-projection and the CFL time step (grid-wide min).
+//   k_update   kinetic flux at the quadrature nodes of every face, projected
+//              onto the basis and applied as the explicit Euler update
+//              (expliciteuler.cpp:17-74), plus the residual of
+//              momentsolver.cpp:149-152 and the time/loop control, finished
+//              by the last CTA.
+//   k_init     initial moments and duals (momentsolver.cpp:463-563).
+//   k_meanvar  mean and variance per cell (momentsolver.cpp:302-328).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "physics.cuh"
+#include "uqc.h"
+
+namespace uqc {
+
+constexpr int MAXLEV = 16;
+
+// Grid-wide loop state kept on the device so a step needs no host round trip.
+struct Control {
+    double t, tEnd, minResidual, residual, dt;
+    unsigned long long dtBits;     // atomicMin of the positive dt as integer bits
+    unsigned int workCounter;      // closure work stealing
+    unsigned int doneBlocks;       // last-block detection in k_update
+    int active;                    // the loop condition of momentsolver.cpp:79
+    int steps;
+    int failedCells;
+    int activeCells;      // cells with Newton iterations in the running step
+    int activeCellsLast;  // ... in the last finished step
+    unsigned long long newtonIters, lineSearchTrials;
+};
+
+struct KParams {
+    int nS, nT, nQ, ld;       // ld: row stride of the tables (odd, >= nT)
+    int nLevels;
+    int nTLevel[MAXLEV];
+    int nCells, nFaces, dimXi;
+    double eps;
+    int maxIter, newtonMode;
+    PhysParams phys;
+    // tables
+    const double* phi;       // nQ x ld
+    const double* phiWf;     // nQ x ld
+    const double* xi;        // nQ x dimXi
+    bool tablesInSmem;
+    // geometry
+    const double *area, *dx, *center, *unitN, *scaledN;
+    const int *nbr, *boundary;
+    // state
+    double *u, *lam, *uQ, *uOld0;
+    unsigned* level;
+    const unsigned* nTotalCell;  // closure-only calls: moments per cell (else from level)
+    int *status, *iters;
+    double* blockPartial;     // one per CTA of k_update
+    Control* ctl;
+};
+
+// ------------------------------------------------------------------ groups
+
+template <int GROUP> struct Grp {
+    int r;
+    __device__ __forceinline__ void sync() const {
+        if constexpr( GROUP == 32 )
+            __syncwarp();
+        else
+            __syncthreads();
+    }
+};
+
+// Sum over the group, same value returned to every member. scratch: >= GROUP/32 doubles.
+template <int GROUP> __device__ double group_sum( const Grp<GROUP>& g, double v, double* scratch ) {
+    for( int o = 16; o > 0; o >>= 1 ) v += __shfl_xor_sync( 0xffffffffu, v, o );
+    if constexpr( GROUP == 32 ) {
+        return v;
+    }
+    else {
+        if( ( g.r & 31 ) == 0 ) scratch[g.r >> 5] = v;
+        g.sync();
+        double s = 0.0;
+        for( int w = 0; w < GROUP / 32; ++w ) s += scratch[w];
+        g.sync();
+        return s;
+    }
+}
+
+template <int GROUP> __device__ double group_min( const Grp<GROUP>& g, double v, double* scratch ) {
+    for( int o = 16; o > 0; o >>= 1 ) v = fmin( v, __shfl_xor_sync( 0xffffffffu, v, o ) );
+    if constexpr( GROUP == 32 ) {
+        return v;
+    }
+    else {
+        if( ( g.r & 31 ) == 0 ) scratch[g.r >> 5] = v;
+        g.sync();
+        double s = scratch[0];
+        for( int w = 1; w < GROUP / 32; ++w ) s = fmin( s, scratch[w] );
+        g.sync();
+        return s;
+    }
+}
+
+__device__ __forceinline__ int packed( int row, int col ) { return col * ( col + 1 ) / 2 + row; }
+
+// ------------------------------------------------------------------ workspace
+
+// Shared-memory workspace of one cell (doubles), sizes for the finest level.
+struct CellWs {
+    double *lam, *lamN, *uh, *g, *gN, *d;   // n each
+    double *LA, *LB, *uk;                   // nS nQ each
+    double* du;                             // NP nQ
+    double* H;                              // n (n + 1) / 2 packed upper
+    double* red;                            // reduction scratch (16) + broadcast (16)
+};
+
+__host__ __device__ inline size_t cell_ws_doubles( int nS, int nT, int nQ, int NP ) {
+    size_t n = size_t( nS ) * nT;
+    size_t s = 6 * n + 3 * size_t( nS ) * nQ + size_t( NP ) * nQ + n * ( n + 1 ) / 2 + 32;
+    return ( s + 3 ) & ~size_t( 3 );
+}
+
+__device__ inline CellWs carve( double* p, int nS, int nT, int nQ, int NP ) {
+    CellWs w;
+    size_t n = size_t( nS ) * nT;
+    w.lam    = p;
+    w.lamN   = w.lam + n;
+    w.uh     = w.lamN + n;
+    w.g      = w.uh + n;
+    w.gN     = w.g + n;
+    w.d      = w.gN + n;
+    w.LA     = w.d + n;
+    w.LB     = w.LA + size_t( nS ) * nQ;
+    w.uk     = w.LB + size_t( nS ) * nQ;
+    w.du     = w.uk + size_t( nS ) * nQ;
+    w.H      = w.du + size_t( NP ) * nQ;
+    w.red    = w.H + n * ( n + 1 ) / 2;
+    return w;
+}
+
+// ------------------------------------------------------------------ building blocks
+
+// Lambda_k[s] = sum_{i < nTj} lam[s nT + i] phi(k, i)   (closure.cpp:205-213)
+template <int NS, int GROUP>
+__device__ void eval_lambda( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* lam, int nTj, double* L ) {
+    for( int idx = g.r; idx < NS * P.nQ; idx += GROUP ) {
+        int s = idx / P.nQ, k = idx - s * P.nQ;
+        const double* row = phi + size_t( k ) * P.ld;
+        const double* ls  = lam + s * P.nT;
+        double a          = 0.0;
+        for( int i = 0; i < nTj; ++i ) a = fma( ls[i], row[i], a );
+        L[s * P.nQ + k] = a;
+    }
+}
+
+// U at every node from Lambda (node-major loop, one node per thread).
+template <int CL, int GROUP>
+__device__ void eval_u( const Grp<GROUP>& g, const KParams& P, const double* L, double* uk, bool vecForm ) {
+    constexpr int NS = Closure<CL>::NS;
+    for( int k = g.r; k < P.nQ; k += GROUP ) {
+        double Lk[NS], y[NS];
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) Lk[s] = L[s * P.nQ + k];
+        Closure<CL>::U( Lk, y, vecForm, P.phys );
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) uk[s * P.nQ + k] = y[s];
+    }
+}
+
+// Gradient (closure.cpp:234-253) at the duals whose Lambda is in L:
+// gout[s nTj + i] = sum_k U_s(k) phiWf(k, i) - uh[s nT + i]; returns ||gout||_2.
+// Vectors of the Newton system use the level's compact stride nTj.
+template <int CL, int GROUP>
+__device__ double gradient( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* L, const double* uh, int nTj,
+                            double* uk, double* gout, double* red ) {
+    constexpr int NS = Closure<CL>::NS;
+    eval_u<CL, GROUP>( g, P, L, uk, true );
+    g.sync();
+    double sq = 0.0;
+    for( int idx = g.r; idx < NS * nTj; idx += GROUP ) {
+        int s = idx / nTj, i = idx - s * nTj;
+        const double* us = uk + s * P.nQ;
+        double a         = 0.0;
+        for( int k = 0; k < P.nQ; ++k ) a = fma( us[k], phiWf[size_t( k ) * P.ld + i], a );
+        a         = a - uh[s * P.nT + i];
+        gout[idx] = a;
+        sq += a * a;
+    }
+    return sqrt( group_sum<GROUP>( g, sq, red ) );
+}
+
+// Hessian (closure.cpp:255-271), packed upper triangle of the n x n matrix,
+// n = NS nTj: H(m nTj + j, l nTj + i) = sum_k phi(k,j) phiWf(k,i) DU(l,m)(k).
+// Register tiles of 4 x 4 entries per thread, m <= l (and j <= i on the diagonal).
+template <int CL, int GROUP>
+__device__ void hessian( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* phiWf, const double* L, int nTj,
+                         double* du, double* H ) {
+    constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP;
+    for( int k = g.r; k < P.nQ; k += GROUP ) {
+        double Lk[NS], y[NP];
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) Lk[s] = L[s * P.nQ + k];
+        Closure<CL>::DU( Lk, y, P.phys );
+#pragma unroll
+        for( int p = 0; p < NP; ++p ) du[p * P.nQ + k] = y[p];
+    }
+    g.sync();
+    const int nTiles = ( nTj + 3 ) >> 2;
+    const int tDiag = nTiles * ( nTiles + 1 ) / 2, tOff = nTiles * nTiles;
+    const int total = NS * tDiag + ( NS * ( NS - 1 ) / 2 ) * tOff;
+    for( int t = g.r; t < total; t += GROUP ) {
+        // decode tile -> block (m, l), m <= l, and tile (tj, ti)
+        int m = 0, l = 0, tj = 0, ti = 0, rem = t;
+        for( m = 0; m < NS; ++m ) {
+            if( rem < tDiag ) {
+                l = m;
+                int c = 0;
+                while( ( c + 1 ) * ( c + 2 ) / 2 <= rem ) ++c;
+                ti = c;
+                tj = rem - c * ( c + 1 ) / 2;
+                break;
+            }
+            rem -= tDiag;
+            int offHere = ( NS - 1 - m ) * tOff;
+            if( rem < offHere ) {
+                l  = m + 1 + rem / tOff;
+                rem = rem % tOff;
+                tj = rem / nTiles;
+                ti = rem % nTiles;
+                break;
+            }
+            rem -= offHere;
+        }
+        const int j0 = tj * 4, i0 = ti * 4;
+        const double* dup = du + pair_index<NS>( l, m ) * P.nQ;
+        double acc[4][4];
+#pragma unroll
+        for( int a = 0; a < 4; ++a )
+#pragma unroll
+            for( int b = 0; b < 4; ++b ) acc[a][b] = 0.0;
+        for( int k = 0; k < P.nQ; ++k ) {
+            const double* pr  = phi + size_t( k ) * P.ld;
+            const double* pwr = phiWf + size_t( k ) * P.ld;
+            double dk         = dup[k];
+            double aj[4], bi[4];
+#pragma unroll
+            for( int a = 0; a < 4; ++a ) aj[a] = pr[j0 + a];
+#pragma unroll
+            for( int b = 0; b < 4; ++b ) bi[b] = pwr[i0 + b] * dk;
+#pragma unroll
+            for( int a = 0; a < 4; ++a )
+#pragma unroll
+                for( int b = 0; b < 4; ++b ) acc[a][b] = fma( aj[a], bi[b], acc[a][b] );
+        }
+#pragma unroll
+        for( int a = 0; a < 4; ++a )
+#pragma unroll
+            for( int b = 0; b < 4; ++b ) {
+                int j = j0 + a, i = i0 + b;
+                if( j < nTj && i < nTj && ( m < l || j <= i ) ) H[packed( m * nTj + j, l * nTj + i )] = acc[a][b];
+            }
+    }
+}
+
+// Cholesky H = U^T U of the packed upper matrix (LAPACK dpotrf semantics,
+// called through posv, vectorspace.cpp:152-171), right-looking with one group
+// barrier per column: at step j every thread forms U(j,r) = A(j,r) / sqrt(A(j,j))
+// itself and updates its share of the trailing triangle; row j is written
+// scaled one step later, when nobody reads it. Returns 0 or j + 1 of the first
+// non-positive pivot (posv's info > 0).
+template <int GROUP> __device__ int cholesky( const Grp<GROUP>& g, double* H, int n ) {
+    constexpr int TX = GROUP == 32 ? 8 : 16, TY = GROUP / TX;
+    const int tx = g.r % TX, ty = g.r / TX;
+    double prevInv = 0.0, prevD = 0.0;
+    for( int j = 0; j < n; ++j ) {
+        double ajj = H[packed( j, j )];
+        if( !( ajj > 0.0 ) ) return j + 1;    // uniform: every thread reads the same value
+        double d = sqrt( ajj ), inv = 1.0 / d;
+        if( j > 0 ) {
+            // finalise row j-1: U(j-1, c) = A(j-1, c) / d_{j-1}
+            for( int c = j - 1 + g.r; c < n; c += GROUP ) H[packed( j - 1, c )] = ( c == j - 1 ) ? prevD : H[packed( j - 1, c )] * prevInv;
+        }
+        for( int c = j + 1 + ty; c < n; c += TY ) {
+            double ujc = H[packed( j, c )] * inv;
+            for( int r = j + 1 + tx; r <= c; r += TX ) H[packed( r, c )] -= ( H[packed( j, r )] * inv ) * ujc;
+        }
+        prevInv = inv;
+        prevD   = d;
+        g.sync();
+    }
+    for( int c = n - 1 + g.r; c < n; c += GROUP ) H[packed( n - 1, c )] = prevD;
+    g.sync();
+    return 0;
+}
+
+// Solves U^T U x = b in place (x = b on entry) by one warp (dpotrs:
+// forward with U^T, then backward with U, sequential order of dtrsm).
+template <int GROUP> __device__ void chol_solve( const Grp<GROUP>& g, const double* H, int n, double* x ) {
+    if( g.r >= 32 ) return;
+    const int lane = g.r;
+    constexpr int MAXR = 8;    // rows per lane: n <= 256
+    double y[MAXR];
+#pragma unroll
+    for( int q = 0; q < MAXR; ++q ) y[q] = ( lane + 32 * q < n ) ? x[lane + 32 * q] : 0.0;
+    for( int i = 0; i < n; ++i ) {
+        double yi = 0.0;
+        int own = i & 31, q0 = i >> 5;
+#pragma unroll
+        for( int q = 0; q < MAXR; ++q )
+            if( q == q0 && lane == own ) {
+                y[q] = y[q] / H[packed( i, i )];
+                yi   = y[q];
+            }
+        yi = __shfl_sync( 0xffffffffu, yi, own );
+#pragma unroll
+        for( int q = 0; q < MAXR; ++q ) {
+            int r = lane + 32 * q;
+            if( r > i && r < n ) y[q] = y[q] - H[packed( i, r )] * yi;
+        }
+    }
+    for( int k = n - 1; k >= 0; --k ) {
+        double xk = 0.0;
+        int own = k & 31, q0 = k >> 5;
+#pragma unroll
+        for( int q = 0; q < MAXR; ++q )
+            if( q == q0 && lane == own ) {
+                if( y[q] != 0.0 ) y[q] = y[q] / H[packed( k, k )];
+                xk = y[q];
+            }
+        xk = __shfl_sync( 0xffffffffu, xk, own );
+        if( xk != 0.0 ) {
+#pragma unroll
+            for( int q = 0; q < MAXR; ++q ) {
+                int r = lane + 32 * q;
+                if( r < k ) y[q] = y[q] - xk * H[packed( r, k )];
+            }
+        }
+    }
+#pragma unroll
+    for( int q = 0; q < MAXR; ++q )
+        if( lane + 32 * q < n ) x[lane + 32 * q] = y[q];
+}
+
+// lamOut[s nT + i] = lamIn[s nT + i] + c d[s nTj + i], i < nTj (closure.cpp:273-279)
+template <int GROUP> __device__ void add_step( const Grp<GROUP>& g, const KParams& P, int nTj, const double* lamIn, double c, const double* d, double* lamOut ) {
+    for( int idx = g.r; idx < P.nS * nTj; idx += GROUP ) {
+        int s = idx / nTj, i = idx - s * nTj;
+        lamOut[s * P.nT + i] = lamIn[s * P.nT + i] + c * d[idx];
+    }
+}
+
+// Damped Newton on one cell in shared memory. On return w.lam holds the duals
+// and w.LA the Lambda of w.lam at all nodes (laValid). Returns a uqc_cell_code.
+template <int CL, int GROUP>
+__device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* phiWf, CellWs& w, int nTj, int& iters,
+                            int& lsTrials ) {
+    const int n      = P.nS * nTj;
+    const double eps = P.eps;
+    const bool guard = P.newtonMode != 0;
+    iters            = 0;
+    lsTrials         = 0;
+    double* LA = w.LA;
+    double* LB = w.LB;
+    auto accept = [&]() {    // lam <- lamN, LA <- LB
+        for( int idx = g.r; idx < P.nS * P.nT; idx += GROUP ) w.lam[idx] = w.lamN[idx];
+        double* t = LA;
+        LA        = LB;
+        LB        = t;
+    };
+    int rc = UQC_CELL_MAX_ITER;
+    eval_lambda<Closure<CL>::NS, GROUP>( g, P, phi, w.lam, nTj, LA );
+    g.sync();
+    if( P.newtonMode == 2 ) {
+        // Closure::SolveClosureSafe (closure.cpp:297-339)
+        for( int l = 0; l < P.maxIter; ++l ) {
+            double stepSize = 1.0;
+            double gn       = gradient<CL, GROUP>( g, P, phiWf, LA, w.uh, nTj, w.uk, w.g, w.red );
+            hessian<CL, GROUP>( g, P, phi, phiWf, LA, nTj, w.du, w.H );
+            g.sync();
+            if( cholesky<GROUP>( g, w.H, n ) ) {
+                rc = UQC_CELL_NOT_PD;
+                goto out;
+            }
+            for( int idx = g.r; idx < n; idx += GROUP ) w.d[idx] = w.g[idx];
+            g.sync();
+            chol_solve<GROUP>( g, w.H, n, w.d );
+            g.sync();
+            ++iters;
+            for( int idx = g.r; idx < P.nS * P.nT; idx += GROUP ) w.lamN[idx] = w.lam[idx];
+            add_step<GROUP>( g, P, nTj, w.lam, -stepSize, w.d, w.lamN );
+            g.sync();
+            eval_lambda<Closure<CL>::NS, GROUP>( g, P, phi, w.lamN, nTj, LB );
+            g.sync();
+            double gnN = gradient<CL, GROUP>( g, P, phiWf, LB, w.uh, nTj, w.uk, w.gN, w.red );
+            int refine = 0;
+            while( gn < gnN || !isfinite( gnN ) ) {
+                stepSize *= 0.5;
+                ++lsTrials;
+                add_step<GROUP>( g, P, nTj, w.lam, -stepSize, w.d, w.lamN );
+                g.sync();
+                eval_lambda<Closure<CL>::NS, GROUP>( g, P, phi, w.lamN, nTj, LB );
+                g.sync();
+                gnN = gradient<CL, GROUP>( g, P, phiWf, LB, w.uh, nTj, w.uk, w.gN, w.red );
+                if( gnN < eps ) {
+                    accept();
+                    rc = UQC_CELL_CONVERGED;
+                    goto out;
+                }
+                if( ++refine > 1000 ) {
+                    rc = UQC_CELL_LINE_SEARCH;
+                    goto out;
+                }
+            }
+            accept();
+            g.sync();
+            if( gnN < eps ) {
+                rc = UQC_CELL_CONVERGED;
+                goto out;
+            }
+        }
+        goto out;
+    }
+    {
+        // Closure::SolveClosure (closure.cpp:133-193); guard = the finiteness test of :318
+        double gn = gradient<CL, GROUP>( g, P, phiWf, LA, w.uh, nTj, w.uk, w.g, w.red );
+        if( gn < eps ) {
+            rc = UQC_CELL_CONVERGED;
+            goto out;
+        }
+        double gnN = 0.0;
+        for( int l = 0; l < P.maxIter; ++l ) {
+            double stepSize = 1.0;
+            if( l != 0 ) {
+                // the gradient at lam is the accepted trial gradient (same duals, same arithmetic)
+                for( int idx = g.r; idx < n; idx += GROUP ) w.g[idx] = w.gN[idx];
+                gn = gnN;
+            }
+            hessian<CL, GROUP>( g, P, phi, phiWf, LA, nTj, w.du, w.H );
+            g.sync();
+            if( cholesky<GROUP>( g, w.H, n ) ) {
+                rc = UQC_CELL_NOT_PD;
+                goto out;
+            }
+            for( int idx = g.r; idx < n; idx += GROUP ) w.d[idx] = w.g[idx];
+            g.sync();
+            chol_solve<GROUP>( g, w.H, n, w.d );
+            g.sync();
+            ++iters;
+            if( P.maxIter == 1 ) {
+                // One-Shot IPM: lam -= alpha H^-1 g, no line search (closure.cpp:151-154)
+                add_step<GROUP>( g, P, nTj, w.lam, -1.0, w.d, w.lam );
+                g.sync();
+                eval_lambda<Closure<CL>::NS, GROUP>( g, P, phi, w.lam, nTj, LA );
+                g.sync();
+                rc = UQC_CELL_CONVERGED;
+                goto out;
+            }
+            for( int idx = g.r; idx < P.nS * P.nT; idx += GROUP ) w.lamN[idx] = w.lam[idx];
+            add_step<GROUP>( g, P, nTj, w.lam, -stepSize, w.d, w.lamN );
+            g.sync();
+            eval_lambda<Closure<CL>::NS, GROUP>( g, P, phi, w.lamN, nTj, LB );
+            g.sync();
+            gnN        = gradient<CL, GROUP>( g, P, phiWf, LB, w.uh, nTj, w.uk, w.gN, w.red );
+            int refine = 0;
+            while( gn < gnN || ( guard && !isfinite( gnN ) ) ) {
+                stepSize *= 0.5;
+                ++lsTrials;
+                add_step<GROUP>( g, P, nTj, w.lam, -stepSize, w.d, w.lamN );
+                g.sync();
+                eval_lambda<Closure<CL>::NS, GROUP>( g, P, phi, w.lamN, nTj, LB );
+                g.sync();
+                gnN = gradient<CL, GROUP>( g, P, phiWf, LB, w.uh, nTj, w.uk, w.gN, w.red );
+                if( gnN < eps ) {
+                    accept();
+                    rc = UQC_CELL_CONVERGED;
+                    goto out;
+                }
+                if( ++refine > 1000 ) {
+                    rc = UQC_CELL_LINE_SEARCH;
+                    goto out;
+                }
+            }
+            accept();
+            g.sync();
+            if( gnN < eps ) {
+                rc = UQC_CELL_CONVERGED;
+                goto out;
+            }
+        }
+    }
+out:
+    g.sync();
+    w.LA = LA;
+    w.LB = LB;
+    return rc;
+}
+
+// ------------------------------------------------------------------ kernels
+
+__device__ __forceinline__ void atomic_min_pos_double( unsigned long long* addr, double v ) {
+    if( v >= 0.0 ) atomicMin( addr, (unsigned long long)__double_as_longlong( v ) );
+}
+
+// Persistent closure kernel. mode 0: closure only; mode 1: closure + fused
+// epilogue of a time step. Tables are staged in shared memory when they fit.
+template <int CL, int GROUP>
+__global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_closure( KParams P, int mode ) {
+    constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP;
+    extern __shared__ __align__( 16 ) double smem[];
+    if( mode == 1 && !P.ctl->active ) return;
+    const int groups = blockDim.x / GROUP;
+    Grp<GROUP> g{int( threadIdx.x % GROUP )};
+    const int gid = threadIdx.x / GROUP;
+    const double *phi = P.phi, *phiWf = P.phiWf;
+    double* base = smem;
+    if( P.tablesInSmem ) {
+        size_t tn = size_t( P.nQ ) * P.ld + 4;
+        for( size_t i = threadIdx.x; i < tn; i += blockDim.x ) {
+            base[i]      = i < size_t( P.nQ ) * P.ld ? P.phi[i] : 0.0;
+            base[tn + i] = i < size_t( P.nQ ) * P.ld ? P.phiWf[i] : 0.0;
+        }
+        phi   = base;
+        phiWf = base + tn;
+        base += 2 * tn;
+        __syncthreads();
+    }
+    CellWs w = carve( base + gid * cell_ws_doubles( NS, P.nT, P.nQ, NP ), NS, P.nT, P.nQ, NP );
+    const size_t ldc = size_t( NS ) * P.nT;
+    double* bc       = w.red + 16;    // broadcast slot
+    unsigned long long itSum = 0, lsSum = 0;
+    int failSum = 0, activeSum = 0;
+    double dtMin = 1e300;
+    for( ;; ) {
+        int cell;
+        if( g.r == 0 ) bc[0] = double( atomicAdd( &P.ctl->workCounter, 1u ) );
+        g.sync();
+        cell = int( bc[0] );
+        g.sync();
+        if( cell >= P.nCells ) break;
+        const int lev = P.level ? int( P.level[cell] ) : P.nLevels - 1;
+        const int nTj = P.nTotalCell ? int( P.nTotalCell[cell] ) : P.nTLevel[lev];
+        // load duals and moments (state-major, finest stride)
+        for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
+            w.lam[idx] = P.lam[cell * ldc + idx];
+            w.uh[idx]  = P.u[cell * ldc + idx];
+        }
+        g.sync();
+        int iters = 0, ls = 0, rc;
+        bool finite = true;
+        for( int idx = 0; idx < int( ldc ); ++idx ) finite = finite && isfinite( w.uh[idx] ) && isfinite( w.lam[idx] );
+        if( !finite )
+            rc = UQC_CELL_NONFINITE;
+        else
+            rc = newton_cell<CL, GROUP>( g, P, phi, phiWf, w, nTj, iters, ls );
+        if( g.r == 0 ) {
+            P.status[cell] = rc;
+            P.iters[cell]  = iters;
+            itSum += iters;
+            lsSum += ls;
+            failSum += rc != 0;
+            activeSum += iters > 0;
+        }
+        for( int idx = g.r; idx < int( ldc ); idx += GROUP ) P.lam[cell * ldc + idx] = w.lam[idx];
+        if( mode == 1 ) {
+            // [C] uQ = U(Lambda(lam)) with the matrix-form ansatz; w.LA is Lambda(lam) at level nTj
+            if( rc != 0 ) {
+                eval_lambda<NS, GROUP>( g, P, phi, w.lam, nTj, w.LA );
+                g.sync();
+            }
+            eval_u<CL, GROUP>( g, P, w.LA, w.uk, false );
+            // [D] refinement level from the moments before re-projection (momentsolver.cpp:104-112, 271-289)
+            int newLev = lev;
+            if( P.nLevels > 1 ) {
+                double ind = 0.0;
+                if( P.dimXi == 1 )
+                    ind = fabs( w.uh[nTj - 1] ) + fabs( w.uh[nTj - 2] );
+                else {
+                    int prev = lev == 0 ? 1 : P.nTLevel[lev - 1];
+                    for( int i = prev; i < nTj; ++i ) ind += fabs( w.uh[i] );
+                }
+                if( ind > 0.02 && lev < P.nLevels - 1 )
+                    newLev = lev + 1;
+                else if( ind < 0.004 && lev > 0 )
+                    newLev = lev - 1;
+            }
+            const int nTn = P.nTLevel[newLev];
+            if( g.r == 0 ) {
+                P.uOld0[cell] = w.uh[0];
+                P.level[cell] = unsigned( newLev );
+            }
+            g.sync();
+            double* uq = P.uQ + size_t( cell ) * NS * P.nQ;
+            for( int idx = g.r; idx < NS * P.nQ; idx += GROUP ) uq[idx] = w.uk[idx];
+            // [E] moments re-projected: u(s, i) = sum_k uQ(s, k) phiWf(k, i), i < nT(new level)
+            for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
+                int s = idx / P.nT, i = idx - s * P.nT;
+                double a = 0.0;
+                if( i < nTn ) {
+                    const double* us = w.uk + s * P.nQ;
+                    for( int k = 0; k < P.nQ; ++k ) a = fma( us[k], phiWf[size_t( k ) * P.ld + i], a );
+                }
+                P.u[cell * ldc + idx] = a;
+            }
+            // [F] time step of this cell (min over its nodes)
+            double dloc = 1e300;
+            for( int k = g.r; k < P.nQ; k += GROUP ) {
+                double uqk[NS];
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) uqk[s] = w.uk[s * P.nQ + k];
+                double d = Problem<CL>::dt( uqk, P.dx[cell], P.phys );
+                dloc     = d < dloc ? d : dloc;
+            }
+            dloc  = group_min<GROUP>( g, dloc, w.red );
+            dtMin = dloc < dtMin ? dloc : dtMin;
+        }
+        g.sync();
+    }
+    if( g.r == 0 ) {
+        if( itSum ) atomicAdd( &P.ctl->newtonIters, itSum );
+        if( lsSum ) atomicAdd( &P.ctl->lineSearchTrials, lsSum );
+        if( failSum ) atomicAdd( &P.ctl->failedCells, failSum );
+        if( activeSum ) atomicAdd( &P.ctl->activeCells, activeSum );
+        if( mode == 1 && dtMin < 1e300 ) atomic_min_pos_double( &P.ctl->dtBits, dtMin );
+    }
+}
+
+// Flux + explicit Euler update, one group per cell (grid-stride), and the
+// residual / time control finished by the last CTA.
+template <int CL, int GROUP>
+__global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_update( KParams P ) {
+    constexpr int NS = Closure<CL>::NS;
+    extern __shared__ __align__( 16 ) double smem[];
+    __shared__ double blockRes[32];
+    __shared__ int isLast;
+    if( !P.ctl->active ) return;
+    const int groups = blockDim.x / GROUP;
+    Grp<GROUP> g{int( threadIdx.x % GROUP )};
+    const int gid = threadIdx.x / GROUP;
+    const double* phiWf = P.phiWf;
+    double* base        = smem;
+    if( P.tablesInSmem ) {
+        size_t tn = size_t( P.nQ ) * P.ld;
+        for( size_t i = threadIdx.x; i < tn; i += blockDim.x ) base[i] = P.phiWf[i];
+        phiWf = base;
+        base += tn + 4;
+        __syncthreads();
+    }
+    double* G     = base + size_t( gid ) * ( size_t( P.nFaces ) * NS * P.nQ + 32 );
+    double* red   = G + size_t( P.nFaces ) * NS * P.nQ;
+    const double dt = __longlong_as_double( (long long)P.ctl->dtBits );
+    const size_t ldc = size_t( NS ) * P.nT;
+    double res       = 0.0;
+    for( int cell = blockIdx.x * groups + gid; cell < P.nCells; cell += gridDim.x * groups ) {
+        if( P.boundary[cell] ) {
+            // Dirichlet cell: uNew = u (expliciteuler.cpp:21-23)
+            if( g.r == 0 ) res += fabs( P.u[cell * ldc] - P.uOld0[cell] ) * P.area[cell];
+            continue;
+        }
+        const int nTj    = P.nTLevel[P.level[cell]];
+        const double* ua = P.uQ + size_t( cell ) * NS * P.nQ;
+        for( int idx = g.r; idx < P.nFaces * P.nQ; idx += GROUP ) {
+            int f = idx / P.nQ, k = idx - f * P.nQ;
+            int nb = P.nbr[cell * P.nFaces + f];
+            const double* ub = P.uQ + size_t( nb ) * NS * P.nQ;
+            double a[NS], b[NS], y[NS];
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) {
+                a[s] = ua[s * P.nQ + k];
+                b[s] = ub[s * P.nQ + k];
+            }
+            Problem<CL>::flux( a, b, P.unitN + ( cell * P.nFaces + f ) * 2, P.scaledN + ( cell * P.nFaces + f ) * 2, y, P.phys );
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) G[( f * NS + s ) * P.nQ + k] = y[s];
+        }
+        g.sync();
+        const double c = dt / P.area[cell];
+        for( int idx = g.r; idx < NS * nTj; idx += GROUP ) {
+            int s = idx / nTj, i = idx - s * nTj;
+            double rhs = 0.0;
+            for( int f = 0; f < P.nFaces; ++f ) {
+                const double* gs = G + ( f * NS + s ) * P.nQ;
+                for( int k = 0; k < P.nQ; ++k ) rhs = fma( gs[k], phiWf[size_t( k ) * P.ld + i], rhs );
+            }
+            double* up = P.u + cell * ldc + s * P.nT + i;
+            double nu  = *up - rhs * c;
+            *up        = nu;
+            if( idx == 0 ) res += fabs( nu - P.uOld0[cell] ) * P.area[cell];
+        }
+        g.sync();
+    }
+    // deterministic residual: per-thread partials -> CTA sum -> per-CTA slot -> last CTA sums in order
+    for( int o = 16; o > 0; o >>= 1 ) res += __shfl_xor_sync( 0xffffffffu, res, o );
+    if( ( threadIdx.x & 31 ) == 0 ) blockRes[threadIdx.x >> 5] = res;
+    __syncthreads();
+    if( threadIdx.x == 0 ) {
+        double s = 0.0;
+        for( int w = 0; w < int( blockDim.x >> 5 ); ++w ) s += blockRes[w];
+        P.blockPartial[blockIdx.x] = s;
+        __threadfence();
+        unsigned done = atomicAdd( &P.ctl->doneBlocks, 1u );
+        isLast        = done == gridDim.x - 1;
+    }
+    __syncthreads();
+    if( isLast && threadIdx.x == 0 ) {
+        __threadfence();
+        double s = 0.0;
+        for( unsigned b = 0; b < gridDim.x; ++b ) s += ( (volatile double*)P.blockPartial )[b];
+        Control* C    = P.ctl;
+        C->residual   = s;
+        C->dt         = dt;
+        C->t          = C->t + dt;
+        C->steps      = C->steps + 1;
+        C->active     = ( C->t < C->tEnd && C->residual > C->minResidual ) ? 1 : 0;
+        C->activeCellsLast = C->activeCells;
+        C->activeCells     = 0;
+        C->dtBits     = 0x7FF0000000000000ull;    // +inf for the next step's min
+        C->workCounter = 0;
+        C->doneBlocks  = 0;
+    }
+}
+
+// Initial moments u_j = U_IC(x_j, xi_k) phiWf and duals lambda_j(:,0) = DS(u_j(:,0)).
+template <int CL, int GROUP> __global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_init( KParams P ) {
+    constexpr int NS = Closure<CL>::NS;
+    extern __shared__ __align__( 16 ) double smem[];
+    const int groups = blockDim.x / GROUP;
+    Grp<GROUP> g{int( threadIdx.x % GROUP )};
+    const int gid   = threadIdx.x / GROUP;
+    double* uic     = smem + size_t( gid ) * ( size_t( NS ) * P.nQ + 8 );
+    const size_t ldc = size_t( NS ) * P.nT;
+    for( int cell = blockIdx.x * groups + gid; cell < P.nCells; cell += gridDim.x * groups ) {
+        for( int k = g.r; k < P.nQ; k += GROUP ) {
+            double y[NS];
+            Problem<CL>::ic( P.center + 2 * cell, P.xi + size_t( k ) * P.dimXi, y, P.phys );
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) uic[s * P.nQ + k] = y[s];
+        }
+        g.sync();
+        for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
+            int s = idx / P.nT, i = idx - s * P.nT;
+            double a = 0.0;
+            for( int k = 0; k < P.nQ; ++k ) a = fma( uic[s * P.nQ + k], P.phiWf[size_t( k ) * P.ld + i], a );
+            P.u[cell * ldc + idx]   = a;
+            P.lam[cell * ldc + idx] = 0.0;
+        }
+        g.sync();
+        if( g.r == 0 ) {
+            double u0[NS], ds[NS];
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) u0[s] = P.u[cell * ldc + s * P.nT];
+            Closure<CL>::DS( u0, ds, P.phys );
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) P.lam[cell * ldc + s * P.nT] = ds[s];
+            P.level[cell] = unsigned( P.nLevels - 1 );
+        }
+        g.sync();
+    }
+}
+
+// Mean and variance (vector-form ansatz), out[cell 2 NS + r].
+template <int CL, int GROUP> __global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_meanvar( KParams P, double* out ) {
+    constexpr int NS = Closure<CL>::NS;
+    extern __shared__ __align__( 16 ) double smem[];
+    const int groups = blockDim.x / GROUP;
+    Grp<GROUP> g{int( threadIdx.x % GROUP )};
+    const int gid    = threadIdx.x / GROUP;
+    double* L        = smem + size_t( gid ) * ( 2 * size_t( NS ) * P.nQ + 8 );
+    double* uk       = L + size_t( NS ) * P.nQ;
+    const size_t ldc = size_t( NS ) * P.nT;
+    for( int cell = blockIdx.x * groups + gid; cell < P.nCells; cell += gridDim.x * groups ) {
+        const int nTj = P.nTLevel[P.level[cell]];
+        eval_lambda<NS, GROUP>( g, P, P.phi, P.lam + cell * ldc, nTj, L );
+        g.sync();
+        eval_u<CL, GROUP>( g, P, L, uk, true );
+        g.sync();
+        for( int s = g.r; s < NS; s += GROUP ) {
+            double e = 0.0, v = 0.0;
+            for( int k = 0; k < P.nQ; ++k ) e = fma( uk[s * P.nQ + k], P.phiWf[size_t( k ) * P.ld], e );
+            for( int k = 0; k < P.nQ; ++k ) {
+                double dv = uk[s * P.nQ + k] - e;
+                v         = fma( dv * dv, P.phiWf[size_t( k ) * P.ld], v );
+            }
+            out[cell * 2 * NS + s]      = e;
+            out[cell * 2 * NS + NS + s] = v;
+        }
+        g.sync();
+    }
+}
+
+}    // namespace uqc

@@ -1,0 +1,227 @@
+// Device physics of the hot path: entropy ansatz U, its Jacobian DU and the
+// entropy gradient DS of each closure, numerical fluxes, time-step rules and
+// initial states. Formulas and their evaluation order follow the reference
+// files cited per function; CUDA's exp/pow/log/sqrt are called as is.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace uqc {
+
+struct PhysParams {
+    double bbMinus, bbPlus;   // bounded barrier bounds
+    double gamma;             // Euler
+    double cfl;
+    double ic[8];
+    double sigma[4];
+    int dimXi;
+    double dtFixed;           // shallow water: TimeSolver's dx CFL / 12
+};
+
+template <int CL> struct Closure;
+
+// ---------------------------------------------------------------- bounded barrier
+// U and DU of BoundedBarrier (boundedbarrier.cpp:19-31, 67-80), one state.
+template <> struct Closure<0> {
+    static constexpr int NS = 1, NP = 1;
+    __device__ static void U( const double* L, double* u, bool, const PhysParams& p ) {
+        double ePos = exp( L[0] ), eNeg = 1.0 / ePos;
+        if( L[0] > 0.0 )
+            u[0] = p.bbPlus / ( eNeg + 1.0 ) + p.bbMinus * eNeg / ( 1.0 + eNeg );
+        else
+            u[0] = p.bbMinus / ( ePos + 1.0 ) + p.bbPlus * ePos / ( 1.0 + ePos );
+    }
+    // packed symmetric DU: du[0] = DU(0,0)
+    __device__ static void DU( const double* L, double* du, const PhysParams& p ) {
+        double ePos = exp( L[0] ), eNeg = 1 / ePos;
+        if( L[0] > 0 )
+            du[0] = eNeg * ( p.bbPlus - p.bbMinus ) / ( exp( -2.0 * L[0] ) + 2.0 * eNeg + 1.0 );
+        else
+            du[0] = ePos * ( p.bbPlus - p.bbMinus ) / ( 1.0 + 2.0 * ePos + exp( 2.0 * L[0] ) );
+    }
+    // Closure::DS of the base class leaves the guess unchanged (zero)
+    __device__ static void DS( const double*, double* ds, const PhysParams& ) { ds[0] = 0.0; }
+};
+
+// ---------------------------------------------------------------- Euler 2-D
+// EulerClosure2D (eulerclosure2d.cpp); the class stores g = -gamma (:3).
+template <> struct Closure<1> {
+    static constexpr int NS = 4, NP = 10;
+    // vecForm: U(Vector&, ...) of :7-18 (gradient, mean/variance); otherwise the
+    // U(const Matrix&) form of :27-32 (nodal reconstruction, momentsolver.cpp:99-101).
+    __device__ static void U( const double* L, double* u, bool vecForm, const PhysParams& p ) {
+        const double g = -p.gamma;
+        double v1 = L[0], v2 = L[1], v3 = L[2], v4 = L[3];
+        double q  = ( v2 * v2 + v3 * v3 - 2.0 * v1 * v4 - 2.0 * v4 * g ) / ( 2.0 * v4 );
+        double e;
+        if( vecForm )
+            e = exp( 1.0 / ( 1.0 + g ) * q ) * pow( -v4, 1.0 / ( 1.0 + g ) );
+        else
+            e = pow( -exp( q ) * v4, 1.0 / ( 1.0 + g ) );
+        u[0] = e;
+        u[1] = -( ( v2 * e ) / v4 );
+        u[2] = -( ( v3 * e ) / v4 );
+        u[3] = -( ( e * ( -( v2 * v2 ) - v3 * v3 + 2.0 * v4 ) ) / ( 2.0 * ( v4 * v4 ) ) );
+    }
+    // packed upper DU (:54-88): order (0,0)(0,1)(0,2)(0,3)(1,1)(1,2)(1,3)(2,2)(2,3)(3,3)
+    __device__ static void DU( const double* L, double* y, const PhysParams& p ) {
+        const double g = -p.gamma;
+        double v1 = L[0], v2 = L[1], v3 = L[2], v4 = L[3];
+        double v4p2 = v4 * v4, v4p3 = v4p2 * v4, v4i2 = 1.0 / v4p2, v3p2 = v3 * v3, v2p2 = v2 * v2;
+        double e = exp( 1.0 / ( 1.0 + g ) * ( ( v2p2 + v3p2 - 2.0 * v1 * v4 - 2.0 * v4 * g ) / ( 2.0 * v4 ) ) ) * pow( -v4, 1.0 / ( 1.0 + g ) ) / ( 1.0 + g );
+        double vTerm = e * ( v2p2 + v3p2 + 2.0 * v4 * g ) / ( 2 * v4p3 );
+        y[0] = -( e );
+        y[1] = ( v2 * e ) / ( v4 );
+        y[2] = ( v3 * e ) / ( v4 );
+        y[3] = -( 0.5 * ( ( v2p2 + v3p2 - 2.0 * v4 ) * e ) * v4i2 );
+        y[4] = -( ( e * ( v2p2 + ( g + 1.0 ) * v4 ) ) * v4i2 );
+        y[5] = -( ( v2 * v3 * e ) * v4i2 );
+        y[6] = v2 * vTerm;
+        y[7] = -( ( e * ( v3p2 + ( g + 1.0 ) * v4 ) ) * v4i2 );
+        y[8] = v3 * vTerm;
+        y[9] = -( e * ( v2p2 * v2p2 + v3p2 * v3p2 + 4.0 * v3p2 * v4 * g - 4.0 * v4p2 * g + 2.0 * v2p2 * ( v3p2 + 2.0 * v4 * g ) ) ) / ( 4.0 * ( v4p2 * v4p2 ) );
+    }
+    // EulerClosure2D::DS (:90-106)
+    __device__ static void DS( const double* u, double* ds, const PhysParams& p ) {
+        const double gamma = -p.gamma;
+        double rho = u[0], rhoU = u[1], rhoV = u[2], rhoE = u[3];
+        double rhoV2 = rhoV * rhoV, rhoU2 = rhoU * rhoU;
+        ds[0] = ( rhoU2 + rhoV2 + gamma * ( 2 * rho * rhoE - rhoU2 - rhoV2 ) ) / ( -2 * rho * rhoE + rhoU2 + rhoV2 ) -
+                log( pow( rho, gamma ) * ( rhoE - ( rhoU2 + rhoV2 ) / ( 2 * rho ) ) );
+        ds[1] = -( ( 2 * rho * rhoU ) / ( -2 * rho * rhoE + rhoU2 + rhoV2 ) );
+        ds[2] = -( ( 2 * rho * rhoV ) / ( -2 * rho * rhoE + rhoU2 + rhoV2 ) );
+        ds[3] = -( rho / ( rhoE - ( rhoU2 + rhoV2 ) / ( 2 * rho ) ) );
+    }
+};
+
+// ---------------------------------------------------------------- shallow water 1-D
+// ShallowWaterClosure (shallowwaterclosure.cpp:10-42), g = 9.81.
+template <> struct Closure<2> {
+    static constexpr int NS = 2, NP = 3;
+    __device__ static void U( const double* L, double* u, bool, const PhysParams& ) {
+        const double gr = 9.81;
+        u[0] = ( 0.5 * ( 2 * L[0] + L[1] * L[1] ) ) / gr;
+        u[1] = ( 0.5 * ( 2 * L[0] * L[1] + L[1] * L[1] * L[1] ) ) / gr;
+    }
+    __device__ static void DU( const double* L, double* y, const PhysParams& ) {
+        const double gr = 9.81;
+        y[0] = 1.0 / gr;
+        y[1] = L[1] / gr;
+        y[2] = ( L[0] + 1.5 * ( L[1] * L[1] ) ) / gr;
+    }
+    __device__ static void DS( const double* u, double* ds, const PhysParams& ) {
+        const double gr = 9.81;
+        ds[0] = ( gr * ( u[0] * u[0] * u[0] ) - 0.5 * ( u[1] * u[1] ) ) / ( u[0] * u[0] );
+        ds[1] = u[1] / u[0];
+    }
+};
+
+// packed index of the symmetric pair (a, b)
+template <int NS> __device__ __forceinline__ int pair_index( int a, int b ) {
+    int lo = a < b ? a : b, hi = a < b ? b : a;
+    return lo * NS - ( lo * ( lo - 1 ) ) / 2 + ( hi - lo );
+}
+
+// ---------------------------------------------------------------- problems
+// Numerical flux g(u, v) for face unit normal nu and scaled normal n.
+template <int CL> struct Problem;
+
+// Burgers with the local Lax-Friedrichs flux (julia/Tensorization/IPMSolver.jl:38-42)
+// and CFL rule of burgers.cpp:114-122; ramp initial state (burgers.cpp:48-68).
+template <> struct Problem<0> {
+    __device__ static void flux( const double* u, const double* v, const double*, const double* n, double* y, const PhysParams& ) {
+        double beta = fabs( u[0] ) < fabs( v[0] ) ? fabs( v[0] ) : fabs( u[0] );
+        y[0]        = 0.5 * ( 0.5 * u[0] * u[0] + 0.5 * v[0] * v[0] ) * n[0] - 0.5 * beta * ( v[0] - u[0] ) * fabs( n[0] );
+    }
+    __device__ static double dt( const double* uq, double dx, const PhysParams& p ) { return p.cfl * dx / fabs( uq[0] ); }
+    __device__ static void ic( const double* x, const double* xi, double* y, const PhysParams& p ) {
+        double uL = p.ic[0], uR = p.ic[1], x0 = p.ic[2], x1 = p.ic[3], s = p.sigma[0];
+        if( x[0] < x0 + s * xi[0] )
+            y[0] = uL;
+        else if( x[0] < x1 + s * xi[0] )
+            y[0] = uL + ( uR - uL ) * ( x0 + s * xi[0] - x[0] ) / ( x0 - x1 );
+        else
+            y[0] = uR;
+    }
+};
+
+// Euler 2-D: HLL flux (euler2d.cpp:52-87), physical flux F (:89-106), CFL rule
+// (:114-134); Sod-type initial state with uncertain interface, density, pressure.
+template <> struct Problem<1> {
+    __device__ static void Fn( double gm, const double* u, const double* n, double* out ) {
+        double rhoInv = 1.0 / u[0], v1 = u[1] * rhoInv, v2 = u[2] * rhoInv;
+        double p = ( gm - 1.0 ) * ( u[3] - 0.5 * u[0] * ( v1 * v1 + v2 * v2 ) );
+        out[0]   = u[1] * n[0] + u[2] * n[1];
+        out[1]   = ( u[1] * v1 + p ) * n[0] + ( u[2] * v1 ) * n[1];
+        out[2]   = ( u[1] * v2 ) * n[0] + ( u[2] * v2 + p ) * n[1];
+        out[3]   = ( ( u[3] + p ) * v1 ) * n[0] + ( ( u[3] + p ) * v2 ) * n[1];
+    }
+    __device__ static void flux( const double* u, const double* v, const double* nu, const double* n, double* y, const PhysParams& P ) {
+        const double gm = P.gamma;
+        double rhoInv = 1.0 / u[0], uU = u[1] * rhoInv, vU = u[2] * rhoInv;
+        double p  = ( gm - 1.0 ) * ( u[3] - 0.5 * u[0] * ( uU * uU + vU * vU ) );
+        double aU = sqrt( gm * p * rhoInv );
+        rhoInv    = 1.0 / v[0];
+        double uV = v[1] * rhoInv, vV = v[2] * rhoInv;
+        p         = ( gm - 1.0 ) * ( v[3] - 0.5 * v[0] * ( uV * uV + vV * vV ) );
+        double aV = sqrt( gm * p * rhoInv );
+        double lmin = ( nu[0] * uU + nu[1] * vU ) - aU;
+        double lmax = ( nu[0] * uV + nu[1] * vV ) + aV;
+        if( lmin >= 0 )
+            Fn( gm, u, n, y );
+        else if( lmax <= 0 )
+            Fn( gm, v, n, y );
+        else {
+            double fu[4], fv[4];
+            Fn( gm, u, n, fu );
+            Fn( gm, v, n, fv );
+            double nn = sqrt( n[0] * n[0] + n[1] * n[1] ), ll = lmax * lmin, inv = 1.0 / ( lmax - lmin );
+            for( int i = 0; i < 4; ++i ) y[i] = inv * ( ( lmax * fu[i] - lmin * fv[i] ) + ll * ( v[i] - u[i] ) * nn );
+        }
+    }
+    __device__ static double dt( const double* uq, double dx, const PhysParams& P ) {
+        const double gm = P.gamma;
+        double rhoInv = 1.0 / uq[0], uU = uq[1] * rhoInv, vU = uq[2] * rhoInv;
+        double p = ( gm - 1.0 ) * ( uq[3] - 0.5 * uq[0] * ( uU * uU + vU * vU ) );
+        double a = sqrt( gm * p * rhoInv );
+        double t0 = fabs( 1.0 / ( vU - a ) ), t1 = fabs( 1.0 / ( vU + a ) );
+        double m1 = t1 < t0 ? t1 : t0;
+        double t2 = fabs( 1.0 / ( uU + a ) ), t3 = fabs( 1.0 / ( uU - a ) );
+        double m2 = t3 < t2 ? t3 : t2;
+        return ( P.cfl / dx ) * ( m2 < m1 ? m2 : m1 );
+    }
+    __device__ static void ic( const double* x, const double* xi, double* y, const PhysParams& P ) {
+        double rho, pr;
+        if( x[0] < P.ic[0] + P.sigma[0] * xi[0] ) {
+            rho = P.ic[1] * ( 1.0 + ( P.dimXi > 1 ? P.sigma[1] * xi[1] : 0.0 ) );
+            pr  = P.ic[2] * ( 1.0 + ( P.dimXi > 2 ? P.sigma[2] * xi[2] : 0.0 ) );
+        }
+        else {
+            rho = P.ic[3];
+            pr  = P.ic[4];
+        }
+        y[0] = rho;
+        y[1] = 0.0;
+        y[2] = 0.0;
+        y[3] = pr / ( P.gamma - 1.0 );
+    }
+};
+
+// Shallow water 1-D: Lax-Friedrichs with dx/dt = 12 / CFL (shallowwater.cpp:21-35);
+// time step Settings::GetDT (problem.cpp:44); dam-break initial state.
+template <> struct Problem<2> {
+    __device__ static void flux( const double* u, const double* v, const double*, const double* n, double* y, const PhysParams& P ) {
+        const double gr = 9.81;
+        double s        = 0.5 / ( P.cfl / 12.0 );
+        double fl1 = ( u[1] * u[1] ) / u[0] + 0.5 * gr * ( u[0] * u[0] );
+        double fr1 = ( v[1] * v[1] ) / v[0] + 0.5 * gr * ( v[0] * v[0] );
+        y[0]       = 0.5 * ( u[1] * n[0] + v[1] * n[0] ) - s * ( v[0] - u[0] );
+        y[1]       = 0.5 * ( fl1 * n[0] + fr1 * n[0] ) - s * ( v[1] - u[1] );
+    }
+    __device__ static double dt( const double*, double, const PhysParams& P ) { return P.dtFixed; }
+    __device__ static void ic( const double* x, const double* xi, double* y, const PhysParams& P ) {
+        y[0] = x[0] < P.ic[0] ? P.ic[1] * ( 1.0 + P.sigma[0] * xi[0] ) : P.ic[2];
+        y[1] = 0.0;
+    }
+};
+
+}    // namespace uqc

@@ -1,0 +1,811 @@
+// Host orchestration and C ABI (include/uqc.h) of the B200 IPM solver.
+//
+// One uqc_solver = the reference's Settings + Mesh + Problem + Closure +
+// MomentSolver for one run, with the whole state resident in HBM:
+//   u, lambda   cell-major, state-major inside a cell (nS * nT doubles per cell)
+//   uQ          nodal states, nS * nQ doubles per cell (FP64)
+//   geometry    structure-of-arrays per cell / face
+// A time step is two kernel launches (k_closure in step mode, k_update); the
+// loop condition, dt and residual live in a device Control block, so steps
+// need no host synchronisation and are captured into a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "host.h"
+#include "ipm_kernels.cuh"
+#include "mixed.cuh"
+#include "uqc.h"
+
+using namespace uqc;
+
+struct uqc_solver {
+    Config cfg;
+    Tables tab;
+    Mesh mesh;
+    cudaStream_t stream     = nullptr;
+    cudaStream_t userStream = nullptr;
+    bool ownStream          = false;
+    bool deviceReady        = false;
+    int nS = 1, ld = 1, group = 32, numSMs = 148;
+    size_t ldc = 1;
+    // device buffers
+    double *d_phi = nullptr, *d_phiWf = nullptr, *d_xi = nullptr;
+    double *d_area = nullptr, *d_dx = nullptr, *d_center = nullptr, *d_unitN = nullptr, *d_scaledN = nullptr;
+    int *d_nbr = nullptr, *d_boundary = nullptr;
+    double *d_u = nullptr, *d_lam = nullptr, *d_uQ = nullptr, *d_uOld0 = nullptr, *d_blockPartial = nullptr;
+    unsigned* d_level = nullptr;
+    int *d_status = nullptr, *d_iters = nullptr;
+    Control* d_ctl = nullptr;
+    Control* h_ctl = nullptr;    // pinned mirror
+    // closure-only scratch for caller-owned batches (grow-only)
+    double *d_xLam = nullptr, *d_xU = nullptr;
+    unsigned* d_xNt = nullptr;
+    int *d_xStatus = nullptr, *d_xIters = nullptr;
+    size_t xCap = 0;
+    // launch shapes
+    int closureBlock = 256, closureGrid = 0, updateBlock = 256, updateGrid = 0, auxGrid = 0;
+    size_t closureSmem = 0, updateSmem = 0, initSmem = 0, mvSmem = 0;
+    bool tablesInSmem = false;
+    // mixed precision
+    MixedPlan mixed;
+    // bookkeeping
+    bool stateReady = false;
+    int precision   = 0;
+    int launches    = 0;
+    unsigned long long lastIters = 0, lastLs = 0;
+    int lastFailed = 0;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    float lastMs[3] = {0, 0, 0};
+    cudaGraphExec_t graph = nullptr;
+    std::string err;
+};
+
+namespace {
+
+struct CudaError : public std::runtime_error {
+    explicit CudaError( const std::string& m ) : std::runtime_error( m ) {}
+};
+#define CK( x )                                                                                                                      \
+    do {                                                                                                                             \
+        cudaError_t e_ = ( x );                                                                                                      \
+        if( e_ != cudaSuccess ) throw CudaError( std::string( #x ) + ": " + cudaGetErrorName( e_ ) + " " + cudaGetErrorString( e_ ) ); \
+    } while( 0 )
+
+int fail( uqc_solver* h, int code, const std::string& m ) {
+    if( h ) h->err = m;
+    return code;
+}
+
+template <class F> int guarded( uqc_solver* h, F&& f ) {
+    try {
+        return f();
+    } catch( const ConfigError& e ) {
+        return fail( h, UQC_ERR_CONFIG, e.what() );
+    } catch( const CudaError& e ) {
+        std::string m = e.what();
+        return fail( h, m.find( "MemoryAllocation" ) != std::string::npos ? UQC_ERR_MEMORY : UQC_ERR_CUDA, m );
+    } catch( const std::bad_alloc& ) {
+        return fail( h, UQC_ERR_MEMORY, "host allocation failed" );
+    } catch( const std::exception& e ) {
+        return fail( h, UQC_ERR_ARGUMENT, e.what() );
+    }
+}
+
+void ensure_device( uqc_solver* h );
+
+// guarded() for entry points that touch the device
+template <class F> int guarded_dev( uqc_solver* h, F&& f ) {
+    return guarded( h, [&] {
+        ensure_device( h );
+        return f();
+    } );
+}
+
+template <class T> T* dalloc( size_t n ) {
+    T* p = nullptr;
+    CK( cudaMalloc( &p, std::max<size_t>( n, 1 ) * sizeof( T ) ) );
+    return p;
+}
+template <class T> T* dupload( const std::vector<T>& v, size_t extra = 0 ) {
+    T* p = dalloc<T>( v.size() + extra );
+    if( extra ) CK( cudaMemset( p, 0, ( v.size() + extra ) * sizeof( T ) ) );
+    if( !v.empty() ) CK( cudaMemcpy( p, v.data(), v.size() * sizeof( T ), cudaMemcpyHostToDevice ) );
+    return p;
+}
+
+KParams make_params( const uqc_solver* h ) {
+    KParams P{};
+    P.nS      = h->nS;
+    P.nT      = h->tab.nT;
+    P.nQ      = h->tab.nQ;
+    P.ld      = h->ld;
+    P.nLevels = h->tab.nLevels;
+    for( int l = 0; l < h->tab.nLevels; ++l ) P.nTLevel[l] = h->tab.nTLevel[l];
+    P.nCells     = h->mesh.nCells;
+    P.nFaces     = h->mesh.nFaces;
+    P.dimXi      = h->tab.dimXi;
+    P.eps        = h->cfg.epsilon;
+    P.maxIter    = h->cfg.maxIterations;
+    P.newtonMode = h->cfg.newtonMode;
+    PhysParams& ph = P.phys;
+    ph.bbMinus     = h->cfg.bbMinus;
+    ph.bbPlus      = h->cfg.bbPlus;
+    ph.gamma       = h->cfg.gamma;
+    ph.cfl         = h->cfg.cfl;
+    for( size_t i = 0; i < h->cfg.ic.size() && i < 8; ++i ) ph.ic[i] = h->cfg.ic[i];
+    for( size_t i = 0; i < h->cfg.sigma.size() && i < 4; ++i ) ph.sigma[i] = h->cfg.sigma[i];
+    ph.dimXi   = h->tab.dimXi;
+    ph.dtFixed = h->mesh.area[0] * h->cfg.cfl / 12.0;    // TimeSolver (timesolver.cpp:4-9)
+    P.phi          = h->d_phi;
+    P.phiWf        = h->d_phiWf;
+    P.xi           = h->d_xi;
+    P.tablesInSmem = h->tablesInSmem;
+    P.area         = h->d_area;
+    P.dx           = h->d_dx;
+    P.center       = h->d_center;
+    P.unitN        = h->d_unitN;
+    P.scaledN      = h->d_scaledN;
+    P.nbr          = h->d_nbr;
+    P.boundary     = h->d_boundary;
+    P.u            = h->d_u;
+    P.lam          = h->d_lam;
+    P.uQ           = h->d_uQ;
+    P.uOld0        = h->d_uOld0;
+    P.level        = h->d_level;
+    P.nTotalCell   = nullptr;
+    P.status       = h->d_status;
+    P.iters        = h->d_iters;
+    P.blockPartial = h->d_blockPartial;
+    P.ctl          = h->d_ctl;
+    return P;
+}
+
+// ---- kernel dispatch on (closure kind, group size) ------------------------
+template <int CL, int GROUP> struct Kern {
+    static void* closure() { return (void*)&k_closure<CL, GROUP>; }
+    static void* update() { return (void*)&k_update<CL, GROUP>; }
+    static void* init() { return (void*)&k_init<CL, GROUP>; }
+    static void* meanvar() { return (void*)&k_meanvar<CL, GROUP>; }
+};
+
+void* pick( int cl, int group, int which ) {
+#define PICK( C, G )                                                                                                     \
+    if( cl == C && group == G ) {                                                                                        \
+        switch( which ) {                                                                                                \
+            case 0: return Kern<C, G>::closure();                                                                        \
+            case 1: return Kern<C, G>::update();                                                                         \
+            case 2: return Kern<C, G>::init();                                                                           \
+            default: return Kern<C, G>::meanvar();                                                                       \
+        }                                                                                                                \
+    }
+    PICK( 0, 32 ) PICK( 0, 256 ) PICK( 1, 32 ) PICK( 1, 256 ) PICK( 2, 32 ) PICK( 2, 256 )
+#undef PICK
+    throw ConfigError( "no kernel for this closure" );
+}
+
+int closure_np( int cl ) { return cl == 0 ? 1 : ( cl == 1 ? 10 : 3 ); }
+
+void launch( uqc_solver* h, void* fn, int grid, int block, size_t smem, void** args ) {
+    CK( cudaLaunchKernel( fn, dim3( grid ), dim3( block ), args, smem, h->stream ) );
+    ++h->launches;
+}
+
+void plan_launches( uqc_solver* h ) {
+    int dev;
+    CK( cudaGetDevice( &dev ) );
+    CK( cudaDeviceGetAttribute( &h->numSMs, cudaDevAttrMultiProcessorCount, dev ) );
+    int maxSmem = 0;
+    CK( cudaDeviceGetAttribute( &maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev ) );
+    const int cl = h->cfg.closure, nT = h->tab.nT, nQ = h->tab.nQ, nS = h->nS;
+    const size_t n = size_t( nS ) * nT;
+    h->group        = n <= 32 ? 32 : 256;
+    h->closureBlock = 256;
+    const int groupsPerCta = h->closureBlock / h->group;
+    const size_t tables    = 2 * ( size_t( nQ ) * h->ld + 4 ) * sizeof( double );
+    const size_t ws        = cell_ws_doubles( nS, nT, nQ, closure_np( cl ) ) * sizeof( double ) * groupsPerCta;
+    h->tablesInSmem        = tables + ws <= size_t( maxSmem ) && tables <= 96 * 1024;
+    h->closureSmem         = ws + ( h->tablesInSmem ? tables : 0 );
+    if( h->closureSmem > size_t( maxSmem ) )
+        throw ConfigError( "closure workspace (" + std::to_string( h->closureSmem ) + " B) exceeds shared memory; reduce moments or nodes" );
+    void* kc = pick( cl, h->group, 0 );
+    CK( cudaFuncSetAttribute( kc, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->closureSmem ) ) );
+    int occ = 0;
+    CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kc, h->closureBlock, h->closureSmem ) );
+    h->closureGrid = std::max( 1, occ ) * h->numSMs;
+    // update kernel: phiWf + per-group flux buffers
+    h->updateBlock     = 256;
+    const int ug       = h->updateBlock / h->group;
+    size_t uTables     = h->tablesInSmem ? ( size_t( nQ ) * h->ld + 4 ) * sizeof( double ) : 0;
+    h->updateSmem      = uTables + size_t( ug ) * ( size_t( h->mesh.nFaces ) * nS * nQ + 32 ) * sizeof( double );
+    if( h->updateSmem > size_t( maxSmem ) ) throw ConfigError( "update workspace exceeds shared memory" );
+    void* ku = pick( cl, h->group, 1 );
+    CK( cudaFuncSetAttribute( ku, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->updateSmem ) ) );
+    CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ku, h->updateBlock, h->updateSmem ) );
+    h->updateGrid = std::max( 1, occ ) * h->numSMs;
+    h->updateGrid = std::min( h->updateGrid, std::max( 1, ( h->mesh.nCells + ug - 1 ) / ug ) );
+    h->initSmem   = size_t( ug ) * ( size_t( nS ) * nQ + 8 ) * sizeof( double );
+    h->mvSmem     = size_t( ug ) * ( 2 * size_t( nS ) * nQ + 8 ) * sizeof( double );
+    for( int which : {2, 3} ) {
+        size_t sm = which == 2 ? h->initSmem : h->mvSmem;
+        if( sm > size_t( maxSmem ) ) throw ConfigError( "init/meanvar workspace exceeds shared memory" );
+        CK( cudaFuncSetAttribute( pick( cl, h->group, which ), cudaFuncAttributeMaxDynamicSharedMemorySize, int( sm ) ) );
+    }
+    h->auxGrid = std::min( 4 * h->numSMs, std::max( 1, ( h->mesh.nCells + ug - 1 ) / ug ) );
+    h->mixed   = plan_mixed( cl, nS, nT, nQ, h->ld, maxSmem );
+}
+
+void reset_control( uqc_solver* h, double t ) {
+    Control c{};
+    c.t               = t;
+    c.tEnd            = h->cfg.tEnd;
+    c.minResidual     = h->cfg.minResidual;
+    c.residual        = h->cfg.minResidual + 1.0;    // momentsolver.cpp:76
+    c.dtBits          = 0x7FF0000000000000ull;
+    c.active          = t < h->cfg.tEnd ? 1 : 0;
+    *h->h_ctl         = c;
+    CK( cudaMemcpyAsync( h->d_ctl, h->h_ctl, sizeof( Control ), cudaMemcpyHostToDevice, h->stream ) );
+    CK( cudaStreamSynchronize( h->stream ) );
+}
+
+void read_control( uqc_solver* h ) {
+    CK( cudaMemcpyAsync( h->h_ctl, h->d_ctl, sizeof( Control ), cudaMemcpyDeviceToHost, h->stream ) );
+    CK( cudaStreamSynchronize( h->stream ) );
+}
+
+void build( uqc_solver* h, const std::string& text, void* stream ) {
+    h->cfg = parse_config( text );
+    h->tab = build_tables( h->cfg );
+    h->nS  = h->cfg.closure == CL_BOUNDED_BARRIER ? 1 : ( h->cfg.closure == CL_EULER2D ? 4 : 2 );
+    h->ld  = ( h->tab.nT % 2 ) ? h->tab.nT : h->tab.nT + 1;    // odd row stride: conflict-free column reads
+    h->ldc = size_t( h->nS ) * h->tab.nT;
+    if( h->cfg.meshDim == 1 )
+        h->mesh = build_mesh_1d( h->cfg.nCells1d, h->cfg.a, h->cfg.b );
+    else {
+        int nn = ( h->cfg.nx + 1 ) * ( h->cfg.ny + 1 ), nt = 2 * h->cfg.nx * h->cfg.ny;
+        std::vector<double> xy( 2 * size_t( nn ) );
+        std::vector<int> bnd( nn ), tri( 3 * size_t( nt ) );
+        tri_jitter_nodes( h->cfg.nx, h->cfg.ny, h->cfg.jitter, h->cfg.seed, xy.data(), bnd.data(), tri.data() );
+        h->mesh = build_mesh_tri( nn, xy.data(), bnd.data(), nt, tri.data() );
+    }
+    h->precision = h->cfg.precision;
+    h->userStream = (cudaStream_t)stream;
+}
+
+// Device side of a handle, set up on first use so that configuration, tables
+// and mesh (host code) work without a GPU.
+void ensure_device( uqc_solver* h ) {
+    if( h->deviceReady ) return;
+    if( h->userStream ) {
+        h->stream = h->userStream;
+    }
+    else {
+        CK( cudaStreamCreateWithFlags( &h->stream, cudaStreamNonBlocking ) );
+        h->ownStream = true;
+    }
+    // tables with zero padding rows (row stride ld, 8 spare doubles)
+    const int nQ = h->tab.nQ, nT = h->tab.nT;
+    std::vector<double> phi( size_t( nQ ) * h->ld + 8, 0.0 ), phiWf( size_t( nQ ) * h->ld + 8, 0.0 );
+    for( int k = 0; k < nQ; ++k )
+        for( int i = 0; i < nT; ++i ) {
+            phi[size_t( k ) * h->ld + i]   = h->tab.phi[size_t( k ) * nT + i];
+            phiWf[size_t( k ) * h->ld + i] = h->tab.phiWf[size_t( k ) * nT + i];
+        }
+    h->d_phi   = dupload( phi );
+    h->d_phiWf = dupload( phiWf );
+    h->d_xi    = dupload( h->tab.xi );
+    const Mesh& m = h->mesh;
+    std::vector<double> dx( m.nCells );
+    for( int j = 0; j < m.nCells; ++j ) dx[j] = m.maxEdge[j] / m.area[j];    // momentsolver.cpp:130
+    h->d_area     = dupload( m.area );
+    h->d_dx       = dupload( dx );
+    h->d_center   = dupload( m.center );
+    h->d_unitN    = dupload( m.unitN );
+    h->d_scaledN  = dupload( m.scaledN );
+    h->d_nbr      = dupload( m.nbr );
+    h->d_boundary = dupload( m.boundary );
+    const size_t N = size_t( m.nCells );
+    h->d_u         = dalloc<double>( N * h->ldc );
+    h->d_lam       = dalloc<double>( N * h->ldc );
+    h->d_uQ        = dalloc<double>( ( N + 1 ) * h->nS * nQ );    // +1: ghost cell (never read by Dirichlet runs)
+    CK( cudaMemset( h->d_uQ, 0, ( N + 1 ) * h->nS * nQ * sizeof( double ) ) );
+    h->d_uOld0  = dalloc<double>( N );
+    h->d_level  = dalloc<unsigned>( N );
+    h->d_status = dalloc<int>( N );
+    h->d_iters  = dalloc<int>( N );
+    h->d_ctl    = dalloc<Control>( 1 );
+    CK( cudaMallocHost( &h->h_ctl, sizeof( Control ) ) );
+    for( auto& e : h->ev ) CK( cudaEventCreate( &e ) );
+    plan_launches( h );
+    h->d_blockPartial = dalloc<double>( std::max( h->updateGrid, 1 ) );
+    alloc_mixed( h->mixed, N );
+    h->deviceReady = true;
+    reset_control( h, 0.0 );
+}
+
+void release( uqc_solver* h ) {
+    if( h->graph ) cudaGraphExecDestroy( h->graph );
+    for( void* p : {(void*)h->d_phi, (void*)h->d_phiWf, (void*)h->d_xi, (void*)h->d_area, (void*)h->d_dx, (void*)h->d_center,
+                    (void*)h->d_unitN, (void*)h->d_scaledN, (void*)h->d_nbr, (void*)h->d_boundary, (void*)h->d_u, (void*)h->d_lam,
+                    (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
+                    (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
+                    (void*)h->d_xIters} )
+        if( p ) cudaFree( p );
+    free_mixed( h->mixed );
+    if( h->h_ctl ) cudaFreeHost( h->h_ctl );
+    for( auto& e : h->ev )
+        if( e ) cudaEventDestroy( e );
+    if( h->ownStream && h->stream ) cudaStreamDestroy( h->stream );
+}
+
+// Closure launch: FP64 kernel, or the mixed-precision pipeline.
+void launch_closure( uqc_solver* h, KParams& P, int mode ) {
+    if( h->precision == UQC_MIXED && h->mixed.ok ) {
+        h->launches += launch_mixed_closure( h->mixed, P, mode, h->cfg.closure, h->stream );
+        return;
+    }
+    void* args[] = {&P, &mode};
+    launch( h, pick( h->cfg.closure, h->group, 0 ), h->closureGrid, h->closureBlock, h->closureSmem, args );
+}
+
+void enqueue_step( uqc_solver* h, KParams& P ) {
+    launch_closure( h, P, 1 );
+    void* args[] = {&P};
+    launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
+}
+
+// Reads the control block, fills info with this call's deltas, returns the
+// number of cells that failed during the call.
+int fill_info( uqc_solver* h, uqc_step_info* info, int stepsBefore ) {
+    read_control( h );
+    const Control& c = *h->h_ctl;
+    const int failedNow = c.failedCells - h->lastFailed;
+    if( info ) {
+        info->t                  = c.t;
+        info->dt                 = c.dt;
+        info->residual           = c.residual;
+        info->steps              = c.steps - stepsBefore;
+        info->failed_cells       = c.failedCells - h->lastFailed;
+        info->newton_iterations  = (long long)( c.newtonIters - h->lastIters );
+        info->line_search_trials = (long long)( c.lineSearchTrials - h->lastLs );
+        info->active_cells       = c.activeCellsLast;
+    }
+    h->lastIters  = c.newtonIters;
+    h->lastLs     = c.lineSearchTrials;
+    h->lastFailed = c.failedCells;
+    return failedNow;
+}
+
+void to_layout( const uqc_solver* h, const double* src, double* dst, int layout, bool toDevice ) {
+    // REF: (s, i) at i nS + s ; STATE_MAJOR: s nT + i
+    const size_t N = size_t( h->mesh.nCells ), nT = size_t( h->tab.nT ), nS = size_t( h->nS );
+    for( size_t j = 0; j < N; ++j )
+        for( size_t s = 0; s < nS; ++s )
+            for( size_t i = 0; i < nT; ++i ) {
+                size_t sm = j * nS * nT + s * nT + i, rf = j * nS * nT + i * nS + s;
+                if( toDevice )
+                    dst[sm] = src[rf];
+                else
+                    dst[rf] = src[sm];
+            }
+    (void)layout;
+}
+
+}    // namespace
+
+// ========================================================================== C ABI
+
+extern "C" {
+
+int uqc_create_from_string( const char* toml_text, void* cuda_stream, uqc_solver** out, char* err, int err_len ) {
+    if( !out || !toml_text ) return UQC_ERR_ARGUMENT;
+    *out           = nullptr;
+    uqc_solver* h  = new uqc_solver();
+    int rc         = guarded( h, [&] {
+        build( h, toml_text, cuda_stream );
+        return UQC_OK;
+    } );
+    if( rc != UQC_OK ) {
+        if( err && err_len > 0 ) {
+            std::strncpy( err, h->err.c_str(), size_t( err_len - 1 ) );
+            err[err_len - 1] = 0;
+        }
+        release( h );
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return UQC_OK;
+}
+
+int uqc_create_from_file( const char* toml_path, void* cuda_stream, uqc_solver** out, char* err, int err_len ) {
+    if( !toml_path || !out ) return UQC_ERR_ARGUMENT;
+    std::ifstream f( toml_path );
+    if( !f ) {
+        if( err && err_len > 0 ) std::snprintf( err, size_t( err_len ), "cannot open %s", toml_path );
+        return UQC_ERR_CONFIG;
+    }
+    std::stringstream ss;
+    ss << f.rdbuf();
+    return uqc_create_from_string( ss.str().c_str(), cuda_stream, out, err, err_len );
+}
+
+void uqc_destroy( uqc_solver* h ) {
+    if( !h ) return;
+    if( h->stream ) cudaStreamSynchronize( h->stream );
+    release( h );
+    delete h;
+}
+
+const char* uqc_last_error( const uqc_solver* h ) { return h ? h->err.c_str() : "null handle"; }
+
+int uqc_get_info( const uqc_solver* h, uqc_info* o ) {
+    if( !h || !o ) return UQC_ERR_ARGUMENT;
+    std::memset( o, 0, sizeof( *o ) );
+    o->n_cells  = h->mesh.nCells;
+    o->n_states = h->nS;
+    o->n_total  = h->tab.nT;
+    o->n_quad   = h->tab.nQ;
+    o->n_levels = h->tab.nLevels;
+    o->dim_xi   = h->tab.dimXi;
+    o->n_faces  = h->mesh.nFaces;
+    o->mesh_dim = h->mesh.dim;
+    for( int l = 0; l < h->tab.nLevels && l < 16; ++l ) o->n_total_level[l] = h->tab.nTLevel[l];
+    o->precision   = h->precision;
+    o->newton_mode = h->cfg.newtonMode;
+    o->t           = h->h_ctl ? h->h_ctl->t : 0.0;
+    o->steps       = h->h_ctl ? h->h_ctl->steps : 0;
+    return UQC_OK;
+}
+
+int uqc_set_precision( uqc_solver* h, int precision ) {
+    if( !h || ( precision != UQC_FP64 && precision != UQC_MIXED ) ) return UQC_ERR_ARGUMENT;
+    int rc = guarded( h, [&] {
+        ensure_device( h );
+        return UQC_OK;
+    } );
+    if( rc != UQC_OK ) return rc;
+    if( precision == UQC_MIXED && !h->mixed.ok ) return fail( h, UQC_ERR_CONFIG, "mixed precision not available for this configuration: " + h->mixed.why );
+    h->precision = precision;
+    return UQC_OK;
+}
+
+int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newton_mode ) {
+    if( !h || max_iterations < 1 || !( epsilon > 0 ) || newton_mode < 0 || newton_mode > 2 ) return UQC_ERR_ARGUMENT;
+    h->cfg.maxIterations = max_iterations;
+    h->cfg.epsilon       = epsilon;
+    h->cfg.newtonMode    = newton_mode;
+    return UQC_OK;
+}
+
+int uqc_get_tables( const uqc_solver* h, double* phi, double* phi_wf, double* xi, double* w ) {
+    if( !h ) return UQC_ERR_ARGUMENT;
+    if( phi ) std::memcpy( phi, h->tab.phi.data(), h->tab.phi.size() * sizeof( double ) );
+    if( phi_wf ) std::memcpy( phi_wf, h->tab.phiWf.data(), h->tab.phiWf.size() * sizeof( double ) );
+    if( xi ) std::memcpy( xi, h->tab.xi.data(), h->tab.xi.size() * sizeof( double ) );
+    if( w ) std::memcpy( w, h->tab.w.data(), h->tab.w.size() * sizeof( double ) );
+    return UQC_OK;
+}
+
+int uqc_get_geometry( const uqc_solver* h, double* area, double* max_edge, double* center, double* unit_normal, double* scaled_normal,
+                      int* neighbor, int* boundary ) {
+    if( !h ) return UQC_ERR_ARGUMENT;
+    const Mesh& m = h->mesh;
+    if( area ) std::memcpy( area, m.area.data(), m.area.size() * sizeof( double ) );
+    if( max_edge ) std::memcpy( max_edge, m.maxEdge.data(), m.maxEdge.size() * sizeof( double ) );
+    if( center ) std::memcpy( center, m.center.data(), m.center.size() * sizeof( double ) );
+    if( unit_normal ) std::memcpy( unit_normal, m.unitN.data(), m.unitN.size() * sizeof( double ) );
+    if( scaled_normal ) std::memcpy( scaled_normal, m.scaledN.data(), m.scaledN.size() * sizeof( double ) );
+    if( neighbor ) std::memcpy( neighbor, m.nbr.data(), m.nbr.size() * sizeof( int ) );
+    if( boundary ) std::memcpy( boundary, m.boundary.data(), m.boundary.size() * sizeof( int ) );
+    return UQC_OK;
+}
+
+int uqc_init_state( uqc_solver* h ) {
+    if( !h ) return UQC_ERR_ARGUMENT;
+    return guarded_dev( h, [&] {
+        h->launches  = 0;
+        KParams P    = make_params( h );
+        void* args[] = {&P};
+        launch( h, pick( h->cfg.closure, h->group, 2 ), h->auxGrid, h->updateBlock, h->initSmem, args );
+        CK( cudaGetLastError() );
+        reset_control( h, 0.0 );
+        h->stateReady = true;
+        return UQC_OK;
+    } );
+}
+
+int uqc_upload_state( uqc_solver* h, const double* u, const double* lambda, const unsigned* level, int layout, double t ) {
+    if( !h || ( layout != UQC_LAYOUT_REF && layout != UQC_LAYOUT_STATE_MAJOR ) ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady && ( !u || !lambda ) ) return fail( h, UQC_ERR_STATE, "first upload needs both u and lambda" );
+    return guarded_dev( h, [&] {
+        const size_t N = size_t( h->mesh.nCells ), bytes = N * h->ldc * sizeof( double );
+        std::vector<double> tmp;
+        for( int which = 0; which < 2; ++which ) {
+            const double* src = which == 0 ? u : lambda;
+            double* dst       = which == 0 ? h->d_u : h->d_lam;
+            if( !src ) continue;
+            if( layout == UQC_LAYOUT_REF ) {
+                tmp.resize( N * h->ldc );
+                to_layout( h, src, tmp.data(), layout, true );
+                src = tmp.data();
+                CK( cudaMemcpyAsync( dst, src, bytes, cudaMemcpyHostToDevice, h->stream ) );
+                CK( cudaStreamSynchronize( h->stream ) );
+            }
+            else {
+                CK( cudaMemcpyAsync( dst, src, bytes, cudaMemcpyHostToDevice, h->stream ) );
+            }
+        }
+        if( level ) {
+            for( size_t j = 0; j < N; ++j )
+                if( level[j] >= unsigned( h->tab.nLevels ) ) throw std::invalid_argument( "refinement level out of range" );
+            CK( cudaMemcpyAsync( h->d_level, level, N * sizeof( unsigned ), cudaMemcpyHostToDevice, h->stream ) );
+        }
+        else if( !h->stateReady ) {
+            std::vector<unsigned> lv( N, unsigned( h->tab.nLevels - 1 ) );
+            CK( cudaMemcpyAsync( h->d_level, lv.data(), N * sizeof( unsigned ), cudaMemcpyHostToDevice, h->stream ) );
+            CK( cudaStreamSynchronize( h->stream ) );
+        }
+        reset_control( h, t );
+        h->stateReady = true;
+        return UQC_OK;
+    } );
+}
+
+int uqc_download_state( uqc_solver* h, double* u, double* lambda, unsigned* level, int layout ) {
+    if( !h || ( layout != UQC_LAYOUT_REF && layout != UQC_LAYOUT_STATE_MAJOR ) ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state (call uqc_init_state or uqc_upload_state)" );
+    return guarded_dev( h, [&] {
+        const size_t N = size_t( h->mesh.nCells ), bytes = N * h->ldc * sizeof( double );
+        std::vector<double> tmp;
+        for( int which = 0; which < 2; ++which ) {
+            double* dst       = which == 0 ? u : lambda;
+            const double* src = which == 0 ? h->d_u : h->d_lam;
+            if( !dst ) continue;
+            if( layout == UQC_LAYOUT_REF ) {
+                tmp.resize( N * h->ldc );
+                CK( cudaMemcpyAsync( tmp.data(), src, bytes, cudaMemcpyDeviceToHost, h->stream ) );
+                CK( cudaStreamSynchronize( h->stream ) );
+                to_layout( h, tmp.data(), dst, layout, false );
+            }
+            else {
+                CK( cudaMemcpyAsync( dst, src, bytes, cudaMemcpyDeviceToHost, h->stream ) );
+            }
+        }
+        if( level ) CK( cudaMemcpyAsync( level, h->d_level, N * sizeof( unsigned ), cudaMemcpyDeviceToHost, h->stream ) );
+        CK( cudaStreamSynchronize( h->stream ) );
+        return UQC_OK;
+    } );
+}
+
+int uqc_solve_closure( uqc_solver* h, uqc_step_info* info ) {
+    if( !h ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
+    return guarded_dev( h, [&] {
+        h->launches = 0;
+        read_control( h );
+        int stepsBefore = h->h_ctl->steps;
+        CK( cudaMemsetAsync( &h->d_ctl->workCounter, 0, sizeof( unsigned ), h->stream ) );
+        KParams P = make_params( h );
+        launch_closure( h, P, 0 );
+        CK( cudaGetLastError() );
+        int failed = fill_info( h, info, stepsBefore );
+        return failed ? fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( failed ) + " cells did not converge" ) : UQC_OK;
+    } );
+}
+
+int uqc_cell_status( uqc_solver* h, int* status, int* iterations ) {
+    if( !h ) return UQC_ERR_ARGUMENT;
+    return guarded_dev( h, [&] {
+        size_t N = size_t( h->mesh.nCells );
+        if( status ) CK( cudaMemcpyAsync( status, h->d_status, N * sizeof( int ), cudaMemcpyDeviceToHost, h->stream ) );
+        if( iterations ) CK( cudaMemcpyAsync( iterations, h->d_iters, N * sizeof( int ), cudaMemcpyDeviceToHost, h->stream ) );
+        CK( cudaStreamSynchronize( h->stream ) );
+        return UQC_OK;
+    } );
+}
+
+int uqc_step( uqc_solver* h, int n_steps, uqc_step_info* info ) {
+    if( !h || n_steps < 0 ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state (call uqc_init_state or uqc_upload_state)" );
+    return guarded_dev( h, [&] {
+        h->launches     = 0;
+        int stepsBefore = h->h_ctl->steps;
+        KParams P       = make_params( h );
+        for( int s = 0; s < n_steps; ++s ) {
+            const bool last = s == n_steps - 1;
+            if( last ) CK( cudaEventRecord( h->ev[0], h->stream ) );
+            launch_closure( h, P, 1 );
+            if( last ) CK( cudaEventRecord( h->ev[1], h->stream ) );
+            void* args[] = {&P};
+            launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
+            if( last ) CK( cudaEventRecord( h->ev[2], h->stream ) );
+        }
+        CK( cudaGetLastError() );
+        int failed = fill_info( h, info, stepsBefore );
+        if( n_steps > 0 ) {
+            CK( cudaEventElapsedTime( &h->lastMs[0], h->ev[0], h->ev[1] ) );
+            CK( cudaEventElapsedTime( &h->lastMs[1], h->ev[1], h->ev[2] ) );
+            CK( cudaEventElapsedTime( &h->lastMs[2], h->ev[0], h->ev[2] ) );
+        }
+        return failed ? fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( failed ) + " cells did not converge" ) : UQC_OK;
+    } );
+}
+
+int uqc_run( uqc_solver* h, double t_end, uqc_step_info* info ) {
+    if( !h ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
+    return guarded_dev( h, [&] {
+        if( t_end > 0 ) {
+            h->cfg.tEnd = t_end;
+            read_control( h );
+            h->h_ctl->tEnd   = t_end;
+            h->h_ctl->active = ( h->h_ctl->t < t_end && h->h_ctl->residual > h->h_ctl->minResidual ) ? 1 : 0;
+            CK( cudaMemcpyAsync( h->d_ctl, h->h_ctl, sizeof( Control ), cudaMemcpyHostToDevice, h->stream ) );
+        }
+        read_control( h );
+        int stepsBefore = h->h_ctl->steps;
+        unsigned long long it0 = h->lastIters, ls0 = h->lastLs;
+        int f0 = h->lastFailed;
+        KParams P = make_params( h );
+        while( h->h_ctl->active ) {
+            for( int s = 0; s < 32; ++s ) enqueue_step( h, P );    // kernels turn into no-ops once the loop condition fails
+            read_control( h );
+        }
+        CK( cudaGetLastError() );
+        h->lastIters  = it0;
+        h->lastLs     = ls0;
+        h->lastFailed = f0;
+        int failed    = fill_info( h, info, stepsBefore );
+        return failed ? fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( failed ) + " cells did not converge" ) : UQC_OK;
+    } );
+}
+
+int uqc_mean_var( uqc_solver* h, double* out ) {
+    if( !h || !out ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
+    return guarded_dev( h, [&] {
+        const size_t N = size_t( h->mesh.nCells ), cnt = N * 2 * h->nS;
+        double* d_out  = dalloc<double>( cnt );
+        KParams P      = make_params( h );
+        void* args[]   = {&P, &d_out};
+        launch( h, pick( h->cfg.closure, h->group, 3 ), h->auxGrid, h->updateBlock, h->mvSmem, args );
+        CK( cudaMemcpyAsync( out, d_out, cnt * sizeof( double ), cudaMemcpyDeviceToHost, h->stream ) );
+        CK( cudaStreamSynchronize( h->stream ) );
+        cudaFree( d_out );
+        return UQC_OK;
+    } );
+}
+
+static void ensure_scratch( uqc_solver* h, size_t n ) {
+    if( n <= h->xCap ) return;
+    for( void* p : {(void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus, (void*)h->d_xIters} )
+        if( p ) cudaFree( p );
+    h->d_xLam    = dalloc<double>( n * h->ldc );
+    h->d_xU      = dalloc<double>( n * h->ldc );
+    h->d_xNt     = dalloc<unsigned>( n );
+    h->d_xStatus = dalloc<int>( n );
+    h->d_xIters  = dalloc<int>( n );
+    h->xCap      = n;
+}
+
+static void closure_on( uqc_solver* h, int n, double* d_lam, const double* d_u, const unsigned* d_nt, int* d_status, int* d_iters ) {
+    KParams P     = make_params( h );
+    P.nCells      = n;
+    P.lam         = d_lam;
+    P.u           = const_cast<double*>( d_u );
+    P.level       = nullptr;
+    P.nTotalCell  = d_nt;
+    P.status      = d_status;
+    P.iters       = d_iters;
+    CK( cudaMemsetAsync( &h->d_ctl->workCounter, 0, sizeof( unsigned ), h->stream ) );
+    launch_closure( h, P, 0 );
+    CK( cudaGetLastError() );
+}
+
+int uqc_closure_solve_host( uqc_solver* h, int n, double* lambda, const double* u, const unsigned* n_total, int layout, int* status ) {
+    if( !h || n < 0 || !lambda || !u || ( layout != UQC_LAYOUT_REF && layout != UQC_LAYOUT_STATE_MAJOR ) ) return UQC_ERR_ARGUMENT;
+    if( n == 0 ) return UQC_OK;
+    return guarded_dev( h, [&] {
+        h->launches = 0;
+        ensure_scratch( h, size_t( n ) );
+        const size_t cnt = size_t( n ) * h->ldc, nT = size_t( h->tab.nT ), nS = size_t( h->nS );
+        std::vector<double> L( cnt ), U( cnt );
+        for( size_t j = 0; j < size_t( n ); ++j )
+            for( size_t s = 0; s < nS; ++s )
+                for( size_t i = 0; i < nT; ++i ) {
+                    size_t sm = j * nS * nT + s * nT + i, src = layout == UQC_LAYOUT_REF ? j * nS * nT + i * nS + s : sm;
+                    L[sm] = lambda[src];
+                    U[sm] = u[src];
+                }
+        std::vector<unsigned> nt( n, unsigned( nT ) );
+        if( n_total )
+            for( int j = 0; j < n; ++j ) {
+                if( std::find( h->tab.nTLevel.begin(), h->tab.nTLevel.end(), int( n_total[j] ) ) == h->tab.nTLevel.end() )
+                    throw std::invalid_argument( "n_total[" + std::to_string( j ) + "] is not a refinement level size" );
+                nt[j] = n_total[j];
+            }
+        CK( cudaMemcpyAsync( h->d_xLam, L.data(), cnt * sizeof( double ), cudaMemcpyHostToDevice, h->stream ) );
+        CK( cudaMemcpyAsync( h->d_xU, U.data(), cnt * sizeof( double ), cudaMemcpyHostToDevice, h->stream ) );
+        CK( cudaMemcpyAsync( h->d_xNt, nt.data(), n * sizeof( unsigned ), cudaMemcpyHostToDevice, h->stream ) );
+        closure_on( h, n, h->d_xLam, h->d_xU, h->d_xNt, h->d_xStatus, h->d_xIters );
+        std::vector<int> st( n );
+        CK( cudaMemcpyAsync( L.data(), h->d_xLam, cnt * sizeof( double ), cudaMemcpyDeviceToHost, h->stream ) );
+        CK( cudaMemcpyAsync( st.data(), h->d_xStatus, n * sizeof( int ), cudaMemcpyDeviceToHost, h->stream ) );
+        CK( cudaStreamSynchronize( h->stream ) );
+        for( size_t j = 0; j < size_t( n ); ++j )
+            for( size_t s = 0; s < nS; ++s )
+                for( size_t i = 0; i < nT; ++i ) {
+                    size_t sm = j * nS * nT + s * nT + i, dst = layout == UQC_LAYOUT_REF ? j * nS * nT + i * nS + s : sm;
+                    lambda[dst] = L[sm];
+                }
+        int bad = 0;
+        for( int j = 0; j < n; ++j ) {
+            if( status ) status[j] = st[j];
+            bad += st[j] != 0;
+        }
+        return bad ? fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( bad ) + " cells did not converge" ) : UQC_OK;
+    } );
+}
+
+int uqc_closure_solve_device( uqc_solver* h, int n, double* d_lambda, const double* d_u, const unsigned* d_n_total, int* d_status ) {
+    if( !h || n < 0 || !d_lambda || !d_u ) return UQC_ERR_ARGUMENT;
+    if( n == 0 ) return UQC_OK;
+    return guarded_dev( h, [&] {
+        h->launches = 0;
+        ensure_scratch( h, size_t( n ) );
+        unsigned* nt = const_cast<unsigned*>( d_n_total );
+        if( !nt ) {
+            std::vector<unsigned> v( n, unsigned( h->tab.nT ) );
+            CK( cudaMemcpyAsync( h->d_xNt, v.data(), n * sizeof( unsigned ), cudaMemcpyHostToDevice, h->stream ) );
+            CK( cudaStreamSynchronize( h->stream ) );
+            nt = h->d_xNt;
+        }
+        closure_on( h, n, d_lambda, d_u, nt, d_status ? d_status : h->d_xStatus, h->d_xIters );
+        return UQC_OK;
+    } );
+}
+
+int uqc_last_timing( uqc_solver* h, float* ms3 ) {
+    if( !h || !ms3 ) return UQC_ERR_ARGUMENT;
+    for( int i = 0; i < 3; ++i ) ms3[i] = h->lastMs[i];
+    return UQC_OK;
+}
+
+int uqc_device_state( uqc_solver* h, double** d_u, double** d_lambda ) {
+    if( !h ) return UQC_ERR_ARGUMENT;
+    int rc = guarded( h, [&] {
+        ensure_device( h );
+        return UQC_OK;
+    } );
+    if( rc != UQC_OK ) return rc;
+    if( d_u ) *d_u = h->d_u;
+    if( d_lambda ) *d_lambda = h->d_lam;
+    return UQC_OK;
+}
+
+int uqc_last_launch_count( uqc_solver* h ) { return h ? h->launches : 0; }
+
+void* uqc_stream( uqc_solver* h ) {
+    if( !h || guarded( h, [&] {
+            ensure_device( h );
+            return UQC_OK;
+        } ) != UQC_OK )
+        return nullptr;
+    return (void*)h->stream;
+}
+
+int uqc_mesh_tri_jitter( int nx, int ny, double jitter, unsigned long long seed, double* xy, int* node_boundary, int* tri ) {
+    if( nx < 1 || ny < 1 || !xy || !node_boundary || !tri ) return UQC_ERR_ARGUMENT;
+    tri_jitter_nodes( nx, ny, jitter, seed, xy, node_boundary, tri );
+    return UQC_OK;
+}
+
+}    // extern "C"
