@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Benchmark of the IPM hot path on the 2-D Euler workload (200,000 cells).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: 2-D Euler (gamma 1.4), seeded jittered triangle mesh of 400 x 250
+rectangles x 2 = 200,000 cells on [0,1]^2, uncertain Sod-type interface
+(x = 0.5 + 0.05 xi1, left density 1 + 0.1 xi2), total-degree-5 Legendre basis
+(21 moments x 4 states = 84 duals per cell), 10 x 10 tensor Gauss nodes,
+guarded Newton to |g| < 1e-10. Synthetic, seeded; no dataset is involved.
+
+A step is one explicit time step of the hot path (closure for every cell,
+nodal reconstruction, kinetic flux, update). `value` is cell-steps/s of the
+chosen form with the state resident in HBM; `e2e` is the same metric through
+the C ABI with the state uploaded from and downloaded to pinned host memory
+every step. The plain FP64 form is timed in the same run (`fp64`), from the same
+state, and the chosen form's moments are compared with it after the K steps.
+
+N > 1 (torchrun): replicas only. Each rank runs its own copy of the workload
+on its GPU; there is no data-path collective; time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cell-steps/s mixed vs FP64 GPU at ≤1e-6 moment err; p50/p99 request latency"
+WORKLOAD = dict(nx=400, ny=250, degree=5, nquad=10, dim_xi=2)
+SAMPLE_NY = 10           # CPU sample: a 400 x 10 strip of the same mesh construction (8,000 cells)
+FP64_NOMINAL_TFLOPS = 40.0
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def work_per_cell_step(n_states, n_total, n_quad, n_faces=3):
+    """Algorithmic FP64-equivalent flops of the closure kernel, per unit:
+    F_it per Newton iteration = 2 nQ n^2 (Hessian) + 4 nQ n (ansatz + gradient)
+    + n^3/3 + 2 n^2 (Cholesky + solves); 4 nQ n per extra gradient evaluation
+    (initial check, line-search trial); epilogue 4 nQ n (reconstruction +
+    re-projection)."""
+    n = n_states * n_total
+    f_it = 2 * n_quad * n * n + 4 * n_quad * n + n ** 3 / 3 + 2 * n * n
+    f_grad = 4 * n_quad * n
+    f_epi = 4 * n_quad * n
+    f_flux = n_faces * 2 * n_quad * n
+    return f_it, f_grad, f_epi, f_flux
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during a timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.rows = []
+        if self.p is None:
+            return
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out = ""
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_run(steps, warmup, min_seconds=None, ny=SAMPLE_NY):
+    """UQCreator's own code (oracle/_ref, OpenMP build) on a strip of the workload."""
+    from oracle import refharness
+    from uqcreator_b200 import workloads as W
+    toml = W.euler2d(nx=WORKLOAD["nx"], ny=ny)
+    r = refharness.RefSolver(toml, "Euler2D", [0.5, 1.0, 1.0, 0.125, 0.1], bounds=(3, 12), mesh2d=W.mesh_for(toml),
+                             variant="omp", newton="guarded")
+    r.init_state()
+    for _ in range(warmup):
+        r.step(1)
+    t0 = time.perf_counter()
+    done = 0
+    while True:
+        r.step(1)
+        done += 1
+        el = time.perf_counter() - t0
+        if (min_seconds is None and done >= steps) or (min_seconds is not None and el >= min_seconds and done >= 1):
+            break
+    cores = os.cpu_count()
+    return dict(value=r.n_cells * done / el, unit="cell-steps/s", cores=cores, kind="reference",
+                sample=f"UQCreator C++ (OpenMP, {cores} threads) on a {WORKLOAD['nx']}x{ny}x2 = {r.n_cells}-cell strip of the same "
+                       f"workload after {warmup} warm-up steps, {done} steps in {el:.1f} s"), r.n_cells, done, el
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import refharness
+    if not refharness.available("omp"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libuqcref_omp.so not built (make -C oracle/ref)"}))
+        return
+    cb, cells, done, el = cpu_reference_run(args.steps, args.warmup)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": done,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / done, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "euler2d_sod_2u_deg5_q10x10", "cells": cells, "sample_of_cells": 200000},
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_b200(args, rank, world, local):
+    import torch
+    from uqcreator_b200 import Solver, workloads as W, FP64, MIXED
+
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.Stream(device=dev)
+    toml = W.euler2d(**WORKLOAD)
+    s = Solver(toml, stream=stream.cuda_stream)
+    s.init_state()
+    forms = ["fp64"]
+    try:
+        s.set_precision(MIXED)
+        s.set_precision(FP64)
+        forms.append("mixed")
+    except Exception:
+        pass
+    chosen = "mixed" if "mixed" in forms else "fp64"
+    # warm-up (FP64: the first step from the initial state is the expensive one)
+    warm = s.step(args.warmup)
+    u0, l0, v0 = s.download_state()
+    results = {}
+    for form in forms:
+        s.set_precision(MIXED if form == "mixed" else FP64)
+        s.upload_state(u0, l0, v0, t=warm["t"])
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(dev) as ck:
+            ev0.record(stream)
+            info = s.step(args.steps)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        barrier(world)
+        ms = ev0.elapsed_time(ev1)
+        phase = s.last_timing()
+        results[form] = dict(ms=max_over_ranks(ms, world), info=info, phase=phase, clocks=ck.summary(),
+                             launches=s.last_launch_count(), state=s.download_state())
+    # accuracy of the chosen form vs the FP64 form after the same K steps
+    err = None
+    if chosen != "fp64":
+        uf, ub = results["fp64"]["state"][0], results[chosen]["state"][0]
+        area = s.geometry()["area"][:, None, None]
+        err = float(((np.abs(ub - uf) * area).sum(axis=(0, 2)) / (np.abs(uf) * area).sum(axis=(0, 2))).max())
+    # end to end through the C ABI with pinned host buffers, chosen form
+    s.set_precision(MIXED if chosen == "mixed" else FP64)
+    s.upload_state(u0, l0, v0, t=warm["t"])
+    hu = torch.empty(u0.shape, dtype=torch.float64, pin_memory=True).numpy()
+    hl = torch.empty(l0.shape, dtype=torch.float64, pin_memory=True).numpy()
+    hv = torch.empty(v0.shape, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    hu[...] = u0; hl[...] = l0; hv[...] = v0
+    e2e_steps = max(1, min(args.steps, 10))
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    tcur = warm["t"]
+    for _ in range(e2e_steps):
+        s.upload_state(hu, hl, hv, t=tcur)
+        inf = s.step(1)
+        tcur = inf["t"]
+        s.download_state(out=(hu, hl, hv))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(max(ev0.elapsed_time(ev1), 1e3 * (time.perf_counter() - t0)), world)
+    cells = s.n_cells
+    r = results[chosen]
+    value = cells * args.steps * world / (r["ms"] / 1e3)
+    fp64_value = cells * args.steps * world / (results["fp64"]["ms"] / 1e3)
+    # roofline of the dominant kernel (the closure kernel): algorithmic flops per launch / mean launch time
+    f_it, f_grad, f_epi, f_flux = work_per_cell_step(s.n_states, s.n_total, s.n_quad)
+    inf = r["info"]
+    flops = inf["newton_iterations"] * f_it + (inf["line_search_trials"] + cells * args.steps) * f_grad + cells * args.steps * f_epi
+    closure_ms = r["phase"][0] / args.steps
+    achieved = flops / args.steps / (closure_ms / 1e3) / 1e12
+    hbm, bf16, src = peaks()
+    roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
+            "traffic": None, "peak_source": src, "kernel": "k_closure (Newton + reconstruction)",
+            "closure_ms_per_launch": closure_ms, "update_ms_per_launch": r["phase"][1] / args.steps,
+            "fp64_nominal_tflops": FP64_NOMINAL_TFLOPS, "frac_of_fp64_nominal": achieved / FP64_NOMINAL_TFLOPS,
+            "flops_per_launch": flops / args.steps}
+    state_bytes = cells * s.n_states * s.n_total * 8
+    h2d = 2 * state_bytes + 4 * cells
+    d2h = 2 * state_bytes + 4 * cells
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16+f32+f64" if chosen == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": "euler2d_sod_2u_deg5_q10x10", "cells": cells, "duals_per_cell": s.n_states * s.n_total,
+                   "nodes": s.n_quad, "form": chosen, "parallelism": f"replicas{world}",
+                   "l2": f"inputs larger than L2 (resident state {cells * (2 * s.n_states * s.n_total + s.n_states * s.n_quad) * 8 / 1e9:.2f} GB)"},
+        "fp64": {"value": fp64_value, "ms_per_step": results["fp64"]["ms"] / args.steps},
+        "chosen_over_fp64": value / fp64_value,
+        "moment_rel_l1_vs_fp64": err,
+        "newton": {"iterations_per_step": inf["newton_iterations"] / args.steps, "active_cells_last_step": inf["active_cells"],
+                   "line_search_trials": inf["line_search_trials"]},
+        "roofline": roof,
+        "e2e": {"value": cells * e2e_steps * world / (e2e_ms / 1e3), "unit": "cell-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+        "gpu_launches": r["launches"],
+        "clocks": r["clocks"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb, *_ = cpu_reference_run(0, 2, min_seconds=args.cpu_seconds)
+            line["cpu_baseline"] = cb
+        except Exception as e:  # the reference build is optional on a box without it
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    if rank == 0:
+        print(json.dumps(line))
+    s.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_b200(args, rank, world, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -118,12 +118,13 @@ struct CellWs {
     double *LA, *LB, *uk;                   // nS nQ each
     double* du;                             // NP nQ
     double* H;                              // n (n + 1) / 2 packed upper
+    double *D, *I;                          // Cholesky pivots and their inverses (n each)
     double* red;                            // reduction scratch (16) + broadcast (16)
 };
 
 __host__ __device__ inline size_t cell_ws_doubles( int nS, int nT, int nQ, int NP ) {
     size_t n = size_t( nS ) * nT;
-    size_t s = 6 * n + 3 * size_t( nS ) * nQ + size_t( NP ) * nQ + n * ( n + 1 ) / 2 + 32;
+    size_t s = 8 * n + 3 * size_t( nS ) * nQ + size_t( NP ) * nQ + n * ( n + 1 ) / 2 + 32;
     return ( s + 3 ) & ~size_t( 3 );
 }
 
@@ -141,7 +142,9 @@ __device__ inline CellWs carve( double* p, int nS, int nT, int nQ, int NP ) {
     w.uk     = w.LB + size_t( nS ) * nQ;
     w.du     = w.uk + size_t( nS ) * nQ;
     w.H      = w.du + size_t( NP ) * nQ;
-    w.red    = w.H + n * ( n + 1 ) / 2;
+    w.D      = w.H + n * ( n + 1 ) / 2;
+    w.I      = w.D + n;
+    w.red    = w.I + n;
     return w;
 }
 
@@ -275,34 +278,45 @@ __device__ void hessian( const Grp<GROUP>& g, const KParams& P, const double* ph
 // itself and updates its share of the trailing triangle; row j is written
 // scaled one step later, when nobody reads it. Returns 0 or j + 1 of the first
 // non-positive pivot (posv's info > 0).
-template <int GROUP> __device__ int cholesky( const Grp<GROUP>& g, double* H, int n ) {
+// D[j] = sqrt of the pivot, I[j] = 1 / D[j], computed once per column by the
+// thread that owns the diagonal entry (thread 0 owns (j+1, j+1) in step j).
+template <int GROUP> __device__ int cholesky( const Grp<GROUP>& g, double* H, int n, double* D, double* I ) {
     constexpr int TX = GROUP == 32 ? 8 : 16, TY = GROUP / TX;
     const int tx = g.r % TX, ty = g.r / TX;
-    double prevInv = 0.0, prevD = 0.0;
+    if( g.r == 0 && H[0] > 0.0 ) {
+        D[0] = sqrt( H[0] );
+        I[0] = 1.0 / D[0];
+    }
+    g.sync();
     for( int j = 0; j < n; ++j ) {
         double ajj = H[packed( j, j )];
         if( !( ajj > 0.0 ) ) return j + 1;    // uniform: every thread reads the same value
-        double d = sqrt( ajj ), inv = 1.0 / d;
+        const double inv = I[j];
         if( j > 0 ) {
             // finalise row j-1: U(j-1, c) = A(j-1, c) / d_{j-1}
-            for( int c = j - 1 + g.r; c < n; c += GROUP ) H[packed( j - 1, c )] = ( c == j - 1 ) ? prevD : H[packed( j - 1, c )] * prevInv;
+            for( int c = j - 1 + g.r; c < n; c += GROUP ) H[packed( j - 1, c )] = ( c == j - 1 ) ? D[j - 1] : H[packed( j - 1, c )] * I[j - 1];
         }
         for( int c = j + 1 + ty; c < n; c += TY ) {
             double ujc = H[packed( j, c )] * inv;
             for( int r = j + 1 + tx; r <= c; r += TX ) H[packed( r, c )] -= ( H[packed( j, r )] * inv ) * ujc;
         }
-        prevInv = inv;
-        prevD   = d;
+        if( g.r == 0 && j + 1 < n ) {
+            double a = H[packed( j + 1, j + 1 )];
+            if( a > 0.0 ) {
+                D[j + 1] = sqrt( a );
+                I[j + 1] = 1.0 / D[j + 1];
+            }
+        }
         g.sync();
     }
-    for( int c = n - 1 + g.r; c < n; c += GROUP ) H[packed( n - 1, c )] = prevD;
+    if( g.r == 0 ) H[packed( n - 1, n - 1 )] = D[n - 1];
     g.sync();
     return 0;
 }
 
 // Solves U^T U x = b in place (x = b on entry) by one warp (dpotrs:
 // forward with U^T, then backward with U, sequential order of dtrsm).
-template <int GROUP> __device__ void chol_solve( const Grp<GROUP>& g, const double* H, int n, double* x ) {
+template <int GROUP> __device__ void chol_solve( const Grp<GROUP>& g, const double* H, int n, double* x, const double* I ) {
     if( g.r >= 32 ) return;
     const int lane = g.r;
     constexpr int MAXR = 8;    // rows per lane: n <= 256
@@ -315,7 +329,7 @@ template <int GROUP> __device__ void chol_solve( const Grp<GROUP>& g, const doub
 #pragma unroll
         for( int q = 0; q < MAXR; ++q )
             if( q == q0 && lane == own ) {
-                y[q] = y[q] / H[packed( i, i )];
+                y[q] = y[q] * I[i];
                 yi   = y[q];
             }
         yi = __shfl_sync( 0xffffffffu, yi, own );
@@ -331,7 +345,7 @@ template <int GROUP> __device__ void chol_solve( const Grp<GROUP>& g, const doub
 #pragma unroll
         for( int q = 0; q < MAXR; ++q )
             if( q == q0 && lane == own ) {
-                if( y[q] != 0.0 ) y[q] = y[q] / H[packed( k, k )];
+                if( y[q] != 0.0 ) y[q] = y[q] * I[k];
                 xk = y[q];
             }
         xk = __shfl_sync( 0xffffffffu, xk, own );
@@ -384,13 +398,13 @@ __device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double*
             double gn       = gradient<CL, GROUP>( g, P, phiWf, LA, w.uh, nTj, w.uk, w.g, w.red );
             hessian<CL, GROUP>( g, P, phi, phiWf, LA, nTj, w.du, w.H );
             g.sync();
-            if( cholesky<GROUP>( g, w.H, n ) ) {
+            if( cholesky<GROUP>( g, w.H, n, w.D, w.I ) ) {
                 rc = UQC_CELL_NOT_PD;
                 goto out;
             }
             for( int idx = g.r; idx < n; idx += GROUP ) w.d[idx] = w.g[idx];
             g.sync();
-            chol_solve<GROUP>( g, w.H, n, w.d );
+            chol_solve<GROUP>( g, w.H, n, w.d, w.I );
             g.sync();
             ++iters;
             for( int idx = g.r; idx < P.nS * P.nT; idx += GROUP ) w.lamN[idx] = w.lam[idx];
@@ -444,13 +458,13 @@ __device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double*
             }
             hessian<CL, GROUP>( g, P, phi, phiWf, LA, nTj, w.du, w.H );
             g.sync();
-            if( cholesky<GROUP>( g, w.H, n ) ) {
+            if( cholesky<GROUP>( g, w.H, n, w.D, w.I ) ) {
                 rc = UQC_CELL_NOT_PD;
                 goto out;
             }
             for( int idx = g.r; idx < n; idx += GROUP ) w.d[idx] = w.g[idx];
             g.sync();
-            chol_solve<GROUP>( g, w.H, n, w.d );
+            chol_solve<GROUP>( g, w.H, n, w.d, w.I );
             g.sync();
             ++iters;
             if( P.maxIter == 1 ) {

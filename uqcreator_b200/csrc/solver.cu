@@ -63,6 +63,7 @@ struct uqc_solver {
     unsigned long long lastIters = 0, lastLs = 0;
     int lastFailed = 0;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> stepEvents;
     float lastMs[3] = {0, 0, 0};
     cudaGraphExec_t graph = nullptr;
     std::string err;
@@ -251,6 +252,9 @@ void reset_control( uqc_solver* h, double t ) {
     c.dtBits          = 0x7FF0000000000000ull;
     c.active          = t < h->cfg.tEnd ? 1 : 0;
     *h->h_ctl         = c;
+    h->lastIters      = 0;    // device counters restart from zero
+    h->lastLs         = 0;
+    h->lastFailed     = 0;
     CK( cudaMemcpyAsync( h->d_ctl, h->h_ctl, sizeof( Control ), cudaMemcpyHostToDevice, h->stream ) );
     CK( cudaStreamSynchronize( h->stream ) );
 }
@@ -341,6 +345,8 @@ void release( uqc_solver* h ) {
     free_mixed( h->mixed );
     if( h->h_ctl ) cudaFreeHost( h->h_ctl );
     for( auto& e : h->ev )
+        if( e ) cudaEventDestroy( e );
+    for( auto& e : h->stepEvents )
         if( e ) cudaEventDestroy( e );
     if( h->ownStream && h->stream ) cudaStreamDestroy( h->stream );
 }
@@ -619,21 +625,31 @@ int uqc_step( uqc_solver* h, int n_steps, uqc_step_info* info ) {
         h->launches     = 0;
         int stepsBefore = h->h_ctl->steps;
         KParams P       = make_params( h );
+        // CUDA events around every launch on the handle's stream: per-phase
+        // device time summed over the steps of this call.
+        if( h->stepEvents.size() < size_t( 3 * n_steps ) ) {
+            size_t old = h->stepEvents.size();
+            h->stepEvents.resize( 3 * size_t( n_steps ) );
+            for( size_t i = old; i < h->stepEvents.size(); ++i ) CK( cudaEventCreate( &h->stepEvents[i] ) );
+        }
         for( int s = 0; s < n_steps; ++s ) {
-            const bool last = s == n_steps - 1;
-            if( last ) CK( cudaEventRecord( h->ev[0], h->stream ) );
+            CK( cudaEventRecord( h->stepEvents[3 * s], h->stream ) );
             launch_closure( h, P, 1 );
-            if( last ) CK( cudaEventRecord( h->ev[1], h->stream ) );
+            CK( cudaEventRecord( h->stepEvents[3 * s + 1], h->stream ) );
             void* args[] = {&P};
             launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
-            if( last ) CK( cudaEventRecord( h->ev[2], h->stream ) );
+            CK( cudaEventRecord( h->stepEvents[3 * s + 2], h->stream ) );
         }
         CK( cudaGetLastError() );
         int failed = fill_info( h, info, stepsBefore );
-        if( n_steps > 0 ) {
-            CK( cudaEventElapsedTime( &h->lastMs[0], h->ev[0], h->ev[1] ) );
-            CK( cudaEventElapsedTime( &h->lastMs[1], h->ev[1], h->ev[2] ) );
-            CK( cudaEventElapsedTime( &h->lastMs[2], h->ev[0], h->ev[2] ) );
+        h->lastMs[0] = h->lastMs[1] = h->lastMs[2] = 0.f;
+        for( int s = 0; s < n_steps; ++s ) {
+            float a = 0.f, b = 0.f;
+            CK( cudaEventElapsedTime( &a, h->stepEvents[3 * s], h->stepEvents[3 * s + 1] ) );
+            CK( cudaEventElapsedTime( &b, h->stepEvents[3 * s + 1], h->stepEvents[3 * s + 2] ) );
+            h->lastMs[0] += a;
+            h->lastMs[1] += b;
+            h->lastMs[2] += a + b;
         }
         return failed ? fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( failed ) + " cells did not converge" ) : UQC_OK;
     } );

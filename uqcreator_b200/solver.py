@@ -122,9 +122,14 @@ class Solver:
         lev = None if level is None else np.ascontiguousarray(level, dtype=np.uint32)
         check(self.h, self.lib.uqc_upload_state(self.h, ptr(u), ptr(lam), ptr(lev, L._up), layout, t))
 
-    def download_state(self, layout=L.LAYOUT_STATE_MAJOR):
+    def download_state(self, layout=L.LAYOUT_STATE_MAJOR, out=None):
+        """(u, lambda, level); out = caller-owned (e.g. pinned) arrays to fill."""
         shape = (self.n_cells, self.n_states, self.n_total)
-        u = np.zeros(shape); lam = np.zeros(shape); lev = np.zeros(self.n_cells, dtype=np.uint32)
+        if out is not None:
+            u, lam, lev = out
+            assert u.shape == shape and lam.shape == shape and lev.dtype == np.uint32 and u.flags.c_contiguous
+        else:
+            u = np.zeros(shape); lam = np.zeros(shape); lev = np.zeros(self.n_cells, dtype=np.uint32)
         check(self.h, self.lib.uqc_download_state(self.h, ptr(u), ptr(lam), ptr(lev, L._up), layout))
         return u, lam, lev
 
