@@ -146,6 +146,40 @@ int uqc_closure_solve_host( uqc_solver* h, int n, double* lambda, const double* 
 int uqc_closure_solve_device( uqc_solver* h, int n, double* d_lambda, const double* d_u, const unsigned* d_n_total,
                               int* d_status );
 
+/* For callers that must not allocate GPU memory: the same batched closure as
+ * uqc_closure_solve_device, on caller-owned DEVICE arrays, without any
+ * cudaMalloc/cudaFree, not even on its first call. No counterpart in the
+ * reference (its closure runs on the host).
+ *
+ * Who needs it: code that runs inside a framework owning all device memory
+ * (its own arena or pool), code enqueued while another thread captures a CUDA
+ * graph in global mode, and latency-critical loops that may not hit the
+ * allocator. The handle may be freshly created (its own device state is never
+ * touched); its configuration and basis tables come from host memory.
+ *
+ * Scratch lives in one statically allocated device array inside this library
+ * (UQC_NOALLOC_SCRATCH_BYTES, held on every GPU that loads the library until
+ * the process exits): the loop-control block, per-cell iteration counts for at
+ * most UQC_NOALLOC_MAX_CELLS cells, and a copy of the two basis tables of at
+ * most UQC_NOALLOC_MAX_TABLE doubles each (nQ rows of an odd stride >= nT, plus
+ * 8). Larger requests return UQC_ERR_CAPACITY. Every call overwrites the whole
+ * array, so calls whose work overlaps on the GPU (different streams, or
+ * different host threads, at the same time) race and must be serialised by
+ * the caller.
+ *
+ * d_lambda (in/out), d_u: n cells, UQC_LAYOUT_STATE_MAJOR; d_n_total: moments
+ * per cell or NULL (finest level); d_status: n uqc_cell_code values (required);
+ * cuda_stream: the stream to enqueue on (NULL = the legacy default stream).
+ * Asynchronous: results are valid once the stream has reached this point.
+ * The first call on each device looks up the array's device address and sets
+ * the kernel's shared-memory limit; make that first call before any stream
+ * capture begins. */
+#define UQC_NOALLOC_MAX_CELLS 65536
+#define UQC_NOALLOC_MAX_TABLE 8192
+#define UQC_NOALLOC_SCRATCH_BYTES ( 256 + 4 * UQC_NOALLOC_MAX_CELLS + 16 * UQC_NOALLOC_MAX_TABLE )
+int uqc_closure_solve_device_noalloc( uqc_solver* h, int n, double* d_lambda, const double* d_u, const unsigned* d_n_total,
+                                      int* d_status, void* cuda_stream );
+
 /* ---- introspection ----------------------------------------------------- */
 
 /* Device time (ms) of the kernels of the last uqc_step call, by phase:

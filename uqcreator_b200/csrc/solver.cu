@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -66,6 +67,7 @@ struct uqc_solver {
     std::vector<cudaEvent_t> stepEvents;
     float lastMs[3] = {0, 0, 0};
     cudaGraphExec_t graph = nullptr;
+    std::vector<double> padPhi, padPhiWf;    // host tables in the device layout
     std::string err;
 };
 
@@ -281,6 +283,15 @@ void build( uqc_solver* h, const std::string& text, void* stream ) {
     }
     h->precision = h->cfg.precision;
     h->userStream = (cudaStream_t)stream;
+    // host copies of the tables in the device layout (row stride ld, 8 spare
+    // doubles), used by uqc_closure_solve_device_noalloc
+    h->padPhi.assign( size_t( h->tab.nQ ) * h->ld + 8, 0.0 );
+    h->padPhiWf.assign( size_t( h->tab.nQ ) * h->ld + 8, 0.0 );
+    for( int k = 0; k < h->tab.nQ; ++k )
+        for( int i = 0; i < h->tab.nT; ++i ) {
+            h->padPhi[size_t( k ) * h->ld + i]   = h->tab.phi[size_t( k ) * h->tab.nT + i];
+            h->padPhiWf[size_t( k ) * h->ld + i] = h->tab.phiWf[size_t( k ) * h->tab.nT + i];
+        }
 }
 
 // Device side of a handle, set up on first use so that configuration, tables
@@ -825,3 +836,88 @@ int uqc_mesh_tri_jitter( int nx, int ny, double jitter, unsigned long long seed,
 }
 
 }    // extern "C"
+
+// ===================================================== closure without allocation
+//
+// Statically allocated scratch of uqc_closure_solve_device_noalloc (layout:
+// Control block in the first 256 bytes, then the per-cell iteration counts,
+// then the two padded basis tables). In host code the name below is only a
+// host-side stand-in for the array: kernels get the device address that
+// cudaGetSymbolAddress returns for the current device.
+static __device__ __align__( 256 ) unsigned char g_noallocScratch[UQC_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noallocMutex;
+unsigned char* g_noallocAddr[kMaxDevices] = {};    // device address per device id, set once
+
+unsigned char* noalloc_scratch_address() {
+    int dev = 0;
+    CK( cudaGetDevice( &dev ) );
+    if( dev < 0 || dev >= kMaxDevices ) throw std::invalid_argument( "device id beyond the no-alloc table" );
+    std::lock_guard<std::mutex> lock( g_noallocMutex );
+    if( !g_noallocAddr[dev] ) {
+        void* p = nullptr;
+        CK( cudaGetSymbolAddress( &p, g_noallocScratch ) );
+        g_noallocAddr[dev] = static_cast<unsigned char*>( p );
+    }
+    return g_noallocAddr[dev];
+}
+}    // namespace
+
+extern "C" int uqc_closure_solve_device_noalloc( uqc_solver* h, int n, double* d_lambda, const double* d_u, const unsigned* d_n_total,
+                                                 int* d_status, void* cuda_stream ) {
+    if( !h || n < 0 || ( n > 0 && ( !d_lambda || !d_u || !d_status ) ) ) return UQC_ERR_ARGUMENT;
+    if( n > UQC_NOALLOC_MAX_CELLS )
+        return fail( h, UQC_ERR_CAPACITY,
+                     "uqc_closure_solve_device_noalloc: " + std::to_string( n ) + " cells exceed UQC_NOALLOC_MAX_CELLS = " +
+                         std::to_string( UQC_NOALLOC_MAX_CELLS ) + "; split the batch" );
+    const size_t tableLen = size_t( h->tab.nQ ) * h->ld + 8;
+    if( tableLen > size_t( UQC_NOALLOC_MAX_TABLE ) )
+        return fail( h, UQC_ERR_CAPACITY,
+                     "uqc_closure_solve_device_noalloc: basis tables of " + std::to_string( tableLen ) + " doubles exceed UQC_NOALLOC_MAX_TABLE = " +
+                         std::to_string( UQC_NOALLOC_MAX_TABLE ) + "; use uqc_closure_solve_device" );
+    if( n == 0 ) return UQC_OK;
+    return guarded( h, [&] {
+        cudaStream_t st      = (cudaStream_t)cuda_stream;
+        unsigned char* base  = noalloc_scratch_address();
+        Control* ctl         = reinterpret_cast<Control*>( base );
+        int* iters           = reinterpret_cast<int*>( base + 256 );
+        double* tPhi         = reinterpret_cast<double*>( base + 256 + 4 * size_t( UQC_NOALLOC_MAX_CELLS ) );
+        double* tPhiWf       = tPhi + UQC_NOALLOC_MAX_TABLE;
+        // the array keeps the previous call's contents: the control block must start at zero
+        CK( cudaMemsetAsync( ctl, 0, sizeof( Control ), st ) );
+        CK( cudaMemcpyAsync( tPhi, h->padPhi.data(), tableLen * sizeof( double ), cudaMemcpyHostToDevice, st ) );
+        CK( cudaMemcpyAsync( tPhiWf, h->padPhiWf.data(), tableLen * sizeof( double ), cudaMemcpyHostToDevice, st ) );
+        KParams P      = make_params( h );
+        P.nCells       = n;
+        P.phi          = tPhi;
+        P.phiWf        = tPhiWf;
+        P.lam          = d_lambda;
+        P.u            = const_cast<double*>( d_u );
+        P.level        = nullptr;
+        P.nTotalCell   = d_n_total;
+        P.status       = d_status;
+        P.iters        = iters;
+        P.ctl          = ctl;
+        // launch shape of k_closure, as plan_launches chooses it
+        int dev = 0, maxSmem = 0, sms = 0, occ = 0;
+        CK( cudaGetDevice( &dev ) );
+        CK( cudaDeviceGetAttribute( &maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev ) );
+        CK( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev ) );
+        const int nS = h->nS, nT = h->tab.nT, nQ = h->tab.nQ, cl = h->cfg.closure;
+        const int group = size_t( nS ) * nT <= 32 ? 32 : 256, block = 256;
+        const size_t tables = 2 * ( size_t( nQ ) * h->ld + 4 ) * sizeof( double );
+        const size_t ws     = cell_ws_doubles( nS, nT, nQ, closure_np( cl ) ) * sizeof( double ) * ( block / group );
+        P.tablesInSmem      = tables + ws <= size_t( maxSmem ) && tables <= 96 * 1024;
+        const size_t smem   = ws + ( P.tablesInSmem ? tables : 0 );
+        if( smem > size_t( maxSmem ) ) throw ConfigError( "closure workspace exceeds shared memory" );
+        void* fn = pick( cl, group, 0 );
+        CK( cudaFuncSetAttribute( fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) ) );
+        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, fn, block, smem ) );
+        int mode     = 0;
+        void* args[] = {&P, &mode};
+        CK( cudaLaunchKernel( fn, dim3( std::max( 1, occ ) * sms ), dim3( block ), args, smem, st ) );
+        return UQC_OK;
+    } );
+}
