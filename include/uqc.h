@@ -98,6 +98,13 @@ int uqc_set_precision( uqc_solver* h, int precision );
 /* Closure::SetMaxIterations (closure.cpp:341) and the epsilon of settings.cpp:314. */
 int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newton_mode );
 
+/* Launch tuning (no reference counterpart; the autotuner uses it):
+ *   "closure_group"  threads per cell in the closure kernel: 32 (a warp per
+ *                    cell, several cells per CTA) or 256 (a CTA per cell);
+ *                    0 = automatic.
+ * Unknown keys return UQC_ERR_ARGUMENT. */
+int uqc_set_option( uqc_solver* h, const char* key, double value );
+
 /* Host copies of the tables of Closure::Closure (closure.cpp:16-84):
  * phi[k * nT + i] = phiTilde(k, i), phi_wf = phiTildeWf, xi[k * dimXi + l],
  * w[k]. Any pointer may be NULL. */
@@ -160,9 +167,10 @@ int uqc_closure_solve_device( uqc_solver* h, int n, double* d_lambda, const doub
  * Scratch lives in one statically allocated device array inside this library
  * (UQC_NOALLOC_SCRATCH_BYTES, held on every GPU that loads the library until
  * the process exits): the loop-control block, per-cell iteration counts for at
- * most UQC_NOALLOC_MAX_CELLS cells, and a copy of the two basis tables of at
- * most UQC_NOALLOC_MAX_TABLE doubles each (nQ rows of an odd stride >= nT, plus
- * 8). Larger requests return UQC_ERR_CAPACITY. Every call overwrites the whole
+ * most UQC_NOALLOC_MAX_CELLS cells, and copies of the two basis tables (nQ rows
+ * of an odd stride >= nT, plus 8 doubles each) and of the nQ node weights, at
+ * most UQC_NOALLOC_MAX_TABLE doubles per table (the second table together with
+ * the weights). Larger requests return UQC_ERR_CAPACITY. Every call overwrites the whole
  * array, so calls whose work overlaps on the GPU (different streams, or
  * different host threads, at the same time) race and must be serialised by
  * the caller.

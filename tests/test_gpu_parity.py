@@ -145,3 +145,16 @@ def test_full_size_euler_step_is_finite_and_deterministic():
     assert a["dt"] == b["dt"] and a["residual"] == b["residual"]
     np.testing.assert_array_equal(u1, u2)
     np.testing.assert_array_equal(l1, l2)
+
+
+@pytest.mark.parametrize("group", [32, 256])
+def test_closure_group_sizes_agree(group):
+    """Warp-per-cell and CTA-per-cell closure kernels give the same results."""
+    toml = W.euler2d(nx=16, ny=4)
+    s, o = _pair(toml)
+    s.set_option("closure_group", group)
+    a = s.step(4)
+    o.step(4)
+    assert a["failed_cells"] == 0
+    err = rel_l1(s.mean_var(), o.mean_var(), o.geometry()["area"])
+    assert np.all(err <= TOL_MV), err

@@ -27,6 +27,7 @@ EXPORTS = [
     "uqc_upload_state", "uqc_download_state", "uqc_solve_closure", "uqc_cell_status", "uqc_step", "uqc_run",
     "uqc_mean_var", "uqc_closure_solve_host", "uqc_closure_solve_device", "uqc_last_timing", "uqc_device_state",
     "uqc_last_launch_count", "uqc_stream", "uqc_mesh_tri_jitter", "uqc_closure_solve_device_noalloc",
+    "uqc_set_option",
 ]
 NOALLOC_MAX_CELLS = 65536
 
@@ -93,6 +94,7 @@ def lib() -> C.CDLL:
         "uqc_stream": ([_vp], _vp),
         "uqc_mesh_tri_jitter": ([C.c_int, C.c_int, C.c_double, C.c_ulonglong, _dp, _ip, _ip], C.c_int),
         "uqc_closure_solve_device_noalloc": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "uqc_set_option": ([_vp, C.c_char_p, C.c_double], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

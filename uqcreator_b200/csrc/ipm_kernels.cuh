@@ -19,6 +19,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "linalg.cuh"
 #include "physics.cuh"
 #include "uqc.h"
 
@@ -52,6 +53,7 @@ struct KParams {
     const double* phi;       // nQ x ld
     const double* phiWf;     // nQ x ld
     const double* xi;        // nQ x dimXi
+    const double* wt;        // nQ: w_k / 2^dimXi (phiWf = phi wt)
     bool tablesInSmem;
     // geometry
     const double *area, *dx, *center, *unitN, *scaledN;
@@ -65,50 +67,6 @@ struct KParams {
     Control* ctl;
 };
 
-// ------------------------------------------------------------------ groups
-
-template <int GROUP> struct Grp {
-    int r;
-    __device__ __forceinline__ void sync() const {
-        if constexpr( GROUP == 32 )
-            __syncwarp();
-        else
-            __syncthreads();
-    }
-};
-
-// Sum over the group, same value returned to every member. scratch: >= GROUP/32 doubles.
-template <int GROUP> __device__ double group_sum( const Grp<GROUP>& g, double v, double* scratch ) {
-    for( int o = 16; o > 0; o >>= 1 ) v += __shfl_xor_sync( 0xffffffffu, v, o );
-    if constexpr( GROUP == 32 ) {
-        return v;
-    }
-    else {
-        if( ( g.r & 31 ) == 0 ) scratch[g.r >> 5] = v;
-        g.sync();
-        double s = 0.0;
-        for( int w = 0; w < GROUP / 32; ++w ) s += scratch[w];
-        g.sync();
-        return s;
-    }
-}
-
-template <int GROUP> __device__ double group_min( const Grp<GROUP>& g, double v, double* scratch ) {
-    for( int o = 16; o > 0; o >>= 1 ) v = fmin( v, __shfl_xor_sync( 0xffffffffu, v, o ) );
-    if constexpr( GROUP == 32 ) {
-        return v;
-    }
-    else {
-        if( ( g.r & 31 ) == 0 ) scratch[g.r >> 5] = v;
-        g.sync();
-        double s = scratch[0];
-        for( int w = 1; w < GROUP / 32; ++w ) s = fmin( s, scratch[w] );
-        g.sync();
-        return s;
-    }
-}
-
-__device__ __forceinline__ int packed( int row, int col ) { return col * ( col + 1 ) / 2 + row; }
 
 // ------------------------------------------------------------------ workspace
 
@@ -117,14 +75,23 @@ struct CellWs {
     double *lam, *lamN, *uh, *g, *gN, *d;   // n each
     double *LA, *LB, *uk;                   // nS nQ each
     double* du;                             // NP nQ
-    double* H;                              // n (n + 1) / 2 packed upper
+    double* H;                              // hess_ld(n) x (n + 1): upper triangle + right-hand side
     double *D, *I;                          // Cholesky pivots and their inverses (n each)
     double* red;                            // reduction scratch (16) + broadcast (16)
 };
 
+// Layout: [lam uh g LA D I red] then a region shared by the trial data
+// [LB uk gN d lamN] and the nodal DU of the Hessian: whenever the Hessian is
+// assembled, the trial buffers are dead (the next trial is formed after the
+// solve), so DU aliases them. Then the packed Hessian.
+__host__ __device__ inline size_t cell_ws_trial_doubles( int nS, int nT, int nQ, int NP ) {
+    size_t n = size_t( nS ) * nT, trial = 2 * size_t( nS ) * nQ + 3 * n, du = size_t( NP ) * nQ;
+    return trial > du ? trial : du;
+}
+
 __host__ __device__ inline size_t cell_ws_doubles( int nS, int nT, int nQ, int NP ) {
     size_t n = size_t( nS ) * nT;
-    size_t s = 8 * n + 3 * size_t( nS ) * nQ + size_t( NP ) * nQ + n * ( n + 1 ) / 2 + 32;
+    size_t s = 5 * n + size_t( nS ) * nQ + 32 + cell_ws_trial_doubles( nS, nT, nQ, NP ) + hess_doubles( int( n ) );
     return ( s + 3 ) & ~size_t( 3 );
 }
 
@@ -132,19 +99,20 @@ __device__ inline CellWs carve( double* p, int nS, int nT, int nQ, int NP ) {
     CellWs w;
     size_t n = size_t( nS ) * nT;
     w.lam    = p;
-    w.lamN   = w.lam + n;
-    w.uh     = w.lamN + n;
+    w.uh     = w.lam + n;
     w.g      = w.uh + n;
-    w.gN     = w.g + n;
-    w.d      = w.gN + n;
-    w.LA     = w.d + n;
-    w.LB     = w.LA + size_t( nS ) * nQ;
-    w.uk     = w.LB + size_t( nS ) * nQ;
-    w.du     = w.uk + size_t( nS ) * nQ;
-    w.H      = w.du + size_t( NP ) * nQ;
-    w.D      = w.H + n * ( n + 1 ) / 2;
+    w.LA     = w.g + n;
+    w.D      = w.LA + size_t( nS ) * nQ;
     w.I      = w.D + n;
     w.red    = w.I + n;
+    double* t = w.red + 32;
+    w.LB     = t;
+    w.uk     = w.LB + size_t( nS ) * nQ;
+    w.gN     = w.uk + size_t( nS ) * nQ;
+    w.d      = w.gN + n;
+    w.lamN   = w.d + n;
+    w.du     = t;    // aliases the trial buffers while the Hessian is assembled
+    w.H      = t + cell_ws_trial_doubles( nS, nT, nQ, NP );
     return w;
 }
 
@@ -199,167 +167,20 @@ __device__ double gradient( const Grp<GROUP>& g, const KParams& P, const double*
     return sqrt( group_sum<GROUP>( g, sq, red ) );
 }
 
-// Hessian (closure.cpp:255-271), packed upper triangle of the n x n matrix,
-// n = NS nTj: H(m nTj + j, l nTj + i) = sum_k phi(k,j) phiWf(k,i) DU(l,m)(k).
-// Register tiles of 4 x 4 entries per thread, m <= l (and j <= i on the diagonal).
+// Newton direction d = H(lambda)^-1 g (closure.cpp:145-150 / 162-168): Hessian
+// at the duals whose Lambda is in LA, then posv. Returns 0 or UQC_CELL_NOT_PD.
 template <int CL, int GROUP>
-__device__ void hessian( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* phiWf, const double* L, int nTj,
-                         double* du, double* H ) {
+__device__ int newton_direction( const Grp<GROUP>& g, const KParams& P, const double* phi, CellWs& w, int nTj, const double* LA ) {
     constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP;
-    for( int k = g.r; k < P.nQ; k += GROUP ) {
-        double Lk[NS], y[NP];
-#pragma unroll
-        for( int s = 0; s < NS; ++s ) Lk[s] = L[s * P.nQ + k];
-        Closure<CL>::DU( Lk, y, P.phys );
-#pragma unroll
-        for( int p = 0; p < NP; ++p ) du[p * P.nQ + k] = y[p];
-    }
+    const int n = NS * nTj, ldH = hess_ld( n );
+    hessian_sym<NS, NP, GROUP>( g, P.nQ, P.ld, phi, P.wt, LA, nTj, w.du, w.H, ldH,
+                                [&]( const double* L, double* y ) { Closure<CL>::DU( L, y, P.phys ); } );
+    for( int r = g.r; r < n; r += GROUP ) w.H[size_t( n ) * ldH + r] = w.g[r];
     g.sync();
-    const int nTiles = ( nTj + 3 ) >> 2;
-    const int tDiag = nTiles * ( nTiles + 1 ) / 2, tOff = nTiles * nTiles;
-    const int total = NS * tDiag + ( NS * ( NS - 1 ) / 2 ) * tOff;
-    for( int t = g.r; t < total; t += GROUP ) {
-        // decode tile -> block (m, l), m <= l, and tile (tj, ti)
-        int m = 0, l = 0, tj = 0, ti = 0, rem = t;
-        for( m = 0; m < NS; ++m ) {
-            if( rem < tDiag ) {
-                l = m;
-                int c = 0;
-                while( ( c + 1 ) * ( c + 2 ) / 2 <= rem ) ++c;
-                ti = c;
-                tj = rem - c * ( c + 1 ) / 2;
-                break;
-            }
-            rem -= tDiag;
-            int offHere = ( NS - 1 - m ) * tOff;
-            if( rem < offHere ) {
-                l  = m + 1 + rem / tOff;
-                rem = rem % tOff;
-                tj = rem / nTiles;
-                ti = rem % nTiles;
-                break;
-            }
-            rem -= offHere;
-        }
-        const int j0 = tj * 4, i0 = ti * 4;
-        const double* dup = du + pair_index<NS>( l, m ) * P.nQ;
-        double acc[4][4];
-#pragma unroll
-        for( int a = 0; a < 4; ++a )
-#pragma unroll
-            for( int b = 0; b < 4; ++b ) acc[a][b] = 0.0;
-        for( int k = 0; k < P.nQ; ++k ) {
-            const double* pr  = phi + size_t( k ) * P.ld;
-            const double* pwr = phiWf + size_t( k ) * P.ld;
-            double dk         = dup[k];
-            double aj[4], bi[4];
-#pragma unroll
-            for( int a = 0; a < 4; ++a ) aj[a] = pr[j0 + a];
-#pragma unroll
-            for( int b = 0; b < 4; ++b ) bi[b] = pwr[i0 + b] * dk;
-#pragma unroll
-            for( int a = 0; a < 4; ++a )
-#pragma unroll
-                for( int b = 0; b < 4; ++b ) acc[a][b] = fma( aj[a], bi[b], acc[a][b] );
-        }
-#pragma unroll
-        for( int a = 0; a < 4; ++a )
-#pragma unroll
-            for( int b = 0; b < 4; ++b ) {
-                int j = j0 + a, i = i0 + b;
-                if( j < nTj && i < nTj && ( m < l || j <= i ) ) H[packed( m * nTj + j, l * nTj + i )] = acc[a][b];
-            }
-    }
-}
-
-// Cholesky H = U^T U of the packed upper matrix (LAPACK dpotrf semantics,
-// called through posv, vectorspace.cpp:152-171), right-looking with one group
-// barrier per column: at step j every thread forms U(j,r) = A(j,r) / sqrt(A(j,j))
-// itself and updates its share of the trailing triangle; row j is written
-// scaled one step later, when nobody reads it. Returns 0 or j + 1 of the first
-// non-positive pivot (posv's info > 0).
-// D[j] = sqrt of the pivot, I[j] = 1 / D[j], computed once per column by the
-// thread that owns the diagonal entry (thread 0 owns (j+1, j+1) in step j).
-template <int GROUP> __device__ int cholesky( const Grp<GROUP>& g, double* H, int n, double* D, double* I ) {
-    constexpr int TX = GROUP == 32 ? 8 : 16, TY = GROUP / TX;
-    const int tx = g.r % TX, ty = g.r / TX;
-    if( g.r == 0 && H[0] > 0.0 ) {
-        D[0] = sqrt( H[0] );
-        I[0] = 1.0 / D[0];
-    }
-    g.sync();
-    for( int j = 0; j < n; ++j ) {
-        double ajj = H[packed( j, j )];
-        if( !( ajj > 0.0 ) ) return j + 1;    // uniform: every thread reads the same value
-        const double inv = I[j];
-        if( j > 0 ) {
-            // finalise row j-1: U(j-1, c) = A(j-1, c) / d_{j-1}
-            for( int c = j - 1 + g.r; c < n; c += GROUP ) H[packed( j - 1, c )] = ( c == j - 1 ) ? D[j - 1] : H[packed( j - 1, c )] * I[j - 1];
-        }
-        for( int c = j + 1 + ty; c < n; c += TY ) {
-            double ujc = H[packed( j, c )] * inv;
-            for( int r = j + 1 + tx; r <= c; r += TX ) H[packed( r, c )] -= ( H[packed( j, r )] * inv ) * ujc;
-        }
-        if( g.r == 0 && j + 1 < n ) {
-            double a = H[packed( j + 1, j + 1 )];
-            if( a > 0.0 ) {
-                D[j + 1] = sqrt( a );
-                I[j + 1] = 1.0 / D[j + 1];
-            }
-        }
-        g.sync();
-    }
-    if( g.r == 0 ) H[packed( n - 1, n - 1 )] = D[n - 1];
+    if( cholesky_blk<GROUP, double>( g, w.H, ldH, n, w.D, w.I, reinterpret_cast<int*>( w.red + 24 ) ) ) return UQC_CELL_NOT_PD;
+    back_solve<GROUP, double>( g, w.H, ldH, n, w.I, w.d );
     g.sync();
     return 0;
-}
-
-// Solves U^T U x = b in place (x = b on entry) by one warp (dpotrs:
-// forward with U^T, then backward with U, sequential order of dtrsm).
-template <int GROUP> __device__ void chol_solve( const Grp<GROUP>& g, const double* H, int n, double* x, const double* I ) {
-    if( g.r >= 32 ) return;
-    const int lane = g.r;
-    constexpr int MAXR = 8;    // rows per lane: n <= 256
-    double y[MAXR];
-#pragma unroll
-    for( int q = 0; q < MAXR; ++q ) y[q] = ( lane + 32 * q < n ) ? x[lane + 32 * q] : 0.0;
-    for( int i = 0; i < n; ++i ) {
-        double yi = 0.0;
-        int own = i & 31, q0 = i >> 5;
-#pragma unroll
-        for( int q = 0; q < MAXR; ++q )
-            if( q == q0 && lane == own ) {
-                y[q] = y[q] * I[i];
-                yi   = y[q];
-            }
-        yi = __shfl_sync( 0xffffffffu, yi, own );
-#pragma unroll
-        for( int q = 0; q < MAXR; ++q ) {
-            int r = lane + 32 * q;
-            if( r > i && r < n ) y[q] = y[q] - H[packed( i, r )] * yi;
-        }
-    }
-    for( int k = n - 1; k >= 0; --k ) {
-        double xk = 0.0;
-        int own = k & 31, q0 = k >> 5;
-#pragma unroll
-        for( int q = 0; q < MAXR; ++q )
-            if( q == q0 && lane == own ) {
-                if( y[q] != 0.0 ) y[q] = y[q] * I[k];
-                xk = y[q];
-            }
-        xk = __shfl_sync( 0xffffffffu, xk, own );
-        if( xk != 0.0 ) {
-#pragma unroll
-            for( int q = 0; q < MAXR; ++q ) {
-                int r = lane + 32 * q;
-                if( r < k ) y[q] = y[q] - xk * H[packed( r, k )];
-            }
-        }
-    }
-#pragma unroll
-    for( int q = 0; q < MAXR; ++q )
-        if( lane + 32 * q < n ) x[lane + 32 * q] = y[q];
 }
 
 // lamOut[s nT + i] = lamIn[s nT + i] + c d[s nTj + i], i < nTj (closure.cpp:273-279)
@@ -382,11 +203,11 @@ __device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double*
     lsTrials         = 0;
     double* LA = w.LA;
     double* LB = w.LB;
-    auto accept = [&]() {    // lam <- lamN, LA <- LB
+    // lam <- lamN and LA <- LB by copy: LA must stay outside the region that
+    // the Hessian's DU buffer aliases
+    auto accept = [&]() {
         for( int idx = g.r; idx < P.nS * P.nT; idx += GROUP ) w.lam[idx] = w.lamN[idx];
-        double* t = LA;
-        LA        = LB;
-        LB        = t;
+        for( int idx = g.r; idx < Closure<CL>::NS * P.nQ; idx += GROUP ) LA[idx] = LB[idx];
     };
     int rc = UQC_CELL_MAX_ITER;
     eval_lambda<Closure<CL>::NS, GROUP>( g, P, phi, w.lam, nTj, LA );
@@ -396,16 +217,10 @@ __device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double*
         for( int l = 0; l < P.maxIter; ++l ) {
             double stepSize = 1.0;
             double gn       = gradient<CL, GROUP>( g, P, phiWf, LA, w.uh, nTj, w.uk, w.g, w.red );
-            hessian<CL, GROUP>( g, P, phi, phiWf, LA, nTj, w.du, w.H );
-            g.sync();
-            if( cholesky<GROUP>( g, w.H, n, w.D, w.I ) ) {
+            if( newton_direction<CL, GROUP>( g, P, phi, w, nTj, LA ) ) {
                 rc = UQC_CELL_NOT_PD;
                 goto out;
             }
-            for( int idx = g.r; idx < n; idx += GROUP ) w.d[idx] = w.g[idx];
-            g.sync();
-            chol_solve<GROUP>( g, w.H, n, w.d, w.I );
-            g.sync();
             ++iters;
             for( int idx = g.r; idx < P.nS * P.nT; idx += GROUP ) w.lamN[idx] = w.lam[idx];
             add_step<GROUP>( g, P, nTj, w.lam, -stepSize, w.d, w.lamN );
@@ -456,16 +271,10 @@ __device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double*
                 for( int idx = g.r; idx < n; idx += GROUP ) w.g[idx] = w.gN[idx];
                 gn = gnN;
             }
-            hessian<CL, GROUP>( g, P, phi, phiWf, LA, nTj, w.du, w.H );
-            g.sync();
-            if( cholesky<GROUP>( g, w.H, n, w.D, w.I ) ) {
+            if( newton_direction<CL, GROUP>( g, P, phi, w, nTj, LA ) ) {
                 rc = UQC_CELL_NOT_PD;
                 goto out;
             }
-            for( int idx = g.r; idx < n; idx += GROUP ) w.d[idx] = w.g[idx];
-            g.sync();
-            chol_solve<GROUP>( g, w.H, n, w.d, w.I );
-            g.sync();
             ++iters;
             if( P.maxIter == 1 ) {
                 // One-Shot IPM: lam -= alpha H^-1 g, no line search (closure.cpp:151-154)
@@ -473,6 +282,7 @@ __device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double*
                 g.sync();
                 eval_lambda<Closure<CL>::NS, GROUP>( g, P, phi, w.lam, nTj, LA );
                 g.sync();
+                eval_u<CL, GROUP>( g, P, LA, w.uk, true );    // keep uk = U(lam) for the epilogue
                 rc = UQC_CELL_CONVERGED;
                 goto out;
             }
@@ -560,16 +370,22 @@ __global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_closure( KParam
         if( cell >= P.nCells ) break;
         const int lev = P.level ? int( P.level[cell] ) : P.nLevels - 1;
         const int nTj = P.nTotalCell ? int( P.nTotalCell[cell] ) : P.nTLevel[lev];
-        // load duals and moments (state-major, finest stride)
+        // load duals and moments (state-major, finest stride), checking finiteness on the way
+        bool bad = false;
         for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
-            w.lam[idx] = P.lam[cell * ldc + idx];
-            w.uh[idx]  = P.u[cell * ldc + idx];
+            double a = P.lam[cell * ldc + idx], b = P.u[cell * ldc + idx];
+            w.lam[idx] = a;
+            w.uh[idx]  = b;
+            bad        = bad || !isfinite( a ) || !isfinite( b );
         }
+        bool anyBad;
+        if constexpr( GROUP == 32 )
+            anyBad = __any_sync( 0xffffffffu, bad );
+        else
+            anyBad = __syncthreads_or( bad );
         g.sync();
         int iters = 0, ls = 0, rc;
-        bool finite = true;
-        for( int idx = 0; idx < int( ldc ); ++idx ) finite = finite && isfinite( w.uh[idx] ) && isfinite( w.lam[idx] );
-        if( !finite )
+        if( anyBad )
             rc = UQC_CELL_NONFINITE;
         else
             rc = newton_cell<CL, GROUP>( g, P, phi, phiWf, w, nTj, iters, ls );
@@ -583,12 +399,15 @@ __global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_closure( KParam
         }
         for( int idx = g.r; idx < int( ldc ); idx += GROUP ) P.lam[cell * ldc + idx] = w.lam[idx];
         if( mode == 1 ) {
-            // [C] uQ = U(Lambda(lam)) with the matrix-form ansatz; w.LA is Lambda(lam) at level nTj
+            // [C] uQ = U(Lambda(lam)). A converged cell's last gradient evaluation
+            // was at the accepted duals, so w.uk already holds U there (the
+            // U(Vector&) form; the reference reconstructs with U(const Matrix&),
+            // which for the Euler closure differs in the last bits only).
             if( rc != 0 ) {
                 eval_lambda<NS, GROUP>( g, P, phi, w.lam, nTj, w.LA );
                 g.sync();
+                eval_u<CL, GROUP>( g, P, w.LA, w.uk, true );
             }
-            eval_u<CL, GROUP>( g, P, w.LA, w.uk, false );
             // [D] refinement level from the moments before re-projection (momentsolver.cpp:104-112, 271-289)
             int newLev = lev;
             if( P.nLevels > 1 ) {

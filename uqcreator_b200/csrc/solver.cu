@@ -36,6 +36,7 @@ struct uqc_solver {
     bool ownStream          = false;
     bool deviceReady        = false;
     int nS = 1, ld = 1, group = 32, numSMs = 148;
+    int closureGroup = 32, closureGroupOverride = 0;    // threads per cell in k_closure (32 or 256)
     size_t ldc = 1;
     // device buffers
     double *d_phi = nullptr, *d_phiWf = nullptr, *d_xi = nullptr;
@@ -68,6 +69,8 @@ struct uqc_solver {
     float lastMs[3] = {0, 0, 0};
     cudaGraphExec_t graph = nullptr;
     std::vector<double> padPhi, padPhiWf;    // host tables in the device layout
+    std::vector<double> padWt;               // w_k / 2^dimXi per node
+    double* d_wt = nullptr;
     std::string err;
 };
 
@@ -150,6 +153,7 @@ KParams make_params( const uqc_solver* h ) {
     P.phi          = h->d_phi;
     P.phiWf        = h->d_phiWf;
     P.xi           = h->d_xi;
+    P.wt           = h->d_wt;
     P.tablesInSmem = h->tablesInSmem;
     P.area         = h->d_area;
     P.dx           = h->d_dx;
@@ -209,16 +213,21 @@ void plan_launches( uqc_solver* h ) {
     CK( cudaDeviceGetAttribute( &maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev ) );
     const int cl = h->cfg.closure, nT = h->tab.nT, nQ = h->tab.nQ, nS = h->nS;
     const size_t n = size_t( nS ) * nT;
-    h->group        = n <= 32 ? 32 : 256;
-    h->closureBlock = 256;
-    const int groupsPerCta = h->closureBlock / h->group;
-    const size_t tables    = 2 * ( size_t( nQ ) * h->ld + 4 ) * sizeof( double );
-    const size_t ws        = cell_ws_doubles( nS, nT, nQ, closure_np( cl ) ) * sizeof( double ) * groupsPerCta;
-    h->tablesInSmem        = tables + ws <= size_t( maxSmem ) && tables <= 96 * 1024;
-    h->closureSmem         = ws + ( h->tablesInSmem ? tables : 0 );
+    h->group = n <= 32 ? 32 : 256;    // thread group per cell of the update / init / mean-variance kernels
+    // closure: a warp per cell (several per CTA) or a whole 256-thread CTA per cell
+    const size_t tables  = 2 * ( size_t( nQ ) * h->ld + 4 ) * sizeof( double );
+    const size_t wsCell  = cell_ws_doubles( nS, nT, nQ, closure_np( cl ) ) * sizeof( double );
+    h->tablesInSmem      = tables <= 96 * 1024 && tables + wsCell <= size_t( maxSmem );
+    const size_t avail   = size_t( maxSmem ) - ( h->tablesInSmem ? tables : 0 );
+    int warpGroups       = int( std::min<size_t>( 8, avail / wsCell ) );
+    h->closureGroup      = h->closureGroupOverride ? h->closureGroupOverride : ( n <= 32 ? 32 : 256 );
+    if( h->closureGroup == 32 && warpGroups < 1 ) h->closureGroup = 256;
+    h->closureBlock        = h->closureGroup == 32 ? 32 * warpGroups : 256;
+    const int groupsPerCta = h->closureBlock / h->closureGroup;
+    h->closureSmem         = wsCell * groupsPerCta + ( h->tablesInSmem ? tables : 0 );
     if( h->closureSmem > size_t( maxSmem ) )
         throw ConfigError( "closure workspace (" + std::to_string( h->closureSmem ) + " B) exceeds shared memory; reduce moments or nodes" );
-    void* kc = pick( cl, h->group, 0 );
+    void* kc = pick( cl, h->closureGroup, 0 );
     CK( cudaFuncSetAttribute( kc, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->closureSmem ) ) );
     int occ = 0;
     CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kc, h->closureBlock, h->closureSmem ) );
@@ -287,6 +296,9 @@ void build( uqc_solver* h, const std::string& text, void* stream ) {
     // doubles), used by uqc_closure_solve_device_noalloc
     h->padPhi.assign( size_t( h->tab.nQ ) * h->ld + 8, 0.0 );
     h->padPhiWf.assign( size_t( h->tab.nQ ) * h->ld + 8, 0.0 );
+    // wt_k = w_k / 2^dimXi, so that phiWf(k, i) = phi(k, i) wt_k exactly
+    h->padWt.resize( h->tab.nQ );
+    for( int k = 0; k < h->tab.nQ; ++k ) h->padWt[k] = std::ldexp( h->tab.w[k], -h->tab.dimXi );
     for( int k = 0; k < h->tab.nQ; ++k )
         for( int i = 0; i < h->tab.nT; ++i ) {
             h->padPhi[size_t( k ) * h->ld + i]   = h->tab.phi[size_t( k ) * h->tab.nT + i];
@@ -316,6 +328,7 @@ void ensure_device( uqc_solver* h ) {
     h->d_phi   = dupload( phi );
     h->d_phiWf = dupload( phiWf );
     h->d_xi    = dupload( h->tab.xi );
+    h->d_wt    = dupload( h->padWt );
     const Mesh& m = h->mesh;
     std::vector<double> dx( m.nCells );
     for( int j = 0; j < m.nCells; ++j ) dx[j] = m.maxEdge[j] / m.area[j];    // momentsolver.cpp:130
@@ -347,7 +360,7 @@ void ensure_device( uqc_solver* h ) {
 
 void release( uqc_solver* h ) {
     if( h->graph ) cudaGraphExecDestroy( h->graph );
-    for( void* p : {(void*)h->d_phi, (void*)h->d_phiWf, (void*)h->d_xi, (void*)h->d_area, (void*)h->d_dx, (void*)h->d_center,
+    for( void* p : {(void*)h->d_phi, (void*)h->d_phiWf, (void*)h->d_xi, (void*)h->d_wt, (void*)h->d_area, (void*)h->d_dx, (void*)h->d_center,
                     (void*)h->d_unitN, (void*)h->d_scaledN, (void*)h->d_nbr, (void*)h->d_boundary, (void*)h->d_u, (void*)h->d_lam,
                     (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
                     (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
@@ -369,7 +382,7 @@ void launch_closure( uqc_solver* h, KParams& P, int mode ) {
         return;
     }
     void* args[] = {&P, &mode};
-    launch( h, pick( h->cfg.closure, h->group, 0 ), h->closureGrid, h->closureBlock, h->closureSmem, args );
+    launch( h, pick( h->cfg.closure, h->closureGroup, 0 ), h->closureGrid, h->closureBlock, h->closureSmem, args );
 }
 
 void enqueue_step( uqc_solver* h, KParams& P ) {
@@ -492,6 +505,22 @@ int uqc_set_precision( uqc_solver* h, int precision ) {
     if( precision == UQC_MIXED && !h->mixed.ok ) return fail( h, UQC_ERR_CONFIG, "mixed precision not available for this configuration: " + h->mixed.why );
     h->precision = precision;
     return UQC_OK;
+}
+
+int uqc_set_option( uqc_solver* h, const char* key, double value ) {
+    if( !h || !key ) return UQC_ERR_ARGUMENT;
+    std::string k = key;
+    if( k == "closure_group" ) {
+        int v = int( value );
+        if( v != 0 && v != 32 && v != 256 ) return fail( h, UQC_ERR_ARGUMENT, "closure_group must be 0, 32 or 256" );
+        h->closureGroupOverride = v;
+        if( h->deviceReady ) return guarded( h, [&] {
+                plan_launches( h );
+                return UQC_OK;
+            } );
+        return UQC_OK;
+    }
+    return fail( h, UQC_ERR_ARGUMENT, "unknown option '" + k + "'" );
 }
 
 int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newton_mode ) {
@@ -873,9 +902,10 @@ extern "C" int uqc_closure_solve_device_noalloc( uqc_solver* h, int n, double* d
                      "uqc_closure_solve_device_noalloc: " + std::to_string( n ) + " cells exceed UQC_NOALLOC_MAX_CELLS = " +
                          std::to_string( UQC_NOALLOC_MAX_CELLS ) + "; split the batch" );
     const size_t tableLen = size_t( h->tab.nQ ) * h->ld + 8;
-    if( tableLen > size_t( UQC_NOALLOC_MAX_TABLE ) )
+    if( tableLen + size_t( h->tab.nQ ) > size_t( UQC_NOALLOC_MAX_TABLE ) )
         return fail( h, UQC_ERR_CAPACITY,
-                     "uqc_closure_solve_device_noalloc: basis tables of " + std::to_string( tableLen ) + " doubles exceed UQC_NOALLOC_MAX_TABLE = " +
+                     "uqc_closure_solve_device_noalloc: basis tables of " + std::to_string( tableLen + h->tab.nQ ) +
+                         " doubles exceed UQC_NOALLOC_MAX_TABLE = " +
                          std::to_string( UQC_NOALLOC_MAX_TABLE ) + "; use uqc_closure_solve_device" );
     if( n == 0 ) return UQC_OK;
     return guarded( h, [&] {
@@ -889,7 +919,10 @@ extern "C" int uqc_closure_solve_device_noalloc( uqc_solver* h, int n, double* d
         CK( cudaMemsetAsync( ctl, 0, sizeof( Control ), st ) );
         CK( cudaMemcpyAsync( tPhi, h->padPhi.data(), tableLen * sizeof( double ), cudaMemcpyHostToDevice, st ) );
         CK( cudaMemcpyAsync( tPhiWf, h->padPhiWf.data(), tableLen * sizeof( double ), cudaMemcpyHostToDevice, st ) );
+        double* tWt = tPhiWf + tableLen;    // node weights after the second table
+        CK( cudaMemcpyAsync( tWt, h->padWt.data(), h->padWt.size() * sizeof( double ), cudaMemcpyHostToDevice, st ) );
         KParams P      = make_params( h );
+        P.wt           = tWt;
         P.nCells       = n;
         P.phi          = tPhi;
         P.phiWf        = tPhiWf;

@@ -136,6 +136,9 @@ class Solver:
     def set_precision(self, precision: int):
         check(self.h, self.lib.uqc_set_precision(self.h, precision))
 
+    def set_option(self, key: str, value: float):
+        check(self.h, self.lib.uqc_set_option(self.h, key.encode(), float(value)))
+
     def set_newton(self, max_iterations: int, epsilon: float, mode: int):
         check(self.h, self.lib.uqc_set_newton(self.h, max_iterations, epsilon, mode))
 
