@@ -47,10 +47,12 @@ enum uqc_layout { UQC_LAYOUT_REF = 0, UQC_LAYOUT_STATE_MAJOR = 1 };
 
 /* Hessian precision of the Newton closure.
  * UQC_FP64:  all-FP64 (the reference's arithmetic).
- * UQC_MIXED: Hessian assembled on tensor cores (BF16 inputs, FP32
- *            accumulation in TMEM) and factored in FP32; the residual, the
- *            line-search test and the moment update stay FP64; cells whose FP32
- *            pivot test fails are refactored in FP64. */
+ * UQC_MIXED: Hessian assembled, factored and solved in FP32; the gradient,
+ *            the convergence and line-search tests, the duals and the moment
+ *            update stay FP64, so a converged cell meets the same FP64
+ *            tolerance. Cells whose FP32 Newton does not converge (FP32
+ *            factor not positive definite, line-search or iteration limit)
+ *            continue from their last accepted duals in the FP64 form. */
 enum uqc_precision { UQC_FP64 = 0, UQC_MIXED = 1 };
 
 /* Per-cell closure status (uqc_cell_status). */
@@ -78,6 +80,7 @@ typedef struct uqc_step_info {
     long long newton_iterations; /* summed over cells and steps of this call */
     long long line_search_trials;
     int active_cells;         /* cells that needed Newton iterations in the last step */
+    long long fallback_cells; /* UQC_MIXED: cells handed to the FP64 form during this call */
 } uqc_step_info;
 
 /* ---- lifecycle and configuration ------------------------------------ */
@@ -100,8 +103,12 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
 
 /* Launch tuning (no reference counterpart; the autotuner uses it):
  *   "closure_group"  threads per cell in the closure kernel: 32 (a warp per
- *                    cell, several cells per CTA) or 256 (a CTA per cell);
+ *                    cell, several cells per CTA), 64 (two warps per cell,
+ *                    up to six cells per CTA) or 256 (a CTA per cell);
  *                    0 = automatic.
+ *   "mixed_max_iterations"  UQC_MIXED: Newton iterations of the FP32 pass
+ *                    after which a cell continues in the FP64 form (>= 2;
+ *                    0 = the configured maxIterations).
  * Unknown keys return UQC_ERR_ARGUMENT. */
 int uqc_set_option( uqc_solver* h, const char* key, double value );
 

@@ -147,7 +147,7 @@ def test_full_size_euler_step_is_finite_and_deterministic():
     np.testing.assert_array_equal(l1, l2)
 
 
-@pytest.mark.parametrize("group", [32, 256])
+@pytest.mark.parametrize("group", [32, 64, 256])
 def test_closure_group_sizes_agree(group):
     """Warp-per-cell and CTA-per-cell closure kernels give the same results."""
     toml = W.euler2d(nx=16, ny=4)

@@ -48,7 +48,7 @@ class Info(C.Structure):
 class StepInfo(C.Structure):
     _fields_ = [("t", C.c_double), ("dt", C.c_double), ("residual", C.c_double), ("steps", C.c_int),
                 ("failed_cells", C.c_int), ("newton_iterations", C.c_longlong), ("line_search_trials", C.c_longlong),
-                ("active_cells", C.c_int)]
+                ("active_cells", C.c_int), ("fallback_cells", C.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -27,18 +27,35 @@ namespace uqc {
 
 constexpr int MAXLEV = 16;
 
+// Phase counters (slots 0-7 of g_phaseCycles, diagnostic builds; rank 0 of
+// each thread group accumulates clock64 deltas): 0 newton, 1 initial
+// gradient, 2 Hessian, 3 Cholesky, 4 back substitution, 5 trial gradients,
+// 6 epilogue, 7 load.
+#ifdef UQC_PHASE_TIMERS
+#define PT_BEGIN( v ) long long v = clock64();
+#define PT_END( v, id ) \
+    if( g.r == 0 ) atomicAdd( &g_phaseCycles[id], (unsigned long long)( clock64() - v ) );
+#else
+#define PT_BEGIN( v )
+#define PT_END( v, id )
+#endif
+
 // Grid-wide loop state kept on the device so a step needs no host round trip.
 struct Control {
     double t, tEnd, minResidual, residual, dt;
     unsigned long long dtBits;     // atomicMin of the positive dt as integer bits
     unsigned int workCounter;      // closure work stealing
+    unsigned int workCounter2;     // ... of the FP64 pass over the mixed form's fallback cells
+    unsigned int nFallback;        // length of that fallback list
     unsigned int doneBlocks;       // last-block detection in k_update
     int active;                    // the loop condition of momentsolver.cpp:79
     int steps;
     int failedCells;
     int activeCells;      // cells with Newton iterations in the running step
     int activeCellsLast;  // ... in the last finished step
+    unsigned int nActive; // length of the active-cell list of the running step
     unsigned long long newtonIters, lineSearchTrials;
+    unsigned long long fallbackCells;    // mixed form: cells handed to the FP64 form
 };
 
 struct KParams {
@@ -54,6 +71,7 @@ struct KParams {
     const double* phiWf;     // nQ x ld
     const double* xi;        // nQ x dimXi
     const double* wt;        // nQ: w_k / 2^dimXi (phiWf = phi wt)
+    const float* phiF;       // nQ x ld: phi rounded to FP32 (mixed form)
     bool tablesInSmem;
     // geometry
     const double *area, *dx, *center, *unitN, *scaledN;
@@ -64,6 +82,11 @@ struct KParams {
     const unsigned* nTotalCell;  // closure-only calls: moments per cell (else from level)
     int *status, *iters;
     double* blockPartial;     // one per CTA of k_update
+    int* activeList;          // step mode: cells that need Newton (filled by k_check), or null
+    unsigned* activeCount;
+    unsigned* workCounter;    // work-stealing counter of k_closure (in ctl)
+    int* fallbackList;        // mixed form: cells handed to the FP64 form (non-PD FP32 factor, ...)
+    unsigned* fallbackCount;
     Control* ctl;
 };
 
@@ -75,7 +98,7 @@ struct CellWs {
     double *lam, *lamN, *uh, *g, *gN, *d;   // n each
     double *LA, *LB, *uk;                   // nS nQ each
     double* du;                             // NP nQ
-    double* H;                              // hess_ld(n) x (n + 1): upper triangle + right-hand side
+    double* H;                              // block-packed upper triangle + right-hand side (hess_doubles(n))
     double *D, *I;                          // Cholesky pivots and their inverses (n each)
     double* red;                            // reduction scratch (16) + broadcast (16)
 };
@@ -83,36 +106,62 @@ struct CellWs {
 // Layout: [lam uh g LA D I red] then a region shared by the trial data
 // [LB uk gN d lamN] and the nodal DU of the Hessian: whenever the Hessian is
 // assembled, the trial buffers are dead (the next trial is formed after the
-// solve), so DU aliases them. Then the packed Hessian.
-__host__ __device__ inline size_t cell_ws_trial_doubles( int nS, int nT, int nQ, int NP ) {
-    size_t n = size_t( nS ) * nT, trial = 2 * size_t( nS ) * nQ + 3 * n, du = size_t( NP ) * nQ;
-    return trial > du ? trial : du;
+// solve), so DU aliases them. Then the block-packed Hessian. Every buffer
+// starts on a 32-byte boundary; D and I are padded to whole tiles.
+struct WsLayout {
+    size_t lam, uh, g, LA, D, I, red, LB, uk, gN, d, lamN, du, H, total;    // offsets in doubles
+};
+
+// hElem: bytes of a Hessian element (8 FP64 form, 4 mixed form)
+__host__ __device__ inline WsLayout ws_layout( int nS, int nT, int nQ, int NP, int hElem ) {
+    auto a4          = []( size_t x ) { return ( x + 3 ) & ~size_t( 3 ); };
+    const size_t n   = size_t( nS ) * nT, n8 = size_t( hnb( int( n ) ) ) * 8, sq = size_t( nS ) * nQ;
+    const size_t npp = size_t( ( NP + 1 ) & ~1 );
+    WsLayout L;
+    size_t o = 0;
+    L.lam    = o, o += a4( n );
+    L.uh     = o, o += a4( n );
+    L.g      = o, o += a4( n );
+    L.LA     = o, o += a4( sq );
+    L.D      = o, o += a4( n8 );
+    L.I      = o, o += a4( n8 );
+    L.red    = o, o += 32;
+    const size_t t = o;
+    L.du           = t;
+    L.LB           = t;
+    L.uk           = L.LB + a4( sq );
+    L.gN           = L.uk + a4( sq );
+    L.d            = L.gN + a4( n );
+    L.lamN         = L.d + a4( n );
+    const size_t trialEnd = L.lamN + a4( n ), duEnd = t + a4( size_t( nQ ) * npp );
+    o       = trialEnd > duEnd ? trialEnd : duEnd;
+    L.H     = o;
+    o += a4( ( hess_doubles( int( n ) ) * size_t( hElem ) + 7 ) / 8 );
+    L.total = o;
+    return L;
 }
 
-__host__ __device__ inline size_t cell_ws_doubles( int nS, int nT, int nQ, int NP ) {
-    size_t n = size_t( nS ) * nT;
-    size_t s = 5 * n + size_t( nS ) * nQ + 32 + cell_ws_trial_doubles( nS, nT, nQ, NP ) + hess_doubles( int( n ) );
-    return ( s + 3 ) & ~size_t( 3 );
+__host__ __device__ inline size_t cell_ws_doubles( int nS, int nT, int nQ, int NP, int hElem = 8 ) {
+    return ws_layout( nS, nT, nQ, NP, hElem ).total;
 }
 
-__device__ inline CellWs carve( double* p, int nS, int nT, int nQ, int NP ) {
+__device__ inline CellWs carve( double* p, int nS, int nT, int nQ, int NP, int hElem ) {
+    const WsLayout L = ws_layout( nS, nT, nQ, NP, hElem );
     CellWs w;
-    size_t n = size_t( nS ) * nT;
-    w.lam    = p;
-    w.uh     = w.lam + n;
-    w.g      = w.uh + n;
-    w.LA     = w.g + n;
-    w.D      = w.LA + size_t( nS ) * nQ;
-    w.I      = w.D + n;
-    w.red    = w.I + n;
-    double* t = w.red + 32;
-    w.LB     = t;
-    w.uk     = w.LB + size_t( nS ) * nQ;
-    w.gN     = w.uk + size_t( nS ) * nQ;
-    w.d      = w.gN + n;
-    w.lamN   = w.d + n;
-    w.du     = t;    // aliases the trial buffers while the Hessian is assembled
-    w.H      = t + cell_ws_trial_doubles( nS, nT, nQ, NP );
+    w.lam  = p + L.lam;
+    w.uh   = p + L.uh;
+    w.g    = p + L.g;
+    w.LA   = p + L.LA;
+    w.D    = p + L.D;
+    w.I    = p + L.I;
+    w.red  = p + L.red;
+    w.LB   = p + L.LB;
+    w.uk   = p + L.uk;
+    w.gN   = p + L.gN;
+    w.d    = p + L.d;
+    w.lamN = p + L.lamN;
+    w.du   = p + L.du;    // aliases the trial buffers while the Hessian is assembled
+    w.H    = p + L.H;
     return w;
 }
 
@@ -169,17 +218,30 @@ __device__ double gradient( const Grp<GROUP>& g, const KParams& P, const double*
 
 // Newton direction d = H(lambda)^-1 g (closure.cpp:145-150 / 162-168): Hessian
 // at the duals whose Lambda is in LA, then posv. Returns 0 or UQC_CELL_NOT_PD.
-template <int CL, int GROUP>
-__device__ int newton_direction( const Grp<GROUP>& g, const KParams& P, const double* phi, CellWs& w, int nTj, const double* LA ) {
+// HT = double: the FP64 form. HT = float (mixed form): Hessian, factor and
+// triangular solves in FP32 from phiH = phi in FP32, the gradient g and the
+// direction d in FP64; the FP64 gradient test of the caller decides
+// convergence, so an FP32 direction costs at most extra iterations.
+template <int CL, int GROUP, class HT>
+__device__ int newton_direction( const Grp<GROUP>& g, const KParams& P, const double* phi, const HT* phiH, CellWs& w, int nTj,
+                                 const double* LA ) {
     constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP;
-    const int n = NS * nTj, ldH = hess_ld( n );
-    hessian_sym<NS, NP, GROUP>( g, P.nQ, P.ld, phi, P.wt, LA, nTj, w.du, w.H, ldH,
-                                [&]( const double* L, double* y ) { Closure<CL>::DU( L, y, P.phys ); } );
-    for( int r = g.r; r < n; r += GROUP ) w.H[size_t( n ) * ldH + r] = w.g[r];
+    const int n = NS * nTj, rhs = hrhs( hnb( n ) );
+    HT* H = reinterpret_cast<HT*>( w.H );
+    HT* D = reinterpret_cast<HT*>( w.D );
+    HT* I = reinterpret_cast<HT*>( w.I );
+    PT_BEGIN( t0 );
+    hessian_sym<NS, NP, GROUP, HT>( g, P.nQ, P.ld, phiH, P.wt, LA, nTj, reinterpret_cast<HT*>( w.du ), H,
+                                    [&]( const double* L, double* y ) { Closure<CL>::DU( L, y, P.phys ); } );
+    for( int r = g.r; r < n; r += GROUP ) H[rhs + r] = HT( w.g[r] );
     g.sync();
-    if( cholesky_blk<GROUP, double>( g, w.H, ldH, n, w.D, w.I, reinterpret_cast<int*>( w.red + 24 ) ) ) return UQC_CELL_NOT_PD;
-    back_solve<GROUP, double>( g, w.H, ldH, n, w.I, w.d );
-    g.sync();
+    PT_END( t0, 2 );
+    PT_BEGIN( t1 );
+    if( cholesky_la<GROUP, HT>( g, H, n, D, I, reinterpret_cast<int*>( w.red + 24 ) ) ) return UQC_CELL_NOT_PD;
+    PT_END( t1, 3 );
+    PT_BEGIN( t2 );
+    back_solve_warp<GROUP, HT>( g, H, n, I, w.d );
+    PT_END( t2, 4 );
     return 0;
 }
 
@@ -193,9 +255,9 @@ template <int GROUP> __device__ void add_step( const Grp<GROUP>& g, const KParam
 
 // Damped Newton on one cell in shared memory. On return w.lam holds the duals
 // and w.LA the Lambda of w.lam at all nodes (laValid). Returns a uqc_cell_code.
-template <int CL, int GROUP>
-__device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* phiWf, CellWs& w, int nTj, int& iters,
-                            int& lsTrials ) {
+template <int CL, int GROUP, class HT>
+__device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* phiWf, const HT* phiH, CellWs& w, int nTj,
+                            int& iters, int& lsTrials ) {
     const int n      = P.nS * nTj;
     const double eps = P.eps;
     const bool guard = P.newtonMode != 0;
@@ -217,7 +279,7 @@ __device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double*
         for( int l = 0; l < P.maxIter; ++l ) {
             double stepSize = 1.0;
             double gn       = gradient<CL, GROUP>( g, P, phiWf, LA, w.uh, nTj, w.uk, w.g, w.red );
-            if( newton_direction<CL, GROUP>( g, P, phi, w, nTj, LA ) ) {
+            if( newton_direction<CL, GROUP, HT>( g, P, phi, phiH, w, nTj, LA ) ) {
                 rc = UQC_CELL_NOT_PD;
                 goto out;
             }
@@ -258,7 +320,9 @@ __device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double*
     }
     {
         // Closure::SolveClosure (closure.cpp:133-193); guard = the finiteness test of :318
+        PT_BEGIN( tg );
         double gn = gradient<CL, GROUP>( g, P, phiWf, LA, w.uh, nTj, w.uk, w.g, w.red );
+        PT_END( tg, 1 );
         if( gn < eps ) {
             rc = UQC_CELL_CONVERGED;
             goto out;
@@ -271,7 +335,7 @@ __device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double*
                 for( int idx = g.r; idx < n; idx += GROUP ) w.g[idx] = w.gN[idx];
                 gn = gnN;
             }
-            if( newton_direction<CL, GROUP>( g, P, phi, w, nTj, LA ) ) {
+            if( newton_direction<CL, GROUP, HT>( g, P, phi, phiH, w, nTj, LA ) ) {
                 rc = UQC_CELL_NOT_PD;
                 goto out;
             }
@@ -286,12 +350,14 @@ __device__ int newton_cell( const Grp<GROUP>& g, const KParams& P, const double*
                 rc = UQC_CELL_CONVERGED;
                 goto out;
             }
+            PT_BEGIN( tt );
             for( int idx = g.r; idx < P.nS * P.nT; idx += GROUP ) w.lamN[idx] = w.lam[idx];
             add_step<GROUP>( g, P, nTj, w.lam, -stepSize, w.d, w.lamN );
             g.sync();
             eval_lambda<Closure<CL>::NS, GROUP>( g, P, phi, w.lamN, nTj, LB );
             g.sync();
             gnN        = gradient<CL, GROUP>( g, P, phiWf, LB, w.uh, nTj, w.uk, w.gN, w.red );
+            PT_END( tt, 5 );
             int refine = 0;
             while( gn < gnN || ( guard && !isfinite( gnN ) ) ) {
                 stepSize *= 0.5;
@@ -328,20 +394,208 @@ out:
 
 // ------------------------------------------------------------------ kernels
 
+// Epilogue of a cell whose closure is done, phases [C]-[F] of
+// MomentSolver::Solve (momentsolver.cpp:99-133): uk holds U(Lambda(lam)) at
+// the nodes, uh the moments before re-projection. Writes uQ, the new
+// refinement level (indicator of :271-289, thresholds of :104-112) and the
+// re-projected moments, and returns the cell's CFL time step.
+template <int CL, int GROUP>
+__device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* uh, const double* uk, int cell,
+                                 int lev, int nTj, double* red ) {
+    constexpr int NS = Closure<CL>::NS;
+    const size_t ldc = size_t( NS ) * P.nT;
+    int newLev       = lev;
+    if( P.nLevels > 1 ) {
+        double ind = 0.0;
+        if( P.dimXi == 1 )
+            ind = fabs( uh[nTj - 1] ) + fabs( uh[nTj - 2] );
+        else {
+            int prev = lev == 0 ? 1 : P.nTLevel[lev - 1];
+            for( int i = prev; i < nTj; ++i ) ind += fabs( uh[i] );
+        }
+        if( ind > 0.02 && lev < P.nLevels - 1 )
+            newLev = lev + 1;
+        else if( ind < 0.004 && lev > 0 )
+            newLev = lev - 1;
+    }
+    const int nTn = P.nTLevel[newLev];
+    if( g.r == 0 ) {
+        P.uOld0[cell] = uh[0];
+        P.level[cell] = unsigned( newLev );
+    }
+    double* uq = P.uQ + size_t( cell ) * NS * P.nQ;
+    for( int idx = g.r; idx < NS * P.nQ; idx += GROUP ) uq[idx] = uk[idx];
+    // [E] u(s, i) = sum_k uQ(s, k) phiWf(k, i) for i < nT(new level), 0 beyond
+    for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
+        int s = idx / P.nT, i = idx - s * P.nT;
+        double a = 0.0;
+        if( i < nTn ) {
+            const double* us = uk + s * P.nQ;
+            for( int k = 0; k < P.nQ; ++k ) a = fma( us[k], phiWf[size_t( k ) * P.ld + i], a );
+        }
+        P.u[cell * ldc + idx] = a;
+    }
+    // [F] the cell's time step (min over its nodes)
+    double dloc = 1e300;
+    for( int k = g.r; k < P.nQ; k += GROUP ) {
+        double uqk[NS];
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) uqk[s] = uk[s * P.nQ + k];
+        double d = Problem<CL>::dt( uqk, P.dx[cell], P.phys );
+        dloc     = d < dloc ? d : dloc;
+    }
+    return group_min<GROUP>( g, dloc, red );
+}
+
 __device__ __forceinline__ void atomic_min_pos_double( unsigned long long* addr, double v ) {
     if( v >= 0.0 ) atomicMin( addr, (unsigned long long)__double_as_longlong( v ) );
 }
 
+// Threads per CTA of k_closure: up to 8 warp groups, 6 two-warp groups.
+template <int GROUP> constexpr int closure_max_block() { return GROUP == 32 ? 256 : ( GROUP == 64 ? 384 : GROUP ); }
+
 // Persistent closure kernel. mode 0: closure only; mode 1: closure + fused
 // epilogue of a time step. Tables are staged in shared memory when they fit.
-template <int CL, int GROUP>
-__global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_closure( KParams P, int mode ) {
+// HT = float is the mixed form: cells whose FP32 Newton does not converge
+// (FP32 factor not positive definite, line search or iteration limit) are
+// appended to P.fallbackList, with their last accepted duals written back,
+// for a pass of the FP64 form; they get no status or epilogue here.
+template <int CL, int GROUP, class HT>
+__global__ void __launch_bounds__( closure_max_block<GROUP>() ) k_closure( KParams P, int mode ) {
     constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP;
+    constexpr bool MIXED = sizeof( HT ) == 4;
     extern __shared__ __align__( 16 ) double smem[];
     if( mode == 1 && !P.ctl->active ) return;
-    const int groups = blockDim.x / GROUP;
-    Grp<GROUP> g{int( threadIdx.x % GROUP )};
     const int gid = threadIdx.x / GROUP;
+    Grp<GROUP> g{int( threadIdx.x % GROUP ), 1 + gid};
+    const double *phi = P.phi, *phiWf = P.phiWf;
+    const HT* phiH;
+    if constexpr( MIXED )
+        phiH = P.phiF;
+    else
+        phiH = P.phi;
+    double* base = smem;
+    if( P.tablesInSmem ) {
+        const size_t tn = size_t( P.nQ ) * P.ld + 4;
+        for( size_t i = threadIdx.x; i < tn; i += blockDim.x ) {
+            base[i]      = i < size_t( P.nQ ) * P.ld ? P.phi[i] : 0.0;
+            base[tn + i] = i < size_t( P.nQ ) * P.ld ? P.phiWf[i] : 0.0;
+        }
+        phi   = base;
+        phiWf = base + tn;
+        base += 2 * tn;
+        if constexpr( MIXED ) {
+            float* f = reinterpret_cast<float*>( base );
+            for( size_t i = threadIdx.x; i < tn; i += blockDim.x ) f[i] = i < size_t( P.nQ ) * P.ld ? P.phiF[i] : 0.0f;
+            phiH = f;
+            base += ( tn + 1 ) / 2;
+        }
+        else {
+            phiH = phi;
+        }
+        __syncthreads();
+    }
+    CellWs w = carve( base + gid * cell_ws_doubles( NS, P.nT, P.nQ, NP, sizeof( HT ) ), NS, P.nT, P.nQ, NP, sizeof( HT ) );
+    const size_t ldc = size_t( NS ) * P.nT;
+    double* bc       = w.red + 16;    // broadcast slot
+    unsigned long long itSum = 0, lsSum = 0;
+    int failSum = 0, activeSum = 0, fbSum = 0;
+    double dtMin = 1e300;
+    // work items: all cells, or the cells k_check found unconverged
+    const int nWork = P.activeList ? int( *P.activeCount ) : P.nCells;
+    for( ;; ) {
+        int item;
+        if( g.r == 0 ) bc[0] = double( atomicAdd( P.workCounter, 1u ) );
+        g.sync();
+        item = int( bc[0] );
+        g.sync();
+        if( item >= nWork ) break;
+        const int cell = P.activeList ? P.activeList[item] : item;
+        const int lev = P.level ? int( P.level[cell] ) : P.nLevels - 1;
+        const int nTj = P.nTotalCell ? int( P.nTotalCell[cell] ) : P.nTLevel[lev];
+        // load duals and moments (state-major, finest stride), checking finiteness on the way
+        bool bad = false;
+        for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
+            double a = P.lam[cell * ldc + idx], b = P.u[cell * ldc + idx];
+            w.lam[idx] = a;
+            w.uh[idx]  = b;
+            bad        = bad || !isfinite( a ) || !isfinite( b );
+        }
+        const bool anyBad = group_any<GROUP>( g, bad, w.red );
+        g.sync();
+        int iters = 0, ls = 0, rc;
+        if( anyBad )
+            rc = UQC_CELL_NONFINITE;
+        else
+        {
+            PT_BEGIN( tn );
+            rc = newton_cell<CL, GROUP, HT>( g, P, phi, phiWf, phiH, w, nTj, iters, ls );
+            PT_END( tn, 0 );
+        }
+        if( MIXED && rc != UQC_CELL_CONVERGED && rc != UQC_CELL_NONFINITE ) {
+            for( int idx = g.r; idx < int( ldc ); idx += GROUP ) P.lam[cell * ldc + idx] = w.lam[idx];
+            if( g.r == 0 ) {
+                P.fallbackList[atomicAdd( P.fallbackCount, 1u )] = cell;
+                ++fbSum;
+                itSum += iters;
+                lsSum += ls;
+            }
+            g.sync();
+            continue;
+        }
+        if( g.r == 0 ) {
+            P.status[cell] = rc;
+            P.iters[cell]  = iters;
+            itSum += iters;
+            lsSum += ls;
+            failSum += rc != 0;
+            activeSum += iters > 0;
+        }
+        for( int idx = g.r; idx < int( ldc ); idx += GROUP ) P.lam[cell * ldc + idx] = w.lam[idx];
+        PT_BEGIN( te );
+        if( mode == 1 ) {
+            // [C] uQ = U(Lambda(lam)). A converged cell's last gradient evaluation
+            // was at the accepted duals, so w.uk already holds U there (the
+            // U(Vector&) form; the reference reconstructs with U(const Matrix&),
+            // which for the Euler closure differs in the last bits only).
+            if( rc != 0 ) {
+                eval_lambda<NS, GROUP>( g, P, phi, w.lam, nTj, w.LA );
+                g.sync();
+                eval_u<CL, GROUP>( g, P, w.LA, w.uk, true );
+            }
+            g.sync();
+            const double dloc = cell_epilogue<CL, GROUP>( g, P, phiWf, w.uh, w.uk, cell, lev, nTj, w.red );
+            dtMin             = dloc < dtMin ? dloc : dtMin;
+        }
+        PT_END( te, 6 );
+        g.sync();
+    }
+    if( g.r == 0 ) {
+        if( itSum ) atomicAdd( &P.ctl->newtonIters, itSum );
+        if( lsSum ) atomicAdd( &P.ctl->lineSearchTrials, lsSum );
+        if( failSum ) atomicAdd( &P.ctl->failedCells, failSum );
+        if( activeSum ) atomicAdd( &P.ctl->activeCells, activeSum );
+        if( fbSum ) atomicAdd( &P.ctl->fallbackCells, (unsigned long long)fbSum );
+        if( mode == 1 && dtMin < 1e300 ) atomic_min_pos_double( &P.ctl->dtBits, dtMin );
+    }
+}
+
+__host__ __device__ inline size_t check_ws_doubles( int nS, int nT, int nQ ) {
+    size_t ldc = size_t( nS ) * nT;
+    return ( ( 3 * ldc + 2 * size_t( nS ) * nQ + 32 ) + 3 ) & ~size_t( 3 );
+}
+
+// Step mode, first half of the closure: one warp per cell evaluates the
+// gradient at the current duals (the initial test of closure.cpp:139-142).
+// Converged cells are finished here (epilogue [C]-[F]); the others are
+// appended to P.activeList for k_closure. Many cells per SM are in flight, so
+// the latency of this per-cell work is hidden.
+template <int CL> __global__ void __launch_bounds__( 256 ) k_check( KParams P ) {
+    constexpr int NS = Closure<CL>::NS;
+    extern __shared__ __align__( 16 ) double smem[];
+    if( !P.ctl->active ) return;
+    Grp<32> g{int( threadIdx.x & 31 ), 0};
+    const int warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
     const double *phi = P.phi, *phiWf = P.phiWf;
     double* base = smem;
     if( P.tablesInSmem ) {
@@ -355,178 +609,141 @@ __global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_closure( KParam
         base += 2 * tn;
         __syncthreads();
     }
-    CellWs w = carve( base + gid * cell_ws_doubles( NS, P.nT, P.nQ, NP ), NS, P.nT, P.nQ, NP );
     const size_t ldc = size_t( NS ) * P.nT;
-    double* bc       = w.red + 16;    // broadcast slot
-    unsigned long long itSum = 0, lsSum = 0;
-    int failSum = 0, activeSum = 0;
-    double dtMin = 1e300;
-    for( ;; ) {
-        int cell;
-        if( g.r == 0 ) bc[0] = double( atomicAdd( &P.ctl->workCounter, 1u ) );
-        g.sync();
-        cell = int( bc[0] );
-        g.sync();
-        if( cell >= P.nCells ) break;
-        const int lev = P.level ? int( P.level[cell] ) : P.nLevels - 1;
-        const int nTj = P.nTotalCell ? int( P.nTotalCell[cell] ) : P.nTLevel[lev];
-        // load duals and moments (state-major, finest stride), checking finiteness on the way
+    double* lam      = base + warp * check_ws_doubles( NS, P.nT, P.nQ );
+    double* uh       = lam + ldc;
+    double* gbuf     = uh + ldc;
+    double* LA       = gbuf + ldc;
+    double* uk       = LA + size_t( NS ) * P.nQ;
+    double* red      = uk + size_t( NS ) * P.nQ;
+    double dtMin     = 1e300;
+    for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
+        const int lev = int( P.level[cell] ), nTj = P.nTLevel[lev];
         bool bad = false;
-        for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
+        for( int idx = g.r; idx < int( ldc ); idx += 32 ) {
             double a = P.lam[cell * ldc + idx], b = P.u[cell * ldc + idx];
-            w.lam[idx] = a;
-            w.uh[idx]  = b;
-            bad        = bad || !isfinite( a ) || !isfinite( b );
+            lam[idx] = a;
+            uh[idx]  = b;
+            bad      = bad || !isfinite( a ) || !isfinite( b );
         }
-        bool anyBad;
-        if constexpr( GROUP == 32 )
-            anyBad = __any_sync( 0xffffffffu, bad );
-        else
-            anyBad = __syncthreads_or( bad );
-        g.sync();
-        int iters = 0, ls = 0, rc;
-        if( anyBad )
-            rc = UQC_CELL_NONFINITE;
-        else
-            rc = newton_cell<CL, GROUP>( g, P, phi, phiWf, w, nTj, iters, ls );
-        if( g.r == 0 ) {
-            P.status[cell] = rc;
-            P.iters[cell]  = iters;
-            itSum += iters;
-            lsSum += ls;
-            failSum += rc != 0;
-            activeSum += iters > 0;
+        bad = __any_sync( 0xffffffffu, bad );
+        __syncwarp();
+        bool converged = false;
+        if( !bad ) {
+            eval_lambda<NS, 32>( g, P, phi, lam, nTj, LA );
+            __syncwarp();
+            converged = gradient<CL, 32>( g, P, phiWf, LA, uh, nTj, uk, gbuf, red ) < P.eps;
         }
-        for( int idx = g.r; idx < int( ldc ); idx += GROUP ) P.lam[cell * ldc + idx] = w.lam[idx];
-        if( mode == 1 ) {
-            // [C] uQ = U(Lambda(lam)). A converged cell's last gradient evaluation
-            // was at the accepted duals, so w.uk already holds U there (the
-            // U(Vector&) form; the reference reconstructs with U(const Matrix&),
-            // which for the Euler closure differs in the last bits only).
-            if( rc != 0 ) {
-                eval_lambda<NS, GROUP>( g, P, phi, w.lam, nTj, w.LA );
-                g.sync();
-                eval_u<CL, GROUP>( g, P, w.LA, w.uk, true );
-            }
-            // [D] refinement level from the moments before re-projection (momentsolver.cpp:104-112, 271-289)
-            int newLev = lev;
-            if( P.nLevels > 1 ) {
-                double ind = 0.0;
-                if( P.dimXi == 1 )
-                    ind = fabs( w.uh[nTj - 1] ) + fabs( w.uh[nTj - 2] );
-                else {
-                    int prev = lev == 0 ? 1 : P.nTLevel[lev - 1];
-                    for( int i = prev; i < nTj; ++i ) ind += fabs( w.uh[i] );
-                }
-                if( ind > 0.02 && lev < P.nLevels - 1 )
-                    newLev = lev + 1;
-                else if( ind < 0.004 && lev > 0 )
-                    newLev = lev - 1;
-            }
-            const int nTn = P.nTLevel[newLev];
+        if( converged ) {
             if( g.r == 0 ) {
-                P.uOld0[cell] = w.uh[0];
-                P.level[cell] = unsigned( newLev );
+                P.status[cell] = UQC_CELL_CONVERGED;
+                P.iters[cell]  = 0;
             }
-            g.sync();
-            double* uq = P.uQ + size_t( cell ) * NS * P.nQ;
-            for( int idx = g.r; idx < NS * P.nQ; idx += GROUP ) uq[idx] = w.uk[idx];
-            // [E] moments re-projected: u(s, i) = sum_k uQ(s, k) phiWf(k, i), i < nT(new level)
-            for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
-                int s = idx / P.nT, i = idx - s * P.nT;
-                double a = 0.0;
-                if( i < nTn ) {
-                    const double* us = w.uk + s * P.nQ;
-                    for( int k = 0; k < P.nQ; ++k ) a = fma( us[k], phiWf[size_t( k ) * P.ld + i], a );
-                }
-                P.u[cell * ldc + idx] = a;
-            }
-            // [F] time step of this cell (min over its nodes)
-            double dloc = 1e300;
-            for( int k = g.r; k < P.nQ; k += GROUP ) {
-                double uqk[NS];
-#pragma unroll
-                for( int s = 0; s < NS; ++s ) uqk[s] = w.uk[s * P.nQ + k];
-                double d = Problem<CL>::dt( uqk, P.dx[cell], P.phys );
-                dloc     = d < dloc ? d : dloc;
-            }
-            dloc  = group_min<GROUP>( g, dloc, w.red );
-            dtMin = dloc < dtMin ? dloc : dtMin;
+            __syncwarp();
+            const double d = cell_epilogue<CL, 32>( g, P, phiWf, uh, uk, cell, lev, nTj, red );
+            dtMin          = d < dtMin ? d : dtMin;
         }
-        g.sync();
+        else if( g.r == 0 ) {
+            P.activeList[atomicAdd( P.activeCount, 1u )] = cell;
+        }
+        __syncwarp();
     }
-    if( g.r == 0 ) {
-        if( itSum ) atomicAdd( &P.ctl->newtonIters, itSum );
-        if( lsSum ) atomicAdd( &P.ctl->lineSearchTrials, lsSum );
-        if( failSum ) atomicAdd( &P.ctl->failedCells, failSum );
-        if( activeSum ) atomicAdd( &P.ctl->activeCells, activeSum );
-        if( mode == 1 && dtMin < 1e300 ) atomic_min_pos_double( &P.ctl->dtBits, dtMin );
-    }
+    if( g.r == 0 && dtMin < 1e300 ) atomic_min_pos_double( &P.ctl->dtBits, dtMin );
 }
 
-// Flux + explicit Euler update, one group per cell (grid-stride), and the
-// residual / time control finished by the last CTA.
-template <int CL, int GROUP>
-__global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_update( KParams P ) {
+// Flux + explicit Euler update (expliciteuler.cpp:17-74), one warp per cell
+// (grid-stride over cells, many warps per SM), and the residual / time
+// control finished by the last CTA. Per node the kinetic fluxes of the cell's
+// faces are summed first (sum_f G_f), then projected once onto the basis:
+// rhs(s, i) = sum_k Gsum(s, k) phiWf(k, i). The reference accumulates the
+// projection face by face (momentsolver.cpp:413-416); the sums agree up to
+// reassociation. Each lane carries two outputs with two partial sums each.
+template <int CL>
+__global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
     __shared__ double blockRes[32];
     __shared__ int isLast;
     if( !P.ctl->active ) return;
-    const int groups = blockDim.x / GROUP;
-    Grp<GROUP> g{int( threadIdx.x % GROUP )};
-    const int gid = threadIdx.x / GROUP;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
     const double* phiWf = P.phiWf;
     double* base        = smem;
     if( P.tablesInSmem ) {
         size_t tn = size_t( P.nQ ) * P.ld;
         for( size_t i = threadIdx.x; i < tn; i += blockDim.x ) base[i] = P.phiWf[i];
         phiWf = base;
-        base += tn + 4;
+        base += ( tn + 4 ) & ~size_t( 3 );
         __syncthreads();
     }
-    double* G     = base + size_t( gid ) * ( size_t( P.nFaces ) * NS * P.nQ + 32 );
-    double* red   = G + size_t( P.nFaces ) * NS * P.nQ;
-    const double dt = __longlong_as_double( (long long)P.ctl->dtBits );
+    double* Gs       = base + size_t( warp ) * ( ( size_t( NS ) * P.nQ + 3 ) & ~size_t( 3 ) );
+    const double dt  = __longlong_as_double( (long long)P.ctl->dtBits );
     const size_t ldc = size_t( NS ) * P.nT;
     double res       = 0.0;
-    for( int cell = blockIdx.x * groups + gid; cell < P.nCells; cell += gridDim.x * groups ) {
+    for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
         if( P.boundary[cell] ) {
             // Dirichlet cell: uNew = u (expliciteuler.cpp:21-23)
-            if( g.r == 0 ) res += fabs( P.u[cell * ldc] - P.uOld0[cell] ) * P.area[cell];
+            if( lane == 0 ) res += fabs( P.u[cell * ldc] - P.uOld0[cell] ) * P.area[cell];
             continue;
         }
         const int nTj    = P.nTLevel[P.level[cell]];
         const double* ua = P.uQ + size_t( cell ) * NS * P.nQ;
-        for( int idx = g.r; idx < P.nFaces * P.nQ; idx += GROUP ) {
-            int f = idx / P.nQ, k = idx - f * P.nQ;
-            int nb = P.nbr[cell * P.nFaces + f];
-            const double* ub = P.uQ + size_t( nb ) * NS * P.nQ;
-            double a[NS], b[NS], y[NS];
+        for( int k = lane; k < P.nQ; k += 32 ) {
+            double a[NS], gsum[NS];
 #pragma unroll
             for( int s = 0; s < NS; ++s ) {
-                a[s] = ua[s * P.nQ + k];
-                b[s] = ub[s * P.nQ + k];
+                a[s]    = ua[s * P.nQ + k];
+                gsum[s] = 0.0;
             }
-            Problem<CL>::flux( a, b, P.unitN + ( cell * P.nFaces + f ) * 2, P.scaledN + ( cell * P.nFaces + f ) * 2, y, P.phys );
-#pragma unroll
-            for( int s = 0; s < NS; ++s ) G[( f * NS + s ) * P.nQ + k] = y[s];
-        }
-        g.sync();
-        const double c = dt / P.area[cell];
-        for( int idx = g.r; idx < NS * nTj; idx += GROUP ) {
-            int s = idx / nTj, i = idx - s * nTj;
-            double rhs = 0.0;
             for( int f = 0; f < P.nFaces; ++f ) {
-                const double* gs = G + ( f * NS + s ) * P.nQ;
-                for( int k = 0; k < P.nQ; ++k ) rhs = fma( gs[k], phiWf[size_t( k ) * P.ld + i], rhs );
+                const int nb      = P.nbr[cell * P.nFaces + f];
+                const double* ub  = P.uQ + size_t( nb ) * NS * P.nQ;
+                double b[NS], y[NS];
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) b[s] = ub[s * P.nQ + k];
+                Problem<CL>::flux( a, b, P.unitN + ( cell * P.nFaces + f ) * 2, P.scaledN + ( cell * P.nFaces + f ) * 2, y, P.phys );
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) gsum[s] += y[s];
             }
-            double* up = P.u + cell * ldc + s * P.nT + i;
-            double nu  = *up - rhs * c;
-            *up        = nu;
-            if( idx == 0 ) res += fabs( nu - P.uOld0[cell] ) * P.area[cell];
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) Gs[s * P.nQ + k] = gsum[s];
         }
-        g.sync();
+        __syncwarp();
+        const double c = dt / P.area[cell];
+        const int nOut = NS * nTj;
+        for( int o0 = 0; o0 < nOut; o0 += 64 ) {
+            const int idxA = o0 + lane, idxB = o0 + 32 + lane;
+            const bool okA = idxA < nOut, okB = idxB < nOut;
+            const int sA = okA ? idxA / nTj : 0, iA = okA ? idxA - sA * nTj : 0;
+            const int sB = okB ? idxB / nTj : 0, iB = okB ? idxB - sB * nTj : 0;
+            const double* gA = Gs + sA * P.nQ;
+            const double* gB = Gs + sB * P.nQ;
+            double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+            int k = 0;
+            for( ; k + 1 < P.nQ; k += 2 ) {
+                const double* r0 = phiWf + size_t( k ) * P.ld;
+                const double* r1 = r0 + P.ld;
+                a0 = fma( gA[k], r0[iA], a0 );
+                a1 = fma( gA[k + 1], r1[iA], a1 );
+                b0 = fma( gB[k], r0[iB], b0 );
+                b1 = fma( gB[k + 1], r1[iB], b1 );
+            }
+            if( k < P.nQ ) {
+                const double* r0 = phiWf + size_t( k ) * P.ld;
+                a0 = fma( gA[k], r0[iA], a0 );
+                b0 = fma( gB[k], r0[iB], b0 );
+            }
+            if( okA ) {
+                double* up = P.u + cell * ldc + sA * P.nT + iA;
+                double nu  = *up - ( a0 + a1 ) * c;
+                *up        = nu;
+                if( idxA == 0 ) res += fabs( nu - P.uOld0[cell] ) * P.area[cell];
+            }
+            if( okB ) {
+                double* up = P.u + cell * ldc + sB * P.nT + iB;
+                *up        = *up - ( b0 + b1 ) * c;
+            }
+        }
+        __syncwarp();
     }
     // deterministic residual: per-thread partials -> CTA sum -> per-CTA slot -> last CTA sums in order
     for( int o = 16; o > 0; o >>= 1 ) res += __shfl_xor_sync( 0xffffffffu, res, o );
@@ -554,7 +771,10 @@ __global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_update( KParams
         C->activeCellsLast = C->activeCells;
         C->activeCells     = 0;
         C->dtBits     = 0x7FF0000000000000ull;    // +inf for the next step's min
-        C->workCounter = 0;
+        C->workCounter  = 0;
+        C->workCounter2 = 0;
+        C->nFallback    = 0;
+        C->nActive      = 0;
         C->doneBlocks  = 0;
     }
 }
@@ -564,7 +784,7 @@ template <int CL, int GROUP> __global__ void __launch_bounds__( GROUP == 32 ? 25
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
     const int groups = blockDim.x / GROUP;
-    Grp<GROUP> g{int( threadIdx.x % GROUP )};
+    Grp<GROUP> g{int( threadIdx.x % GROUP ), 1 + int( threadIdx.x / GROUP )};
     const int gid   = threadIdx.x / GROUP;
     double* uic     = smem + size_t( gid ) * ( size_t( NS ) * P.nQ + 8 );
     const size_t ldc = size_t( NS ) * P.nT;
@@ -602,7 +822,7 @@ template <int CL, int GROUP> __global__ void __launch_bounds__( GROUP == 32 ? 25
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
     const int groups = blockDim.x / GROUP;
-    Grp<GROUP> g{int( threadIdx.x % GROUP )};
+    Grp<GROUP> g{int( threadIdx.x % GROUP ), 1 + int( threadIdx.x / GROUP )};
     const int gid    = threadIdx.x / GROUP;
     double* L        = smem + size_t( gid ) * ( 2 * size_t( NS ) * P.nQ + 8 );
     double* uk       = L + size_t( NS ) * P.nQ;

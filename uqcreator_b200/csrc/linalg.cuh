@@ -1,23 +1,52 @@
 // Per-cell dense linear algebra of the Newton step, for one thread group
-// (a warp, or a whole CTA) working on one cell in shared memory.
+// (a warp, two warps, or a whole CTA) working on one cell in shared memory.
 //
-//   hessian_sym   H = sum_k DU(Lambda_k) (x) phi_k phiWf_k^T, upper triangle
-//   cholesky_blk  H = U^T U of [H | g] (g appended as column n), blocked
-//   back_solve    x = U^-1 y (y = column n after cholesky_blk)
+//   hessian_sym       H = sum_k DU(Lambda_k) (x) phi_k phiWf_k^T, upper triangle
+//   cholesky_la       H = U^T U, right-hand side appended, by 8 x 8 tiles with
+//                     look-ahead (one group barrier per tile column)
+//   back_solve_warp   x = U^-1 y
 //
 // Together they compute posv(H, g) of the reference (vectorspace.cpp:152-171,
 // LAPACK dposv with uplo 'U'): a Cholesky factorisation and two triangular
 // solves, the forward one fused into the factorisation.
+//
+// Storage ("block-packed upper"): the n x n matrix is padded to nb = ceil(n/8)
+// tiles of 8 x 8, the padding being the identity, so every tile is full. Only
+// tiles (R, C) with R <= C are stored, in column-major tile order; inside a
+// tile, element (k, c) sits at 8 c + (k ^ c): column-major with the row index
+// XOR-swizzled by the column, so that both a tile column and a tile row read
+// by eight lanes fall in distinct shared-memory banks. The right-hand side
+// follows as nb segments of 8.
 #pragma once
 #include <cuda_runtime.h>
 
 namespace uqc {
 
+// Optional cycle counters of the closure kernel (diagnostic builds compiled
+// with -DUQC_PHASE_TIMERS): slots 0-7 are phases of the Newton step, 8-15
+// parts of the factorisation (8 critical warp, 9 trailing warp, 10 barrier
+// wait of the critical warp, 11 barrier wait of a trailing warp, 12 tile
+// factor, 13 tile inverse, 14 tile-row update, 15 panel solve).
+#ifdef UQC_PHASE_TIMERS
+__device__ unsigned long long g_phaseCycles[16];
+#define CT_BEGIN( v ) long long v = clock64();
+#define CT_END( v, id, cond ) \
+    if( cond ) atomicAdd( &g_phaseCycles[id], (unsigned long long)( clock64() - v ) );
+#else
+#define CT_BEGIN( v )
+#define CT_END( v, id, cond )
+#endif
+
+// A thread group working on one cell: GROUP = 32 (a warp), 64 (two warps,
+// several groups per CTA, synchronised by named barrier `bar`) or the CTA.
 template <int GROUP> struct Grp {
-    int r;
+    int r;      // rank in the group
+    int bar;    // named barrier id (GROUP == 64)
     __device__ __forceinline__ void sync() const {
         if constexpr( GROUP == 32 )
             __syncwarp();
+        else if constexpr( GROUP == 64 )
+            asm volatile( "bar.sync %0, 64;" ::"r"( bar ) : "memory" );
         else
             __syncthreads();
     }
@@ -54,11 +83,47 @@ template <int GROUP> __device__ double group_min( const Grp<GROUP>& g, double v,
     }
 }
 
-// Row stride of the full Hessian storage for n unknowns plus one right-hand
-// side: odd, so that a warp reading a row of the column-major matrix hits 32
-// different banks.
-__host__ __device__ inline int hess_ld( int n ) { return ( ( n + 1 ) & 1 ) ? n + 1 : n + 2; }
-__host__ __device__ inline size_t hess_doubles( int n ) { return size_t( hess_ld( n ) ) * ( n + 1 ); }
+template <int GROUP> __device__ bool group_any( const Grp<GROUP>& g, bool v, double* scratch ) {
+    bool w = __any_sync( 0xffffffffu, v );
+    if constexpr( GROUP == 32 ) {
+        return w;
+    }
+    else {
+        if( ( g.r & 31 ) == 0 ) scratch[g.r >> 5] = w ? 1.0 : 0.0;
+        g.sync();
+        bool any = false;
+        for( int i = 0; i < GROUP / 32; ++i ) any = any || scratch[i] != 0.0;
+        g.sync();
+        return any;
+    }
+}
+
+// 1/sqrt(a) for a > 0 on the Cholesky critical path: the single-precision
+// hardware estimate (relative error below 2^-22) refined by one Newton-Raphson
+// step for f(y) = 1/y^2 - a, y <- y (3 - a y^2) / 2, which squares the relative
+// error (below 2^-43, about 1e-13: the pivots, and through them the Newton
+// direction, are exact to far below the closure tolerance; convergence is
+// decided by the FP64 gradient). Arguments beyond single-precision range use
+// rsqrt().
+__device__ __forceinline__ double rsqrt_nr( double a ) {
+    if( !( a > 1e-30 && a < 1e30 ) ) return rsqrt( a );
+    const double y = double( rsqrtf( float( a ) ) );
+    return y * fma( -0.5 * a * y, y, 1.5 );
+}
+__device__ __forceinline__ float rsqrt_nr( float a ) { return rsqrtf( a ); }
+
+// ---- block-packed storage
+__host__ __device__ inline int hnb( int n ) { return ( n + 7 ) >> 3; }
+__host__ __device__ inline size_t hess_doubles( int n ) {
+    const size_t nb = size_t( hnb( n ) );
+    return nb * ( nb + 1 ) / 2 * 64 + nb * 8;
+}
+// in-tile offset of element (row k, column c)
+__device__ __forceinline__ int tix( int k, int c ) { return ( c << 3 ) | ( k ^ c ); }
+__device__ __forceinline__ int htile( int R, int C ) { return ( ( ( C * ( C + 1 ) ) >> 1 ) + R ) * 64; }
+// offset of element (r, c), tile row r/8 <= tile column c/8
+__device__ __forceinline__ int hblk( int r, int c ) { return htile( r >> 3, c >> 3 ) + tix( r & 7, c & 7 ); }
+__device__ __forceinline__ int hrhs( int nb ) { return ( ( nb * ( nb + 1 ) ) >> 1 ) * 64; }
 
 // Upper-triangular pair index e -> (j, i), j <= i, column-major packed order.
 __device__ __forceinline__ void unpack_pair( int e, int& j, int& i ) {
@@ -69,17 +134,27 @@ __device__ __forceinline__ void unpack_pair( int e, int& j, int& i ) {
     j = e - c * ( c + 1 ) / 2;
 }
 
+template <class T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
 // Hessian of the dual problem (closure.cpp:255-271): block (m, l) of H is
 // sum_k phi(k, .) phiWf(k, .)^T DU(l, m)(Lambda_k). With phiWf(k, i) =
 // phi(k, i) wt_k (wt_k = w_k / 2^dimXi, an exact identity in binary floating
 // point) every block is phi^T diag(wt DU_lm) phi: symmetric, and the product
-// phi(k,j) phi(k,i) is shared by all NS(NS+1)/2 blocks. One thread owns a pair
-// j <= i and accumulates it for every block; off-diagonal blocks are mirrored.
-// du (NP x nQ) receives wt_k DU(Lambda_k). Writes the upper triangle of H
-// (column-major, row stride ldH); the lower triangle is never read.
-template <int NS, int NP, int GROUP, class DUF>
-__device__ void hessian_sym( const Grp<GROUP>& g, int nQ, int ld, const double* phi, const double* wt, const double* L, int nTj, double* du,
-                             double* H, int ldH, DUF&& duf ) {
+// phi(k,j) phi(k,i) is shared by all NS(NS+1)/2 blocks. A thread owns the two
+// pairs (j, i0) and (j, i0 + 1), i0 even, j <= i0 + 1, and accumulates them for
+// every block; off-diagonal blocks are mirrored. du (nQ x np_pad(NP), node-
+// major) receives wt_k DU(Lambda_k). Writes the upper triangle of H and the
+// identity padding (the right-hand side is written by the caller). T = double
+// (FP64 form) or float (mixed form: DU evaluated in FP64 and rounded, products
+// and sums in FP32, phi the FP32 copy of the table).
+template <int NS, int NP, int GROUP, class T, class DUF>
+__device__ void hessian_sym( const Grp<GROUP>& g, int nQ, int ld, const T* phi, const double* wt, const double* L, int nTj, T* du, T* H,
+                             DUF&& duf ) {
+    constexpr int NPP = ( NP + 1 ) & ~1;    // node-major DU rows padded to pairs
+    using V2          = typename Vec2<T>::type;
+    const int n = NS * nTj, nb = hnb( n );
     for( int k = g.r; k < nQ; k += GROUP ) {
         double Lk[NS], y[NP];
 #pragma unroll
@@ -87,167 +162,341 @@ __device__ void hessian_sym( const Grp<GROUP>& g, int nQ, int ld, const double* 
         duf( Lk, y );
         const double w = wt[k];
 #pragma unroll
-        for( int p = 0; p < NP; ++p ) du[p * nQ + k] = w * y[p];
+        for( int p = 0; p < NPP; ++p ) du[k * NPP + p] = p < NP ? T( w * y[p] ) : T( 0 );
+    }
+    // identity padding of the last tile column (rows and columns >= n) and of the right-hand side
+    if( n & 7 ) {
+        const int C = nb - 1;
+        for( int e = g.r; e < nb * 64; e += GROUP ) {
+            const int R = e >> 6, col = C * 8 + ( ( e >> 3 ) & 7 ), row = R * 8 + ( e & 7 );
+            if( col >= n && row <= col ) H[hblk( row, col )] = row == col ? T( 1 ) : T( 0 );
+        }
+        for( int r = n + g.r; r < nb * 8; r += GROUP ) H[hrhs( nb ) + r] = T( 0 );
     }
     g.sync();
-    const int pairs = nTj * ( nTj + 1 ) / 2;
-    for( int e = g.r; e < pairs; e += GROUP ) {
-        int j, i;
-        unpack_pair( e, j, i );
-        double acc[NP];
+    // pair blocks: i-pair q (i0 = 2q) has min(2q + 2, nTj) values of j
+    const int nq = ( nTj + 1 ) >> 1, last = nq - 1;
+    const int blocks = last * ( last + 1 ) + ( 2 * last + 2 < nTj ? 2 * last + 2 : nTj );
+    for( int b = g.r; b < blocks; b += GROUP ) {
+        int q = int( ( sqrtf( 4.0f * float( b ) + 1.0f ) - 1.0f ) * 0.5f );
+        while( q * ( q + 1 ) > b ) --q;
+        while( ( q + 1 ) * ( q + 2 ) <= b ) ++q;
+        const int j = b - q * ( q + 1 ), i0 = 2 * q;
+        T acc0[NPP], acc1[NPP];
 #pragma unroll
-        for( int p = 0; p < NP; ++p ) acc[p] = 0.0;
-        const double* pj = phi + j;
-        const double* pi = phi + i;
-        for( int k = 0; k < nQ; ++k ) {
-            const double prod = pj[size_t( k ) * ld] * pi[size_t( k ) * ld];
+        for( int p = 0; p < NPP; ++p ) acc0[p] = acc1[p] = T( 0 );
+        const T* rowp = phi;
+        for( int k = 0; k < nQ; ++k, rowp += ld ) {
+            const T pj = rowp[j], prod0 = pj * rowp[i0], prod1 = pj * rowp[i0 + 1];
+            const V2* d2 = reinterpret_cast<const V2*>( du + k * NPP );
 #pragma unroll
-            for( int p = 0; p < NP; ++p ) acc[p] = fma( prod, du[p * nQ + k], acc[p] );
-        }
-        int p = 0;
-#pragma unroll
-        for( int m = 0; m < NS; ++m )
-#pragma unroll
-            for( int l = m; l < NS; ++l, ++p ) {
-                const int row = m * nTj + j, col = l * nTj + i;
-                H[size_t( col ) * ldH + row] = acc[p];
-                if( m < l && j != i ) H[size_t( l * nTj + j ) * ldH + ( m * nTj + i )] = acc[p];
+            for( int p = 0; p < NPP / 2; ++p ) {
+                const V2 v      = d2[p];
+                acc0[2 * p]     = fma( prod0, v.x, acc0[2 * p] );
+                acc0[2 * p + 1] = fma( prod0, v.y, acc0[2 * p + 1] );
+                acc1[2 * p]     = fma( prod1, v.x, acc1[2 * p] );
+                acc1[2 * p + 1] = fma( prod1, v.y, acc1[2 * p + 1] );
             }
+        }
+#pragma unroll
+        for( int h = 0; h < 2; ++h ) {
+            const int i = i0 + h;
+            if( j > i || i >= nTj ) continue;
+            int p = 0;
+#pragma unroll
+            for( int m = 0; m < NS; ++m )
+#pragma unroll
+                for( int l = m; l < NS; ++l, ++p ) {
+                    const T a = h ? acc1[p] : acc0[p];
+                    H[hblk( m * nTj + j, l * nTj + i )] = a;
+                    if( m < l && j != i ) H[hblk( m * nTj + i, l * nTj + j )] = a;
+                }
+        }
     }
 }
 
-// Blocked right-looking Cholesky of the n x n upper-stored matrix with the
-// right-hand side in column n: on return the upper triangle holds U (U^T U =
-// H), column n holds y = U^-T b, D[j] = U(j,j), I[j] = 1/U(j,j). Per panel of
-// B columns: (1) one warp factors the diagonal block, (2) the panel rows are
-// solved column by column (one thread per column, right-hand side included),
-// (3) the trailing upper triangle (and right-hand side) is updated with 2 x 2
-// register tiles. Three group barriers per panel. Returns 0, or j + 1 for the
-// first pivot that is not positive (posv's info > 0). flag: one int in shared
-// memory.
+// ---- tile kernels of the factorisation; `lane` of one warp
+
+// One thread: Cholesky of the (updated) diagonal tile in registers. Writes
+// U_JJ over its upper triangle, D = diag(U), I = 1/diag(U); sets *flag to
+// j0 + jj + 1 at the first pivot that is not positive.
+template <class T> __device__ void tile_factor( T* DT, T* D, T* I, int j0, int* flag ) {
+    T a[8][8];
+#pragma unroll
+    for( int r = 0; r < 8; ++r )
+#pragma unroll
+        for( int c = r; c < 8; ++c ) a[r][c] = DT[tix( r, c )];
+    int bad = 0;
+#pragma unroll
+    for( int jj = 0; jj < 8; ++jj ) {
+        if( !bad ) {
+            const T ajj = a[jj][jj];
+            if( !( ajj > T( 0 ) ) ) {
+                bad = j0 + jj + 1;
+            }
+            else {
+                const T inv = rsqrt_nr( ajj ), d = ajj * inv;
+                a[jj][jj]   = d;
+                D[j0 + jj]  = d;
+                I[j0 + jj]  = inv;
+#pragma unroll
+                for( int c = jj + 1; c < 8; ++c ) a[jj][c] *= inv;
+#pragma unroll
+                for( int r = jj + 1; r < 8; ++r )
+#pragma unroll
+                    for( int c = r; c < 8; ++c ) a[r][c] -= a[jj][r] * a[jj][c];
+            }
+        }
+    }
+    if( bad ) *flag = bad;
+#pragma unroll
+    for( int r = 0; r < 8; ++r )
+#pragma unroll
+        for( int c = r; c < 8; ++c ) DT[tix( r, c )] = a[r][c];
+}
+
+// Lanes 0..7: row i of X = U_JJ^-1 (upper triangular) into the strictly lower
+// half of the diagonal tile, X(i, c) at element (c, i):
+// X(i,i) = I[i], X(i,c) = -I[c] sum_{k=i}^{c-1} X(i,k) U(k,c). The strictly
+// upper part of U and I are read into registers first (the stores go to the
+// lower half), so the chain is FMA latency only.
+template <class T> __device__ void tile_inverse( T* DT, const T* I, int j0, int lane ) {
+    if( lane >= 8 ) return;
+    const int i = lane;
+    T u[8][8], iv[8];
+#pragma unroll
+    for( int c = 1; c < 8; ++c )
+#pragma unroll
+        for( int k = 0; k < c; ++k ) u[k][c] = DT[tix( k, c )];
+#pragma unroll
+    for( int c = 0; c < 8; ++c ) iv[c] = I[j0 + c];
+    T x[8];
+#pragma unroll
+    for( int c = 0; c < 8; ++c ) x[c] = c == i ? iv[c] : T( 0 );
+#pragma unroll
+    for( int c = 1; c < 8; ++c ) {
+        T s = 0;
+#pragma unroll
+        for( int k = 0; k < c; ++k ) s = fma( x[k], u[k][c], s );    // x[k] = 0 for k < i
+        if( c > i ) x[c] = -s * iv[c];
+    }
+#pragma unroll
+    for( int c = 1; c < 8; ++c )
+        if( c > i ) DT[tix( c, i )] = x[c];
+}
+
+// Panel of tile row J: U(J, C) = X^T A(J, C) for C in (J, nb), and y_J = X^T b_J.
+// Lane (r, c0 = lane / 8) computes elements (r, c0) and (r, c0 + 4) of a tile;
+// two tiles at a time, all reads before the writes.
+template <class T> __device__ void tile_row_solve( T* H, int J, int nb, const T* I, int lane ) {
+    const int r = lane & 7, c0 = lane >> 3, c1 = c0 + 4;
+    const T* DT = H + htile( J, J );
+    T xr[8];    // X(k, r), k <= r
+#pragma unroll
+    for( int k = 0; k < 8; ++k ) xr[k] = k < r ? DT[tix( r, k )] : ( k == r ? I[J * 8 + r] : T( 0 ) );
+    T* b = H + hrhs( nb ) + J * 8;
+    for( int C = J + 1; C < nb + 1; C += 2 ) {
+        // tiles C and C + 1; index nb stands for the right-hand side segment
+        T u[2][2];
+#pragma unroll
+        for( int h = 0; h < 2; ++h ) {
+            const int CC = C + h;
+            T p0 = 0, p1 = 0, q0 = 0, q1 = 0;
+            if( CC < nb ) {
+                const T* A = H + htile( J, CC );
+#pragma unroll
+                for( int k = 0; k < 8; k += 2 ) {
+                    p0 = fma( xr[k], A[tix( k, c0 )], p0 );
+                    q0 = fma( xr[k + 1], A[tix( k + 1, c0 )], q0 );
+                    p1 = fma( xr[k], A[tix( k, c1 )], p1 );
+                    q1 = fma( xr[k + 1], A[tix( k + 1, c1 )], q1 );
+                }
+            }
+            else if( CC == nb ) {
+#pragma unroll
+                for( int k = 0; k < 8; k += 2 ) {
+                    p0 = fma( xr[k], b[k], p0 );
+                    q0 = fma( xr[k + 1], b[k + 1], q0 );
+                }
+            }
+            u[h][0] = p0 + q0;
+            u[h][1] = p1 + q1;
+        }
+        __syncwarp();
+#pragma unroll
+        for( int h = 0; h < 2; ++h ) {
+            const int CC = C + h;
+            if( CC < nb ) {
+                T* A            = H + htile( J, CC );
+                A[tix( r, c0 )] = u[h][0];
+                A[tix( r, c1 )] = u[h][1];
+            }
+            else if( CC == nb && lane < 8 ) {
+                b[r] = u[h][0];
+            }
+        }
+    }
+}
+
+// Tiles (R, Ca) and (R, Cb) -= U(J, R)^T U(J, C.) (Cb < 0: one tile); lane
+// layout of tile_row_solve. All reads before the writes.
+template <class T> __device__ __forceinline__ void tile_update2( T* H, int J, int R, int Ca, int Cb, int lane ) {
+    const int r = lane & 7, c0 = lane >> 3, c1 = c0 + 4;
+    const T* A = H + htile( J, R );
+    T a[8];
+#pragma unroll
+    for( int k = 0; k < 8; ++k ) a[k] = A[tix( k, r )];
+    T s[2][2];
+    T o[2][2];
+#pragma unroll
+    for( int h = 0; h < 2; ++h ) {
+        const int C = h ? Cb : Ca;
+        s[h][0] = s[h][1] = o[h][0] = o[h][1] = 0;
+        if( C >= 0 ) {
+            const T* B = H + htile( J, C );
+            const T* O = H + htile( R, C );
+            T p0 = 0, p1 = 0, q0 = 0, q1 = 0;
+#pragma unroll
+            for( int k = 0; k < 8; k += 2 ) {
+                p0 = fma( a[k], B[tix( k, c0 )], p0 );
+                q0 = fma( a[k + 1], B[tix( k + 1, c0 )], q0 );
+                p1 = fma( a[k], B[tix( k, c1 )], p1 );
+                q1 = fma( a[k + 1], B[tix( k + 1, c1 )], q1 );
+            }
+            s[h][0] = p0 + q0;
+            s[h][1] = p1 + q1;
+            o[h][0] = O[tix( r, c0 )];
+            o[h][1] = O[tix( r, c1 )];
+        }
+    }
+#pragma unroll
+    for( int h = 0; h < 2; ++h ) {
+        const int C = h ? Cb : Ca;
+        if( C >= 0 ) {
+            T* O            = H + htile( R, C );
+            O[tix( r, c0 )] = o[h][0] - s[h][0];
+            O[tix( r, c1 )] = o[h][1] - s[h][1];
+        }
+    }
+}
+
+// Right-hand side segment R -= U(J, R)^T y_J (lanes 0..7).
+template <class T> __device__ __forceinline__ void rhs_update( T* H, int J, int R, int nb, int lane ) {
+    if( lane >= 8 ) return;
+    const T* A  = H + htile( J, R );
+    const T* yJ = H + hrhs( nb ) + J * 8;
+    T s         = 0;
+#pragma unroll
+    for( int k = 0; k < 8; ++k ) s += A[tix( k, lane )] * yJ[k];
+    H[hrhs( nb ) + R * 8 + lane] -= s;
+}
+
+// Blocked right-looking Cholesky H = U^T U with look-ahead, right-hand side b
+// appended (y = U^-T b in its place). Per tile column J one warp (warp 0)
+// carries the critical path: it applies row J's update to tile row J + 1,
+// factors and inverts the diagonal tile J + 1 and solves tile row J + 1 (the
+// panel); meanwhile the other warps (all of the group's warps but warp 0, or
+// warp 0 itself afterwards when the group is one warp) apply row J's update
+// to the trailing tiles (R, C), J + 2 <= R <= C, and right-hand side segments.
+// One group barrier per tile column. On return the upper tiles hold U, D[j] =
+// U(j,j), I[j] = 1/U(j,j) (padded to 8 nb entries), and the strictly lower
+// half of each diagonal tile holds the transposed inverse of its U block.
+// Returns 0, or j + 1 for the first pivot that is not positive (posv's
+// info > 0). flag: one int in shared memory.
 template <int GROUP, class T>
-__device__ int cholesky_blk( const Grp<GROUP>& g, T* H, int ldH, int n, T* D, T* I, int* flag ) {
-    constexpr int B = 8;
-    if( g.r == 0 ) *flag = 0;
+__device__ int cholesky_la( const Grp<GROUP>& g, T* H, int n, T* D, T* I, int* flag ) {
+    constexpr int W = GROUP / 32;
+    const int nb = hnb( n ), warp = g.r >> 5, lane = g.r & 31;
+    if( warp == 0 ) {
+        if( lane == 0 ) {
+            *flag = 0;
+            tile_factor<T>( H, D, I, 0, flag );
+        }
+        __syncwarp();
+        tile_inverse<T>( H, I, 0, lane );
+        __syncwarp();
+        if( !*flag ) tile_row_solve<T>( H, 0, nb, I, lane );
+    }
     g.sync();
-    for( int j0 = 0; j0 < n; j0 += B ) {
-        const int jb = n - j0 < B ? n - j0 : B;
-        // (1) diagonal block, warp 0
-        if( g.r < 32 ) {
-            const int lane = g.r;
-            for( int jj = 0; jj < jb; ++jj ) {
-                const int j = j0 + jj;
-                const T a   = H[size_t( j ) * ldH + j];
-                if( !( a > T( 0 ) ) ) {
-                    if( lane == 0 ) *flag = j + 1;
-                    break;
-                }
-                const T d = sqrt( a ), inv = T( 1 ) / d;
-                const int c = j + 1 + lane;
-                if( c < j0 + jb ) H[size_t( c ) * ldH + j] *= inv;
-                if( lane == 0 ) {
-                    H[size_t( j ) * ldH + j] = d;
-                    D[j]                     = d;
-                    I[j]                     = inv;
-                }
-                __syncwarp();
-                // rank-1 update of the rest of the diagonal block: (r, c), j < r <= c < j0 + jb
-                const int m = j0 + jb - j - 1, cnt = m * ( m + 1 ) / 2;
-                for( int e = lane; e < cnt; e += 32 ) {
-                    int rr, cc;
-                    unpack_pair( e, rr, cc );
-                    const int r = j + 1 + rr, c2 = j + 1 + cc;
-                    H[size_t( c2 ) * ldH + r] -= H[size_t( r ) * ldH + j] * H[size_t( c2 ) * ldH + j];
-                }
-                __syncwarp();
-            }
+    if( *flag ) return *flag;
+    for( int J = 0; J + 1 < nb; ++J ) {
+        const int K = J + 1;
+        CT_BEGIN( tc );
+        if( warp == 0 ) {
+            CT_BEGIN( t0 );
+            for( int C = K; C < nb; C += 2 ) tile_update2<T>( H, J, K, C, C + 1 < nb ? C + 1 : -1, lane );
+            rhs_update<T>( H, J, K, nb, lane );
+            __syncwarp();
+            CT_END( t0, 14, g.r == 0 );
+            CT_BEGIN( t1 );
+            if( lane == 0 ) tile_factor<T>( H + htile( K, K ), D, I, K * 8, flag );
+            __syncwarp();
+            CT_END( t1, 12, g.r == 0 );
+            CT_BEGIN( t2 );
+            tile_inverse<T>( H + htile( K, K ), I, K * 8, lane );
+            __syncwarp();
+            CT_END( t2, 13, g.r == 0 );
+            CT_BEGIN( t3 );
+            if( !*flag ) tile_row_solve<T>( H, K, nb, I, lane );
+            CT_END( t3, 15, g.r == 0 );
         }
+        CT_END( tc, 8, g.r == 0 );
+        CT_BEGIN( tw );
+        if( W == 1 || warp > 0 ) {
+            const int worker = W == 1 ? 0 : warp - 1, workers = W == 1 ? 1 : W - 1;
+            if( W == 1 ) __syncwarp();
+            // items: tile pairs (R, C), (R, C + 1) of one tile row, then rhs segments
+            for( int R = J + 2, e = 0; R < nb; ++R ) {
+                for( int C = R; C < nb; C += 2, ++e )
+                    if( e % workers == worker ) tile_update2<T>( H, J, R, C, C + 1 < nb ? C + 1 : -1, lane );
+            }
+            for( int R = J + 2 + worker; R < nb; R += workers ) rhs_update<T>( H, J, R, nb, lane );
+        }
+        CT_END( tw, 9, g.r == 32 );
+        CT_BEGIN( tb );
         g.sync();
+        CT_END( tb, 10, g.r == 0 );
+        CT_END( tb, 11, g.r == 32 );
         if( *flag ) return *flag;
-        // (2) panel rows: U(J, c) = U_JJ^-T A(J, c) for c in [j0 + jb, n]
-        const int s = j0 + jb;
-        for( int c = s + g.r; c <= n; c += GROUP ) {
-            T x[B];
-#pragma unroll
-            for( int jj = 0; jj < B; ++jj ) {
-                if( jj < jb ) {
-                    const int j = j0 + jj;
-                    T v         = H[size_t( c ) * ldH + j];
-#pragma unroll
-                    for( int kk = 0; kk < B; ++kk )
-                        if( kk < jj ) v -= H[size_t( j ) * ldH + j0 + kk] * x[kk];
-                    x[jj]                    = v * I[j];
-                    H[size_t( c ) * ldH + j] = x[jj];
-                }
-            }
-        }
-        g.sync();
-        // (3) trailing update: A(r, c) -= sum_{k in J} U(k, r) U(k, c), s <= r <= c, r < n, c <= n
-        const int m = n - s;    // trailing rows
-        if( m > 0 ) {
-            const int mt = ( m + 2 ) / 2;    // column tiles over m + 1 columns
-            const int tiles = mt * ( mt + 1 ) / 2;
-            for( int t = g.r; t < tiles; t += GROUP ) {
-                int tr, tc;
-                unpack_pair( t, tr, tc );
-                const int r0 = s + 2 * tr, c0 = s + 2 * tc;
-                if( r0 >= n ) continue;
-                const int r1 = r0 + 1 < n ? r0 + 1 : r0, c1 = c0 + 1 <= n ? c0 + 1 : c0;
-                T a00 = 0, a01 = 0, a10 = 0, a11 = 0;
-#pragma unroll
-                for( int kk = 0; kk < B; ++kk ) {
-                    if( kk < jb ) {
-                        const int k = j0 + kk;
-                        const T u0 = H[size_t( r0 ) * ldH + k], u1 = H[size_t( r1 ) * ldH + k];
-                        const T v0 = H[size_t( c0 ) * ldH + k], v1 = H[size_t( c1 ) * ldH + k];
-                        a00 += u0 * v0;
-                        a01 += u0 * v1;
-                        a10 += u1 * v0;
-                        a11 += u1 * v1;
-                    }
-                }
-                H[size_t( c0 ) * ldH + r0] -= a00;
-                if( c1 != c0 ) H[size_t( c1 ) * ldH + r0] -= a01;
-                if( r1 != r0 && r1 <= c0 ) H[size_t( c0 ) * ldH + r1] -= a10;
-                if( r1 != r0 && c1 != c0 ) H[size_t( c1 ) * ldH + r1] -= a11;
-            }
-        }
-        g.sync();
     }
     return 0;
 }
 
-// Back substitution U x = y by one warp (y in column n of H, LAPACK dtrsm
-// 'Left','Upper','No transpose' order), x written to out[0..n).
-template <int GROUP, class T> __device__ void back_solve( const Grp<GROUP>& g, const T* H, int ldH, int n, const T* I, double* out ) {
-    if( g.r >= 32 ) return;
-    const int lane     = g.r;
-    constexpr int MAXR = 8;    // rows per lane: n <= 256
-    T y[MAXR];
+// Back substitution U x = y by warp 0, tile rows last first: r_J = y_J -
+// sum_{C > J} U(J, C) x_C (lane (r, q) sums columns q, q + 4 of each tile,
+// then two shuffles), x_J = X_J r_J with the stored tile inverse. Only x[0..n)
+// is written; the group synchronises at the end.
+template <int GROUP, class T>
+__device__ void back_solve_warp( const Grp<GROUP>& g, const T* H, int n, const T* I, double* x ) {
+    const int nb = hnb( n ), warp = g.r >> 5, lane = g.r & 31;
+    if( warp == 0 ) {
+        const int r = lane & 7, q = lane >> 3;
+        const T* y = H + hrhs( nb );
+        for( int J = nb - 1; J >= 0; --J ) {
+            T acc = 0;
+            for( int C = J + 1; C < nb; ++C ) {
+                const T* A = H + htile( J, C );
 #pragma unroll
-    for( int q = 0; q < MAXR; ++q ) y[q] = ( lane + 32 * q < n ) ? H[size_t( n ) * ldH + lane + 32 * q] : T( 0 );
-    for( int k = n - 1; k >= 0; --k ) {
-        T xk     = 0;
-        const int own = k & 31, q0 = k >> 5;
-#pragma unroll
-        for( int q = 0; q < MAXR; ++q )
-            if( q == q0 && lane == own ) {
-                if( y[q] != T( 0 ) ) y[q] = y[q] * I[k];
-                xk = y[q];
+                for( int cc = q; cc < 8; cc += 4 ) {
+                    const int c = C * 8 + cc;
+                    if( c < n ) acc += A[tix( r, cc )] * T( x[c] );
+                }
             }
-        xk = __shfl_sync( 0xffffffffu, xk, own );
-        if( xk != T( 0 ) ) {
-            const T* col = H + size_t( k ) * ldH;
+            acc += __shfl_xor_sync( 0xffffffffu, acc, 8 );
+            acc += __shfl_xor_sync( 0xffffffffu, acc, 16 );
+            const T rr  = y[J * 8 + r] - acc;
+            const T* DT = H + htile( J, J );
+            T v         = I[J * 8 + r] * rr;
 #pragma unroll
-            for( int q = 0; q < MAXR; ++q ) {
-                const int r = lane + 32 * q;
-                if( r < k ) y[q] = y[q] - xk * col[r];
+            for( int k = 1; k < 8; ++k ) {
+                const T rk = __shfl_sync( 0xffffffffu, rr, k );
+                if( k > r ) v += DT[tix( k, r )] * rk;
             }
+            if( q == 0 && J * 8 + r < n ) x[J * 8 + r] = double( v );
+            __syncwarp();
         }
     }
-#pragma unroll
-    for( int q = 0; q < MAXR; ++q )
-        if( lane + 32 * q < n ) out[lane + 32 * q] = double( y[q] );
+    g.sync();
 }
 
 }    // namespace uqc

@@ -22,7 +22,6 @@
 
 #include "host.h"
 #include "ipm_kernels.cuh"
-#include "mixed.cuh"
 #include "uqc.h"
 
 using namespace uqc;
@@ -36,7 +35,7 @@ struct uqc_solver {
     bool ownStream          = false;
     bool deviceReady        = false;
     int nS = 1, ld = 1, group = 32, numSMs = 148;
-    int closureGroup = 32, closureGroupOverride = 0;    // threads per cell in k_closure (32 or 256)
+    int closureGroup = 32, closureGroupOverride = 0;    // threads per cell in k_closure (32, 64 or 256)
     size_t ldc = 1;
     // device buffers
     double *d_phi = nullptr, *d_phiWf = nullptr, *d_xi = nullptr;
@@ -53,16 +52,25 @@ struct uqc_solver {
     int *d_xStatus = nullptr, *d_xIters = nullptr;
     size_t xCap = 0;
     // launch shapes
-    int closureBlock = 256, closureGrid = 0, updateBlock = 256, updateGrid = 0, auxGrid = 0;
-    size_t closureSmem = 0, updateSmem = 0, initSmem = 0, mvSmem = 0;
+    int closureBlock = 256, closureGrid = 0, updateBlock = 256, updateGrid = 0, auxGrid = 0, auxBlock = 256;
+    size_t closureSmem = 0, updateSmem = 0, initSmem = 0, mvSmem = 0, checkSmem = 0;
+    int checkBlock = 256, checkGrid = 0;
+    int* d_activeList = nullptr;    // cells that need Newton in the running step
     bool tablesInSmem = false;
-    // mixed precision
-    MixedPlan mixed;
+    // mixed form: FP32 Hessian / factor / solves, FP64 gradient and update
+    float* d_phiF        = nullptr;    // phi rounded to FP32, row stride ld
+    int* d_fallbackList  = nullptr;    // cells the mixed form hands to the FP64 form
+    bool mixedOk         = false;
+    std::string mixedWhy = "not planned";
+    int mixedGroup = 64, mixedBlock = 256, mixedGrid = 0;
+    int mixedMaxIter = 0;    // Newton iterations of the FP32 pass before the FP64 form takes over (0: the configured limit)
+    size_t mixedSmem       = 0;
+    bool mixedTablesInSmem = false;
     // bookkeeping
     bool stateReady = false;
     int precision   = 0;
     int launches    = 0;
-    unsigned long long lastIters = 0, lastLs = 0;
+    unsigned long long lastIters = 0, lastLs = 0, lastFallback = 0;
     int lastFailed = 0;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> stepEvents;
@@ -154,6 +162,7 @@ KParams make_params( const uqc_solver* h ) {
     P.phiWf        = h->d_phiWf;
     P.xi           = h->d_xi;
     P.wt           = h->d_wt;
+    P.phiF         = h->d_phiF;
     P.tablesInSmem = h->tablesInSmem;
     P.area         = h->d_area;
     P.dx           = h->d_dx;
@@ -170,15 +179,19 @@ KParams make_params( const uqc_solver* h ) {
     P.nTotalCell   = nullptr;
     P.status       = h->d_status;
     P.iters        = h->d_iters;
-    P.blockPartial = h->d_blockPartial;
-    P.ctl          = h->d_ctl;
+    P.blockPartial  = h->d_blockPartial;
+    P.ctl           = h->d_ctl;
+    P.workCounter   = h->d_ctl ? &h->d_ctl->workCounter : nullptr;
+    P.fallbackList  = h->d_fallbackList;
+    P.fallbackCount = h->d_ctl ? &h->d_ctl->nFallback : nullptr;
     return P;
 }
 
 // ---- kernel dispatch on (closure kind, group size) ------------------------
 template <int CL, int GROUP> struct Kern {
-    static void* closure() { return (void*)&k_closure<CL, GROUP>; }
-    static void* update() { return (void*)&k_update<CL, GROUP>; }
+    static void* closure() { return (void*)&k_closure<CL, GROUP, double>; }
+    static void* closure_mixed() { return (void*)&k_closure<CL, GROUP, float>; }
+    static void* update() { return (void*)&k_update<CL>; }
     static void* init() { return (void*)&k_init<CL, GROUP>; }
     static void* meanvar() { return (void*)&k_meanvar<CL, GROUP>; }
 };
@@ -193,8 +206,32 @@ void* pick( int cl, int group, int which ) {
             default: return Kern<C, G>::meanvar();                                                                       \
         }                                                                                                                \
     }
+    if( which == 0 && group == 64 ) {    // two warps per cell: closure kernel only
+        if( cl == 0 ) return Kern<0, 64>::closure();
+        if( cl == 1 ) return Kern<1, 64>::closure();
+        if( cl == 2 ) return Kern<2, 64>::closure();
+    }
+    if( which == 4 ) {    // mixed-form closure kernel, warp or two-warp groups
+        if( group == 32 ) {
+            if( cl == 0 ) return Kern<0, 32>::closure_mixed();
+            if( cl == 1 ) return Kern<1, 32>::closure_mixed();
+            if( cl == 2 ) return Kern<2, 32>::closure_mixed();
+        }
+        if( group == 64 ) {
+            if( cl == 0 ) return Kern<0, 64>::closure_mixed();
+            if( cl == 1 ) return Kern<1, 64>::closure_mixed();
+            if( cl == 2 ) return Kern<2, 64>::closure_mixed();
+        }
+    }
     PICK( 0, 32 ) PICK( 0, 256 ) PICK( 1, 32 ) PICK( 1, 256 ) PICK( 2, 32 ) PICK( 2, 256 )
 #undef PICK
+    throw ConfigError( "no kernel for this closure" );
+}
+
+void* pick_check( int cl ) {
+    if( cl == 0 ) return (void*)&k_check<0>;
+    if( cl == 1 ) return (void*)&k_check<1>;
+    if( cl == 2 ) return (void*)&k_check<2>;
     throw ConfigError( "no kernel for this closure" );
 }
 
@@ -203,6 +240,35 @@ int closure_np( int cl ) { return cl == 0 ? 1 : ( cl == 1 ? 10 : 3 ); }
 void launch( uqc_solver* h, void* fn, int grid, int block, size_t smem, void** args ) {
     CK( cudaLaunchKernel( fn, dim3( grid ), dim3( block ), args, smem, h->stream ) );
     ++h->launches;
+}
+
+// Mixed-form closure: the FP32 Hessian halves the per-cell shared memory, so
+// more cells share an SM: a warp per cell (n <= 32) or two warps per cell, up
+// to 8 or 6 cells per CTA; the tables gain an FP32 copy of phi.
+void plan_mixed( uqc_solver* h, int maxSmem ) {
+    const int cl = h->cfg.closure, nT = h->tab.nT, nQ = h->tab.nQ, nS = h->nS;
+    const size_t n       = size_t( nS ) * nT;
+    const size_t tn      = size_t( nQ ) * h->ld + 4;
+    const size_t tables  = 2 * tn * sizeof( double ) + ( tn + 1 ) / 2 * sizeof( double );
+    const size_t wsCell  = cell_ws_doubles( nS, nT, nQ, closure_np( cl ), 4 ) * sizeof( double );
+    h->mixedTablesInSmem = tables <= 112 * 1024 && tables + 2 * wsCell <= size_t( maxSmem );
+    const size_t avail   = size_t( maxSmem ) - ( h->mixedTablesInSmem ? tables : 0 );
+    const int fit        = int( std::min<size_t>( 8, avail / wsCell ) );
+    if( fit < 1 ) {
+        h->mixedOk  = false;
+        h->mixedWhy = "mixed-form closure workspace (" + std::to_string( wsCell ) + " B per cell) exceeds shared memory";
+        return;
+    }
+    h->mixedGroup = n <= 32 ? 32 : 64;
+    h->mixedBlock = h->mixedGroup * std::min( h->mixedGroup == 32 ? 8 : 6, fit );
+    h->mixedSmem  = wsCell * ( h->mixedBlock / h->mixedGroup ) + ( h->mixedTablesInSmem ? tables : 0 );
+    void* k       = pick( cl, h->mixedGroup, 4 );
+    CK( cudaFuncSetAttribute( k, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->mixedSmem ) ) );
+    int occ = 0;
+    CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, k, h->mixedBlock, h->mixedSmem ) );
+    h->mixedGrid = std::max( 1, occ ) * h->numSMs;
+    h->mixedOk   = true;
+    h->mixedWhy.clear();
 }
 
 void plan_launches( uqc_solver* h ) {
@@ -219,10 +285,13 @@ void plan_launches( uqc_solver* h ) {
     const size_t wsCell  = cell_ws_doubles( nS, nT, nQ, closure_np( cl ) ) * sizeof( double );
     h->tablesInSmem      = tables <= 96 * 1024 && tables + wsCell <= size_t( maxSmem );
     const size_t avail   = size_t( maxSmem ) - ( h->tablesInSmem ? tables : 0 );
-    int warpGroups       = int( std::min<size_t>( 8, avail / wsCell ) );
-    h->closureGroup      = h->closureGroupOverride ? h->closureGroupOverride : ( n <= 32 ? 32 : 256 );
-    if( h->closureGroup == 32 && warpGroups < 1 ) h->closureGroup = 256;
-    h->closureBlock        = h->closureGroup == 32 ? 32 * warpGroups : 256;
+    // small systems: a warp per cell, up to 8 per CTA; larger: two warps per
+    // cell (named barriers), up to 4 per CTA; a whole CTA per cell otherwise
+    const int fit        = int( std::min<size_t>( 8, avail / wsCell ) );
+    h->closureGroup      = h->closureGroupOverride ? h->closureGroupOverride : ( n <= 32 ? 32 : 64 );
+    if( h->closureGroup == 32 && fit < 1 ) h->closureGroup = 256;
+    if( h->closureGroup == 64 && fit < ( h->closureGroupOverride ? 1 : 2 ) ) h->closureGroup = 256;
+    h->closureBlock        = h->closureGroup == 32 ? 32 * fit : ( h->closureGroup == 64 ? 64 * std::min( 6, fit ) : 256 );
     const int groupsPerCta = h->closureBlock / h->closureGroup;
     h->closureSmem         = wsCell * groupsPerCta + ( h->tablesInSmem ? tables : 0 );
     if( h->closureSmem > size_t( maxSmem ) )
@@ -232,17 +301,21 @@ void plan_launches( uqc_solver* h ) {
     int occ = 0;
     CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kc, h->closureBlock, h->closureSmem ) );
     h->closureGrid = std::max( 1, occ ) * h->numSMs;
-    // update kernel: phiWf + per-group flux buffers
-    h->updateBlock     = 256;
-    const int ug       = h->updateBlock / h->group;
-    size_t uTables     = h->tablesInSmem ? ( size_t( nQ ) * h->ld + 4 ) * sizeof( double ) : 0;
-    h->updateSmem      = uTables + size_t( ug ) * ( size_t( h->mesh.nFaces ) * nS * nQ + 32 ) * sizeof( double );
-    if( h->updateSmem > size_t( maxSmem ) ) throw ConfigError( "update workspace exceeds shared memory" );
-    void* ku = pick( cl, h->group, 1 );
-    CK( cudaFuncSetAttribute( ku, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->updateSmem ) ) );
-    CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ku, h->updateBlock, h->updateSmem ) );
-    h->updateGrid = std::max( 1, occ ) * h->numSMs;
-    h->updateGrid = std::min( h->updateGrid, std::max( 1, ( h->mesh.nCells + ug - 1 ) / ug ) );
+    // update kernel: a warp per cell; phiWf + one node-flux buffer per warp
+    {
+        const size_t uTables = h->tablesInSmem ? ( ( size_t( nQ ) * h->ld + 4 + 3 ) & ~size_t( 3 ) ) * sizeof( double ) : 0;
+        const size_t perWarp = ( ( size_t( nS ) * nQ + 3 ) & ~size_t( 3 ) ) * sizeof( double );
+        const int warps      = int( std::min<size_t>( 8, ( size_t( maxSmem ) - uTables ) / perWarp ) );
+        if( warps < 1 ) throw ConfigError( "update workspace exceeds shared memory" );
+        h->updateBlock = 32 * warps;
+        h->updateSmem  = uTables + size_t( warps ) * perWarp;
+        void* ku       = pick( cl, h->group, 1 );
+        CK( cudaFuncSetAttribute( ku, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->updateSmem ) ) );
+        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ku, h->updateBlock, h->updateSmem ) );
+        h->updateGrid = std::max( 1, occ ) * h->numSMs;
+        h->updateGrid = std::min( h->updateGrid, std::max( 1, ( h->mesh.nCells + warps - 1 ) / warps ) );
+    }
+    const int ug = h->auxBlock / h->group;    // groups per CTA of the init / mean-variance kernels
     h->initSmem   = size_t( ug ) * ( size_t( nS ) * nQ + 8 ) * sizeof( double );
     h->mvSmem     = size_t( ug ) * ( 2 * size_t( nS ) * nQ + 8 ) * sizeof( double );
     for( int which : {2, 3} ) {
@@ -251,7 +324,20 @@ void plan_launches( uqc_solver* h ) {
         CK( cudaFuncSetAttribute( pick( cl, h->group, which ), cudaFuncAttributeMaxDynamicSharedMemorySize, int( sm ) ) );
     }
     h->auxGrid = std::min( 4 * h->numSMs, std::max( 1, ( h->mesh.nCells + ug - 1 ) / ug ) );
-    h->mixed   = plan_mixed( cl, nS, nT, nQ, h->ld, maxSmem );
+    // check kernel: a warp per cell, as many warps per CTA (up to 8) as shared memory allows
+    {
+        const size_t wsc = check_ws_doubles( nS, nT, nQ ) * sizeof( double );
+        const size_t av  = size_t( maxSmem ) - ( h->tablesInSmem ? tables : 0 );
+        const int warps  = int( std::min<size_t>( 8, av / wsc ) );
+        if( warps < 1 ) throw ConfigError( "check workspace exceeds shared memory" );
+        h->checkBlock = 32 * warps;
+        h->checkSmem  = wsc * warps + ( h->tablesInSmem ? tables : 0 );
+        void* kk      = pick_check( cl );
+        CK( cudaFuncSetAttribute( kk, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->checkSmem ) ) );
+        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kk, h->checkBlock, h->checkSmem ) );
+        h->checkGrid = std::min( std::max( 1, occ ) * h->numSMs, std::max( 1, ( h->mesh.nCells + warps - 1 ) / warps ) );
+    }
+    plan_mixed( h, maxSmem );
 }
 
 void reset_control( uqc_solver* h, double t ) {
@@ -266,6 +352,7 @@ void reset_control( uqc_solver* h, double t ) {
     h->lastIters      = 0;    // device counters restart from zero
     h->lastLs         = 0;
     h->lastFailed     = 0;
+    h->lastFallback   = 0;
     CK( cudaMemcpyAsync( h->d_ctl, h->h_ctl, sizeof( Control ), cudaMemcpyHostToDevice, h->stream ) );
     CK( cudaStreamSynchronize( h->stream ) );
 }
@@ -327,6 +414,9 @@ void ensure_device( uqc_solver* h ) {
         }
     h->d_phi   = dupload( phi );
     h->d_phiWf = dupload( phiWf );
+    std::vector<float> phiF( phi.size() );
+    for( size_t i = 0; i < phi.size(); ++i ) phiF[i] = float( phi[i] );
+    h->d_phiF = dupload( phiF );
     h->d_xi    = dupload( h->tab.xi );
     h->d_wt    = dupload( h->padWt );
     const Mesh& m = h->mesh;
@@ -348,12 +438,14 @@ void ensure_device( uqc_solver* h ) {
     h->d_level  = dalloc<unsigned>( N );
     h->d_status = dalloc<int>( N );
     h->d_iters  = dalloc<int>( N );
+    h->d_activeList   = dalloc<int>( N );
+    h->d_fallbackList = dalloc<int>( N );
     h->d_ctl    = dalloc<Control>( 1 );
     CK( cudaMallocHost( &h->h_ctl, sizeof( Control ) ) );
     for( auto& e : h->ev ) CK( cudaEventCreate( &e ) );
     plan_launches( h );
+    if( h->precision == UQC_MIXED && !h->mixedOk ) throw ConfigError( "mixed precision not available for this configuration: " + h->mixedWhy );
     h->d_blockPartial = dalloc<double>( std::max( h->updateGrid, 1 ) );
-    alloc_mixed( h->mixed, N );
     h->deviceReady = true;
     reset_control( h, 0.0 );
 }
@@ -364,9 +456,8 @@ void release( uqc_solver* h ) {
                     (void*)h->d_unitN, (void*)h->d_scaledN, (void*)h->d_nbr, (void*)h->d_boundary, (void*)h->d_u, (void*)h->d_lam,
                     (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
                     (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
-                    (void*)h->d_xIters} )
+                    (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_phiF, (void*)h->d_fallbackList} )
         if( p ) cudaFree( p );
-    free_mixed( h->mixed );
     if( h->h_ctl ) cudaFreeHost( h->h_ctl );
     for( auto& e : h->ev )
         if( e ) cudaEventDestroy( e );
@@ -375,18 +466,50 @@ void release( uqc_solver* h ) {
     if( h->ownStream && h->stream ) cudaStreamDestroy( h->stream );
 }
 
-// Closure launch: FP64 kernel, or the mixed-precision pipeline.
+// Closure launch: the FP64 kernel; or the mixed-form kernel followed by the
+// FP64 kernel over the cells the mixed form handed back (a launch that finds
+// an empty list returns at once). The work counters and the fallback list
+// length must be zero on entry (k_update resets them after every step).
 void launch_closure( uqc_solver* h, KParams& P, int mode ) {
-    if( h->precision == UQC_MIXED && h->mixed.ok ) {
-        h->launches += launch_mixed_closure( h->mixed, P, mode, h->cfg.closure, h->stream );
+    if( h->precision == UQC_MIXED && h->mixedOk ) {
+        KParams M      = P;
+        M.tablesInSmem = h->mixedTablesInSmem;
+        if( h->mixedMaxIter > 1 && P.maxIter > 1 ) M.maxIter = std::min( P.maxIter, h->mixedMaxIter );
+        void* margs[]  = {&M, &mode};
+        launch( h, pick( h->cfg.closure, h->mixedGroup, 4 ), h->mixedGrid, h->mixedBlock, h->mixedSmem, margs );
+        KParams F     = P;
+        F.activeList  = h->d_fallbackList;
+        F.activeCount = &h->d_ctl->nFallback;
+        F.workCounter = &h->d_ctl->workCounter2;
+        void* fargs[] = {&F, &mode};
+        launch( h, pick( h->cfg.closure, h->closureGroup, 0 ), h->closureGrid, h->closureBlock, h->closureSmem, fargs );
         return;
     }
     void* args[] = {&P, &mode};
     launch( h, pick( h->cfg.closure, h->closureGroup, 0 ), h->closureGrid, h->closureBlock, h->closureSmem, args );
 }
 
-void enqueue_step( uqc_solver* h, KParams& P ) {
+// Zeroes the closure work counters and the fallback list length (three
+// consecutive fields of Control) before a closure-only launch.
+void reset_work( uqc_solver* h ) {
+    CK( cudaMemsetAsync( &h->d_ctl->workCounter, 0, 3 * sizeof( unsigned ), h->stream ) );
+}
+
+// Closure half of a time step: k_check (warp per cell) finishes converged
+// cells and lists the others, then k_closure runs Newton on the list. In
+// SolveClosureSafe mode every cell takes a Newton step, so k_closure gets all.
+void enqueue_closure_phase( uqc_solver* h, KParams P ) {
+    if( h->cfg.newtonMode != 2 ) {
+        P.activeList  = h->d_activeList;
+        P.activeCount = &h->d_ctl->nActive;
+        void* args[]  = {&P};
+        launch( h, pick_check( h->cfg.closure ), h->checkGrid, h->checkBlock, h->checkSmem, args );
+    }
     launch_closure( h, P, 1 );
+}
+
+void enqueue_step( uqc_solver* h, KParams& P ) {
+    enqueue_closure_phase( h, P );
     void* args[] = {&P};
     launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
 }
@@ -406,7 +529,9 @@ int fill_info( uqc_solver* h, uqc_step_info* info, int stepsBefore ) {
         info->newton_iterations  = (long long)( c.newtonIters - h->lastIters );
         info->line_search_trials = (long long)( c.lineSearchTrials - h->lastLs );
         info->active_cells       = c.activeCellsLast;
+        info->fallback_cells     = (long long)( c.fallbackCells - h->lastFallback );
     }
+    h->lastFallback = c.fallbackCells;
     h->lastIters  = c.newtonIters;
     h->lastLs     = c.lineSearchTrials;
     h->lastFailed = c.failedCells;
@@ -502,7 +627,7 @@ int uqc_set_precision( uqc_solver* h, int precision ) {
         return UQC_OK;
     } );
     if( rc != UQC_OK ) return rc;
-    if( precision == UQC_MIXED && !h->mixed.ok ) return fail( h, UQC_ERR_CONFIG, "mixed precision not available for this configuration: " + h->mixed.why );
+    if( precision == UQC_MIXED && !h->mixedOk ) return fail( h, UQC_ERR_CONFIG, "mixed precision not available for this configuration: " + h->mixedWhy );
     h->precision = precision;
     return UQC_OK;
 }
@@ -512,12 +637,18 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
     std::string k = key;
     if( k == "closure_group" ) {
         int v = int( value );
-        if( v != 0 && v != 32 && v != 256 ) return fail( h, UQC_ERR_ARGUMENT, "closure_group must be 0, 32 or 256" );
+        if( v != 0 && v != 32 && v != 64 && v != 256 ) return fail( h, UQC_ERR_ARGUMENT, "closure_group must be 0, 32, 64 or 256" );
         h->closureGroupOverride = v;
         if( h->deviceReady ) return guarded( h, [&] {
                 plan_launches( h );
                 return UQC_OK;
             } );
+        return UQC_OK;
+    }
+    if( k == "mixed_max_iterations" ) {
+        int v = int( value );
+        if( v != 0 && v < 2 ) return fail( h, UQC_ERR_ARGUMENT, "mixed_max_iterations must be 0 or >= 2" );
+        h->mixedMaxIter = v;
         return UQC_OK;
     }
     return fail( h, UQC_ERR_ARGUMENT, "unknown option '" + k + "'" );
@@ -560,7 +691,7 @@ int uqc_init_state( uqc_solver* h ) {
         h->launches  = 0;
         KParams P    = make_params( h );
         void* args[] = {&P};
-        launch( h, pick( h->cfg.closure, h->group, 2 ), h->auxGrid, h->updateBlock, h->initSmem, args );
+        launch( h, pick( h->cfg.closure, h->group, 2 ), h->auxGrid, h->auxBlock, h->initSmem, args );
         CK( cudaGetLastError() );
         reset_control( h, 0.0 );
         h->stateReady = true;
@@ -638,7 +769,7 @@ int uqc_solve_closure( uqc_solver* h, uqc_step_info* info ) {
         h->launches = 0;
         read_control( h );
         int stepsBefore = h->h_ctl->steps;
-        CK( cudaMemsetAsync( &h->d_ctl->workCounter, 0, sizeof( unsigned ), h->stream ) );
+        reset_work( h );
         KParams P = make_params( h );
         launch_closure( h, P, 0 );
         CK( cudaGetLastError() );
@@ -674,7 +805,7 @@ int uqc_step( uqc_solver* h, int n_steps, uqc_step_info* info ) {
         }
         for( int s = 0; s < n_steps; ++s ) {
             CK( cudaEventRecord( h->stepEvents[3 * s], h->stream ) );
-            launch_closure( h, P, 1 );
+            enqueue_closure_phase( h, P );
             CK( cudaEventRecord( h->stepEvents[3 * s + 1], h->stream ) );
             void* args[] = {&P};
             launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
@@ -732,7 +863,7 @@ int uqc_mean_var( uqc_solver* h, double* out ) {
         double* d_out  = dalloc<double>( cnt );
         KParams P      = make_params( h );
         void* args[]   = {&P, &d_out};
-        launch( h, pick( h->cfg.closure, h->group, 3 ), h->auxGrid, h->updateBlock, h->mvSmem, args );
+        launch( h, pick( h->cfg.closure, h->group, 3 ), h->auxGrid, h->auxBlock, h->mvSmem, args );
         CK( cudaMemcpyAsync( out, d_out, cnt * sizeof( double ), cudaMemcpyDeviceToHost, h->stream ) );
         CK( cudaStreamSynchronize( h->stream ) );
         cudaFree( d_out );
@@ -761,7 +892,7 @@ static void closure_on( uqc_solver* h, int n, double* d_lam, const double* d_u, 
     P.nTotalCell  = d_nt;
     P.status      = d_status;
     P.iters       = d_iters;
-    CK( cudaMemsetAsync( &h->d_ctl->workCounter, 0, sizeof( unsigned ), h->stream ) );
+    reset_work( h );
     launch_closure( h, P, 0 );
     CK( cudaGetLastError() );
 }
@@ -866,6 +997,18 @@ int uqc_mesh_tri_jitter( int nx, int ny, double jitter, unsigned long long seed,
 
 }    // extern "C"
 
+#ifdef UQC_PHASE_TIMERS
+// Diagnostic builds only: the per-phase cycle counters of k_closure (summed
+// over CTAs since the last call), then reset.
+extern "C" int uqc_debug_phase_cycles( double* out16 ) {
+    unsigned long long v[16];
+    if( cudaMemcpyFromSymbol( v, g_phaseCycles, sizeof( v ) ) != cudaSuccess ) return UQC_ERR_CUDA;
+    for( int i = 0; i < 16; ++i ) out16[i] = double( v[i] );
+    std::memset( v, 0, sizeof( v ) );
+    return cudaMemcpyToSymbol( g_phaseCycles, v, sizeof( v ) ) == cudaSuccess ? UQC_OK : UQC_ERR_CUDA;
+}
+#endif
+
 // ===================================================== closure without allocation
 //
 // Statically allocated scratch of uqc_closure_solve_device_noalloc (layout:
@@ -933,6 +1076,9 @@ extern "C" int uqc_closure_solve_device_noalloc( uqc_solver* h, int n, double* d
         P.status       = d_status;
         P.iters        = iters;
         P.ctl          = ctl;
+        P.workCounter  = &ctl->workCounter;
+        P.activeList   = nullptr;
+        P.fallbackList = nullptr;
         // launch shape of k_closure, as plan_launches chooses it
         int dev = 0, maxSmem = 0, sms = 0, occ = 0;
         CK( cudaGetDevice( &dev ) );
