@@ -104,8 +104,11 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
 /* Launch tuning (no reference counterpart; the autotuner uses it):
  *   "closure_group"  threads per cell in the closure kernel: 32 (a warp per
  *                    cell, several cells per CTA), 64 (two warps per cell,
- *                    up to six cells per CTA) or 256 (a CTA per cell);
+ *                    up to four cells per CTA) or 256 (a CTA per cell);
  *                    0 = automatic.
+ *   "closure_tables_smem"  1: the closure kernels stage the basis tables in
+ *                    shared memory; 0: they read them through the L1 cache
+ *                    (more cells per SM); -1 = automatic.
  *   "mixed_max_iterations"  UQC_MIXED: Newton iterations of the FP32 pass
  *                    after which a cell continues in the FP64 form (>= 2;
  *                    0 = the configured maxIterations).

@@ -451,8 +451,9 @@ __device__ __forceinline__ void atomic_min_pos_double( unsigned long long* addr,
     if( v >= 0.0 ) atomicMin( addr, (unsigned long long)__double_as_longlong( v ) );
 }
 
-// Threads per CTA of k_closure: up to 8 warp groups, 6 two-warp groups.
-template <int GROUP> constexpr int closure_max_block() { return GROUP == 32 ? 256 : ( GROUP == 64 ? 384 : GROUP ); }
+// Threads per CTA of k_closure: up to 8 warp groups or 4 two-warp groups
+// (256 threads: up to 255 registers per thread).
+template <int GROUP> constexpr int closure_max_block() { return GROUP <= 64 ? 256 : GROUP; }
 
 // Persistent closure kernel. mode 0: closure only; mode 1: closure + fused
 // epilogue of a time step. Tables are staged in shared memory when they fit.
@@ -461,7 +462,7 @@ template <int GROUP> constexpr int closure_max_block() { return GROUP == 32 ? 25
 // appended to P.fallbackList, with their last accepted duals written back,
 // for a pass of the FP64 form; they get no status or epilogue here.
 template <int CL, int GROUP, class HT>
-__global__ void __launch_bounds__( closure_max_block<GROUP>() ) k_closure( KParams P, int mode ) {
+__global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KParams P, int mode ) {
     constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP;
     constexpr bool MIXED = sizeof( HT ) == 4;
     extern __shared__ __align__( 16 ) double smem[];

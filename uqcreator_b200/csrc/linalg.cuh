@@ -221,7 +221,7 @@ __device__ void hessian_sym( const Grp<GROUP>& g, int nQ, int ld, const T* phi, 
 // U_JJ over its upper triangle, D = diag(U), I = 1/diag(U); sets *flag to
 // j0 + jj + 1 at the first pivot that is not positive.
 template <class T> __device__ void tile_factor( T* DT, T* D, T* I, int j0, int* flag ) {
-    T a[8][8];
+    double a[8][8];
 #pragma unroll
     for( int r = 0; r < 8; ++r )
 #pragma unroll
@@ -230,15 +230,15 @@ template <class T> __device__ void tile_factor( T* DT, T* D, T* I, int j0, int* 
 #pragma unroll
     for( int jj = 0; jj < 8; ++jj ) {
         if( !bad ) {
-            const T ajj = a[jj][jj];
-            if( !( ajj > T( 0 ) ) ) {
+            const double ajj = a[jj][jj];
+            if( !( ajj > 0.0 ) ) {
                 bad = j0 + jj + 1;
             }
             else {
-                const T inv = rsqrt_nr( ajj ), d = ajj * inv;
-                a[jj][jj]   = d;
-                D[j0 + jj]  = d;
-                I[j0 + jj]  = inv;
+                const double inv = rsqrt_nr( ajj ), d = ajj * inv;
+                a[jj][jj]        = d;
+                D[j0 + jj]       = T( d );
+                I[j0 + jj]       = T( inv );
 #pragma unroll
                 for( int c = jj + 1; c < 8; ++c ) a[jj][c] *= inv;
 #pragma unroll
@@ -252,7 +252,7 @@ template <class T> __device__ void tile_factor( T* DT, T* D, T* I, int j0, int* 
 #pragma unroll
     for( int r = 0; r < 8; ++r )
 #pragma unroll
-        for( int c = r; c < 8; ++c ) DT[tix( r, c )] = a[r][c];
+        for( int c = r; c < 8; ++c ) DT[tix( r, c )] = T( a[r][c] );
 }
 
 // Lanes 0..7: row i of X = U_JJ^-1 (upper triangular) into the strictly lower
@@ -285,99 +285,57 @@ template <class T> __device__ void tile_inverse( T* DT, const T* I, int j0, int 
         if( c > i ) DT[tix( c, i )] = x[c];
 }
 
-// Panel of tile row J: U(J, C) = X^T A(J, C) for C in (J, nb), and y_J = X^T b_J.
-// Lane (r, c0 = lane / 8) computes elements (r, c0) and (r, c0 + 4) of a tile;
-// two tiles at a time, all reads before the writes.
-template <class T> __device__ void tile_row_solve( T* H, int J, int nb, const T* I, int lane ) {
-    const int r = lane & 7, c0 = lane >> 3, c1 = c0 + 4;
-    const T* DT = H + htile( J, J );
-    T xr[8];    // X(k, r), k <= r
-#pragma unroll
-    for( int k = 0; k < 8; ++k ) xr[k] = k < r ? DT[tix( r, k )] : ( k == r ? I[J * 8 + r] : T( 0 ) );
-    T* b = H + hrhs( nb ) + J * 8;
-    for( int C = J + 1; C < nb + 1; C += 2 ) {
-        // tiles C and C + 1; index nb stands for the right-hand side segment
-        T u[2][2];
-#pragma unroll
-        for( int h = 0; h < 2; ++h ) {
-            const int CC = C + h;
-            T p0 = 0, p1 = 0, q0 = 0, q1 = 0;
-            if( CC < nb ) {
-                const T* A = H + htile( J, CC );
-#pragma unroll
-                for( int k = 0; k < 8; k += 2 ) {
-                    p0 = fma( xr[k], A[tix( k, c0 )], p0 );
-                    q0 = fma( xr[k + 1], A[tix( k + 1, c0 )], q0 );
-                    p1 = fma( xr[k], A[tix( k, c1 )], p1 );
-                    q1 = fma( xr[k + 1], A[tix( k + 1, c1 )], q1 );
-                }
-            }
-            else if( CC == nb ) {
-#pragma unroll
-                for( int k = 0; k < 8; k += 2 ) {
-                    p0 = fma( xr[k], b[k], p0 );
-                    q0 = fma( xr[k + 1], b[k + 1], q0 );
-                }
-            }
-            u[h][0] = p0 + q0;
-            u[h][1] = p1 + q1;
-        }
-        __syncwarp();
-#pragma unroll
-        for( int h = 0; h < 2; ++h ) {
-            const int CC = C + h;
-            if( CC < nb ) {
-                T* A            = H + htile( J, CC );
-                A[tix( r, c0 )] = u[h][0];
-                A[tix( r, c1 )] = u[h][1];
-            }
-            else if( CC == nb && lane < 8 ) {
-                b[r] = u[h][0];
-            }
-        }
-    }
+// D = A B + C on the FP64 tensor cores, one 8 x 8 x 4 product per warp
+// (mma.sync m8n8k4, A row-major 8 x 4, B column-major 4 x 8). Lane 4 g + t
+// holds a = A(g, t), b = B(t, g), c0 = C(g, 2t), c1 = C(g, 2t + 1).
+__device__ __forceinline__ void dmma_8x8x4( double& c0, double& c1, double a, double b ) {
+    asm( "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n" : "+d"( c0 ), "+d"( c1 ) : "d"( a ), "d"( b ) );
 }
 
-// Tiles (R, Ca) and (R, Cb) -= U(J, R)^T U(J, C.) (Cb < 0: one tile); lane
-// layout of tile_row_solve. All reads before the writes.
-template <class T> __device__ __forceinline__ void tile_update2( T* H, int J, int R, int Ca, int Cb, int lane ) {
-    const int r = lane & 7, c0 = lane >> 3, c1 = c0 + 4;
-    const T* A = H + htile( J, R );
-    T a[8];
-#pragma unroll
-    for( int k = 0; k < 8; ++k ) a[k] = A[tix( k, r )];
-    T s[2][2];
-    T o[2][2];
-#pragma unroll
-    for( int h = 0; h < 2; ++h ) {
-        const int C = h ? Cb : Ca;
-        s[h][0] = s[h][1] = o[h][0] = o[h][1] = 0;
-        if( C >= 0 ) {
-            const T* B = H + htile( J, C );
-            const T* O = H + htile( R, C );
-            T p0 = 0, p1 = 0, q0 = 0, q1 = 0;
-#pragma unroll
-            for( int k = 0; k < 8; k += 2 ) {
-                p0 = fma( a[k], B[tix( k, c0 )], p0 );
-                q0 = fma( a[k + 1], B[tix( k + 1, c0 )], q0 );
-                p1 = fma( a[k], B[tix( k, c1 )], p1 );
-                q1 = fma( a[k + 1], B[tix( k + 1, c1 )], q1 );
-            }
-            s[h][0] = p0 + q0;
-            s[h][1] = p1 + q1;
-            o[h][0] = O[tix( r, c0 )];
-            o[h][1] = O[tix( r, c1 )];
-        }
+// Tile (R, C) -= U(J, R)^T U(J, C) on the FP64 tensor cores: two mma k-steps
+// with A(g, t) = -U(J, R)(t, g), B(t, g) = U(J, C)(t, g), C = the tile; one
+// shared-memory value per lane and operand per k-step. T = double, or float
+// (mixed form: FP32 storage, FP64 products).
+template <class T> __device__ __forceinline__ void tile_update_mma( T* H, int J, int R, int C, int lane ) {
+    const int g = lane >> 2, t = lane & 3;
+    const T* A      = H + htile( J, R );
+    const T* B      = H + htile( J, C );
+    T* O            = H + htile( R, C );
+    const double a0 = -double( A[tix( t, g )] ), a1 = -double( A[tix( t + 4, g )] );
+    const double b0 = B[tix( t, g )], b1 = B[tix( t + 4, g )];
+    double c0 = O[tix( g, 2 * t )], c1 = O[tix( g, 2 * t + 1 )];
+    dmma_8x8x4( c0, c1, a0, b0 );
+    dmma_8x8x4( c0, c1, a1, b1 );
+    O[tix( g, 2 * t )]     = T( c0 );
+    O[tix( g, 2 * t + 1 )] = T( c1 );
+}
+
+// Panel of tile row J on the FP64 tensor cores: U(J, C) = X^T A(J, C) with
+// A(g, t) = X(t, g) (the stored inverse; X^T is lower triangular), B(t, g) =
+// A(J, C)(t, g). The right-hand side segment by lanes 0..7.
+template <class T> __device__ void tile_row_solve_mma( T* H, int J, int nb, const T* I, int lane ) {
+    const int g = lane >> 2, t = lane & 3;
+    const T* DT = H + htile( J, J );
+    auto xt     = [&]( int k ) { return k < g ? double( DT[tix( g, k )] ) : ( k == g ? double( I[J * 8 + g] ) : 0.0 ); };    // X(k, g)
+    const double a0 = xt( t ), a1 = xt( t + 4 );
+    for( int C = J + 1; C < nb; ++C ) {
+        T* A            = H + htile( J, C );
+        const double b0 = A[tix( t, g )], b1 = A[tix( t + 4, g )];
+        double c0 = 0.0, c1 = 0.0;
+        dmma_8x8x4( c0, c1, a0, b0 );
+        dmma_8x8x4( c0, c1, a1, b1 );
+        A[tix( g, 2 * t )]     = T( c0 );
+        A[tix( g, 2 * t + 1 )] = T( c1 );
     }
+    T* b     = H + hrhs( nb ) + J * 8;
+    double y = 0.0;
+    if( lane < 8 ) {
 #pragma unroll
-    for( int h = 0; h < 2; ++h ) {
-        const int C = h ? Cb : Ca;
-        if( C >= 0 ) {
-            T* O            = H + htile( R, C );
-            O[tix( r, c0 )] = o[h][0] - s[h][0];
-            O[tix( r, c1 )] = o[h][1] - s[h][1];
-        }
+        for( int k = 0; k < 8; ++k )
+            y += ( k < lane ? double( DT[tix( lane, k )] ) : ( k == lane ? double( I[J * 8 + lane] ) : 0.0 ) ) * double( b[k] );
     }
+    __syncwarp();
+    if( lane < 8 ) b[lane] = T( y );
 }
 
 // Right-hand side segment R -= U(J, R)^T y_J (lanes 0..7).
@@ -415,7 +373,7 @@ __device__ int cholesky_la( const Grp<GROUP>& g, T* H, int n, T* D, T* I, int* f
         __syncwarp();
         tile_inverse<T>( H, I, 0, lane );
         __syncwarp();
-        if( !*flag ) tile_row_solve<T>( H, 0, nb, I, lane );
+        if( !*flag ) tile_row_solve_mma<T>( H, 0, nb, I, lane );
     }
     g.sync();
     if( *flag ) return *flag;
@@ -424,7 +382,7 @@ __device__ int cholesky_la( const Grp<GROUP>& g, T* H, int n, T* D, T* I, int* f
         CT_BEGIN( tc );
         if( warp == 0 ) {
             CT_BEGIN( t0 );
-            for( int C = K; C < nb; C += 2 ) tile_update2<T>( H, J, K, C, C + 1 < nb ? C + 1 : -1, lane );
+            for( int C = K; C < nb; ++C ) tile_update_mma<T>( H, J, K, C, lane );
             rhs_update<T>( H, J, K, nb, lane );
             __syncwarp();
             CT_END( t0, 14, g.r == 0 );
@@ -437,7 +395,7 @@ __device__ int cholesky_la( const Grp<GROUP>& g, T* H, int n, T* D, T* I, int* f
             __syncwarp();
             CT_END( t2, 13, g.r == 0 );
             CT_BEGIN( t3 );
-            if( !*flag ) tile_row_solve<T>( H, K, nb, I, lane );
+            if( !*flag ) tile_row_solve_mma<T>( H, K, nb, I, lane );
             CT_END( t3, 15, g.r == 0 );
         }
         CT_END( tc, 8, g.r == 0 );
@@ -445,10 +403,10 @@ __device__ int cholesky_la( const Grp<GROUP>& g, T* H, int n, T* D, T* I, int* f
         if( W == 1 || warp > 0 ) {
             const int worker = W == 1 ? 0 : warp - 1, workers = W == 1 ? 1 : W - 1;
             if( W == 1 ) __syncwarp();
-            // items: tile pairs (R, C), (R, C + 1) of one tile row, then rhs segments
+            // items: tiles (R, C), J + 2 <= R <= C, then rhs segments
             for( int R = J + 2, e = 0; R < nb; ++R ) {
-                for( int C = R; C < nb; C += 2, ++e )
-                    if( e % workers == worker ) tile_update2<T>( H, J, R, C, C + 1 < nb ? C + 1 : -1, lane );
+                for( int C = R; C < nb; ++C, ++e )
+                    if( e % workers == worker ) tile_update_mma<T>( H, J, R, C, lane );
             }
             for( int R = J + 2 + worker; R < nb; R += workers ) rhs_update<T>( H, J, R, nb, lane );
         }

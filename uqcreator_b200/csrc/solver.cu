@@ -56,7 +56,9 @@ struct uqc_solver {
     size_t closureSmem = 0, updateSmem = 0, initSmem = 0, mvSmem = 0, checkSmem = 0;
     int checkBlock = 256, checkGrid = 0;
     int* d_activeList = nullptr;    // cells that need Newton in the running step
-    bool tablesInSmem = false;
+    bool tablesInSmem        = false;    // check / update / init kernels stage the tables in shared memory
+    bool closureTablesInSmem = false;    // ... the FP64 closure kernel
+    int closureTablesOpt     = -1;       // option closure_tables_smem: -1 automatic, 0 read through L1, 1 stage
     // mixed form: FP32 Hessian / factor / solves, FP64 gradient and update
     float* d_phiF        = nullptr;    // phi rounded to FP32, row stride ld
     int* d_fallbackList  = nullptr;    // cells the mixed form hands to the FP64 form
@@ -244,14 +246,14 @@ void launch( uqc_solver* h, void* fn, int grid, int block, size_t smem, void** a
 
 // Mixed-form closure: the FP32 Hessian halves the per-cell shared memory, so
 // more cells share an SM: a warp per cell (n <= 32) or two warps per cell, up
-// to 8 or 6 cells per CTA; the tables gain an FP32 copy of phi.
+// to 8 or 4 cells per CTA; the tables gain an FP32 copy of phi.
 void plan_mixed( uqc_solver* h, int maxSmem ) {
     const int cl = h->cfg.closure, nT = h->tab.nT, nQ = h->tab.nQ, nS = h->nS;
     const size_t n       = size_t( nS ) * nT;
     const size_t tn      = size_t( nQ ) * h->ld + 4;
     const size_t tables  = 2 * tn * sizeof( double ) + ( tn + 1 ) / 2 * sizeof( double );
     const size_t wsCell  = cell_ws_doubles( nS, nT, nQ, closure_np( cl ), 4 ) * sizeof( double );
-    h->mixedTablesInSmem = tables <= 112 * 1024 && tables + 2 * wsCell <= size_t( maxSmem );
+    h->mixedTablesInSmem = h->closureTablesOpt != 0 && tables <= 112 * 1024 && tables + 2 * wsCell <= size_t( maxSmem );
     const size_t avail   = size_t( maxSmem ) - ( h->mixedTablesInSmem ? tables : 0 );
     const int fit        = int( std::min<size_t>( 8, avail / wsCell ) );
     if( fit < 1 ) {
@@ -260,7 +262,7 @@ void plan_mixed( uqc_solver* h, int maxSmem ) {
         return;
     }
     h->mixedGroup = n <= 32 ? 32 : 64;
-    h->mixedBlock = h->mixedGroup * std::min( h->mixedGroup == 32 ? 8 : 6, fit );
+    h->mixedBlock = h->mixedGroup * std::min( h->mixedGroup == 32 ? 8 : 4, fit );
     h->mixedSmem  = wsCell * ( h->mixedBlock / h->mixedGroup ) + ( h->mixedTablesInSmem ? tables : 0 );
     void* k       = pick( cl, h->mixedGroup, 4 );
     CK( cudaFuncSetAttribute( k, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->mixedSmem ) ) );
@@ -283,17 +285,25 @@ void plan_launches( uqc_solver* h ) {
     // closure: a warp per cell (several per CTA) or a whole 256-thread CTA per cell
     const size_t tables  = 2 * ( size_t( nQ ) * h->ld + 4 ) * sizeof( double );
     const size_t wsCell  = cell_ws_doubles( nS, nT, nQ, closure_np( cl ) ) * sizeof( double );
-    h->tablesInSmem      = tables <= 96 * 1024 && tables + wsCell <= size_t( maxSmem );
-    const size_t avail   = size_t( maxSmem ) - ( h->tablesInSmem ? tables : 0 );
+    h->tablesInSmem = tables <= 96 * 1024 && tables + wsCell <= size_t( maxSmem );
+    {
+        // automatic: read the tables through L1 when that lets more cells share a CTA
+        const int cap     = n <= 32 ? 8 : 4;
+        const int staged  = int( std::min<size_t>( cap, ( size_t( maxSmem ) - tables ) / wsCell ) );
+        const int through = int( std::min<size_t>( cap, size_t( maxSmem ) / wsCell ) );
+        h->closureTablesInSmem =
+            h->tablesInSmem && ( h->closureTablesOpt == 1 || ( h->closureTablesOpt == -1 && staged >= through ) );
+    }
+    const size_t avail = size_t( maxSmem ) - ( h->closureTablesInSmem ? tables : 0 );
     // small systems: a warp per cell, up to 8 per CTA; larger: two warps per
     // cell (named barriers), up to 4 per CTA; a whole CTA per cell otherwise
     const int fit        = int( std::min<size_t>( 8, avail / wsCell ) );
     h->closureGroup      = h->closureGroupOverride ? h->closureGroupOverride : ( n <= 32 ? 32 : 64 );
     if( h->closureGroup == 32 && fit < 1 ) h->closureGroup = 256;
     if( h->closureGroup == 64 && fit < ( h->closureGroupOverride ? 1 : 2 ) ) h->closureGroup = 256;
-    h->closureBlock        = h->closureGroup == 32 ? 32 * fit : ( h->closureGroup == 64 ? 64 * std::min( 6, fit ) : 256 );
+    h->closureBlock        = h->closureGroup == 32 ? 32 * fit : ( h->closureGroup == 64 ? 64 * std::min( 4, fit ) : 256 );
     const int groupsPerCta = h->closureBlock / h->closureGroup;
-    h->closureSmem         = wsCell * groupsPerCta + ( h->tablesInSmem ? tables : 0 );
+    h->closureSmem         = wsCell * groupsPerCta + ( h->closureTablesInSmem ? tables : 0 );
     if( h->closureSmem > size_t( maxSmem ) )
         throw ConfigError( "closure workspace (" + std::to_string( h->closureSmem ) + " B) exceeds shared memory; reduce moments or nodes" );
     void* kc = pick( cl, h->closureGroup, 0 );
@@ -480,12 +490,15 @@ void launch_closure( uqc_solver* h, KParams& P, int mode ) {
         KParams F     = P;
         F.activeList  = h->d_fallbackList;
         F.activeCount = &h->d_ctl->nFallback;
-        F.workCounter = &h->d_ctl->workCounter2;
-        void* fargs[] = {&F, &mode};
+        F.workCounter  = &h->d_ctl->workCounter2;
+        F.tablesInSmem = h->closureTablesInSmem;
+        void* fargs[]  = {&F, &mode};
         launch( h, pick( h->cfg.closure, h->closureGroup, 0 ), h->closureGrid, h->closureBlock, h->closureSmem, fargs );
         return;
     }
-    void* args[] = {&P, &mode};
+    KParams Q      = P;
+    Q.tablesInSmem = h->closureTablesInSmem;
+    void* args[]   = {&Q, &mode};
     launch( h, pick( h->cfg.closure, h->closureGroup, 0 ), h->closureGrid, h->closureBlock, h->closureSmem, args );
 }
 
@@ -639,6 +652,16 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
         int v = int( value );
         if( v != 0 && v != 32 && v != 64 && v != 256 ) return fail( h, UQC_ERR_ARGUMENT, "closure_group must be 0, 32, 64 or 256" );
         h->closureGroupOverride = v;
+        if( h->deviceReady ) return guarded( h, [&] {
+                plan_launches( h );
+                return UQC_OK;
+            } );
+        return UQC_OK;
+    }
+    if( k == "closure_tables_smem" ) {
+        int v = int( value );
+        if( v < -1 || v > 1 ) return fail( h, UQC_ERR_ARGUMENT, "closure_tables_smem must be -1, 0 or 1" );
+        h->closureTablesOpt = v;
         if( h->deviceReady ) return guarded( h, [&] {
                 plan_launches( h );
                 return UQC_OK;
