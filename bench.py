@@ -39,6 +39,14 @@ METRIC = "cell-steps/s mixed vs FP64 GPU at ≤1e-6 moment err; p50/p99 request 
 WORKLOAD = dict(nx=400, ny=250, degree=5, nquad=10, dim_xi=2)
 SAMPLE_NY = 10           # CPU sample: a 400 x 10 strip of the same mesh construction (8,000 cells)
 FP64_NOMINAL_TFLOPS = 40.0
+# FP64 FMA throughput measured on this pool's B200s with a register-only
+# micro-benchmark (independent DFMA chains, 16 warps/SM; mma.sync m8n8k4 f64
+# reaches the same rate): the ceiling of an FP64 kernel.
+FP64_MEASURED_TFLOPS = 36.5
+# DRAM bytes (read + write) of one k_closure launch per cell that takes Newton
+# iterations, from an ncu capture of a 12,000-cell step (2.35 MB for 1,532
+# active cells); the launch's traffic is this times its active cells.
+CLOSURE_DRAM_BYTES_PER_ACTIVE_CELL = 2.345472e6 / 1532
 
 
 def peaks():
@@ -255,9 +263,11 @@ def run_b200(args, rank, world, local):
     achieved = flops / args.steps / (closure_ms / 1e3) / 1e12
     hbm, bf16, src = peaks()
     roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
-            "traffic": None, "peak_source": src, "kernel": "k_closure (Newton + reconstruction)",
+            "traffic": CLOSURE_DRAM_BYTES_PER_ACTIVE_CELL * inf["active_cells"], "traffic_unit": "bytes per launch (scaled)",
+            "peak_source": src, "kernel": "k_closure (Newton + reconstruction)",
             "closure_ms_per_launch": closure_ms, "update_ms_per_launch": r["phase"][1] / args.steps,
             "fp64_nominal_tflops": FP64_NOMINAL_TFLOPS, "frac_of_fp64_nominal": achieved / FP64_NOMINAL_TFLOPS,
+            "fp64_measured_tflops": FP64_MEASURED_TFLOPS, "frac_of_fp64_measured": achieved / FP64_MEASURED_TFLOPS,
             "flops_per_launch": flops / args.steps}
     state_bytes = cells * s.n_states * s.n_total * 8
     h2d = 2 * state_bytes + 4 * cells
@@ -265,7 +275,7 @@ def run_b200(args, rank, world, local):
     line = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "bf16+f32+f64" if chosen == "mixed" else "f64", "data": "synthetic",
+        "dtype": "f32+f64" if chosen == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": "euler2d_sod_2u_deg5_q10x10", "cells": cells, "duals_per_cell": s.n_states * s.n_total,
                    "nodes": s.n_quad, "form": chosen, "parallelism": f"replicas{world}",
                    "l2": f"inputs larger than L2 (resident state {cells * (2 * s.n_states * s.n_total + s.n_states * s.n_quad) * 8 / 1e9:.2f} GB)"},
