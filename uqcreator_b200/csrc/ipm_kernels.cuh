@@ -167,16 +167,57 @@ __device__ inline CellWs carve( double* p, int nS, int nT, int nQ, int NP, int h
 
 // ------------------------------------------------------------------ building blocks
 
-// Lambda_k[s] = sum_{i < nTj} lam[s nT + i] phi(k, i)   (closure.cpp:205-213)
+// sum_k u[k] tab(k, i) over nQ nodes (table row stride ld). Long sums (256
+// nodes and more) use four partial sums (nodes k = 0, 1, 2, 3 mod 4): a
+// quarter of the dependent FMA chain; short ones one chain, which issues
+// fewer instructions (measured faster at 100 nodes, slower at 512).
+__device__ __forceinline__ double node_dot( const double* u, const double* tab, int ld, int i, int nQ ) {
+    if( nQ < 256 ) {
+        double a = 0.0;
+        for( int k = 0; k < nQ; ++k ) a = fma( u[k], tab[size_t( k ) * ld + i], a );
+        return a;
+    }
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    const double* t = tab + i;
+    int k           = 0;
+    for( ; k + 3 < nQ; k += 4, t += 4 * size_t( ld ) ) {
+        a0 = fma( u[k], t[0], a0 );
+        a1 = fma( u[k + 1], t[ld], a1 );
+        a2 = fma( u[k + 2], t[2 * ld], a2 );
+        a3 = fma( u[k + 3], t[3 * ld], a3 );
+    }
+    for( ; k < nQ; ++k, t += ld ) a0 = fma( u[k], t[0], a0 );
+    return ( a0 + a1 ) + ( a2 + a3 );
+}
+
+// Lambda_k[s] = sum_{i < nTj} lam[s nT + i] phi(k, i)   (closure.cpp:205-213).
+// Warp groups: one node per thread, the NS states as independent chains
+// sharing the row. CTA groups: one (state, node) per thread.
 template <int NS, int GROUP>
-__device__ void eval_lambda( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* lam, int nTj, double* L ) {
-    for( int idx = g.r; idx < NS * P.nQ; idx += GROUP ) {
-        int s = idx / P.nQ, k = idx - s * P.nQ;
+__device__ __forceinline__ void eval_lambda_body( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* lam, int nTj, double* L ) {
+    if constexpr( GROUP >= 256 ) {
+        for( int idx = g.r; idx < NS * P.nQ; idx += GROUP ) {
+            const int s       = idx / P.nQ, k = idx - s * P.nQ;
+            const double* row = phi + size_t( k ) * P.ld;
+            const double* ls  = lam + s * P.nT;
+            double a          = 0.0;
+            for( int i = 0; i < nTj; ++i ) a = fma( ls[i], row[i], a );
+            L[s * P.nQ + k] = a;
+        }
+        return;
+    }
+    for( int k = g.r; k < P.nQ; k += GROUP ) {
         const double* row = phi + size_t( k ) * P.ld;
-        const double* ls  = lam + s * P.nT;
-        double a          = 0.0;
-        for( int i = 0; i < nTj; ++i ) a = fma( ls[i], row[i], a );
-        L[s * P.nQ + k] = a;
+        double a[NS];
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) a[s] = 0.0;
+        for( int i = 0; i < nTj; ++i ) {
+            const double r = row[i];
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) a[s] = fma( lam[s * P.nT + i], r, a[s] );
+        }
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) L[s * P.nQ + k] = a[s];
     }
 }
 
@@ -198,22 +239,48 @@ __device__ void eval_u( const Grp<GROUP>& g, const KParams& P, const double* L, 
 // gout[s nTj + i] = sum_k U_s(k) phiWf(k, i) - uh[s nT + i]; returns ||gout||_2.
 // Vectors of the Newton system use the level's compact stride nTj.
 template <int CL, int GROUP>
-__device__ double gradient( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* L, const double* uh, int nTj,
-                            double* uk, double* gout, double* red ) {
+__device__ __forceinline__ double gradient_body( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* L, const double* uh,
+                                                 int nTj, double* uk, double* gout, double* red ) {
     constexpr int NS = Closure<CL>::NS;
     eval_u<CL, GROUP>( g, P, L, uk, true );
     g.sync();
     double sq = 0.0;
     for( int idx = g.r; idx < NS * nTj; idx += GROUP ) {
-        int s = idx / nTj, i = idx - s * nTj;
-        const double* us = uk + s * P.nQ;
-        double a         = 0.0;
-        for( int k = 0; k < P.nQ; ++k ) a = fma( us[k], phiWf[size_t( k ) * P.ld + i], a );
-        a         = a - uh[s * P.nT + i];
+        int s    = idx / nTj, i = idx - s * nTj;
+        double a = node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) - uh[s * P.nT + i];
         gout[idx] = a;
         sq += a * a;
     }
     return sqrt( group_sum<GROUP>( g, sq, red ) );
+}
+
+// Out-of-line copies for the CTA-per-cell closure kernel: its Newton loop
+// calls these at several sites, and one copy of each (instead of one per
+// call site) measured faster there (512-node cells); the warp-group kernels
+// inline them.
+template <int NS, int GROUP>
+__device__ __noinline__ void eval_lambda_ool( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* lam, int nTj, double* L ) {
+    eval_lambda_body<NS, GROUP>( g, P, phi, lam, nTj, L );
+}
+template <int CL, int GROUP>
+__device__ __noinline__ double gradient_ool( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* L, const double* uh, int nTj,
+                                             double* uk, double* gout, double* red ) {
+    return gradient_body<CL, GROUP>( g, P, phiWf, L, uh, nTj, uk, gout, red );
+}
+template <int NS, int GROUP>
+__device__ __forceinline__ void eval_lambda( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* lam, int nTj, double* L ) {
+    if constexpr( GROUP >= 256 )
+        eval_lambda_ool<NS, GROUP>( g, P, phi, lam, nTj, L );
+    else
+        eval_lambda_body<NS, GROUP>( g, P, phi, lam, nTj, L );
+}
+template <int CL, int GROUP>
+__device__ __forceinline__ double gradient( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* L, const double* uh, int nTj,
+                                            double* uk, double* gout, double* red ) {
+    if constexpr( GROUP >= 256 )
+        return gradient_ool<CL, GROUP>( g, P, phiWf, L, uh, nTj, uk, gout, red );
+    else
+        return gradient_body<CL, GROUP>( g, P, phiWf, L, uh, nTj, uk, gout, red );
 }
 
 // Newton direction d = H(lambda)^-1 g (closure.cpp:145-150 / 162-168): Hessian
@@ -428,12 +495,7 @@ __device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const do
     // [E] u(s, i) = sum_k uQ(s, k) phiWf(k, i) for i < nT(new level), 0 beyond
     for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
         int s = idx / P.nT, i = idx - s * P.nT;
-        double a = 0.0;
-        if( i < nTn ) {
-            const double* us = uk + s * P.nQ;
-            for( int k = 0; k < P.nQ; ++k ) a = fma( us[k], phiWf[size_t( k ) * P.ld + i], a );
-        }
-        P.u[cell * ldc + idx] = a;
+        P.u[cell * ldc + idx] = i < nTn ? node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) : 0.0;
     }
     // [F] the cell's time step (min over its nodes)
     double dloc = 1e300;
@@ -583,15 +645,16 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
 
 __host__ __device__ inline size_t check_ws_doubles( int nS, int nT, int nQ ) {
     size_t ldc = size_t( nS ) * nT;
-    return ( ( 3 * ldc + 2 * size_t( nS ) * nQ + 32 ) + 3 ) & ~size_t( 3 );
+    return ( ( 2 * ldc + size_t( nS ) * nQ + 32 ) + 3 ) & ~size_t( 3 );
 }
 
 // Step mode, first half of the closure: one warp per cell evaluates the
 // gradient at the current duals (the initial test of closure.cpp:139-142).
 // Converged cells are finished here (epilogue [C]-[F]); the others are
-// appended to P.activeList for k_closure. Many cells per SM are in flight, so
-// the latency of this per-cell work is hidden.
-template <int CL> __global__ void __launch_bounds__( 256 ) k_check( KParams P ) {
+// appended to P.activeList for k_closure. Lambda is formed node by node in
+// registers and U(Lambda) stored (no nodal Lambda buffer), so up to 16 warps
+// share a CTA and the latency of this per-cell work is hidden.
+template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) {
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
     if( !P.ctl->active ) return;
@@ -613,9 +676,7 @@ template <int CL> __global__ void __launch_bounds__( 256 ) k_check( KParams P ) 
     const size_t ldc = size_t( NS ) * P.nT;
     double* lam      = base + warp * check_ws_doubles( NS, P.nT, P.nQ );
     double* uh       = lam + ldc;
-    double* gbuf     = uh + ldc;
-    double* LA       = gbuf + ldc;
-    double* uk       = LA + size_t( NS ) * P.nQ;
+    double* uk       = uh + ldc;
     double* red      = uk + size_t( NS ) * P.nQ;
     double dtMin     = 1e300;
     for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
@@ -631,9 +692,29 @@ template <int CL> __global__ void __launch_bounds__( 256 ) k_check( KParams P ) 
         __syncwarp();
         bool converged = false;
         if( !bad ) {
-            eval_lambda<NS, 32>( g, P, phi, lam, nTj, LA );
+            // U(Lambda_k) at every node, Lambda_k in registers (closure.cpp:205-213, 234-253)
+            for( int k = g.r; k < P.nQ; k += 32 ) {
+                const double* row = phi + size_t( k ) * P.ld;
+                double Lk[NS], y[NS];
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) Lk[s] = 0.0;
+                for( int i = 0; i < nTj; ++i ) {
+                    const double r = row[i];
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) Lk[s] = fma( lam[s * P.nT + i], r, Lk[s] );
+                }
+                Closure<CL>::U( Lk, y, true, P.phys );
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) uk[s * P.nQ + k] = y[s];
+            }
             __syncwarp();
-            converged = gradient<CL, 32>( g, P, phiWf, LA, uh, nTj, uk, gbuf, red ) < P.eps;
+            double sq = 0.0;
+            for( int idx = g.r; idx < NS * nTj; idx += 32 ) {
+                const int s    = idx / nTj, i = idx - s * nTj;
+                const double a = node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) - uh[s * P.nT + i];
+                sq += a * a;
+            }
+            converged = sqrt( group_sum<32>( g, sq, red ) ) < P.eps;
         }
         if( converged ) {
             if( g.r == 0 ) {

@@ -334,11 +334,11 @@ void plan_launches( uqc_solver* h ) {
         CK( cudaFuncSetAttribute( pick( cl, h->group, which ), cudaFuncAttributeMaxDynamicSharedMemorySize, int( sm ) ) );
     }
     h->auxGrid = std::min( 4 * h->numSMs, std::max( 1, ( h->mesh.nCells + ug - 1 ) / ug ) );
-    // check kernel: a warp per cell, as many warps per CTA (up to 8) as shared memory allows
+    // check kernel: a warp per cell, as many warps per CTA (up to 16) as shared memory allows
     {
         const size_t wsc = check_ws_doubles( nS, nT, nQ ) * sizeof( double );
         const size_t av  = size_t( maxSmem ) - ( h->tablesInSmem ? tables : 0 );
-        const int warps  = int( std::min<size_t>( 8, av / wsc ) );
+        const int warps  = int( std::min<size_t>( 16, av / wsc ) );
         if( warps < 1 ) throw ConfigError( "check workspace exceeds shared memory" );
         h->checkBlock = 32 * warps;
         h->checkSmem  = wsc * warps + ( h->tablesInSmem ? tables : 0 );
