@@ -81,6 +81,7 @@ typedef struct uqc_step_info {
     long long line_search_trials;
     int active_cells;         /* cells that needed Newton iterations in the last step */
     long long fallback_cells; /* UQC_MIXED: cells handed to the FP64 form during this call */
+    int running;              /* 1 while the loop condition of momentsolver.cpp:79 holds */
 } uqc_step_info;
 
 /* ---- lifecycle and configuration ------------------------------------ */
@@ -197,6 +198,58 @@ int uqc_closure_solve_device( uqc_solver* h, int n, double* d_lambda, const doub
 #define UQC_NOALLOC_SCRATCH_BYTES ( 256 + 4 * UQC_NOALLOC_MAX_CELLS + 16 * UQC_NOALLOC_MAX_TABLE )
 int uqc_closure_solve_device_noalloc( uqc_solver* h, int n, double* d_lambda, const double* d_u, const unsigned* d_n_total,
                                       int* d_status, void* cuda_stream );
+
+/* ---- asynchronous stepping and serving ----------------------------------
+ * No reference counterpart: the reference runs one MomentSolver::Solve per
+ * process. These entry points let one process keep many solves resident on
+ * the device and interleave their time steps. */
+
+/* Enqueues n_steps time steps and a copy of the loop state on the handle's
+ * stream and returns at once. Steps after the loop condition fails do no work. */
+int uqc_step_async( uqc_solver* h, int n_steps );
+/* 1 when the work of the last uqc_step_async has finished (info filled as by
+ * uqc_step, for the steps since the previous query), 0 while it runs. */
+int uqc_step_query( uqc_solver* h, uqc_step_info* info );
+/* Device memory (bytes) the handle holds once its device side is set up. */
+int uqc_device_bytes( const uqc_solver* h, unsigned long long* bytes );
+
+/* Request server: continuous batching of whole UQ solves (each request is a
+ * TOML configuration run to its tEnd). Requests wait in submission order and
+ * are admitted, first fit, while their device memory fits the budget and
+ * fewer than max_active run; each admitted request owns a stream and its
+ * state stays on the device; every progress call advances each running
+ * request by one slice of steps_per_slice time steps (its kernels overlap on
+ * the device with the other requests'), retires finished ones (mean and
+ * variance are computed and the device memory freed) and admits waiting
+ * ones. A request's result does not depend on what else runs. Times are ms
+ * since the server was created. Not thread safe: one thread drives a server. */
+typedef struct uqc_server uqc_server;
+enum uqc_request_state { UQC_REQ_QUEUED = 0, UQC_REQ_RUNNING = 1, UQC_REQ_DONE = 2, UQC_REQ_FAILED = 3 };
+typedef struct uqc_request_info {
+    long long id;
+    int state;              /* uqc_request_state */
+    int status;             /* uqc_status_code of the solve (UQC_OK when done) */
+    int n_cells, n_states;  /* mean_var holds n_cells x 2 n_states doubles */
+    int steps;              /* time steps taken */
+    double t;               /* simulated time reached */
+    long long newton_iterations;
+    unsigned long long device_bytes;
+    double submit_ms, admit_ms, done_ms;
+} uqc_request_info;
+int uqc_server_create( unsigned long long device_budget_bytes, int max_active, int steps_per_slice, uqc_server** out );
+void uqc_server_destroy( uqc_server* s );
+const char* uqc_server_last_error( const uqc_server* s );
+/* precision: uqc_precision of the request. */
+int uqc_server_submit( uqc_server* s, const char* toml_text, int precision, long long* id );
+/* One scheduling pass; counts after it (any pointer may be NULL). */
+int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_done );
+/* State of a request; mean_var (or NULL) receives E and Var per cell and
+ * state (the layout of uqc_mean_var) once it is done. */
+int uqc_server_request( const uqc_server* s, long long id, uqc_request_info* info, double* mean_var );
+/* Error message of a failed request ("" otherwise; valid until it is released). */
+const char* uqc_server_request_error( const uqc_server* s, long long id );
+/* Forgets a finished request and its result. */
+int uqc_server_release( uqc_server* s, long long id );
 
 /* ---- introspection ----------------------------------------------------- */
 

@@ -1,0 +1,115 @@
+"""Asynchronous stepping and the request server (needs a B200).
+
+A request's result must not depend on what else runs: the kernels of one
+handle use only that handle's buffers and reduce in a fixed order, so the
+mean and variance of a request served in a mix equal those of the same
+request solved alone, bit for bit.
+"""
+import time
+
+import numpy as np
+import pytest
+
+from uqcreator_b200 import Solver, workloads as W, FP64, MIXED
+from uqcreator_b200.serve import Server, latency_percentiles
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests():
+    return [
+        W.burgers1d(ncells=400, degree=3, nquad=16, tend=0.004, x0=0.6),
+        W.euler2d(nx=16, ny=8, degree=2, nquad=4, tend=0.01, xs=0.4),
+        W.burgers1d(ncells=900, degree=5, nquad=24, tend=0.002, x0=0.7),
+        W.euler2d(nx=24, ny=10, degree=3, nquad=6, tend=0.006, xs=0.3),
+        W.shallow_water1d(ncells=2000, max_degree=4, nquad=12, tend=0.002),
+    ]
+
+
+def _alone(toml, precision=FP64):
+    s = Solver(toml)
+    s.init_state()
+    if precision == MIXED:
+        s.set_precision(MIXED)
+    info = s.run()
+    return s.mean_var(), info
+
+
+def test_step_async_matches_step():
+    toml = W.euler2d(nx=16, ny=8, degree=3, nquad=6)
+    a = Solver(toml); a.init_state()
+    b = Solver(toml); b.init_state()
+    ia = a.step(5)
+    b.step_async(5)
+    ib = None
+    t0 = time.time()
+    while ib is None and time.time() - t0 < 60:
+        ib = b.step_query()
+    assert ib is not None
+    for k in ("t", "dt", "residual", "steps", "newton_iterations", "running"):
+        assert ia[k] == ib[k], k
+    ua, la, _ = a.download_state()
+    ub, lb, _ = b.download_state()
+    np.testing.assert_array_equal(ua, ub)
+    np.testing.assert_array_equal(la, lb)
+
+
+def test_server_results_same_alone_and_in_mix():
+    reqs = _requests()
+    alone = [_alone(t)[0] for t in reqs]
+    srv = Server(budget_bytes=8 << 30, max_active=len(reqs), steps_per_slice=2)
+    ids = [srv.submit(t) for t in reqs]
+    srv.drain()
+    for rid, ref in zip(ids, alone):
+        r = srv.result(rid)
+        assert r["state"] == "done" and r["status"] == 0, r
+        assert r["latency_ms"] >= 0 and r["steps"] > 0
+        np.testing.assert_array_equal(r["mean_var"], ref)
+    srv.close()
+
+
+def test_server_mixed_precision_request_within_tolerance():
+    toml = W.euler2d(nx=16, ny=8, degree=3, nquad=6, tend=0.01)
+    ref, _ = _alone(toml)
+    srv = Server(budget_bytes=4 << 30, max_active=2, steps_per_slice=3)
+    rid = srv.submit(toml, precision=MIXED)
+    other = srv.submit(_requests()[0])
+    srv.drain()
+    r = srv.result(rid)
+    assert r["state"] == "done"
+    assert np.abs(r["mean_var"] - ref).sum() / np.abs(ref).sum() <= 1e-6
+    assert srv.result(other)["state"] == "done"
+
+
+def test_server_admits_by_device_budget():
+    reqs = _requests()
+    sizes = []
+    for t in reqs:
+        s = Solver(t)
+        sizes.append(s.device_bytes())
+        s.close()
+    budget = sum(sorted(sizes)[-2:])    # room for the two largest at once, not for all
+    srv = Server(budget_bytes=budget, max_active=len(reqs), steps_per_slice=1)
+    ids = [srv.submit(t) for t in reqs]
+    peak = 0
+    while True:
+        q, r, d = srv.progress()
+        used = sum(srv.info(i)["device_bytes"] for i in ids if srv.info(i)["state"] == "running")
+        assert used <= budget
+        peak = max(peak, r)
+        if q == 0 and r == 0:
+            break
+    assert peak < len(reqs)
+    lat = [srv.result(i, mean_var=False)["latency_ms"] for i in ids]
+    assert all(srv.info(i)["state"] == "done" for i in ids)
+    p = latency_percentiles(lat)
+    assert p["p50_ms"] <= p["p99_ms"]
+
+
+def test_handles_with_different_shared_memory_needs_coexist():
+    """Kernel launch limits are process-wide: a handle with a small workspace
+    set up after one with a large workspace must not break the latter."""
+    big = Solver(W.euler2d(nx=8, ny=4, degree=5, nquad=10)); big.init_state(); big.step(1)
+    small = Solver(W.euler2d(nx=8, ny=4, degree=2, nquad=4)); small.init_state(); small.step(1)
+    assert big.step(2)["steps"] == 2
+    assert small.step(2)["steps"] == 2

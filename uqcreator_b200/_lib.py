@@ -27,8 +27,11 @@ EXPORTS = [
     "uqc_upload_state", "uqc_download_state", "uqc_solve_closure", "uqc_cell_status", "uqc_step", "uqc_run",
     "uqc_mean_var", "uqc_closure_solve_host", "uqc_closure_solve_device", "uqc_last_timing", "uqc_device_state",
     "uqc_last_launch_count", "uqc_stream", "uqc_mesh_tri_jitter", "uqc_closure_solve_device_noalloc",
-    "uqc_set_option",
+    "uqc_set_option", "uqc_step_async", "uqc_step_query", "uqc_device_bytes", "uqc_server_create",
+    "uqc_server_destroy", "uqc_server_last_error", "uqc_server_submit", "uqc_server_progress",
+    "uqc_server_request", "uqc_server_release", "uqc_server_request_error",
 ]
+REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
 NOALLOC_MAX_CELLS = 65536
 
 
@@ -48,10 +51,22 @@ class Info(C.Structure):
 class StepInfo(C.Structure):
     _fields_ = [("t", C.c_double), ("dt", C.c_double), ("residual", C.c_double), ("steps", C.c_int),
                 ("failed_cells", C.c_int), ("newton_iterations", C.c_longlong), ("line_search_trials", C.c_longlong),
-                ("active_cells", C.c_int), ("fallback_cells", C.c_longlong)]
+                ("active_cells", C.c_int), ("fallback_cells", C.c_longlong), ("running", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("id", C.c_longlong), ("state", C.c_int), ("status", C.c_int), ("n_cells", C.c_int),
+                ("n_states", C.c_int), ("steps", C.c_int), ("t", C.c_double), ("newton_iterations", C.c_longlong),
+                ("device_bytes", C.c_ulonglong), ("submit_ms", C.c_double), ("admit_ms", C.c_double),
+                ("done_ms", C.c_double)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["state"] = REQ_STATES.get(d["state"], d["state"])
+        return d
 
 
 _dp = C.POINTER(C.c_double)
@@ -95,6 +110,17 @@ def lib() -> C.CDLL:
         "uqc_mesh_tri_jitter": ([C.c_int, C.c_int, C.c_double, C.c_ulonglong, _dp, _ip, _ip], C.c_int),
         "uqc_closure_solve_device_noalloc": ([_vp, C.c_int, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "uqc_set_option": ([_vp, C.c_char_p, C.c_double], C.c_int),
+        "uqc_step_async": ([_vp, C.c_int], C.c_int),
+        "uqc_step_query": ([_vp, C.POINTER(StepInfo)], C.c_int),
+        "uqc_device_bytes": ([_vp, C.POINTER(C.c_ulonglong)], C.c_int),
+        "uqc_server_create": ([C.c_ulonglong, C.c_int, C.c_int, C.POINTER(_vp)], C.c_int),
+        "uqc_server_destroy": ([_vp], None),
+        "uqc_server_last_error": ([_vp], C.c_char_p),
+        "uqc_server_submit": ([_vp, C.c_char_p, C.c_int, C.POINTER(C.c_longlong)], C.c_int),
+        "uqc_server_progress": ([_vp, _ip, _ip, _ip], C.c_int),
+        "uqc_server_request": ([_vp, C.c_longlong, C.POINTER(RequestInfo), _dp], C.c_int),
+        "uqc_server_release": ([_vp, C.c_longlong], C.c_int),
+        "uqc_server_request_error": ([_vp, C.c_longlong], C.c_char_p),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

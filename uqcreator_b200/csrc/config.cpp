@@ -237,6 +237,10 @@ Config parse_config( const std::string& text ) {
         else
             throw ConfigError( "[uqc] 'newton' must be reference, guarded or safe" );
     }
+    if( const Value* v = find( d, "uqc", "steps" ) ) {
+        c.maxSteps = int( v->num() );
+        if( c.maxSteps < 0 ) throw ConfigError( "[uqc] 'steps' must be >= 0" );
+    }
     size_t needIc = c.problem == PR_BURGERS ? 4 : ( c.problem == PR_EULER2D ? 5 : 3 );
     if( c.ic.size() < needIc ) throw ConfigError( "[uqc] 'ic' needs " + std::to_string( needIc ) + " values for " + c.problemName );
     if( c.meshDim == 1 ) {

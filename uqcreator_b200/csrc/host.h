@@ -49,6 +49,7 @@ struct Config {
     uint64_t seed = 0;
     int precision = 0;     // uqc_precision
     int newtonMode = 0;    // 0 reference, 1 guarded, 2 safe
+    int maxSteps   = 0;    // [uqc] steps: stop after this many time steps (0: no limit)
 };
 
 Config parse_config( const std::string& tomlText );

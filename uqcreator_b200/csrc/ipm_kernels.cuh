@@ -43,6 +43,7 @@ constexpr int MAXLEV = 16;
 // Grid-wide loop state kept on the device so a step needs no host round trip.
 struct Control {
     double t, tEnd, minResidual, residual, dt;
+    int maxSteps;                  // 0: no limit on the number of steps
     unsigned long long dtBits;     // atomicMin of the positive dt as integer bits
     unsigned int workCounter;      // closure work stealing
     unsigned int workCounter2;     // ... of the FP64 pass over the mixed form's fallback cells
@@ -849,7 +850,7 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
         C->dt         = dt;
         C->t          = C->t + dt;
         C->steps      = C->steps + 1;
-        C->active     = ( C->t < C->tEnd && C->residual > C->minResidual ) ? 1 : 0;
+        C->active     = ( C->t < C->tEnd && C->residual > C->minResidual && ( C->maxSteps == 0 || C->steps < C->maxSteps ) ) ? 1 : 0;
         C->activeCellsLast = C->activeCells;
         C->activeCells     = 0;
         C->dtBits     = 0x7FF0000000000000ull;    // +inf for the next step's min

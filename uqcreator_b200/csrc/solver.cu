@@ -17,6 +17,10 @@
 #include <fstream>
 #include <mutex>
 #include <sstream>
+#include <chrono>
+#include <deque>
+#include <map>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -75,6 +79,9 @@ struct uqc_solver {
     unsigned long long lastIters = 0, lastLs = 0, lastFallback = 0;
     int lastFailed = 0;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t asyncEv   = nullptr;    // end of the last uqc_step_async batch
+    bool asyncPending     = false;
+    int asyncStepsBefore  = 0;
     std::vector<cudaEvent_t> stepEvents;
     float lastMs[3] = {0, 0, 0};
     cudaGraphExec_t graph = nullptr;
@@ -239,6 +246,19 @@ void* pick_check( int cl ) {
 
 int closure_np( int cl ) { return cl == 0 ? 1 : ( cl == 1 ? 10 : 3 ); }
 
+// Dynamic shared memory limit of a kernel: the attribute belongs to the
+// kernel function, for the whole process, so every handle sets it to the
+// device's opt-in maximum (a handle that set its own smaller need would break
+// another handle's larger launch of the same kernel).
+void allow_dynamic_smem( const void* fn ) {
+    int dev = 0, maxSmem = 0;
+    CK( cudaGetDevice( &dev ) );
+    CK( cudaDeviceGetAttribute( &maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev ) );
+    cudaFuncAttributes fa;
+    CK( cudaFuncGetAttributes( &fa, fn ) );    // the limit counts static shared memory too
+    CK( cudaFuncSetAttribute( fn, cudaFuncAttributeMaxDynamicSharedMemorySize, maxSmem - int( fa.sharedSizeBytes ) ) );
+}
+
 void launch( uqc_solver* h, void* fn, int grid, int block, size_t smem, void** args ) {
     CK( cudaLaunchKernel( fn, dim3( grid ), dim3( block ), args, smem, h->stream ) );
     ++h->launches;
@@ -265,7 +285,7 @@ void plan_mixed( uqc_solver* h, int maxSmem ) {
     h->mixedBlock = h->mixedGroup * std::min( h->mixedGroup == 32 ? 8 : 4, fit );
     h->mixedSmem  = wsCell * ( h->mixedBlock / h->mixedGroup ) + ( h->mixedTablesInSmem ? tables : 0 );
     void* k       = pick( cl, h->mixedGroup, 4 );
-    CK( cudaFuncSetAttribute( k, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->mixedSmem ) ) );
+    allow_dynamic_smem( k );
     int occ = 0;
     CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, k, h->mixedBlock, h->mixedSmem ) );
     h->mixedGrid = std::max( 1, occ ) * h->numSMs;
@@ -307,7 +327,7 @@ void plan_launches( uqc_solver* h ) {
     if( h->closureSmem > size_t( maxSmem ) )
         throw ConfigError( "closure workspace (" + std::to_string( h->closureSmem ) + " B) exceeds shared memory; reduce moments or nodes" );
     void* kc = pick( cl, h->closureGroup, 0 );
-    CK( cudaFuncSetAttribute( kc, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->closureSmem ) ) );
+    allow_dynamic_smem( kc );
     int occ = 0;
     CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kc, h->closureBlock, h->closureSmem ) );
     h->closureGrid = std::max( 1, occ ) * h->numSMs;
@@ -320,7 +340,7 @@ void plan_launches( uqc_solver* h ) {
         h->updateBlock = 32 * warps;
         h->updateSmem  = uTables + size_t( warps ) * perWarp;
         void* ku       = pick( cl, h->group, 1 );
-        CK( cudaFuncSetAttribute( ku, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->updateSmem ) ) );
+        allow_dynamic_smem( ku );
         CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ku, h->updateBlock, h->updateSmem ) );
         h->updateGrid = std::max( 1, occ ) * h->numSMs;
         h->updateGrid = std::min( h->updateGrid, std::max( 1, ( h->mesh.nCells + warps - 1 ) / warps ) );
@@ -331,7 +351,7 @@ void plan_launches( uqc_solver* h ) {
     for( int which : {2, 3} ) {
         size_t sm = which == 2 ? h->initSmem : h->mvSmem;
         if( sm > size_t( maxSmem ) ) throw ConfigError( "init/meanvar workspace exceeds shared memory" );
-        CK( cudaFuncSetAttribute( pick( cl, h->group, which ), cudaFuncAttributeMaxDynamicSharedMemorySize, int( sm ) ) );
+        allow_dynamic_smem( pick( cl, h->group, which ) );
     }
     h->auxGrid = std::min( 4 * h->numSMs, std::max( 1, ( h->mesh.nCells + ug - 1 ) / ug ) );
     // check kernel: a warp per cell, as many warps per CTA (up to 16) as shared memory allows
@@ -343,7 +363,7 @@ void plan_launches( uqc_solver* h ) {
         h->checkBlock = 32 * warps;
         h->checkSmem  = wsc * warps + ( h->tablesInSmem ? tables : 0 );
         void* kk      = pick_check( cl );
-        CK( cudaFuncSetAttribute( kk, cudaFuncAttributeMaxDynamicSharedMemorySize, int( h->checkSmem ) ) );
+        allow_dynamic_smem( kk );
         CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kk, h->checkBlock, h->checkSmem ) );
         h->checkGrid = std::min( std::max( 1, occ ) * h->numSMs, std::max( 1, ( h->mesh.nCells + warps - 1 ) / warps ) );
     }
@@ -357,6 +377,7 @@ void reset_control( uqc_solver* h, double t ) {
     c.minResidual     = h->cfg.minResidual;
     c.residual        = h->cfg.minResidual + 1.0;    // momentsolver.cpp:76
     c.dtBits          = 0x7FF0000000000000ull;
+    c.maxSteps        = h->cfg.maxSteps;
     c.active          = t < h->cfg.tEnd ? 1 : 0;
     *h->h_ctl         = c;
     h->lastIters      = 0;    // device counters restart from zero
@@ -471,6 +492,7 @@ void release( uqc_solver* h ) {
     if( h->h_ctl ) cudaFreeHost( h->h_ctl );
     for( auto& e : h->ev )
         if( e ) cudaEventDestroy( e );
+    if( h->asyncEv ) cudaEventDestroy( h->asyncEv );
     for( auto& e : h->stepEvents )
         if( e ) cudaEventDestroy( e );
     if( h->ownStream && h->stream ) cudaStreamDestroy( h->stream );
@@ -529,8 +551,8 @@ void enqueue_step( uqc_solver* h, KParams& P ) {
 
 // Reads the control block, fills info with this call's deltas, returns the
 // number of cells that failed during the call.
-int fill_info( uqc_solver* h, uqc_step_info* info, int stepsBefore ) {
-    read_control( h );
+// fill_info from the host mirror of the control block as it stands.
+int fill_info_host( uqc_solver* h, uqc_step_info* info, int stepsBefore ) {
     const Control& c = *h->h_ctl;
     const int failedNow = c.failedCells - h->lastFailed;
     if( info ) {
@@ -543,12 +565,29 @@ int fill_info( uqc_solver* h, uqc_step_info* info, int stepsBefore ) {
         info->line_search_trials = (long long)( c.lineSearchTrials - h->lastLs );
         info->active_cells       = c.activeCellsLast;
         info->fallback_cells     = (long long)( c.fallbackCells - h->lastFallback );
+        info->running            = c.active;
     }
     h->lastFallback = c.fallbackCells;
     h->lastIters  = c.newtonIters;
     h->lastLs     = c.lineSearchTrials;
     h->lastFailed = c.failedCells;
     return failedNow;
+}
+
+int fill_info( uqc_solver* h, uqc_step_info* info, int stepsBefore ) {
+    read_control( h );
+    return fill_info_host( h, info, stepsBefore );
+}
+
+// Device memory of a handle once ensure_device has run (the allocations of
+// ensure_device and plan_launches; closure-only scratch excluded).
+unsigned long long device_bytes_of( const uqc_solver* h ) {
+    const unsigned long long N = (unsigned long long)h->mesh.nCells, F = (unsigned long long)h->mesh.nFaces;
+    const unsigned long long ldc = h->ldc, sq = (unsigned long long)h->nS * h->tab.nQ;
+    const unsigned long long tab = ( (unsigned long long)h->tab.nQ * h->ld + 8 ) * ( 8 + 8 + 4 ) + h->tab.xi.size() * 8 + h->tab.nQ * 8;
+    const unsigned long long d8  = N * ( 2 * ldc + 1 + 1 + 2 + 4 * F ) + ( N + 1 ) * sq;    // state, uQ, geometry (doubles)
+    const unsigned long long d4  = N * ( F + 1 + 1 + 1 + 1 + 1 + 1 );                         // nbr, boundary, level, status, iters, lists
+    return tab + 8 * d8 + 4 * d4 + sizeof( Control ) + 8 * 4096;
 }
 
 void to_layout( const uqc_solver* h, const double* src, double* dst, int layout, bool toDevice ) {
@@ -983,6 +1022,245 @@ int uqc_closure_solve_device( uqc_solver* h, int n, double* d_lambda, const doub
     } );
 }
 
+// ===================================================== asynchronous stepping
+
+int uqc_step_async( uqc_solver* h, int n_steps ) {
+    if( !h || n_steps < 0 ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state (call uqc_init_state or uqc_upload_state)" );
+    if( h->asyncPending ) return fail( h, UQC_ERR_STATE, "the previous uqc_step_async has not been queried to completion" );
+    return guarded_dev( h, [&] {
+        if( !h->asyncEv ) CK( cudaEventCreateWithFlags( &h->asyncEv, cudaEventDisableTiming ) );
+        h->launches         = 0;
+        h->asyncStepsBefore = h->h_ctl->steps;    // the mirror is current: no work is in flight
+        KParams P           = make_params( h );
+        for( int s = 0; s < n_steps; ++s ) enqueue_step( h, P );
+        CK( cudaMemcpyAsync( h->h_ctl, h->d_ctl, sizeof( Control ), cudaMemcpyDeviceToHost, h->stream ) );
+        CK( cudaEventRecord( h->asyncEv, h->stream ) );
+        CK( cudaGetLastError() );
+        h->asyncPending = true;
+        return UQC_OK;
+    } );
+}
+
+int uqc_step_query( uqc_solver* h, uqc_step_info* info ) {
+    if( !h ) return UQC_ERR_ARGUMENT;
+    if( !h->asyncPending ) return fail( h, UQC_ERR_STATE, "no uqc_step_async in flight" );
+    return guarded( h, [&] {
+        cudaError_t e = cudaEventQuery( h->asyncEv );
+        if( e == cudaErrorNotReady ) return 0;
+        CK( e );
+        h->asyncPending = false;
+        const int failed = fill_info_host( h, info, h->asyncStepsBefore );
+        if( failed ) return fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( failed ) + " cells did not converge" );
+        return 1;
+    } );
+}
+
+int uqc_device_bytes( const uqc_solver* h, unsigned long long* bytes ) {
+    if( !h || !bytes ) return UQC_ERR_ARGUMENT;
+    *bytes = device_bytes_of( h );
+    return UQC_OK;
+}
+
+// ===================================================== request server
+
+struct uqc_request {
+    long long id       = 0;
+    uqc_solver* h      = nullptr;
+    int state          = UQC_REQ_QUEUED;
+    int status         = UQC_OK;
+    int precision      = UQC_FP64;
+    int nCells = 0, nStates = 0, steps = 0;
+    double t           = 0.0;
+    long long iters    = 0;
+    unsigned long long bytes = 0;
+    bool admitted            = false;    // its bytes count against the budget
+    double submitMs = 0, admitMs = 0, doneMs = 0;
+    std::vector<double> meanVar;
+    std::string err;
+};
+
+struct uqc_server {
+    unsigned long long budget = 0, used = 0;
+    int maxActive = 1, slice = 1;
+    long long nextId = 1;
+    std::map<long long, uqc_request> reqs;
+    std::deque<long long> queue;      // waiting, in submission order
+    std::vector<long long> running;
+    int done = 0;
+    std::chrono::steady_clock::time_point t0;
+    std::string err;
+    double now() const { return std::chrono::duration<double, std::milli>( std::chrono::steady_clock::now() - t0 ).count(); }
+};
+
+namespace {
+int sfail( uqc_server* s, int code, const std::string& m ) {
+    s->err = m;
+    return code;
+}
+void retire( uqc_server* s, uqc_request& r, int status, const std::string& err ) {
+    r.status = status;
+    r.err    = err;
+    r.state  = status == UQC_OK ? UQC_REQ_DONE : UQC_REQ_FAILED;
+    r.doneMs = s->now();
+    if( r.h ) {
+        uqc_destroy( r.h );    // frees the request's device memory
+        r.h = nullptr;
+    }
+    if( r.admitted ) {
+        s->used -= r.bytes;
+        r.admitted = false;
+    }
+    ++s->done;
+}
+}    // namespace
+
+int uqc_server_create( unsigned long long device_budget_bytes, int max_active, int steps_per_slice, uqc_server** out ) {
+    if( !out || device_budget_bytes == 0 || max_active < 1 || steps_per_slice < 1 ) return UQC_ERR_ARGUMENT;
+    uqc_server* s = new( std::nothrow ) uqc_server();
+    if( !s ) return UQC_ERR_MEMORY;
+    s->budget    = device_budget_bytes;
+    s->maxActive = max_active;
+    s->slice     = steps_per_slice;
+    s->t0        = std::chrono::steady_clock::now();
+    *out         = s;
+    return UQC_OK;
+}
+
+void uqc_server_destroy( uqc_server* s ) {
+    if( !s ) return;
+    for( auto& kv : s->reqs )
+        if( kv.second.h ) uqc_destroy( kv.second.h );
+    delete s;
+}
+
+const char* uqc_server_last_error( const uqc_server* s ) { return s ? s->err.c_str() : "null server"; }
+
+int uqc_server_submit( uqc_server* s, const char* toml_text, int precision, long long* id ) {
+    if( !s || !toml_text || !id || ( precision != UQC_FP64 && precision != UQC_MIXED ) ) return UQC_ERR_ARGUMENT;
+    uqc_request r;
+    char err[512] = {0};
+    int rc = uqc_create_from_string( toml_text, nullptr, &r.h, err, sizeof( err ) );    // host side only
+    if( rc != UQC_OK ) return sfail( s, rc, err );
+    r.id        = s->nextId++;
+    r.precision = precision;
+    r.nCells    = r.h->mesh.nCells;
+    r.nStates   = r.h->nS;
+    r.bytes     = device_bytes_of( r.h );
+    r.submitMs  = s->now();
+    *id         = r.id;
+    s->queue.push_back( r.id );
+    s->reqs.emplace( r.id, std::move( r ) );
+    return UQC_OK;
+}
+
+int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_done ) {
+    if( !s ) return UQC_ERR_ARGUMENT;
+    // running requests: collect finished slices, retire finished solves, queue the next slice
+    for( size_t k = 0; k < s->running.size(); ) {
+        uqc_request& r = s->reqs[s->running[k]];
+        uqc_step_info info{};
+        const int q = uqc_step_query( r.h, &info );
+        if( q == 0 ) {
+            ++k;
+            continue;
+        }
+        bool finished = false;
+        if( q < 0 ) {
+            retire( s, r, q, uqc_last_error( r.h ) );
+            finished = true;
+        }
+        else {
+            r.steps += info.steps;
+            r.iters += info.newton_iterations;
+            r.t = info.t;
+            if( !info.running ) {
+                r.meanVar.assign( size_t( r.nCells ) * 2 * r.nStates, 0.0 );
+                const int rc = uqc_mean_var( r.h, r.meanVar.data() );
+                retire( s, r, rc, rc == UQC_OK ? "" : uqc_last_error( r.h ) );
+                finished = true;
+            }
+            else {
+                const int rc = uqc_step_async( r.h, s->slice );
+                if( rc != UQC_OK ) {
+                    retire( s, r, rc, uqc_last_error( r.h ) );
+                    finished = true;
+                }
+            }
+        }
+        if( finished )
+            s->running.erase( s->running.begin() + long( k ) );
+        else
+            ++k;
+    }
+    // admission, first fit in submission order
+    for( auto it = s->queue.begin(); it != s->queue.end() && int( s->running.size() ) < s->maxActive; ) {
+        uqc_request& r = s->reqs[*it];
+        if( r.bytes > s->budget ) {
+            retire( s, r, UQC_ERR_CAPACITY,
+                    "request needs " + std::to_string( r.bytes ) + " device bytes, the server budget is " + std::to_string( s->budget ) );
+            it = s->queue.erase( it );
+            continue;
+        }
+        if( s->used + r.bytes > s->budget ) {
+            ++it;
+            continue;
+        }
+        s->used += r.bytes;
+        r.admitted = true;
+        r.state    = UQC_REQ_RUNNING;
+        r.admitMs = s->now();
+        int rc    = uqc_init_state( r.h );
+        if( rc == UQC_OK && r.precision == UQC_MIXED ) rc = uqc_set_precision( r.h, UQC_MIXED );
+        if( rc == UQC_OK ) rc = uqc_step_async( r.h, s->slice );
+        if( rc != UQC_OK )
+            retire( s, r, rc, uqc_last_error( r.h ) );
+        else
+            s->running.push_back( r.id );
+        it = s->queue.erase( it );
+    }
+    if( n_queued ) *n_queued = int( s->queue.size() );
+    if( n_running ) *n_running = int( s->running.size() );
+    if( n_done ) *n_done = s->done;
+    return UQC_OK;
+}
+
+int uqc_server_request( const uqc_server* s, long long id, uqc_request_info* info, double* mean_var ) {
+    if( !s || !info ) return UQC_ERR_ARGUMENT;
+    auto it = s->reqs.find( id );
+    if( it == s->reqs.end() ) return UQC_ERR_ARGUMENT;
+    const uqc_request& r    = it->second;
+    info->id                = r.id;
+    info->state             = r.state;
+    info->status            = r.status;
+    info->n_cells           = r.nCells;
+    info->n_states          = r.nStates;
+    info->steps             = r.steps;
+    info->t                 = r.t;
+    info->newton_iterations = r.iters;
+    info->device_bytes      = r.bytes;
+    info->submit_ms         = r.submitMs;
+    info->admit_ms          = r.admitMs;
+    info->done_ms           = r.doneMs;
+    if( mean_var && r.state == UQC_REQ_DONE ) std::memcpy( mean_var, r.meanVar.data(), r.meanVar.size() * sizeof( double ) );
+    return UQC_OK;
+}
+
+const char* uqc_server_request_error( const uqc_server* s, long long id ) {
+    if( !s ) return "null server";
+    auto it = s->reqs.find( id );
+    return it == s->reqs.end() ? "unknown request" : it->second.err.c_str();
+}
+
+int uqc_server_release( uqc_server* s, long long id ) {
+    if( !s ) return UQC_ERR_ARGUMENT;
+    auto it = s->reqs.find( id );
+    if( it == s->reqs.end() || ( it->second.state != UQC_REQ_DONE && it->second.state != UQC_REQ_FAILED ) )
+        return sfail( s, UQC_ERR_STATE, "request " + std::to_string( id ) + " is not finished" );
+    s->reqs.erase( it );
+    return UQC_OK;
+}
+
 int uqc_last_timing( uqc_solver* h, float* ms3 ) {
     if( !h || !ms3 ) return UQC_ERR_ARGUMENT;
     for( int i = 0; i < 3; ++i ) ms3[i] = h->lastMs[i];
@@ -1115,7 +1393,7 @@ extern "C" int uqc_closure_solve_device_noalloc( uqc_solver* h, int n, double* d
         const size_t smem   = ws + ( P.tablesInSmem ? tables : 0 );
         if( smem > size_t( maxSmem ) ) throw ConfigError( "closure workspace exceeds shared memory" );
         void* fn = pick( cl, group, 0 );
-        CK( cudaFuncSetAttribute( fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int( smem ) ) );
+        allow_dynamic_smem( fn );
         CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, fn, block, smem ) );
         int mode     = 0;
         void* args[] = {&P, &mode};

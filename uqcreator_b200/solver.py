@@ -162,6 +162,25 @@ class Solver:
             check(self.h, rc)
         return info.as_dict()
 
+    def step_async(self, n_steps=1):
+        """Enqueues n_steps steps and returns at once (uqc_step_async)."""
+        check(self.h, self.lib.uqc_step_async(self.h, n_steps))
+
+    def step_query(self):
+        """None while the last step_async runs, else its step info."""
+        info = StepInfo()
+        rc = self.lib.uqc_step_query(self.h, C.byref(info))
+        if rc == 0:
+            return None
+        if rc < 0:
+            check(self.h, rc)
+        return info.as_dict()
+
+    def device_bytes(self):
+        b = C.c_ulonglong()
+        check(self.h, self.lib.uqc_device_bytes(self.h, C.byref(b)))
+        return b.value
+
     def run(self, t_end=0.0, raise_on_failure=True):
         info = StepInfo()
         rc = self.lib.uqc_run(self.h, t_end, C.byref(info))

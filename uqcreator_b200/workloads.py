@@ -10,6 +10,8 @@ a [uqc] table that the reference ignores and this package reads:
               jittered triangle mesh on [0,1]^2, nx x ny rectangles x 2)
   mesh_params [nx, ny, jitter, seed] for tri_jitter
   precision   "fp64" (plain form) or "mixed" (tensor-core Hessian)
+  newton      "reference", "guarded" or "safe" Newton (see euler2d)
+  steps       stop after this many time steps (0: run to tEnd only)
 
 Problems and their ic parameters:
   Burgers1D       [uL, uR, x0, x1]          ramp of code/src/burgers.cpp:48-68
@@ -52,13 +54,14 @@ mesh = "{mesh}"
 mesh_params = [{mesh_params}]
 precision = "{precision}"
 newton = "{newton}"
+steps = {steps}
 """
 
 
 def make_toml(*, name, problem, closure, dim, ncells=0, a=0.0, b=1.0, sigmas, cfl, tend, degrees,
               nquad, ic, bounds=(3.0, 12.0), mesh="uniform1d", mesh_params=(0, 0, 0.0, 0),
               maxit=1000, eps=1e-10, degtype="totalDegree", precision="fp64", gamma=None,
-              newton="reference") -> str:
+              newton="reference", steps=0) -> str:
     degrees = list(degrees)
     quads = [nquad] * len(degrees)
     extra = f"gamma = {gamma!r}\n" if gamma is not None else ""
@@ -70,19 +73,19 @@ def make_toml(*, name, problem, closure, dim, ncells=0, a=0.0, b=1.0, sigmas, cf
         maxit=int(maxit), eps=repr(float(eps)), ic=",".join(repr(float(v)) for v in ic),
         bounds=",".join(repr(float(v)) for v in bounds), mesh=mesh,
         mesh_params=",".join(repr(v) if isinstance(v, float) else str(v) for v in mesh_params),
-        precision=precision, newton=newton)
+        precision=precision, newton=newton, steps=int(steps))
 
 
-def burgers1d(ncells=500, tend=0.11, degree=4, nquad=20, eps=1e-10, **kw) -> str:
-    """Plain IPM FP64 Burgers: x in [0,3], u=12 left of 0.5+0.2 xi, ramp of width 0.1
-    down to 3, bounded barrier (2.5, 12.5), local Lax-Friedrichs flux, CFL 0.5."""
+def burgers1d(ncells=500, tend=0.11, degree=4, nquad=20, eps=1e-10, x0=0.5, **kw) -> str:
+    """Plain IPM FP64 Burgers: x in [0,3], u=12 left of x0+0.2 xi (x0 = 0.5), ramp of
+    width 0.1 down to 3, bounded barrier (2.5, 12.5), local Lax-Friedrichs flux, CFL 0.5."""
     return make_toml(name="burgers1d", problem="Burgers1D", closure="BoundedBarrier", dim=1, ncells=ncells,
                      a=0.0, b=3.0, sigmas=[0.2], cfl=0.5, tend=tend, degrees=[degree], nquad=nquad,
-                     ic=[12.0, 3.0, 0.5, 0.6], bounds=(2.5, 12.5), eps=eps, **kw)
+                     ic=[12.0, 3.0, x0, x0 + 0.1], bounds=(2.5, 12.5), eps=eps, **kw)
 
 
 def euler2d(nx=400, ny=250, degree=5, nquad=10, dim_xi=2, tend=0.2, cfl=0.5, eps=1e-10, seed=7,
-            jitter=0.2, newton="guarded", **kw) -> str:
+            jitter=0.2, newton="guarded", xs=0.5, **kw) -> str:
     """2-D Euler (gamma 1.4) on a jittered triangle mesh of nx*ny*2 cells, Sod-type
     interface x = 0.5 + 0.05 xi1, left density 1 + 0.1 xi2 (and left pressure
     1 + 0.1 xi3 when dim_xi = 3), right state (0.125, 0.1), total-degree basis.
@@ -94,7 +97,7 @@ def euler2d(nx=400, ny=250, degree=5, nquad=10, dim_xi=2, tend=0.2, cfl=0.5, eps
     sig = [0.05, 0.1, 0.1][:dim_xi]
     return make_toml(name="euler2d", problem="Euler2D", closure="Euler2D", dim=2, ncells=nx * ny * 2,
                      sigmas=sig, cfl=cfl, tend=tend, degrees=[degree], nquad=nquad,
-                     ic=[0.5, 1.0, 1.0, 0.125, 0.1], mesh="tri_jitter", mesh_params=(nx, ny, float(jitter), seed),
+                     ic=[xs, 1.0, 1.0, 0.125, 0.1], mesh="tri_jitter", mesh_params=(nx, ny, float(jitter), seed),
                      eps=eps, gamma=1.4, newton=newton, **kw)
 
 
@@ -109,6 +112,37 @@ def shallow_water1d(ncells=1_000_000, max_degree=9, nquad=30, tend=0.05, eps=1e-
 def euler2d_3u(nx=512, ny=256, degree=4, nquad=8, **kw) -> str:
     """Large 2-D Euler with 3 uncertainties, total degree 4 (35 moments x 4 states), 8^3 nodes."""
     return euler2d(nx=nx, ny=ny, degree=degree, nquad=nquad, dim_xi=3, **kw)
+
+
+def serving_stream(n_requests=2000, rate_per_s=50.0, seed=11, steps=(5, 40), euler_fraction=0.5, scale=1.0):
+    """Seeded request stream of the serving workload: Poisson arrivals (rate
+    rate_per_s) of UQ solves mixing 1-D Burgers (200-20k cells, degree 2-9:
+    3-10 moments) and 2-D Euler (10k-200k cells, total degree 2-5: 6-21
+    moments, 2 uncertainties), each with its shock / interface offset drawn from
+    U[0.05, 0.3] and a horizon of `steps` time steps (drawn uniformly, the
+    [uqc] steps limit; tEnd is far beyond). scale < 1 shrinks the meshes.
+    Returns [(arrival_s, kind, toml)]."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for _ in range(n_requests):
+        t += rng.exponential(1.0 / rate_per_s)
+        off = float(rng.uniform(0.05, 0.3))
+        nsteps = int(rng.integers(steps[0], steps[1] + 1))
+        if rng.random() < euler_fraction:
+            cells = int(rng.integers(10_000, 200_001) * scale)
+            deg = int(rng.integers(2, 6))
+            nx = max(4, int(round((cells / 2 * 1.6) ** 0.5)))
+            ny = max(2, cells // (2 * nx))
+            toml = euler2d(nx=nx, ny=ny, degree=deg, nquad=2 * deg, tend=10.0, xs=0.5 - off, steps=nsteps)
+            out.append((t, "euler2d", toml))
+        else:
+            cells = max(20, int(rng.integers(200, 20_001) * scale))
+            deg = int(rng.integers(2, 10))
+            toml = burgers1d(ncells=cells, degree=deg, nquad=4 * deg + 4, tend=10.0, x0=0.5 + off, steps=nsteps)
+            out.append((t, "burgers1d", toml))
+    return out
 
 
 WORKLOADS = {
