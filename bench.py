@@ -16,6 +16,10 @@ the C ABI with the state uploaded from and downloaded to pinned host memory
 every step. The plain FP64 form is timed in the same run (`fp64`), from the same
 state, and the chosen form's moments are compared with it after the K steps.
 
+`serving`: p50/p99 request latency and aggregate cell-steps/s of the request
+server (continuous batching) on the first requests of the seeded serving
+stream, submitted at their Poisson arrival times.
+
 N > 1 (torchrun): replicas only. Each rank runs its own copy of the workload
 on its GPU; there is no data-path collective; time = max over ranks.
 """
@@ -184,6 +188,42 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def run_serving(args, precision):
+    """p50/p99 request latency: the first `serve_requests` requests of the seeded
+    serving stream (Poisson arrivals, Burgers 1-D 200-20k cells / Euler 2-D
+    10k-200k cells, 5-40 steps each) submitted at their arrival times to the
+    request server and driven to completion."""
+    from uqcreator_b200 import workloads as W
+    from uqcreator_b200.serve import Server, latency_percentiles
+    stream = W.serving_stream(args.serve_requests, args.serve_rate, seed=11)
+    srv = Server(budget_bytes=int(args.serve_budget_gb * (1 << 30)), max_active=16, steps_per_slice=4)
+    t0 = time.perf_counter()
+    i, ids = 0, []
+    while True:
+        now = time.perf_counter() - t0
+        while i < len(stream) and stream[i][0] <= now:
+            ids.append((srv.submit(stream[i][2], precision), stream[i][1]))
+            i += 1
+        q, r, _ = srv.progress()
+        if i == len(stream) and q == 0 and r == 0:
+            break
+    el = time.perf_counter() - t0
+    res = [srv.result(k, mean_var=False) for k, _ in ids]
+    srv.close()
+    ok = [x for x in res if x["state"] == "done"]
+    lat = [x["latency_ms"] for x in ok]
+    out = {"requests": len(res), "failed": len(res) - len(ok), "arrival_rate_per_s": args.serve_rate,
+           "elapsed_s": el, "cell_steps_per_s": sum(x["n_cells"] * x["steps"] for x in ok) / el,
+           "stream": "seeded serving stream (seed 11): Poisson arrivals, Burgers1D 200-20k cells deg 2-9, "
+                     "Euler2D 10k-200k cells deg 2-5, offsets U[0.05,0.3], 5-40 steps per request",
+           "budget_gb": args.serve_budget_gb, "max_active": 16, "steps_per_slice": 4}
+    out.update(latency_percentiles(lat))
+    for kind in ("burgers1d", "euler2d"):
+        lk = [x["latency_ms"] for x, (_, k) in zip(res, ids) if k == kind and x["state"] == "done"]
+        out[kind] = dict(n=len(lk), **latency_percentiles(lk))
+    return out
+
+
 def run_b200(args, rank, world, local):
     import torch
     from uqcreator_b200 import Solver, workloads as W, FP64, MIXED
@@ -290,6 +330,8 @@ def run_b200(args, rank, world, local):
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
     }
+    if args.serve_requests > 0:
+        line["serving"] = run_serving(args, MIXED if chosen == "mixed" else FP64)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cb, *_ = cpu_reference_run(0, 2, min_seconds=args.cpu_seconds)
@@ -309,6 +351,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=120, help="requests of the serving stream (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=12.0, help="arrivals per second")
+    ap.add_argument("--serve-budget-gb", type=float, default=100.0)
     args = ap.parse_args()
     rank, world, local = dist_init()
     if args.impl == "reference":
