@@ -110,6 +110,8 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *   "closure_tables_smem"  1: the closure kernels stage the basis tables in
  *                    shared memory; 0: they read them through the L1 cache
  *                    (more cells per SM); -1 = automatic.
+ *   "graphs"         1 (default): uqc_run and uqc_step_async launch cached
+ *                    CUDA graphs of whole time steps; 0: direct launches.
  *   "mixed_max_iterations"  UQC_MIXED: Newton iterations of the FP32 pass
  *                    after which a cell continues in the FP64 form (>= 2;
  *                    0 = the configured maxIterations).

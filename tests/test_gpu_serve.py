@@ -113,3 +113,19 @@ def test_handles_with_different_shared_memory_needs_coexist():
     small = Solver(W.euler2d(nx=8, ny=4, degree=2, nquad=4)); small.init_state(); small.step(1)
     assert big.step(2)["steps"] == 2
     assert small.step(2)["steps"] == 2
+
+
+def test_graph_replay_matches_direct_launches():
+    """uqc_run through cached CUDA graphs gives the same state as direct launches."""
+    toml = W.burgers1d(ncells=500, tend=0.02)
+    a = Solver(toml); a.init_state(); a.set_option("graphs", 0)
+    b = Solver(toml); b.init_state()
+    ia, ib = a.run(), b.run()
+    assert ia["steps"] == ib["steps"] and ia["t"] == ib["t"]
+    np.testing.assert_array_equal(a.download_state()[0], b.download_state()[0])
+    # a settings change between runs re-captures the graph
+    b.set_newton(1000, 1e-11, 0)
+    a.set_newton(1000, 1e-11, 0)
+    ja, jb = a.run(0.03), b.run(0.03)
+    assert ja["newton_iterations"] == jb["newton_iterations"]
+    np.testing.assert_array_equal(a.download_state()[1], b.download_state()[1])

@@ -84,7 +84,11 @@ struct uqc_solver {
     int asyncStepsBefore  = 0;
     std::vector<cudaEvent_t> stepEvents;
     float lastMs[3] = {0, 0, 0};
-    cudaGraphExec_t graph = nullptr;
+    // CUDA graphs of n whole time steps (uqc_run, uqc_step_async), rebuilt
+    // when anything the kernels' arguments hold changes (planGen)
+    std::map<int, std::pair<cudaGraphExec_t, int>> graphs;    // n -> (graph, kernel launches)
+    int planGen = 0, graphGen = 0;
+    bool useGraphs = true;
     std::vector<double> padPhi, padPhiWf;    // host tables in the device layout
     std::vector<double> padWt;               // w_k / 2^dimXi per node
     double* d_wt = nullptr;
@@ -294,6 +298,7 @@ void plan_mixed( uqc_solver* h, int maxSmem ) {
 }
 
 void plan_launches( uqc_solver* h ) {
+    ++h->planGen;
     int dev;
     CK( cudaGetDevice( &dev ) );
     CK( cudaDeviceGetAttribute( &h->numSMs, cudaDevAttrMultiProcessorCount, dev ) );
@@ -482,7 +487,8 @@ void ensure_device( uqc_solver* h ) {
 }
 
 void release( uqc_solver* h ) {
-    if( h->graph ) cudaGraphExecDestroy( h->graph );
+    for( auto& kv : h->graphs ) cudaGraphExecDestroy( kv.second.first );
+    h->graphs.clear();
     for( void* p : {(void*)h->d_phi, (void*)h->d_phiWf, (void*)h->d_xi, (void*)h->d_wt, (void*)h->d_area, (void*)h->d_dx, (void*)h->d_center,
                     (void*)h->d_unitN, (void*)h->d_scaledN, (void*)h->d_nbr, (void*)h->d_boundary, (void*)h->d_u, (void*)h->d_lam,
                     (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
@@ -549,9 +555,50 @@ void enqueue_step( uqc_solver* h, KParams& P ) {
     launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
 }
 
+// n time steps on the handle's stream: one launch of a cached CUDA graph of
+// the n steps (captured on first use, re-captured after a change of launch
+// plan, precision or Newton settings), or direct launches when graphs are
+// off or the stream cannot be captured.
+void launch_steps( uqc_solver* h, int n ) {
+    if( h->useGraphs && h->graphGen != h->planGen ) {
+        for( auto& kv : h->graphs ) CK( cudaGraphExecDestroy( kv.second.first ) );
+        h->graphs.clear();
+        h->graphGen = h->planGen;
+    }
+    if( h->useGraphs ) {
+        auto it = h->graphs.find( n );
+        if( it == h->graphs.end() ) {
+            if( cudaStreamBeginCapture( h->stream, cudaStreamCaptureModeThreadLocal ) != cudaSuccess ) {
+                cudaGetLastError();
+                h->useGraphs = false;    // e.g. the legacy default stream
+            }
+            else {
+                const int l0 = h->launches;
+                KParams P    = make_params( h );
+                for( int s = 0; s < n; ++s ) enqueue_step( h, P );
+                cudaGraph_t g = nullptr;
+                CK( cudaStreamEndCapture( h->stream, &g ) );
+                cudaGraphExec_t ex = nullptr;
+                const cudaError_t e = cudaGraphInstantiate( &ex, g, 0 );
+                cudaGraphDestroy( g );
+                CK( e );
+                it          = h->graphs.emplace( n, std::make_pair( ex, h->launches - l0 ) ).first;
+                h->launches = l0;
+            }
+        }
+        if( h->useGraphs ) {
+            CK( cudaGraphLaunch( it->second.first, h->stream ) );
+            h->launches += it->second.second;
+            return;
+        }
+    }
+    KParams P = make_params( h );
+    for( int s = 0; s < n; ++s ) enqueue_step( h, P );
+}
+
 // Reads the control block, fills info with this call's deltas, returns the
-// number of cells that failed during the call.
-// fill_info from the host mirror of the control block as it stands.
+// number of cells that failed during the call; fill_info_host uses the host
+// mirror of the control block as it stands.
 int fill_info_host( uqc_solver* h, uqc_step_info* info, int stepsBefore ) {
     const Control& c = *h->h_ctl;
     const int failedNow = c.failedCells - h->lastFailed;
@@ -681,6 +728,7 @@ int uqc_set_precision( uqc_solver* h, int precision ) {
     if( rc != UQC_OK ) return rc;
     if( precision == UQC_MIXED && !h->mixedOk ) return fail( h, UQC_ERR_CONFIG, "mixed precision not available for this configuration: " + h->mixedWhy );
     h->precision = precision;
+    ++h->planGen;
     return UQC_OK;
 }
 
@@ -711,6 +759,12 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
         int v = int( value );
         if( v != 0 && v < 2 ) return fail( h, UQC_ERR_ARGUMENT, "mixed_max_iterations must be 0 or >= 2" );
         h->mixedMaxIter = v;
+        ++h->planGen;
+        return UQC_OK;
+    }
+    if( k == "graphs" ) {
+        h->useGraphs = value != 0.0;
+        ++h->planGen;
         return UQC_OK;
     }
     return fail( h, UQC_ERR_ARGUMENT, "unknown option '" + k + "'" );
@@ -721,6 +775,7 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
     h->cfg.maxIterations = max_iterations;
     h->cfg.epsilon       = epsilon;
     h->cfg.newtonMode    = newton_mode;
+    ++h->planGen;
     return UQC_OK;
 }
 
@@ -903,9 +958,8 @@ int uqc_run( uqc_solver* h, double t_end, uqc_step_info* info ) {
         int stepsBefore = h->h_ctl->steps;
         unsigned long long it0 = h->lastIters, ls0 = h->lastLs;
         int f0 = h->lastFailed;
-        KParams P = make_params( h );
         while( h->h_ctl->active ) {
-            for( int s = 0; s < 32; ++s ) enqueue_step( h, P );    // kernels turn into no-ops once the loop condition fails
+            launch_steps( h, 32 );    // kernels turn into no-ops once the loop condition fails
             read_control( h );
         }
         CK( cudaGetLastError() );
@@ -1032,8 +1086,7 @@ int uqc_step_async( uqc_solver* h, int n_steps ) {
         if( !h->asyncEv ) CK( cudaEventCreateWithFlags( &h->asyncEv, cudaEventDisableTiming ) );
         h->launches         = 0;
         h->asyncStepsBefore = h->h_ctl->steps;    // the mirror is current: no work is in flight
-        KParams P           = make_params( h );
-        for( int s = 0; s < n_steps; ++s ) enqueue_step( h, P );
+        launch_steps( h, n_steps );
         CK( cudaMemcpyAsync( h->h_ctl, h->d_ctl, sizeof( Control ), cudaMemcpyDeviceToHost, h->stream ) );
         CK( cudaEventRecord( h->asyncEv, h->stream ) );
         CK( cudaGetLastError() );
