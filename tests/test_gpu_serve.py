@@ -129,3 +129,20 @@ def test_graph_replay_matches_direct_launches():
     ja, jb = a.run(0.03), b.run(0.03)
     assert ja["newton_iterations"] == jb["newton_iterations"]
     np.testing.assert_array_equal(a.download_state()[1], b.download_state()[1])
+
+
+def test_autotune_picks_a_valid_shape_and_keeps_results(tmp_path):
+    from uqcreator_b200.autotune import autotune
+    from oracle.oracle import Oracle
+    from ._util import rel_l1
+    toml = W.euler2d(nx=16, ny=6, degree=4, nquad=8)
+    s = Solver(toml); s.init_state(); s.step(2)
+    r = autotune(s, steps=1, repeats=1, cache=tmp_path / "tune.json")
+    assert r["best"]["closure_group"] in (32, 64, 256) and not r["cached"]
+    assert min(v for v in r["ms_per_step"].values() if v is not None) > 0
+    s.step(2)
+    o = Oracle(toml, W.mesh_for(toml)); o.init_state(); o.step(4)
+    err = rel_l1(s.mean_var(), o.mean_var(), o.geometry()["area"])
+    assert (err <= 1e-10).all(), err
+    s2 = Solver(toml); s2.init_state()
+    assert autotune(s2, cache=tmp_path / "tune.json")["cached"]
