@@ -343,6 +343,72 @@ def run_b200(args, rank, world, local):
     s.close()
 
 
+# The other configurations: (builder, reference problem, reference IC parameters,
+# bounded-barrier bounds, Newton mode, GPU steps, CPU sample builder).
+def _configs():
+    from uqcreator_b200 import workloads as W
+    return {
+        "C1_burgers1d_500": (W.burgers1d, "Burgers1D", [12.0, 3.0, 0.5, 0.6], (2.5, 12.5), "reference", 0,
+                             lambda: W.burgers1d()),
+        "C2_euler2d_200k": (W.euler2d, "Euler2D", [0.5, 1.0, 1.0, 0.125, 0.1], (3, 12), "guarded", 10,
+                            lambda: W.euler2d(nx=400, ny=10)),
+        "C3_sw1d_1M_adaptive": (W.shallow_water1d, "ShallowWater1D", [0.5, 1.0, 0.5], (3, 12), "reference", 10,
+                                lambda: W.shallow_water1d(ncells=50_000)),
+        "C5_euler2d_3u_262k": (W.euler2d_3u, "Euler2D", [0.5, 1.0, 1.0, 0.125, 0.1], (3, 12), "guarded", 3,
+                               lambda: W.euler2d_3u(nx=512, ny=2)),
+    }
+
+
+def run_configs(args):
+    """One JSON line per configuration: GPU FP64 and mixed cell-steps/s from the
+    same state (C1: the whole 0.11 s solve, CUDA graphs), the mixed form's
+    moment error against the FP64 form, and the reference's own C++ (OpenMP)
+    on a sample of the configuration."""
+    import torch
+    from oracle import refharness
+    from uqcreator_b200 import Solver, FP64, MIXED
+    for name, (mk, problem, ic, bounds, newton, steps, sample) in _configs().items():
+        toml = mk()
+        out = {"config": name}
+        states = {}
+        for form in ("fp64", "mixed"):
+            s = Solver(toml)
+            s.init_state()
+            if form == "mixed":
+                s.set_precision(MIXED)
+            if steps == 0:    # whole solve
+                s.run(1e-3)
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize(); t0 = time.perf_counter()
+                info = s.run(s.settings.GetTEnd())
+                torch.cuda.synchronize(); el = time.perf_counter() - t0
+                done = info["steps"]
+            else:
+                s.step(3)
+                s.step(steps)
+                el = sum(s.last_timing()[2:3]) / 1e3
+                done = steps
+            out[form] = {"cell_steps_per_s": s.n_cells * done / el, "ms_per_step": 1e3 * el / done, "steps": done}
+            states[form] = s.download_state()[0]
+            s.close()
+        uf, um = states["fp64"], states["mixed"]
+        out["mixed_over_fp64"] = out["mixed"]["cell_steps_per_s"] / out["fp64"]["cell_steps_per_s"]
+        out["moment_rel_l1_mixed_vs_fp64"] = float(np.abs(um - uf).sum() / np.abs(uf).sum())
+        if refharness.available("omp") and not args.no_cpu_baseline:
+            st = sample()
+            r = refharness.RefSolver(st, problem, ic, bounds=bounds, mesh2d=__import__("uqcreator_b200").workloads.mesh_for(st),
+                                     variant="omp", newton=newton)
+            r.init_state()
+            r.step(1)
+            t0 = time.perf_counter(); n = 0
+            while time.perf_counter() - t0 < args.cpu_seconds / 3 or n == 0:
+                r.step(1); n += 1
+            el = time.perf_counter() - t0
+            out["cpu_reference"] = {"cell_steps_per_s": r.n_cells * n / el, "cells": r.n_cells, "steps": n,
+                                    "cores": os.cpu_count()}
+        print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -354,9 +420,13 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=120, help="requests of the serving stream (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=12.0, help="arrivals per second")
     ap.add_argument("--serve-budget-gb", type=float, default=100.0)
+    ap.add_argument("--configs", action="store_true", help="one line per configuration (C1, C2, C3, C5) instead of the bench line")
     args = ap.parse_args()
     rank, world, local = dist_init()
-    if args.impl == "reference":
+    if args.configs:
+        if rank == 0:
+            run_configs(args)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
         run_b200(args, rank, world, local)
