@@ -10,6 +10,7 @@ namespace uqc {
 struct PhysParams {
     double bbMinus, bbPlus;   // bounded barrier bounds
     double gamma;             // Euler
+    double eulerA;            // Euler: 1 / (1 - gamma), the exponent of the entropy ansatz
     double cfl;
     double ic[8];
     double sigma[4];
@@ -46,39 +47,44 @@ template <> struct Closure<0> {
 // EulerClosure2D (eulerclosure2d.cpp); the class stores g = -gamma (:3).
 template <> struct Closure<1> {
     static constexpr int NS = 4, NP = 10;
-    // vecForm: U(Vector&, ...) of :7-18 (gradient, mean/variance); otherwise the
-    // U(const Matrix&) form of :27-32 (nodal reconstruction, momentsolver.cpp:99-101).
-    __device__ static void U( const double* L, double* u, bool vecForm, const PhysParams& p ) {
+    // The reference has two forms, U(Vector&) of :7-18 (gradient, mean/variance):
+    // rho = exp(A q) (-v4)^A, and U(const Matrix&) of :27-32 (reconstruction):
+    // rho = (-exp(q) v4)^A, with A = 1/(1 + g), g = -gamma. Both equal
+    // exp(A (q + log(-v4))), which is evaluated here with one exponential and
+    // one logarithm instead of exp and pow, and one division (1/v4); the
+    // results agree with the reference's to a few ulps of the exponent.
+    // vecForm is kept for the interface.
+    __device__ static void U( const double* L, double* u, bool /*vecForm*/, const PhysParams& p ) {
         const double g = -p.gamma;
-        double v1 = L[0], v2 = L[1], v3 = L[2], v4 = L[3];
-        double q  = ( v2 * v2 + v3 * v3 - 2.0 * v1 * v4 - 2.0 * v4 * g ) / ( 2.0 * v4 );
-        double e;
-        if( vecForm )
-            e = exp( 1.0 / ( 1.0 + g ) * q ) * pow( -v4, 1.0 / ( 1.0 + g ) );
-        else
-            e = pow( -exp( q ) * v4, 1.0 / ( 1.0 + g ) );
-        u[0] = e;
-        u[1] = -( ( v2 * e ) / v4 );
-        u[2] = -( ( v3 * e ) / v4 );
-        u[3] = -( ( e * ( -( v2 * v2 ) - v3 * v3 + 2.0 * v4 ) ) / ( 2.0 * ( v4 * v4 ) ) );
+        const double v1 = L[0], v2 = L[1], v3 = L[2], v4 = L[3];
+        const double i4 = 1.0 / v4;
+        const double q  = ( v2 * v2 + v3 * v3 - 2.0 * v1 * v4 - 2.0 * v4 * g ) * ( 0.5 * i4 );
+        const double e  = exp( p.eulerA * ( q + log( -v4 ) ) );
+        const double ei = e * i4;
+        u[0]            = e;
+        u[1]            = -( v2 * ei );
+        u[2]            = -( v3 * ei );
+        u[3]            = -( ( -( v2 * v2 ) - v3 * v3 + 2.0 * v4 ) * ( 0.5 * ei * i4 ) );
     }
     // packed upper DU (:54-88): order (0,0)(0,1)(0,2)(0,3)(1,1)(1,2)(1,3)(2,2)(2,3)(3,3)
+    // Same rewriting as U: rho' = A exp(A (q + log(-v4))), powers of 1/v4 from one division.
     __device__ static void DU( const double* L, double* y, const PhysParams& p ) {
         const double g = -p.gamma;
         double v1 = L[0], v2 = L[1], v3 = L[2], v4 = L[3];
-        double v4p2 = v4 * v4, v4p3 = v4p2 * v4, v4i2 = 1.0 / v4p2, v3p2 = v3 * v3, v2p2 = v2 * v2;
-        double e = exp( 1.0 / ( 1.0 + g ) * ( ( v2p2 + v3p2 - 2.0 * v1 * v4 - 2.0 * v4 * g ) / ( 2.0 * v4 ) ) ) * pow( -v4, 1.0 / ( 1.0 + g ) ) / ( 1.0 + g );
-        double vTerm = e * ( v2p2 + v3p2 + 2.0 * v4 * g ) / ( 2 * v4p3 );
+        double i4 = 1.0 / v4, v4i2 = i4 * i4, v3p2 = v3 * v3, v2p2 = v2 * v2, v4p2 = v4 * v4;
+        double q     = ( v2p2 + v3p2 - 2.0 * v1 * v4 - 2.0 * v4 * g ) * ( 0.5 * i4 );
+        double e     = p.eulerA * exp( p.eulerA * ( q + log( -v4 ) ) );
+        double vTerm = e * ( v2p2 + v3p2 + 2.0 * v4 * g ) * ( 0.5 * v4i2 * i4 );
         y[0] = -( e );
-        y[1] = ( v2 * e ) / ( v4 );
-        y[2] = ( v3 * e ) / ( v4 );
+        y[1] = ( v2 * e ) * i4;
+        y[2] = ( v3 * e ) * i4;
         y[3] = -( 0.5 * ( ( v2p2 + v3p2 - 2.0 * v4 ) * e ) * v4i2 );
         y[4] = -( ( e * ( v2p2 + ( g + 1.0 ) * v4 ) ) * v4i2 );
         y[5] = -( ( v2 * v3 * e ) * v4i2 );
         y[6] = v2 * vTerm;
         y[7] = -( ( e * ( v3p2 + ( g + 1.0 ) * v4 ) ) * v4i2 );
         y[8] = v3 * vTerm;
-        y[9] = -( e * ( v2p2 * v2p2 + v3p2 * v3p2 + 4.0 * v3p2 * v4 * g - 4.0 * v4p2 * g + 2.0 * v2p2 * ( v3p2 + 2.0 * v4 * g ) ) ) / ( 4.0 * ( v4p2 * v4p2 ) );
+        y[9] = -( e * ( v2p2 * v2p2 + v3p2 * v3p2 + 4.0 * v3p2 * v4 * g - 4.0 * v4p2 * g + 2.0 * v2p2 * ( v3p2 + 2.0 * v4 * g ) ) ) * ( 0.25 * v4i2 * v4i2 );
     }
     // EulerClosure2D::DS (:90-106)
     __device__ static void DS( const double* u, double* ds, const PhysParams& p ) {

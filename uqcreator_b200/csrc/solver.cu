@@ -166,6 +166,7 @@ KParams make_params( const uqc_solver* h ) {
     ph.bbMinus     = h->cfg.bbMinus;
     ph.bbPlus      = h->cfg.bbPlus;
     ph.gamma       = h->cfg.gamma;
+    ph.eulerA      = 1.0 / ( 1.0 - h->cfg.gamma );
     ph.cfl         = h->cfg.cfl;
     for( size_t i = 0; i < h->cfg.ic.size() && i < 8; ++i ) ph.ic[i] = h->cfg.ic[i];
     for( size_t i = 0; i < h->cfg.sigma.size() && i < 4; ++i ) ph.sigma[i] = h->cfg.sigma[i];
