@@ -469,7 +469,8 @@ out:
 // re-projected moments, and returns the cell's CFL time step.
 template <int CL, int GROUP>
 __device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* uh, const double* uk, int cell,
-                                 int lev, int nTj, double* red ) {
+                                 int lev, int nTj, double* red,
+                                 const double* ugs = nullptr ) {
     constexpr int NS = Closure<CL>::NS;
     const size_t ldc = size_t( NS ) * P.nT;
     int newLev       = lev;
@@ -496,7 +497,8 @@ __device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const do
     // [E] u(s, i) = sum_k uQ(s, k) phiWf(k, i) for i < nT(new level), 0 beyond
     for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
         int s = idx / P.nT, i = idx - s * P.nT;
-        P.u[cell * ldc + idx] = i < nTn ? node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) : 0.0;
+        // ugs: the same sums kept from the gradient test (i < nTj), when the caller has them
+        P.u[cell * ldc + idx] = i < nTn ? ( ugs && i < nTj ? ugs[idx] : node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) ) : 0.0;
     }
     // [F] the cell's time step (min over its nodes)
     double dloc = 1e300;
@@ -646,7 +648,7 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
 
 __host__ __device__ inline size_t check_ws_doubles( int nS, int nT, int nQ ) {
     size_t ldc = size_t( nS ) * nT;
-    return ( ( 2 * ldc + size_t( nS ) * nQ + 32 ) + 3 ) & ~size_t( 3 );
+    return ( ( 3 * ldc + size_t( nS ) * nQ + 32 ) + 3 ) & ~size_t( 3 );
 }
 
 // Step mode, first half of the closure: one warp per cell evaluates the
@@ -677,7 +679,8 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
     const size_t ldc = size_t( NS ) * P.nT;
     double* lam      = base + warp * check_ws_doubles( NS, P.nT, P.nQ );
     double* uh       = lam + ldc;
-    double* uk       = uh + ldc;
+    double* ugs      = uh + ldc;    // sum_k U_s(k) phiWf(k, i), kept for the re-projection
+    double* uk       = ugs + ldc;
     double* red      = uk + size_t( NS ) * P.nQ;
     double dtMin     = 1e300;
     for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
@@ -711,8 +714,10 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
             __syncwarp();
             double sq = 0.0;
             for( int idx = g.r; idx < NS * nTj; idx += 32 ) {
-                const int s    = idx / nTj, i = idx - s * nTj;
-                const double a = node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) - uh[s * P.nT + i];
+                const int s     = idx / nTj, i = idx - s * nTj;
+                const double m  = node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ );
+                ugs[s * P.nT + i] = m;
+                const double a  = m - uh[s * P.nT + i];
                 sq += a * a;
             }
             converged = sqrt( group_sum<32>( g, sq, red ) ) < P.eps;
@@ -723,7 +728,7 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
                 P.iters[cell]  = 0;
             }
             __syncwarp();
-            const double d = cell_epilogue<CL, 32>( g, P, phiWf, uh, uk, cell, lev, nTj, red );
+            const double d = cell_epilogue<CL, 32>( g, P, phiWf, uh, uk, cell, lev, nTj, red, ugs );
             dtMin          = d < dtMin ? d : dtMin;
         }
         else if( g.r == 0 ) {
