@@ -110,6 +110,13 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *   "closure_tables_smem"  1: the closure kernels stage the basis tables in
  *                    shared memory; 0: they read them through the L1 cache
  *                    (more cells per SM); -1 = automatic.
+ *   "mixed_chord"    UQC_MIXED, 1 (default): inexact (chord) Newton that
+ *                    keeps each cell's FP32 factor in device memory (about
+ *                    2 n^2 bytes per cell, n = states x moments) and reuses it
+ *                    across iterations and time steps while it contracts;
+ *                    0: a new factor at every iteration.
+ *   "mixed_chord_theta"  re-factor after a step with the held factor that
+ *                    reduced ||g|| by less than the factor 1/theta (default 0.1).
  *   "graphs"         1 (default): uqc_run and uqc_step_async launch cached
  *                    CUDA graphs of whole time steps; 0: direct launches.
  *   "mixed_max_iterations"  UQC_MIXED: Newton iterations of the FP32 pass

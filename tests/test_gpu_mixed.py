@@ -83,3 +83,27 @@ def test_fp64_and_mixed_switch_on_one_handle():
     s.set_precision(MIXED); s.step(2)
     s.set_precision(FP64); b = s.step(2)
     assert b["fallback_cells"] == 0 and b["failed_cells"] == 0
+
+
+def test_chord_newton_reuses_factors_reproducibly():
+    """The inexact (chord) Newton of the mixed form keeps each cell's factor
+    between steps; results stay within the mixed bound of the FP64 form, and a
+    state uploaded again starts without stored factors, so the same steps give
+    the same result."""
+    toml = W.euler2d(nx=16, ny=6)
+    ref = Solver(toml); ref.init_state(); ref.step(4)
+    s = Solver(toml); s.init_state(); s.set_precision(MIXED)
+    u0, l0, v0 = s.download_state()
+    a = s.step(4)
+    ua = s.download_state()[0]
+    s.upload_state(u0, l0, v0)
+    b = s.step(4)
+    ub = s.download_state()[0]
+    assert a["newton_iterations"] == b["newton_iterations"]
+    np.testing.assert_array_equal(ua, ub)
+    assert _moment_err(ua, ref.download_state()[0]) <= TOL
+    s.set_option("mixed_chord", 0)
+    s.upload_state(u0, l0, v0)
+    c = s.step(4)
+    assert _moment_err(s.download_state()[0], ref.download_state()[0]) <= TOL
+    assert c["newton_iterations"] <= a["newton_iterations"]

@@ -86,6 +86,10 @@ struct KParams {
     int* activeList;          // step mode: cells that need Newton (filled by k_check), or null
     unsigned* activeCount;
     unsigned* workCounter;    // work-stealing counter of k_closure (in ctl)
+    float* factorStore;       // mixed form, step mode: each cell's last FP32 factor (or null)
+    int* factorLevel;         // ... nTj it was formed for, -1 none
+    int factorStride;         // floats per cell in factorStore
+    double chordTheta;        // re-factor after a held-factor step that reduced ||g|| by less than 1/chordTheta
     int* fallbackList;        // mixed form: cells handed to the FP64 form (non-PD FP32 factor, ...)
     unsigned* fallbackCount;
     Control* ctl;
@@ -460,6 +464,105 @@ out:
     return rc;
 }
 
+// Mixed form, step mode: inexact (chord) Newton with a reused FP32 factor.
+// Same loop as newton_cell's SolveClosure path (FP64 gradient, line search,
+// convergence test), but the direction H0^-1 g comes from the factor the cell
+// holds (loaded from the store, formed at an earlier iteration or time step)
+// while it contracts well; the Hessian is re-assembled and factored when there
+// is no factor, when a step with the held factor does not reduce ||g|| at all
+// (the direction is then recomputed, not line-searched), and after a step
+// that reduced ||g|| by less than the factor 1/P.chordTheta. `fresh` reports whether w.H
+// ends with a factor formed in this solve (to store).
+template <int CL, int GROUP>
+__device__ int newton_cell_chord( const Grp<GROUP>& g, const KParams& P, const double* phi, const double* phiWf, const float* phiH, CellWs& w,
+                                  int nTj, bool have, int& iters, int& lsTrials, bool& fresh ) {
+    constexpr int NS = Closure<CL>::NS;
+    const int n      = NS * nTj;
+    const double eps = P.eps;
+    const bool guard = P.newtonMode != 0;
+    iters            = 0;
+    lsTrials         = 0;
+    fresh            = false;
+    double* LA       = w.LA;
+    double* LB       = w.LB;
+    float* H         = reinterpret_cast<float*>( w.H );
+    float* I         = reinterpret_cast<float*>( w.I );
+    auto accept      = [&]() {
+        for( int idx = g.r; idx < P.nS * P.nT; idx += GROUP ) w.lam[idx] = w.lamN[idx];
+        for( int idx = g.r; idx < NS * P.nQ; idx += GROUP ) LA[idx] = LB[idx];
+    };
+    auto trial = [&]( double step ) {
+        add_step<GROUP>( g, P, nTj, w.lam, -step, w.d, w.lamN );
+        g.sync();
+        eval_lambda<NS, GROUP>( g, P, phi, w.lamN, nTj, LB );
+        g.sync();
+        return gradient<CL, GROUP>( g, P, phiWf, LB, w.uh, nTj, w.uk, w.gN, w.red );
+    };
+    int rc = UQC_CELL_MAX_ITER;
+    eval_lambda<NS, GROUP>( g, P, phi, w.lam, nTj, LA );
+    g.sync();
+    double gn = gradient<CL, GROUP>( g, P, phiWf, LA, w.uh, nTj, w.uk, w.g, w.red );
+    if( gn < eps ) return UQC_CELL_CONVERGED;
+    bool refresh = !have;
+    double gnN   = 0.0;
+    for( int l = 0; l < P.maxIter; ++l ) {
+        if( l != 0 ) {
+            for( int idx = g.r; idx < n; idx += GROUP ) w.g[idx] = w.gN[idx];
+            gn = gnN;
+        }
+        for( int idx = g.r; idx < P.nS * P.nT; idx += GROUP ) w.lamN[idx] = w.lam[idx];
+        bool chord = false;
+        for( int attempt = 0; attempt < 2; ++attempt ) {
+            if( refresh ) {
+                if( newton_direction<CL, GROUP, float>( g, P, phi, phiH, w, nTj, LA ) ) return UQC_CELL_NOT_PD;
+                fresh   = true;
+                refresh = false;
+                chord   = false;
+            }
+            else {
+                forward_solve_warp<GROUP, float>( g, H, n, I, w.g );
+                back_solve_warp<GROUP, float>( g, H, n, I, w.d );
+                chord = true;
+            }
+            ++iters;
+            gnN = trial( 1.0 );
+            if( chord && !( gnN < gn ) ) {
+                refresh = true;    // no decrease with the held factor: form the true Newton direction
+                continue;
+            }
+            break;
+        }
+        double stepSize = 1.0;
+        int refine      = 0;
+        while( gn < gnN || ( guard && !isfinite( gnN ) ) ) {
+            stepSize *= 0.5;
+            ++lsTrials;
+            gnN = trial( stepSize );
+            if( gnN < eps ) {
+                accept();
+                rc = UQC_CELL_CONVERGED;
+                goto out;
+            }
+            if( ++refine > 1000 ) {
+                rc = UQC_CELL_LINE_SEARCH;
+                goto out;
+            }
+        }
+        accept();
+        g.sync();
+        if( gnN < eps ) {
+            rc = UQC_CELL_CONVERGED;
+            goto out;
+        }
+        if( chord && gnN > P.chordTheta * gn ) refresh = true;
+    }
+out:
+    g.sync();
+    w.LA = LA;
+    w.LB = LB;
+    return rc;
+}
+
 // ------------------------------------------------------------------ kernels
 
 // Epilogue of a cell whose closure is done, phases [C]-[F] of
@@ -595,7 +698,35 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
         else
         {
             PT_BEGIN( tn );
-            rc = newton_cell<CL, GROUP, HT>( g, P, phi, phiWf, phiH, w, nTj, iters, ls );
+            if constexpr( MIXED ) {
+                if( mode == 1 && P.factorStore && P.newtonMode != 2 && P.maxIter > 1 ) {
+                    // reuse the cell's stored FP32 factor when it was formed for this level
+                    const int nH    = int( ( hess_doubles( NS * nTj ) + 1 ) & ~size_t( 1 ) );    // floats of the tiles
+                    const int n8    = hnb( NS * nTj ) * 8;
+                    float* st       = P.factorStore + size_t( cell ) * P.factorStride;
+                    float* H        = reinterpret_cast<float*>( w.H );
+                    float* Iv       = reinterpret_cast<float*>( w.I );
+                    const bool have = P.factorLevel[cell] == nTj;
+                    if( have ) {
+                        for( int i = g.r; i < nH; i += GROUP ) H[i] = st[i];
+                        for( int i = g.r; i < n8; i += GROUP ) Iv[i] = st[nH + i];
+                    }
+                    g.sync();
+                    bool fresh = false;
+                    rc         = newton_cell_chord<CL, GROUP>( g, P, phi, phiWf, phiH, w, nTj, have, iters, ls, fresh );
+                    if( rc == UQC_CELL_CONVERGED && fresh ) {
+                        for( int i = g.r; i < nH; i += GROUP ) st[i] = H[i];
+                        for( int i = g.r; i < n8; i += GROUP ) st[nH + i] = Iv[i];
+                    }
+                    if( g.r == 0 ) P.factorLevel[cell] = rc == UQC_CELL_CONVERGED ? ( fresh || have ? nTj : -1 ) : -1;
+                }
+                else {
+                    rc = newton_cell<CL, GROUP, HT>( g, P, phi, phiWf, phiH, w, nTj, iters, ls );
+                }
+            }
+            else {
+                rc = newton_cell<CL, GROUP, HT>( g, P, phi, phiWf, phiH, w, nTj, iters, ls );
+            }
             PT_END( tn, 0 );
         }
         if( MIXED && rc != UQC_CELL_CONVERGED && rc != UQC_CELL_NONFINITE ) {

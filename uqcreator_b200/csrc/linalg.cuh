@@ -420,6 +420,42 @@ __device__ int cholesky_la( const Grp<GROUP>& g, T* H, int n, T* D, T* I, int* f
     return 0;
 }
 
+// Forward substitution U^T y = b by warp 0 with a factor that cholesky_la left
+// (tiles, tile inverses, I): y_J = X_J^T (b_J - sum_{K < J} U(K, J)^T y_K),
+// tile rows first to last; y goes to the right-hand side tiles, where
+// back_solve_warp reads it. b: n values (the padding rows are zero).
+template <int GROUP, class T>
+__device__ void forward_solve_warp( const Grp<GROUP>& g, T* H, int n, const T* I, const double* b ) {
+    const int nb = hnb( n ), warp = g.r >> 5, lane = g.r & 31;
+    if( warp == 0 ) {
+        const int r = lane & 7, q = lane >> 3;
+        T* y        = H + hrhs( nb );
+        for( int J = 0; J < nb; ++J ) {
+            T acc = 0;
+            for( int K = 0; K < J; ++K ) {
+                const T* A = H + htile( K, J );
+#pragma unroll
+                for( int kk = q; kk < 8; kk += 4 ) acc += A[tix( kk, r )] * y[K * 8 + kk];
+            }
+            acc += __shfl_xor_sync( 0xffffffffu, acc, 8 );
+            acc += __shfl_xor_sync( 0xffffffffu, acc, 16 );
+            const int row = J * 8 + r;
+            const T rr    = ( row < n ? T( b[row] ) : T( 0 ) ) - acc;
+            const T* DT   = H + htile( J, J );
+            T v           = I[J * 8 + r] * rr;
+#pragma unroll
+            for( int k = 0; k < 7; ++k ) {
+                const T rk = __shfl_sync( 0xffffffffu, rr, k );
+                if( k < r ) v += DT[tix( r, k )] * rk;
+            }
+            __syncwarp();
+            if( q == 0 ) y[J * 8 + r] = v;
+            __syncwarp();
+        }
+    }
+    g.sync();
+}
+
 // Back substitution U x = y by warp 0, tile rows last first: r_J = y_J -
 // sum_{C > J} U(J, C) x_C (lane (r, q) sums columns q, q + 4 of each tile,
 // then two shuffles), x_J = X_J r_J with the stored tile inverse. Only x[0..n)

@@ -70,6 +70,12 @@ struct uqc_solver {
     std::string mixedWhy = "not planned";
     int mixedGroup = 64, mixedBlock = 256, mixedGrid = 0;
     int mixedMaxIter = 0;    // Newton iterations of the FP32 pass before the FP64 form takes over (0: the configured limit)
+    // mixed form: each cell's last FP32 factor, reused by the chord Newton of later iterations and steps
+    float* d_factorStore = nullptr;
+    int* d_factorLevel   = nullptr;
+    int factorStride     = 0;
+    bool chord           = true;
+    double chordTheta    = 0.1;
     size_t mixedSmem       = 0;
     bool mixedTablesInSmem = false;
     // bookkeeping
@@ -197,6 +203,11 @@ KParams make_params( const uqc_solver* h ) {
     P.ctl           = h->d_ctl;
     P.workCounter   = h->d_ctl ? &h->d_ctl->workCounter : nullptr;
     P.fallbackList  = h->d_fallbackList;
+    const bool useStore = h->precision == UQC_MIXED && h->chord && h->d_factorStore;
+    P.factorStore       = useStore ? h->d_factorStore : nullptr;
+    P.factorLevel       = useStore ? h->d_factorLevel : nullptr;
+    P.factorStride      = h->factorStride;
+    P.chordTheta        = h->chordTheta;
     P.fallbackCount = h->d_ctl ? &h->d_ctl->nFallback : nullptr;
     return P;
 }
@@ -267,6 +278,25 @@ void allow_dynamic_smem( const void* fn ) {
 void launch( uqc_solver* h, void* fn, int grid, int block, size_t smem, void** args ) {
     CK( cudaLaunchKernel( fn, dim3( grid ), dim3( block ), args, smem, h->stream ) );
     ++h->launches;
+}
+
+// Factor store of the mixed form: floats per cell (tiles + pivot inverses of
+// the finest level, padded to 16 bytes) and its total bytes.
+int factor_stride( const uqc_solver* h ) {
+    const int n = h->nS * h->tab.nT;
+    return int( ( hess_doubles( n ) + size_t( hnb( n ) ) * 8 + 3 ) & ~size_t( 3 ) );
+}
+unsigned long long factor_store_bytes( const uqc_solver* h ) {
+    return (unsigned long long)h->mesh.nCells * ( (unsigned long long)factor_stride( h ) * 4 + 4 );
+}
+// Allocates the store on first use; marks every stored factor invalid.
+void reset_factor_store( uqc_solver* h ) {
+    if( !h->d_factorStore ) {
+        h->factorStride  = factor_stride( h );
+        h->d_factorStore = dalloc<float>( size_t( h->mesh.nCells ) * h->factorStride );
+        h->d_factorLevel = dalloc<int>( size_t( h->mesh.nCells ) );
+    }
+    CK( cudaMemsetAsync( h->d_factorLevel, 0xFF, size_t( h->mesh.nCells ) * sizeof( int ), h->stream ) );
 }
 
 // Mixed-form closure: the FP32 Hessian halves the per-cell shared memory, so
@@ -482,6 +512,7 @@ void ensure_device( uqc_solver* h ) {
     for( auto& e : h->ev ) CK( cudaEventCreate( &e ) );
     plan_launches( h );
     if( h->precision == UQC_MIXED && !h->mixedOk ) throw ConfigError( "mixed precision not available for this configuration: " + h->mixedWhy );
+    if( h->precision == UQC_MIXED && h->chord ) reset_factor_store( h );
     h->d_blockPartial = dalloc<double>( std::max( h->updateGrid, 1 ) );
     h->deviceReady = true;
     reset_control( h, 0.0 );
@@ -494,7 +525,8 @@ void release( uqc_solver* h ) {
                     (void*)h->d_unitN, (void*)h->d_scaledN, (void*)h->d_nbr, (void*)h->d_boundary, (void*)h->d_u, (void*)h->d_lam,
                     (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
                     (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
-                    (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_phiF, (void*)h->d_fallbackList} )
+                    (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_phiF, (void*)h->d_fallbackList,
+                    (void*)h->d_factorStore, (void*)h->d_factorLevel} )
         if( p ) cudaFree( p );
     if( h->h_ctl ) cudaFreeHost( h->h_ctl );
     for( auto& e : h->ev )
@@ -629,13 +661,14 @@ int fill_info( uqc_solver* h, uqc_step_info* info, int stepsBefore ) {
 
 // Device memory of a handle once ensure_device has run (the allocations of
 // ensure_device and plan_launches; closure-only scratch excluded).
+unsigned long long factor_store_bytes( const uqc_solver* h );
 unsigned long long device_bytes_of( const uqc_solver* h ) {
     const unsigned long long N = (unsigned long long)h->mesh.nCells, F = (unsigned long long)h->mesh.nFaces;
     const unsigned long long ldc = h->ldc, sq = (unsigned long long)h->nS * h->tab.nQ;
     const unsigned long long tab = ( (unsigned long long)h->tab.nQ * h->ld + 8 ) * ( 8 + 8 + 4 ) + h->tab.xi.size() * 8 + h->tab.nQ * 8;
     const unsigned long long d8  = N * ( 2 * ldc + 1 + 1 + 2 + 4 * F ) + ( N + 1 ) * sq;    // state, uQ, geometry (doubles)
     const unsigned long long d4  = N * ( F + 1 + 1 + 1 + 1 + 1 + 1 );                         // nbr, boundary, level, status, iters, lists
-    return tab + 8 * d8 + 4 * d4 + sizeof( Control ) + 8 * 4096;
+    return tab + 8 * d8 + 4 * d4 + sizeof( Control ) + 8 * 4096 + ( h->precision == UQC_MIXED && h->chord ? factor_store_bytes( h ) : 0 );
 }
 
 void to_layout( const uqc_solver* h, const double* src, double* dst, int layout, bool toDevice ) {
@@ -728,6 +761,13 @@ int uqc_set_precision( uqc_solver* h, int precision ) {
     } );
     if( rc != UQC_OK ) return rc;
     if( precision == UQC_MIXED && !h->mixedOk ) return fail( h, UQC_ERR_CONFIG, "mixed precision not available for this configuration: " + h->mixedWhy );
+    if( precision == UQC_MIXED && h->chord ) {
+        rc = guarded( h, [&] {
+            reset_factor_store( h );
+            return UQC_OK;
+        } );
+        if( rc != UQC_OK ) return rc;
+    }
     h->precision = precision;
     ++h->planGen;
     return UQC_OK;
@@ -760,6 +800,24 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
         int v = int( value );
         if( v != 0 && v < 2 ) return fail( h, UQC_ERR_ARGUMENT, "mixed_max_iterations must be 0 or >= 2" );
         h->mixedMaxIter = v;
+        ++h->planGen;
+        return UQC_OK;
+    }
+    if( k == "mixed_chord" ) {
+        h->chord = value != 0.0;
+        if( h->chord && h->precision == UQC_MIXED && h->deviceReady ) {
+            int rc = guarded( h, [&] {
+                reset_factor_store( h );
+                return UQC_OK;
+            } );
+            if( rc != UQC_OK ) return rc;
+        }
+        ++h->planGen;
+        return UQC_OK;
+    }
+    if( k == "mixed_chord_theta" ) {
+        if( !( value > 0.0 && value < 1.0 ) ) return fail( h, UQC_ERR_ARGUMENT, "mixed_chord_theta must be in (0, 1)" );
+        h->chordTheta = value;
         ++h->planGen;
         return UQC_OK;
     }
@@ -811,6 +869,7 @@ int uqc_init_state( uqc_solver* h ) {
         void* args[] = {&P};
         launch( h, pick( h->cfg.closure, h->group, 2 ), h->auxGrid, h->auxBlock, h->initSmem, args );
         CK( cudaGetLastError() );
+        if( h->d_factorLevel ) reset_factor_store( h );
         reset_control( h, 0.0 );
         h->stateReady = true;
         return UQC_OK;
@@ -848,6 +907,7 @@ int uqc_upload_state( uqc_solver* h, const double* u, const double* lambda, cons
             CK( cudaMemcpyAsync( h->d_level, lv.data(), N * sizeof( unsigned ), cudaMemcpyHostToDevice, h->stream ) );
             CK( cudaStreamSynchronize( h->stream ) );
         }
+        if( h->d_factorLevel ) reset_factor_store( h );
         reset_control( h, t );
         h->stateReady = true;
         return UQC_OK;
@@ -1200,7 +1260,7 @@ int uqc_server_submit( uqc_server* s, const char* toml_text, int precision, long
     r.precision = precision;
     r.nCells    = r.h->mesh.nCells;
     r.nStates   = r.h->nS;
-    r.bytes     = device_bytes_of( r.h );
+    r.bytes     = device_bytes_of( r.h ) + ( precision == UQC_MIXED && r.h->chord ? factor_store_bytes( r.h ) : 0 );
     r.submitMs  = s->now();
     *id         = r.id;
     s->queue.push_back( r.id );
