@@ -243,19 +243,56 @@ __device__ void eval_u( const Grp<GROUP>& g, const KParams& P, const double* L, 
 // Gradient (closure.cpp:234-253) at the duals whose Lambda is in L:
 // gout[s nTj + i] = sum_k U_s(k) phiWf(k, i) - uh[s nT + i]; returns ||gout||_2.
 // Vectors of the Newton system use the level's compact stride nTj.
+// The sums m(s, i) = sum_k uk(s, k) phiWf(k, i) of the gradient, and
+// sum_(s,i) (m - uh)^2 of this thread. Warp groups: a thread per basis
+// function i, its NS sums as independent chains sharing each table value (one
+// table load per NS FMAs, one chain of nQ per sum, in node order as
+// node_dot's single chain); CTA groups: a thread per (s, i) with node_dot.
+// gout (compact stride nTj) and ms (stride nT) may be null.
+template <int NS, int GROUP>
+__device__ __forceinline__ double gradient_sums( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* uk, const double* uh,
+                                                 int nTj, double* gout, double* ms ) {
+    double sq = 0.0;
+    if constexpr( GROUP <= 64 ) {
+        for( int i = g.r; i < nTj; i += GROUP ) {
+            double a[NS];
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) a[s] = 0.0;
+            const double* t = phiWf + i;
+            for( int k = 0; k < P.nQ; ++k, t += P.ld ) {
+                const double w = *t;
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) a[s] = fma( uk[s * P.nQ + k], w, a[s] );
+            }
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) {
+                if( ms ) ms[s * P.nT + i] = a[s];
+                const double d = a[s] - uh[s * P.nT + i];
+                if( gout ) gout[s * nTj + i] = d;
+                sq += d * d;
+            }
+        }
+    }
+    else {
+        for( int idx = g.r; idx < NS * nTj; idx += GROUP ) {
+            const int s    = idx / nTj, i = idx - s * nTj;
+            const double m = node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ );
+            if( ms ) ms[s * P.nT + i] = m;
+            const double d = m - uh[s * P.nT + i];
+            if( gout ) gout[idx] = d;
+            sq += d * d;
+        }
+    }
+    return sq;
+}
+
 template <int CL, int GROUP>
 __device__ __forceinline__ double gradient_body( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* L, const double* uh,
                                                  int nTj, double* uk, double* gout, double* red ) {
     constexpr int NS = Closure<CL>::NS;
     eval_u<CL, GROUP>( g, P, L, uk, true );
     g.sync();
-    double sq = 0.0;
-    for( int idx = g.r; idx < NS * nTj; idx += GROUP ) {
-        int s    = idx / nTj, i = idx - s * nTj;
-        double a = node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) - uh[s * P.nT + i];
-        gout[idx] = a;
-        sq += a * a;
-    }
+    const double sq = gradient_sums<NS, GROUP>( g, P, phiWf, uk, uh, nTj, gout, nullptr );
     return sqrt( group_sum<GROUP>( g, sq, red ) );
 }
 
@@ -815,6 +852,8 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
     double* red      = uk + size_t( NS ) * P.nQ;
     double dtMin     = 1e300;
     for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
+        CT_BEGIN( tcell );
+        CT_BEGIN( tload );
         const int lev = int( P.level[cell] ), nTj = P.nTLevel[lev];
         bool bad = false;
         for( int idx = g.r; idx < int( ldc ); idx += 32 ) {
@@ -825,8 +864,10 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
         }
         bad = __any_sync( 0xffffffffu, bad );
         __syncwarp();
+        CT_END( tload, 16, g.r == 0 );
         bool converged = false;
         if( !bad ) {
+            CT_BEGIN( tlu );
             // U(Lambda_k) at every node, Lambda_k in registers (closure.cpp:205-213, 234-253)
             for( int k = g.r; k < P.nQ; k += 32 ) {
                 const double* row = phi + size_t( k ) * P.ld;
@@ -843,15 +884,11 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
                 for( int s = 0; s < NS; ++s ) uk[s * P.nQ + k] = y[s];
             }
             __syncwarp();
-            double sq = 0.0;
-            for( int idx = g.r; idx < NS * nTj; idx += 32 ) {
-                const int s     = idx / nTj, i = idx - s * nTj;
-                const double m  = node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ );
-                ugs[s * P.nT + i] = m;
-                const double a  = m - uh[s * P.nT + i];
-                sq += a * a;
-            }
+            CT_END( tlu, 17, g.r == 0 );
+            CT_BEGIN( tgr );
+            const double sq = gradient_sums<NS, 32>( g, P, phiWf, uk, uh, nTj, nullptr, ugs );
             converged = sqrt( group_sum<32>( g, sq, red ) ) < P.eps;
+            CT_END( tgr, 18, g.r == 0 );
         }
         if( converged ) {
             if( g.r == 0 ) {
@@ -859,13 +896,16 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
                 P.iters[cell]  = 0;
             }
             __syncwarp();
+            CT_BEGIN( tep );
             const double d = cell_epilogue<CL, 32>( g, P, phiWf, uh, uk, cell, lev, nTj, red, ugs );
             dtMin          = d < dtMin ? d : dtMin;
+            CT_END( tep, 19, g.r == 0 );
         }
         else if( g.r == 0 ) {
             P.activeList[atomicAdd( P.activeCount, 1u )] = cell;
         }
         __syncwarp();
+        CT_END( tcell, 20, g.r == 0 );
     }
     if( g.r == 0 && dtMin < 1e300 ) atomic_min_pos_double( &P.ctl->dtBits, dtMin );
 }

@@ -26,9 +26,10 @@ namespace uqc {
 // with -DUQC_PHASE_TIMERS): slots 0-7 are phases of the Newton step, 8-15
 // parts of the factorisation (8 critical warp, 9 trailing warp, 10 barrier
 // wait of the critical warp, 11 barrier wait of a trailing warp, 12 tile
-// factor, 13 tile inverse, 14 tile-row update, 15 panel solve).
+// factor, 13 tile inverse, 14 tile-row update, 15 panel solve), 16-20 parts
+// of the check kernel (load, Lambda and U, gradient sums, epilogue, cell).
 #ifdef UQC_PHASE_TIMERS
-__device__ unsigned long long g_phaseCycles[16];
+__device__ unsigned long long g_phaseCycles[32];
 #define CT_BEGIN( v ) long long v = clock64();
 #define CT_END( v, id, cond ) \
     if( cond ) atomicAdd( &g_phaseCycles[id], (unsigned long long)( clock64() - v ) );

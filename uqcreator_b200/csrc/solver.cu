@@ -1415,10 +1415,10 @@ int uqc_mesh_tri_jitter( int nx, int ny, double jitter, unsigned long long seed,
 #ifdef UQC_PHASE_TIMERS
 // Diagnostic builds only: the per-phase cycle counters of k_closure (summed
 // over CTAs since the last call), then reset.
-extern "C" int uqc_debug_phase_cycles( double* out16 ) {
-    unsigned long long v[16];
+extern "C" int uqc_debug_phase_cycles( double* out32 ) {
+    unsigned long long v[32];
     if( cudaMemcpyFromSymbol( v, g_phaseCycles, sizeof( v ) ) != cudaSuccess ) return UQC_ERR_CUDA;
-    for( int i = 0; i < 16; ++i ) out16[i] = double( v[i] );
+    for( int i = 0; i < 32; ++i ) out32[i] = double( v[i] );
     std::memset( v, 0, sizeof( v ) );
     return cudaMemcpyToSymbol( g_phaseCycles, v, sizeof( v ) ) == cudaSuccess ? UQC_OK : UQC_ERR_CUDA;
 }
