@@ -138,12 +138,22 @@ int uqc_get_geometry( const uqc_solver* h, double* area, double* max_edge, doubl
 /* ---- state ------------------------------------------------------------ */
 
 /* Initial moments and duals on the device: MomentSolver::SetupIC
- * (momentsolver.cpp:535-563) and SetDuals without restart (:463-485). */
+ * (momentsolver.cpp:535-563) and SetDuals without restart (:463-485); with
+ * [general] restartFile = "<prefix>" in the input (settings.cpp:74-79) the
+ * moments come from <prefix>_moments (DetermineMoments, :418-433) and, with
+ * importDualState = true, the duals from <prefix>_duals (:465-466), else the
+ * duals start from DS of the moments. The prefix is relative to the input
+ * file's directory. A restart with another number of moments is refused. */
 int uqc_init_state( uqc_solver* h );
 /* Copies caller-owned host state to the device (u, lambda: n_cells * nS * nT
  * doubles in `layout`; level: n_cells refinement levels or NULL to keep). */
 int uqc_upload_state( uqc_solver* h, const double* u, const double* lambda, const unsigned* level, int layout, double t );
 int uqc_download_state( uqc_solver* h, double* u, double* lambda, unsigned* level, int layout );
+/* MomentSolver::Export (momentsolver.cpp:565-588): writes <prefix>_moments
+ * and <prefix>_duals in the reference's format (a line per cell, nS x nT values
+ * in state-major order with 15 significant digits, each followed by a comma),
+ * the files a restart reads. */
+int uqc_export_state( uqc_solver* h, const char* path_prefix );
 
 /* ---- hot path ----------------------------------------------------------- */
 

@@ -237,6 +237,11 @@ Config parse_config( const std::string& text ) {
         else
             throw ConfigError( "[uqc] 'newton' must be reference, guarded or safe" );
     }
+    if( const Value* v = find( d, "general", "restartFile" ) ) c.restartFile = str( *v, "[general] restartFile" );
+    if( const Value* v = find( d, "general", "importDualState" ) ) {
+        if( v->kind != Value::BOOL ) throw ConfigError( "[general] 'importDualState' must be true or false" );
+        c.importDualState = v->b;
+    }
     if( const Value* v = find( d, "uqc", "steps" ) ) {
         c.maxSteps = int( v->num() );
         if( c.maxSteps < 0 ) throw ConfigError( "[uqc] 'steps' must be >= 0" );

@@ -50,6 +50,9 @@ struct Config {
     int precision = 0;     // uqc_precision
     int newtonMode = 0;    // 0 reference, 1 guarded, 2 safe
     int maxSteps   = 0;    // [uqc] steps: stop after this many time steps (0: no limit)
+    std::string restartFile;       // [general] restartFile (settings.cpp:74-79), relative to the input file's directory
+    bool importDualState = false;  // [general] importDualState: duals from <restartFile>_duals too
+    std::string inputDir = ".";    // directory of the input file (uqc_create_from_file), else "."
 };
 
 Config parse_config( const std::string& tomlText );

@@ -1039,7 +1039,9 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
 }
 
 // Initial moments u_j = U_IC(x_j, xi_k) phiWf and duals lambda_j(:,0) = DS(u_j(:,0)).
-template <int CL, int GROUP> __global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_init( KParams P ) {
+// keepMoments: the moments are already in place (restart without duals,
+// momentsolver.cpp:463-485); only the duals are set.
+template <int CL, int GROUP> __global__ void __launch_bounds__( GROUP == 32 ? 256 : GROUP ) k_init( KParams P, int keepMoments ) {
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
     const int groups = blockDim.x / GROUP;
@@ -1048,7 +1050,7 @@ template <int CL, int GROUP> __global__ void __launch_bounds__( GROUP == 32 ? 25
     double* uic     = smem + size_t( gid ) * ( size_t( NS ) * P.nQ + 8 );
     const size_t ldc = size_t( NS ) * P.nT;
     for( int cell = blockIdx.x * groups + gid; cell < P.nCells; cell += gridDim.x * groups ) {
-        for( int k = g.r; k < P.nQ; k += GROUP ) {
+        for( int k = g.r; k < P.nQ && !keepMoments; k += GROUP ) {
             double y[NS];
             Problem<CL>::ic( P.center + 2 * cell, P.xi + size_t( k ) * P.dimXi, y, P.phys );
 #pragma unroll
@@ -1057,9 +1059,11 @@ template <int CL, int GROUP> __global__ void __launch_bounds__( GROUP == 32 ? 25
         g.sync();
         for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
             int s = idx / P.nT, i = idx - s * P.nT;
-            double a = 0.0;
-            for( int k = 0; k < P.nQ; ++k ) a = fma( uic[s * P.nQ + k], P.phiWf[size_t( k ) * P.ld + i], a );
-            P.u[cell * ldc + idx]   = a;
+            if( !keepMoments ) {
+                double a = 0.0;
+                for( int k = 0; k < P.nQ; ++k ) a = fma( uic[s * P.nQ + k], P.phiWf[size_t( k ) * P.ld + i], a );
+                P.u[cell * ldc + idx] = a;
+            }
             P.lam[cell * ldc + idx] = 0.0;
         }
         g.sync();

@@ -722,7 +722,13 @@ int uqc_create_from_file( const char* toml_path, void* cuda_stream, uqc_solver**
     }
     std::stringstream ss;
     ss << f.rdbuf();
-    return uqc_create_from_string( ss.str().c_str(), cuda_stream, out, err, err_len );
+    const int rc = uqc_create_from_string( ss.str().c_str(), cuda_stream, out, err, err_len );
+    if( rc == UQC_OK ) {
+        const std::string path = toml_path;
+        const size_t slash     = path.find_last_of( '/' );
+        ( *out )->cfg.inputDir = slash == std::string::npos ? "." : path.substr( 0, slash );
+    }
+    return rc;
 }
 
 void uqc_destroy( uqc_solver* h ) {
@@ -861,17 +867,92 @@ int uqc_get_geometry( const uqc_solver* h, double* area, double* max_edge, doubl
     return UQC_OK;
 }
 
+// Reads one of the reference's state files (MomentSolver::Export,
+// momentsolver.cpp:565-588): a line per cell, nS x nT values in state-major
+// order, each followed by a comma (ImportPrevMoments/Duals, :614-650).
+static void read_state_file( const std::string& path, size_t nCells, size_t perCell, std::vector<double>& out ) {
+    std::ifstream f( path );
+    if( !f ) throw ConfigError( "cannot open restart file " + path );
+    out.assign( nCells * perCell, 0.0 );
+    std::string line;
+    for( size_t j = 0; j < nCells; ++j ) {
+        if( !std::getline( f, line ) ) throw ConfigError( path + ": " + std::to_string( nCells ) + " cells expected, file ends at line " + std::to_string( j + 1 ) );
+        std::stringstream ls( line );
+        std::string cell;
+        for( size_t k = 0; k < perCell; ++k ) {
+            if( !std::getline( ls, cell, ',' ) || cell.empty() )
+                throw ConfigError( path + " line " + std::to_string( j + 1 ) + ": " + std::to_string( perCell ) +
+                                   " values expected (a restart with another number of moments is not supported)" );
+            out[j * perCell + k] = std::stod( cell );
+        }
+    }
+}
+
 int uqc_init_state( uqc_solver* h ) {
     if( !h ) return UQC_ERR_ARGUMENT;
     return guarded_dev( h, [&] {
         h->launches  = 0;
         KParams P    = make_params( h );
-        void* args[] = {&P};
-        launch( h, pick( h->cfg.closure, h->group, 2 ), h->auxGrid, h->auxBlock, h->initSmem, args );
+        int keep     = 0;
+        if( !h->cfg.restartFile.empty() ) {
+            // restart (MomentSolver::DetermineMoments / SetDuals, momentsolver.cpp:418-485)
+            const std::string base = h->cfg.restartFile[0] == '/' ? h->cfg.restartFile : h->cfg.inputDir + "/" + h->cfg.restartFile;
+            const size_t N = size_t( h->mesh.nCells );
+            std::vector<double> u, lam;
+            read_state_file( base + "_moments", N, h->ldc, u );
+            CK( cudaMemcpyAsync( h->d_u, u.data(), u.size() * sizeof( double ), cudaMemcpyHostToDevice, h->stream ) );
+            if( h->cfg.importDualState ) {
+                read_state_file( base + "_duals", N, h->ldc, lam );
+                CK( cudaMemcpyAsync( h->d_lam, lam.data(), lam.size() * sizeof( double ), cudaMemcpyHostToDevice, h->stream ) );
+                std::vector<unsigned> lv( N, unsigned( h->tab.nLevels - 1 ) );
+                CK( cudaMemcpyAsync( h->d_level, lv.data(), N * sizeof( unsigned ), cudaMemcpyHostToDevice, h->stream ) );
+                CK( cudaStreamSynchronize( h->stream ) );
+                keep = -1;
+            }
+            else {
+                keep = 1;
+            }
+        }
+        if( keep >= 0 ) {
+            void* args[] = {&P, &keep};
+            launch( h, pick( h->cfg.closure, h->group, 2 ), h->auxGrid, h->auxBlock, h->initSmem, args );
+        }
         CK( cudaGetLastError() );
         if( h->d_factorLevel ) reset_factor_store( h );
         reset_control( h, 0.0 );
         h->stateReady = true;
+        return UQC_OK;
+    } );
+}
+
+int uqc_export_state( uqc_solver* h, const char* path_prefix ) {
+    if( !h || !path_prefix ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
+    return guarded_dev( h, [&] {
+        const size_t N = size_t( h->mesh.nCells ), per = h->ldc;
+        std::vector<double> u( N * per ), lam( N * per );
+        CK( cudaMemcpyAsync( u.data(), h->d_u, u.size() * sizeof( double ), cudaMemcpyDeviceToHost, h->stream ) );
+        CK( cudaMemcpyAsync( lam.data(), h->d_lam, lam.size() * sizeof( double ), cudaMemcpyDeviceToHost, h->stream ) );
+        CK( cudaStreamSynchronize( h->stream ) );
+        for( int which = 0; which < 2; ++which ) {
+            const std::string path = std::string( path_prefix ) + ( which == 0 ? "_moments" : "_duals" );
+            FILE* f                = std::fopen( path.c_str(), "w" );
+            if( !f ) throw ConfigError( "cannot write " + path );
+            const std::vector<double>& v = which == 0 ? u : lam;
+            char buf[64];
+            for( size_t j = 0; j < N; ++j ) {
+                std::string line;
+                line.reserve( per * 24 );
+                for( size_t k = 0; k < per; ++k ) {
+                    // std::setprecision(digits10 = 15) in the default float field: %.15g
+                    std::snprintf( buf, sizeof( buf ), "%.15g,", v[j * per + k] );
+                    line += buf;
+                }
+                line += '\n';
+                std::fputs( line.c_str(), f );
+            }
+            if( std::fclose( f ) != 0 ) throw ConfigError( "cannot write " + path );
+        }
         return UQC_OK;
     } );
 }

@@ -133,6 +133,10 @@ class Solver:
         check(self.h, self.lib.uqc_download_state(self.h, ptr(u), ptr(lam), ptr(lev, L._up), layout))
         return u, lam, lev
 
+    def export_state(self, path_prefix: str):
+        """MomentSolver::Export: <prefix>_moments and <prefix>_duals, the reference's restart files."""
+        check(self.h, self.lib.uqc_export_state(self.h, str(path_prefix).encode()))
+
     def set_precision(self, precision: int):
         check(self.h, self.lib.uqc_set_precision(self.h, precision))
 
