@@ -171,6 +171,12 @@ int uqc_run( uqc_solver* h, double t_end, uqc_step_info* info );
 /* Mean and variance per cell and state (MomentSolver::WriteMeanAndVar,
  * momentsolver.cpp:302-328): out[j * 2 nS + s] = E, out[j * 2 nS + nS + s] = Var. */
 int uqc_mean_var( uqc_solver* h, double* out );
+/* Mesh1D::Export / Mesh2D::Export (mesh1d.cpp:90-220, mesh2d.cpp:399-501):
+ * legacy VTK unstructured grid (ASCII) at `path` (".vtk" appended when
+ * missing) with the reference's arrays E(.) and Var(.) per state as cell data
+ * and averaged to the points; 1-D cells are quads extruded to a tenth of the
+ * domain, and <path>ExpectedValue / <path>Variance text columns are written too. */
+int uqc_write_vtk( uqc_solver* h, const char* path );
 
 /* Drop-in for Closure::SolveClosure on caller-owned HOST arrays (the call a
  * GpuClosure adapter makes): n cells of (lambda, u) in `layout`, solved for

@@ -52,3 +52,36 @@ def test_restart_with_other_moment_count_is_refused(tmp_path):
     with pytest.raises(Exception) as e:
         b.init_state()
     assert "moments" in str(e.value)
+
+
+def _read_vtk_fields(path, section):
+    lines = path.read_text(encoding="utf-8").splitlines()
+    i = next(k for k, l in enumerate(lines) if l.startswith(section))
+    n = int(lines[i].split()[1]); nf = int(lines[i + 1].split()[2])
+    k = i + 2; out = {}
+    for _ in range(nf):
+        name, comps, cnt, _t = lines[k].split(); comps, cnt = int(comps), int(cnt)
+        out[name] = np.array([[float(x) for x in lines[k + 1 + r].split()] for r in range(cnt)])
+        k += 1 + cnt
+    return n, out
+
+
+@pytest.mark.parametrize("toml,dim", [(W.burgers1d(ncells=60), 1), (W.euler2d(nx=6, ny=3, degree=2, nquad=4), 2)])
+def test_vtk_output_holds_mean_and_variance(tmp_path, toml, dim):
+    s = Solver(toml); s.init_state(); s.step(2)
+    s.write_vtk(tmp_path / "out")
+    mv = s.mean_var()
+    n, cell = _read_vtk_fields(tmp_path / "out.vtk", "CELL_DATA")
+    assert n == s.n_cells
+    if dim == 1:
+        np.testing.assert_allclose(cell["E(u)"][:, 0], mv[:, 0], rtol=1e-15)
+        np.testing.assert_allclose(cell["Var(u)"][:, 0], mv[:, 1], rtol=1e-15)
+        ev = np.loadtxt(tmp_path / "outExpectedValue")
+        assert ev.shape == (s.n_cells, 2)
+        np.testing.assert_allclose(ev[:, 1], mv[:, 0], rtol=1e-5)
+    else:
+        np.testing.assert_allclose(cell["E(ρ)"][:, 0], mv[:, 0], rtol=1e-15)
+        np.testing.assert_allclose(cell["E(ρU)"][:, :2], mv[:, 1:3], rtol=1e-15)
+        np.testing.assert_allclose(cell["Var(ρE)"][:, 0], mv[:, 7], rtol=1e-15)
+    npts, pt = _read_vtk_fields(tmp_path / "out.vtk", "POINT_DATA")
+    assert npts > 0 and all(v.shape[0] == npts for v in pt.values())

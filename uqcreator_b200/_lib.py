@@ -29,7 +29,7 @@ EXPORTS = [
     "uqc_last_launch_count", "uqc_stream", "uqc_mesh_tri_jitter", "uqc_closure_solve_device_noalloc",
     "uqc_set_option", "uqc_step_async", "uqc_step_query", "uqc_device_bytes", "uqc_server_create",
     "uqc_server_destroy", "uqc_server_last_error", "uqc_server_submit", "uqc_server_progress",
-    "uqc_server_request", "uqc_server_release", "uqc_server_request_error", "uqc_export_state",
+    "uqc_server_request", "uqc_server_release", "uqc_server_request_error", "uqc_export_state", "uqc_write_vtk",
 ]
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
 NOALLOC_MAX_CELLS = 65536
@@ -122,6 +122,7 @@ def lib() -> C.CDLL:
         "uqc_server_release": ([_vp, C.c_longlong], C.c_int),
         "uqc_server_request_error": ([_vp, C.c_longlong], C.c_char_p),
         "uqc_export_state": ([_vp, C.c_char_p], C.c_int),
+        "uqc_write_vtk": ([_vp, C.c_char_p], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

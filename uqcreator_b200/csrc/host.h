@@ -77,6 +77,8 @@ struct Mesh {
     std::vector<double> unitN, scaledN;              // 2 per face
     std::vector<int> nbr;                            // per face; ghost = nCells
     std::vector<int> boundary;                       // Dirichlet cell flag
+    std::vector<double> nodeXY;                      // node coordinates (x, y), for output
+    std::vector<int> cellNodes;                      // nodes per cell (2 in 1-D, 3 for triangles)
 };
 
 Mesh build_mesh_1d( int nCells, double a, double b );

@@ -38,6 +38,13 @@ Mesh build_mesh_1d( int N, double a, double b ) {
         m.nbr[2 * j]        = m.boundary[j] ? N : j - 1;
         m.nbr[2 * j + 1]    = m.boundary[j] ? N : j + 1;
     }
+    m.nodeXY.assign( 2 * size_t( N + 1 ), 0.0 );
+    for( int j = 0; j <= N; ++j ) m.nodeXY[2 * j] = a + j * ( b - a ) / ( N );
+    m.cellNodes.resize( 2 * size_t( N ) );
+    for( int j = 0; j < N; ++j ) {
+        m.cellNodes[2 * j]     = j;
+        m.cellNodes[2 * j + 1] = j + 1;
+    }
     return m;
 }
 
@@ -152,6 +159,8 @@ Mesh build_mesh_tri( int nNodes, const double* xy, const int* bnd, int N, const 
             m.nbr[keys[i + 1].second] = int( keys[i].second / 3 );
             ++i;
         }
+    m.nodeXY.assign( xy, xy + 2 * size_t( nNodes ) );
+    m.cellNodes.assign( tri, tri + 3 * size_t( N ) );
     return m;
 }
 

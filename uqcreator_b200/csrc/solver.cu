@@ -925,6 +925,131 @@ int uqc_init_state( uqc_solver* h ) {
     } );
 }
 
+// Legacy VTK unstructured grid of E and Var per cell, as Mesh1D::Export
+// (mesh1d.cpp:90-220: cells as quads extruded to a tenth of the domain length,
+// plus <file>ExpectedValue / <file>Variance text columns) and Mesh2D::Export
+// (mesh2d.cpp:399-501: triangles) write it with VTK: the same arrays (names
+// of the reference; momentum as a 3-component vector in 2-D), as cell data
+// and averaged to the points (vtkCellDataToPointData with PassCellData).
+int uqc_write_vtk( uqc_solver* h, const char* path ) {
+    if( !h || !path ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
+    return guarded_dev( h, [&] {
+        const Mesh& m = h->mesh;
+        const int N = m.nCells, nS = h->nS;
+        std::vector<double> mv( size_t( N ) * 2 * nS );
+        if( uqc_mean_var( h, mv.data() ) != UQC_OK ) throw CudaError( h->err );
+        // arrays: name, components, per-cell values (E and Var per state; 2-D Euler momentum as vectors)
+        struct Arr {
+            std::string name;
+            int comps;
+            std::vector<int> cols;    // columns of mv (-1: zero)
+        };
+        std::vector<Arr> arrs;
+        const bool euler = h->cfg.closure == CL_EULER2D;
+        const char* names1[] = {"u"};
+        const char* namesSW[] = {"h", "hu"};
+        for( int part = 0; part < 2; ++part ) {
+            const std::string pre = part == 0 ? "E(" : "Var(";
+            const int off         = part * nS;
+            if( euler ) {
+                arrs.push_back( {pre + "ρ)", 1, {off + 0}} );
+                arrs.push_back( {pre + "ρU)", 3, {off + 1, off + 2, -1}} );
+                arrs.push_back( {pre + "ρE)", 1, {off + 3}} );
+            }
+            else {
+                for( int s2 = 0; s2 < nS; ++s2 ) arrs.push_back( {pre + ( nS == 1 ? names1[0] : namesSW[s2] ) + ")", 1, {off + s2}} );
+            }
+        }
+        const std::string file = ( std::string( path ).size() > 4 && std::string( path ).substr( std::string( path ).size() - 4 ) == ".vtk" ) ? path : std::string( path ) + ".vtk";
+        FILE* f = std::fopen( file.c_str(), "w" );
+        if( !f ) throw ConfigError( "cannot write " + file );
+        // points and cells
+        const int nNodes = int( m.nodeXY.size() / 2 );
+        std::vector<std::vector<int>> cells( N );
+        std::vector<double> pts;
+        int cellType;
+        if( m.dim == 1 ) {
+            const double height = ( m.nodeXY[2 * ( nNodes - 1 )] - m.nodeXY[0] ) / 10;
+            pts.resize( 3 * size_t( 2 * nNodes ), 0.0 );
+            for( int i = 0; i < nNodes; ++i ) {
+                pts[3 * i]                = m.nodeXY[2 * i];
+                pts[3 * ( i + nNodes )]     = m.nodeXY[2 * i];
+                pts[3 * ( i + nNodes ) + 1] = height;
+            }
+            for( int j = 0; j < N; ++j ) {
+                const int a = m.cellNodes[2 * j], b = m.cellNodes[2 * j + 1];
+                cells[j]    = {a, a + nNodes, b + nNodes, b};
+            }
+            cellType = 9;    // VTK_QUAD
+        }
+        else {
+            pts.resize( 3 * size_t( nNodes ), 0.0 );
+            for( int i = 0; i < nNodes; ++i ) {
+                pts[3 * i]     = m.nodeXY[2 * i];
+                pts[3 * i + 1] = m.nodeXY[2 * i + 1];
+            }
+            for( int j = 0; j < N; ++j ) cells[j] = {m.cellNodes[3 * j], m.cellNodes[3 * j + 1], m.cellNodes[3 * j + 2]};
+            cellType = 5;    // VTK_TRIANGLE
+        }
+        const int nPts = int( pts.size() / 3 );
+        std::fprintf( f, "# vtk DataFile Version 3.0\nUQCreator B200 mean and variance\nASCII\nDATASET UNSTRUCTURED_GRID\n" );
+        std::fprintf( f, "POINTS %d double\n", nPts );
+        for( int i = 0; i < nPts; ++i ) std::fprintf( f, "%.17g %.17g %.17g\n", pts[3 * i], pts[3 * i + 1], pts[3 * i + 2] );
+        const int per = int( cells[0].size() );
+        std::fprintf( f, "CELLS %d %d\n", N, N * ( per + 1 ) );
+        for( int j = 0; j < N; ++j ) {
+            std::fprintf( f, "%d", per );
+            for( int v : cells[j] ) std::fprintf( f, " %d", v );
+            std::fprintf( f, "\n" );
+        }
+        std::fprintf( f, "CELL_TYPES %d\n", N );
+        for( int j = 0; j < N; ++j ) std::fprintf( f, "%d\n", cellType );
+        auto value = [&]( int j, int col ) { return col < 0 ? 0.0 : mv[size_t( j ) * 2 * nS + col]; };
+        // cell data
+        std::fprintf( f, "CELL_DATA %d\nFIELD FieldData %d\n", N, int( arrs.size() ) );
+        for( const Arr& a : arrs ) {
+            std::fprintf( f, "%s %d %d double\n", a.name.c_str(), a.comps, N );
+            for( int j = 0; j < N; ++j ) {
+                for( int c = 0; c < a.comps; ++c ) std::fprintf( f, c ? " %.17g" : "%.17g", value( j, a.cols[c] ) );
+                std::fprintf( f, "\n" );
+            }
+        }
+        // point data: mean over the cells that share the point
+        std::vector<int> count( nPts, 0 );
+        for( int j = 0; j < N; ++j )
+            for( int v : cells[j] ) ++count[v];
+        std::fprintf( f, "POINT_DATA %d\nFIELD FieldData %d\n", nPts, int( arrs.size() ) );
+        for( const Arr& a : arrs ) {
+            std::vector<double> acc( size_t( nPts ) * a.comps, 0.0 );
+            for( int j = 0; j < N; ++j )
+                for( int v : cells[j] )
+                    for( int c = 0; c < a.comps; ++c ) acc[size_t( v ) * a.comps + c] += value( j, a.cols[c] );
+            std::fprintf( f, "%s %d %d double\n", a.name.c_str(), a.comps, nPts );
+            for( int i = 0; i < nPts; ++i ) {
+                for( int c = 0; c < a.comps; ++c )
+                    std::fprintf( f, c ? " %.17g" : "%.17g", count[i] ? acc[size_t( i ) * a.comps + c] / count[i] : 0.0 );
+                std::fprintf( f, "\n" );
+            }
+        }
+        if( std::fclose( f ) != 0 ) throw ConfigError( "cannot write " + file );
+        if( m.dim == 1 ) {
+            // <file>ExpectedValue / <file>Variance: x, then the states (default stream format)
+            const std::string stem = file.substr( 0, file.size() - 4 );
+            for( int part = 0; part < 2; ++part ) {
+                std::ofstream out( stem + ( part == 0 ? "ExpectedValue" : "Variance" ) );
+                for( int j = 0; j < N; ++j ) {
+                    out << m.center[2 * j];
+                    for( int s2 = 0; s2 < nS; ++s2 ) out << " " << value( j, part * nS + s2 );
+                    out << std::endl;
+                }
+                if( !out ) throw ConfigError( "cannot write " + stem );
+            }
+        }
+        return UQC_OK;
+    } );
+}
+
 int uqc_export_state( uqc_solver* h, const char* path_prefix ) {
     if( !h || !path_prefix ) return UQC_ERR_ARGUMENT;
     if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );

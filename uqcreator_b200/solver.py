@@ -137,6 +137,10 @@ class Solver:
         """MomentSolver::Export: <prefix>_moments and <prefix>_duals, the reference's restart files."""
         check(self.h, self.lib.uqc_export_state(self.h, str(path_prefix).encode()))
 
+    def write_vtk(self, path: str):
+        """Mesh::Export: legacy VTK file of the mean and variance (cell and point data)."""
+        check(self.h, self.lib.uqc_write_vtk(self.h, str(path).encode()))
+
     def set_precision(self, precision: int):
         check(self.h, self.lib.uqc_set_precision(self.h, precision))
 
