@@ -946,6 +946,19 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
         }
         const int nTj    = P.nTLevel[P.level[cell]];
         const double* ua = P.uQ + size_t( cell ) * NS * P.nQ;
+        // the faces' neighbours and normals, once per cell (nFaces <= 3)
+        const double* ub[3];
+        double nu[3][2], ns[3][2];
+#pragma unroll
+        for( int f = 0; f < 3; ++f ) {
+            if( f < P.nFaces ) {
+                ub[f]    = P.uQ + size_t( P.nbr[cell * P.nFaces + f] ) * NS * P.nQ;
+                nu[f][0] = P.unitN[( cell * P.nFaces + f ) * 2];
+                nu[f][1] = P.unitN[( cell * P.nFaces + f ) * 2 + 1];
+                ns[f][0] = P.scaledN[( cell * P.nFaces + f ) * 2];
+                ns[f][1] = P.scaledN[( cell * P.nFaces + f ) * 2 + 1];
+            }
+        }
         for( int k = lane; k < P.nQ; k += 32 ) {
             double a[NS], gsum[NS];
 #pragma unroll
@@ -953,53 +966,40 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
                 a[s]    = ua[s * P.nQ + k];
                 gsum[s] = 0.0;
             }
-            for( int f = 0; f < P.nFaces; ++f ) {
-                const int nb      = P.nbr[cell * P.nFaces + f];
-                const double* ub  = P.uQ + size_t( nb ) * NS * P.nQ;
-                double b[NS], y[NS];
 #pragma unroll
-                for( int s = 0; s < NS; ++s ) b[s] = ub[s * P.nQ + k];
-                Problem<CL>::flux( a, b, P.unitN + ( cell * P.nFaces + f ) * 2, P.scaledN + ( cell * P.nFaces + f ) * 2, y, P.phys );
+            for( int f = 0; f < 3; ++f ) {
+                if( f < P.nFaces ) {
+                    double b[NS], y[NS];
 #pragma unroll
-                for( int s = 0; s < NS; ++s ) gsum[s] += y[s];
+                    for( int s = 0; s < NS; ++s ) b[s] = ub[f][s * P.nQ + k];
+                    Problem<CL>::flux( a, b, nu[f], ns[f], y, P.phys );
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) gsum[s] += y[s];
+                }
             }
 #pragma unroll
             for( int s = 0; s < NS; ++s ) Gs[s * P.nQ + k] = gsum[s];
         }
         __syncwarp();
+        // projection and update: a lane per basis function i, the NS states as
+        // independent chains sharing each table value
         const double c = dt / P.area[cell];
-        const int nOut = NS * nTj;
-        for( int o0 = 0; o0 < nOut; o0 += 64 ) {
-            const int idxA = o0 + lane, idxB = o0 + 32 + lane;
-            const bool okA = idxA < nOut, okB = idxB < nOut;
-            const int sA = okA ? idxA / nTj : 0, iA = okA ? idxA - sA * nTj : 0;
-            const int sB = okB ? idxB / nTj : 0, iB = okB ? idxB - sB * nTj : 0;
-            const double* gA = Gs + sA * P.nQ;
-            const double* gB = Gs + sB * P.nQ;
-            double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
-            int k = 0;
-            for( ; k + 1 < P.nQ; k += 2 ) {
-                const double* r0 = phiWf + size_t( k ) * P.ld;
-                const double* r1 = r0 + P.ld;
-                a0 = fma( gA[k], r0[iA], a0 );
-                a1 = fma( gA[k + 1], r1[iA], a1 );
-                b0 = fma( gB[k], r0[iB], b0 );
-                b1 = fma( gB[k + 1], r1[iB], b1 );
+        for( int i = lane; i < nTj; i += 32 ) {
+            double r[NS];
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) r[s] = 0.0;
+            const double* t = phiWf + i;
+            for( int k = 0; k < P.nQ; ++k, t += P.ld ) {
+                const double w = *t;
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) r[s] = fma( Gs[s * P.nQ + k], w, r[s] );
             }
-            if( k < P.nQ ) {
-                const double* r0 = phiWf + size_t( k ) * P.ld;
-                a0 = fma( gA[k], r0[iA], a0 );
-                b0 = fma( gB[k], r0[iB], b0 );
-            }
-            if( okA ) {
-                double* up = P.u + cell * ldc + sA * P.nT + iA;
-                double nu  = *up - ( a0 + a1 ) * c;
-                *up        = nu;
-                if( idxA == 0 ) res += fabs( nu - P.uOld0[cell] ) * P.area[cell];
-            }
-            if( okB ) {
-                double* up = P.u + cell * ldc + sB * P.nT + iB;
-                *up        = *up - ( b0 + b1 ) * c;
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) {
+                double* up      = P.u + cell * ldc + s * P.nT + i;
+                const double nu0 = *up - r[s] * c;
+                *up             = nu0;
+                if( s == 0 && i == 0 ) res += fabs( nu0 - P.uOld0[cell] ) * P.area[cell];
             }
         }
         __syncwarp();

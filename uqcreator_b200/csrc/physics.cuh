@@ -189,11 +189,11 @@ template <> struct Problem<1> {
         double rhoInv = 1.0 / uq[0], uU = uq[1] * rhoInv, vU = uq[2] * rhoInv;
         double p = ( gm - 1.0 ) * ( uq[3] - 0.5 * uq[0] * ( uU * uU + vU * vU ) );
         double a = sqrt( gm * p * rhoInv );
-        double t0 = fabs( 1.0 / ( vU - a ) ), t1 = fabs( 1.0 / ( vU + a ) );
-        double m1 = t1 < t0 ? t1 : t0;
-        double t2 = fabs( 1.0 / ( uU + a ) ), t3 = fabs( 1.0 / ( uU - a ) );
-        double m2 = t3 < t2 ? t3 : t2;
-        return ( P.cfl / dx ) * ( m2 < m1 ? m2 : m1 );
+        // the minimum of |1 / (v -+ a)| and |1 / (u +- a)| (euler2d.cpp:114-134)
+        // is 1 / the maximum of the four |.|: the rounded reciprocal is
+        // monotone, so both give the same double
+        const double w = fmax( fmax( fabs( vU - a ), fabs( vU + a ) ), fmax( fabs( uU + a ), fabs( uU - a ) ) );
+        return ( P.cfl / dx ) * ( 1.0 / w );
     }
     __device__ static void ic( const double* x, const double* xi, double* y, const PhysParams& P ) {
         double rho, pr;
