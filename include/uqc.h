@@ -91,9 +91,15 @@ typedef struct uqc_step_info {
  * Mesh::Create (mesh.cpp:19-32) + Closure::Create (closure.cpp:94-131) +
  * MomentSolver(settings, mesh, problem) (momentsolver.h:139). cuda_stream may be
  * NULL (the handle creates its own stream). On error *out is NULL and the
- * message is copied to err (when err != NULL). */
+ * message is copied to err (when err != NULL).
+ * Meshes: 1-D uniform ([mesh] numberOfCells, a, b; Mesh1D), SU2 triangle
+ * meshes ([mesh] format = "SU2", SU2MeshFile relative to the file's directory,
+ * SU2BC = [["marker", "dirichlet" | "noslip" | "swwall"], ...];
+ * Mesh2D::LoadSU2MeshFromFile, mesh2d.cpp:5-259; "neumann" and "periodic"
+ * are refused with UQC_ERR_CONFIG), or the seeded "tri_jitter" mesh of the
+ * [uqc] table. */
 int uqc_create_from_file( const char* toml_path, void* cuda_stream, uqc_solver** out, char* err, int err_len );
-/* Same, from TOML text in memory. */
+/* Same, from TOML text in memory; files it names are relative to the working directory. */
 int uqc_create_from_string( const char* toml_text, void* cuda_stream, uqc_solver** out, char* err, int err_len );
 void uqc_destroy( uqc_solver* h );                        /* ~MomentSolver (momentsolver.cpp:32-35) */
 const char* uqc_last_error( const uqc_solver* h );

@@ -46,6 +46,7 @@ def lib():
         L.uqco_create.restype = C.c_int
         L.uqco_create.argtypes = [C.POINTER(Config), C.c_int, _dp, _ip, C.c_int, _ip, C.POINTER(C.c_void_p)]
         L.uqco_destroy.argtypes = [C.c_void_p]
+        L.uqco_set_cell_bc.argtypes = [C.c_void_p, _ip]
         L.uqco_sizes.argtypes = [C.c_void_p, _ip]
         L.uqco_tables.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.uqco_geometry.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _ip, _ip]
@@ -112,6 +113,8 @@ class Oracle:
             bnd = np.ascontiguousarray(mesh2d["node_boundary"], dtype=np.int32)
             tri = np.ascontiguousarray(mesh2d["tri"], dtype=np.int32)
             self.L.uqco_create(C.byref(self.cfg), len(bnd), _p(xy), _p(bnd, _ip), len(tri), _p(tri, _ip), C.byref(h))
+            if mesh2d.get("cell_bc") is not None:    # SU2 boundary types (oracle/su2.py)
+                self.L.uqco_set_cell_bc(h, _p(np.ascontiguousarray(mesh2d["cell_bc"], dtype=np.int32), _ip))
         else:
             self.L.uqco_create(C.byref(self.cfg), 0, None, None, 0, None, C.byref(h))
         self.h = h

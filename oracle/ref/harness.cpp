@@ -76,6 +76,19 @@ struct HarnessMeshBase : public Mesh {
     HarnessMeshBase( Settings* s, unsigned d ) : Mesh( s, d ) {}
     mutable std::map<std::string, Matrix> exported;
     std::vector<Vector> Import() const override { return {}; }
+    // Boundary types of an SU2 mesh, as Mesh2D::LoadSU2MeshFromFile sets them
+    // (mesh2d.cpp:197-214): each boundary cell takes its given type, and its
+    // boundary normal comes from the reference's Cell::UpdateBoundaryNormal
+    // (mesh2d.cpp:342-344).
+    void SetCellTypes( const int* codes ) {
+        static const BoundaryType types[4] = {BoundaryType::NONE, BoundaryType::DIRICHLET, BoundaryType::NOSLIP, BoundaryType::SWWALL};
+        for( unsigned c = 0; c < _cells.size(); ++c ) {
+            if( !_cells[c]->IsBoundaryCell() || codes[c] < 1 || codes[c] > 3 ) continue;
+            _boundaryType[c] = types[codes[c]];
+            _cells[c]->SetBoundaryType( types[codes[c]] );
+            _cells[c]->UpdateBoundaryNormal();
+        }
+    }
     void Export( const Matrix& results, std::string append ) const override { exported[append] = results; }
     Vector GetNodePositionsX() const override {
         Vector x( unsigned( _nodes.size() ) );
@@ -452,6 +465,20 @@ int uqcref_create( const char* toml,
 }
 
 void uqcref_destroy( uqcref* h ) { delete h; }
+
+// Per-cell boundary types of an SU2 mesh (1 Dirichlet, 2 no-slip, 3 shallow-water wall).
+void uqcref_set_cell_bc( uqcref* h, const int* codes ) { h->mesh->SetCellTypes( codes ); }
+
+// Boundary unit normal of each boundary cell (Cell::GetBoundaryUnitNormal), zero elsewhere.
+void uqcref_boundary_normals( uqcref* h, double* out ) {
+    for( unsigned j = 0; j < h->nCells; ++j ) {
+        Cell* c = h->mesh->GetGrid()[j];
+        Vector n( 2, 0.0 );
+        if( c->IsBoundaryCell() && c->GetBoundaryType() != BoundaryType::NONE ) n = c->GetBoundaryUnitNormal();
+        out[2 * j]     = n[0];
+        out[2 * j + 1] = n[1];
+    }
+}
 
 void uqcref_sizes( uqcref* h, int* out ) {
     out[0] = int( h->nCells );

@@ -44,6 +44,8 @@ def _lib(variant: str = "exact") -> C.CDLL:
     lib.uqcref_create.argtypes = [C.c_char_p, C.c_int, C.c_int, _dp, C.c_double, C.c_double, C.c_int, _dp, _ip,
                                   C.c_int, _ip, C.POINTER(C.c_void_p), C.c_char_p, C.c_int]
     lib.uqcref_destroy.argtypes = [C.c_void_p]
+    lib.uqcref_set_cell_bc.argtypes = [C.c_void_p, _ip]
+    lib.uqcref_boundary_normals.argtypes = [C.c_void_p, _dp]
     lib.uqcref_sizes.argtypes = [C.c_void_p, _ip]
     lib.uqcref_tables.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
     lib.uqcref_geometry.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _ip, _ip]
@@ -88,6 +90,8 @@ class RefSolver:
             tri = np.ascontiguousarray(mesh2d["tri"], dtype=np.int32)
             rc = self.lib.uqcref_create(self.toml_path.encode(), PROBLEM_KIND[problem], NEWTON_MODE[newton], _p(prm), bounds[0], bounds[1],
                                         len(bnd), _p(xy), _p(bnd, _ip), len(tri), _p(tri, _ip), C.byref(h), err, 512)
+            if rc == 0 and mesh2d.get("cell_bc") is not None:    # SU2 boundary types (oracle/su2.py)
+                self.lib.uqcref_set_cell_bc(h, _p(np.ascontiguousarray(mesh2d["cell_bc"], dtype=np.int32), _ip))
         else:
             rc = self.lib.uqcref_create(self.toml_path.encode(), PROBLEM_KIND[problem], NEWTON_MODE[newton], _p(prm), bounds[0], bounds[1],
                                         0, None, None, 0, None, C.byref(h), err, 512)
@@ -123,7 +127,10 @@ class RefSolver:
         un = np.zeros((n, n_faces, 2)); sn = np.zeros((n, n_faces, 2))
         nbr = np.zeros((n, n_faces), dtype=np.int32); bnd = np.zeros(n, dtype=np.int32)
         self.lib.uqcref_geometry(self.h, _p(area), _p(maxe), _p(cen), _p(un), _p(sn), _p(nbr, _ip), _p(bnd, _ip))
-        return dict(area=area, max_edge=maxe, center=cen, unit_normal=un, scaled_normal=sn, nbr=nbr, boundary=bnd)
+        bn = np.zeros((n, 2))
+        self.lib.uqcref_boundary_normals(self.h, _p(bn))
+        return dict(area=area, max_edge=maxe, center=cen, unit_normal=un, scaled_normal=sn, nbr=nbr, boundary=bnd,
+                    boundary_normal=bn)
 
     def init_state(self):
         self.lib.uqcref_init_state(self.h)

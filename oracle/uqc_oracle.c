@@ -22,7 +22,8 @@ struct uqco {
     double *phi, *phiWf, *xi, *w;
     /* geometry */
     double *area, *maxEdge, *center, *unitN, *scaledN;
-    int *nbr, *bnd;
+    int *nbr, *bnd; /* bnd: 0 interior, 1 Dirichlet, 2 no-slip wall, 3 shallow-water wall */
+    double* bndN;   /* unit normal of each cell's ghost face (Cell::UpdateBoundaryNormal) */
     double dtFixed; /* TimeSolver dt = area(0) CFL / 12 (timesolver.cpp:4-9) */
     /* state */
     double *u, *lam, *uQ, *uNew, *uOld;
@@ -797,8 +798,19 @@ int uqco_create( const uqco_config* cfg, int n_nodes, const double* xy, const in
     h->lam     = calloc( h->nCells * n, sizeof( double ) );
     h->uNew    = calloc( h->nCells * n, sizeof( double ) );
     h->uOld    = calloc( h->nCells * n, sizeof( double ) );
-    h->uQ      = calloc( (size_t)h->nCells * h->nS * h->nQ, sizeof( double ) );
+    /* + the ghost row uQ[N], zero as in momentsolver.cpp:50 */
+    h->uQ      = calloc( (size_t)( h->nCells + 1 ) * h->nS * h->nQ, sizeof( double ) );
     h->level   = calloc( h->nCells, sizeof( unsigned ) );
+    /* Cell::UpdateBoundaryNormal (cell.cpp:57-68): the unit normal of the face
+       with the largest neighbour id, the first such face on ties */
+    h->bndN = calloc( 2 * (size_t)h->nCells, sizeof( double ) );
+    for( int c = 0; c < h->nCells; ++c ) {
+        int id = 0;
+        for( int f = 1; f < h->nFaces; ++f )
+            if( h->nbr[c * h->nFaces + f] > h->nbr[c * h->nFaces + id] ) id = f;
+        h->bndN[2 * c]     = h->unitN[( c * h->nFaces + id ) * 2];
+        h->bndN[2 * c + 1] = h->unitN[( c * h->nFaces + id ) * 2 + 1];
+    }
     *out       = h;
     return 0;
 }
@@ -807,9 +819,17 @@ void uqco_destroy( uqco* h ) {
     if( !h ) return;
     free( h->idx ); free( h->phi ); free( h->phiWf ); free( h->xi ); free( h->w );
     free( h->area ); free( h->maxEdge ); free( h->center ); free( h->unitN ); free( h->scaledN );
-    free( h->nbr ); free( h->bnd );
+    free( h->nbr ); free( h->bnd ); free( h->bndN );
     free( h->u ); free( h->lam ); free( h->uNew ); free( h->uOld ); free( h->uQ ); free( h->level );
     free( h );
+}
+
+/* Boundary types of an SU2 mesh (Mesh2D::LoadSU2MeshFromFile,
+   mesh2d.cpp:197-214): codes[c] (1 Dirichlet, 2 no-slip, 3 shallow-water
+   wall) replaces the Dirichlet default of each boundary cell. */
+void uqco_set_cell_bc( uqco* h, const int* codes ) {
+    for( int c = 0; c < h->nCells; ++c )
+        if( h->bnd[c] && codes[c] >= 1 && codes[c] <= 3 ) h->bnd[c] = codes[c];
 }
 
 void uqco_sizes( const uqco* h, int* out ) {
@@ -963,10 +983,12 @@ int uqco_step( uqco* h, int n_steps, double* out ) {
         for( int j = 0; j < N; ++j ) {
             double* un      = h->uNew + j * m;
             const double* u = h->u + j * m;
-            if( h->bnd[j] ) {
+            if( h->bnd[j] == 1 ) {
                 memcpy( un, u, sizeof( double ) * m );
                 continue;
             }
+            /* wall cells: ghost states at each node (expliciteuler.cpp:24-58) */
+            const int wall = h->bnd[j] >= 2 && nS == 4;
             int nTj = h->nTLevel[h->level[j]];
             memset( rhs, 0, sizeof( double ) * m );
             for( int f = 0; f < F; ++f ) {
@@ -978,6 +1000,18 @@ int uqco_step( uqco* h, int n_steps, double* out ) {
                     for( int s = 0; s < nS; ++s ) {
                         a[s] = ua[s * nQ + k];
                         b[s] = ub[s * nQ + k];
+                    }
+                    if( wall && nb == N ) {
+                        /* flux G(ghost, ghost) on the cell's ghost faces (:62-66) */
+                        const double* n = h->bndN + 2 * j;
+                        double v0 = a[1] / a[0], v1 = a[2] / a[0];
+                        double vn = n[0] * v0 + n[1] * v1;
+                        double b0 = -( vn * n[0] ) + v0, b1 = -( vn * n[1] ) + v1;
+                        double rho = a[0];
+                        a[1]       = rho * b0;
+                        a[2]       = rho * b1;
+                        if( h->bnd[j] == 2 ) a[3] += rho * 0.5 * ( ( b0 * b0 + b1 * b1 ) - ( v0 * v0 + v1 * v1 ) );
+                        for( int s = 0; s < nS; ++s ) b[s] = a[s];
                     }
                     num_flux( h, a, b, h->unitN + ( j * F + f ) * 2, h->scaledN + ( j * F + f ) * 2, y );
                     for( int s = 0; s < nS; ++s ) G[s * nQ + k] = y[s];

@@ -45,6 +45,7 @@ typedef struct uqco uqco;
 
 int uqco_create( const uqco_config* cfg, int n_nodes, const double* xy, const int* node_boundary, int n_tri, const int* tri, uqco** out );
 void uqco_destroy( uqco* h );
+void uqco_set_cell_bc( uqco* h, const int* codes );
 /* out: n_cells, n_states, n_total, n_q, n_levels, dim_xi, n_faces, nT per level... */
 void uqco_sizes( const uqco* h, int* out );
 void uqco_tables( const uqco* h, double* phi, double* phiWf, double* xi, double* w );

@@ -13,8 +13,13 @@ sources) on small cases of every workload:
   c3_steps.npz       shallow water, adaptive degree 1..9, 30 nodes, 100 cells, 12 steps.
   c5_steps.npz       2-D Euler, 3 uncertainties, degree 4, 8^3 nodes, 6x2x2 mesh, 1 step.
   c2_closure.npz     batched SolveClosure / SolveClosureSafe from the initial state.
+  su2_steps.npz      2-D Euler on the SU2 channel mesh su2_channel.su2 (6x4x2 cells,
+                     leaning right wall; written by workloads.su2_channel(6, 4)):
+                     Dirichlet inlet, no-slip outlet wall, shallow-water walls
+                     top and bottom, 6 steps: u, lambda, t.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every case
+    python tests/golden/make_golden.py su2      # only the named cases
 """
 from __future__ import annotations
 
@@ -26,6 +31,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
+from oracle import su2  # noqa: E402
 from oracle.refharness import RefSolver  # noqa: E402
 from uqcreator_b200 import workloads as W  # noqa: E402
 
@@ -39,20 +45,33 @@ CASES = {
     "c5": dict(toml=W.euler2d_3u(nx=6, ny=2), problem="Euler2D", ic=[0.5, 1.0, 1.0, 0.125, 0.1], bounds=(3, 12),
                newton="guarded"),
 }
-STEPS = {"c1": 25, "c2": 3, "c3": 12, "c5": 1}
+STEPS = {"c1": 25, "c2": 3, "c3": 12, "c5": 1, "su2": 6}
+SU2_FILE = OUT / "su2_channel.su2"
+SU2_BC = [["inlet", "dirichlet"], ["outlet", "noslip"], ["bottom", "swwall"], ["top", "swwall"]]
+CASES["su2"] = dict(toml=W.euler2d_su2("su2_channel.su2", bcs=SU2_BC), problem="Euler2D", ic=[0.7, 1.0, 1.0, 0.125, 0.1],
+                    bounds=(3, 12), newton="guarded")
+
+
+def su2_mesh():
+    return su2.read_su2(str(SU2_FILE), su2.bc_table(SU2_BC))
 
 
 def ref(name, variant="exact", newton=None):
     c = CASES[name]
-    return RefSolver(c["toml"], c["problem"], c["ic"], bounds=c["bounds"], mesh2d=W.mesh_for(c["toml"]),
+    mesh = su2_mesh() if name == "su2" else W.mesh_for(c["toml"])
+    return RefSolver(c["toml"], c["problem"], c["ic"], bounds=c["bounds"], mesh2d=mesh,
                      variant=variant, newton=newton or c["newton"])
 
 
-def main():
-    r = ref("c1")
-    mv, lam15 = r.full_solve()
-    np.savez_compressed(OUT / "c1_solve.npz", mean_var=mv, lambda15=lam15, toml=CASES["c1"]["toml"])
+def main(only=()):
+    SU2_FILE.write_text(W.su2_channel(6, 4))
+    if not only:
+        r = ref("c1")
+        mv, lam15 = r.full_solve()
+        np.savez_compressed(OUT / "c1_solve.npz", mean_var=mv, lambda15=lam15, toml=CASES["c1"]["toml"])
     for name, n in STEPS.items():
+        if only and name not in only:
+            continue
         r = ref(name)
         r.init_state()
         out = r.step(n)
@@ -60,6 +79,8 @@ def main():
         np.savez_compressed(OUT / f"{name}_steps.npz", u=u, lam=lam, level=lev, t=out["t"], dt=out["dt"],
                             residual=out["residual"], steps=n, mean_var=r.mean_var(), toml=CASES[name]["toml"],
                             newton=CASES[name]["newton"])
+    if only:
+        return
     res = {}
     for mode in ("reference", "guarded", "safe"):
         r = ref("c2", newton=mode)
@@ -74,4 +95,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))    # case names (e.g. su2) regenerate only those

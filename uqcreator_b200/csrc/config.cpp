@@ -211,6 +211,31 @@ Config parse_config( const std::string& text ) {
         c.bbPlus  = v->items.at( 1 ).num();
     }
     if( const Value* v = find( d, "uqc", "mesh" ) ) c.meshKind = str( *v, "[uqc] mesh" );
+    if( const Value* v = find( d, "mesh", "format" ) ) {
+        if( str( *v, "[mesh] format" ) != "SU2" ) throw ConfigError( "[mesh2d] Unsupported mesh format! Please set one of the following formats: SU2" );
+        const Value* f = find( d, "mesh", "SU2MeshFile" );
+        if( !f ) throw ConfigError( "[mesh2d] 'SU2MeshFile' not set!" );
+        c.meshKind = "su2";
+        c.su2File  = str( *f, "[mesh] SU2MeshFile" );
+        const Value* b = find( d, "mesh", "SU2BC" );
+        if( !b || b->kind != Value::ARR ) throw ConfigError( "[mesh2d] 'SU2BC' Not set!" );
+        for( const Value& pair : b->items ) {
+            if( pair.kind != Value::ARR || pair.items.size() != 2 ) throw ConfigError( "[mesh] SU2BC entries are [marker, type]" );
+            const std::string tag = str( pair.items[0], "[mesh] SU2BC marker" ), type = str( pair.items[1], "[mesh] SU2BC type" );
+            int code;
+            if( type == "dirichlet" )
+                code = 1;
+            else if( type == "noslip" )
+                code = 2;
+            else if( type == "swwall" )
+                code = 3;
+            else if( type == "neumann" || type == "periodic" )
+                throw ConfigError( "[mesh2d] boundary condition '" + type + "' on '" + tag + "' is not supported on the hot path" );
+            else
+                throw ConfigError( "[mesh2d] Invalid boundary condition on boundary '" + tag + "'!" );
+            c.su2BC.emplace_back( tag, code );
+        }
+    }
     if( const Value* v = find( d, "uqc", "mesh_params" ) ) {
         c.nx     = int( v->items.at( 0 ).num() );
         c.ny     = int( v->items.at( 1 ).num() );
@@ -253,7 +278,8 @@ Config parse_config( const std::string& text ) {
             throw ConfigError( "[mesh1d] Invalid mesh parameters!" );
     }
     else if( c.meshDim == 2 ) {
-        if( c.meshKind != "tri_jitter" || c.nx < 2 || c.ny < 2 ) throw ConfigError( "[uqc] 2-D runs need mesh = \"tri_jitter\" with mesh_params = [nx, ny, jitter, seed], nx, ny >= 2" );
+        if( c.meshKind != "su2" && ( c.meshKind != "tri_jitter" || c.nx < 2 || c.ny < 2 ) )
+            throw ConfigError( "[uqc] 2-D runs need [mesh] format = \"SU2\" or mesh = \"tri_jitter\" with mesh_params = [nx, ny, jitter, seed], nx, ny >= 2" );
     }
     else
         throw ConfigError( "[mesh] 'dimension' must be 1 or 2" );

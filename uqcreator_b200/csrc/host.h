@@ -44,6 +44,8 @@ struct Config {
     std::vector<double> ic;
     double bbMinus = 3.0, bbPlus = 12.0;
     std::string meshKind = "uniform1d";
+    std::string su2File;                                  // [mesh] format = "SU2": SU2MeshFile (mesh2d.cpp:5-59)
+    std::vector<std::pair<std::string, int>> su2BC;       // [mesh] SU2BC: marker -> BC code (1 dirichlet, 2 noslip, 3 swwall)
     int nx = 0, ny = 0;
     double jitter = 0.0;
     uint64_t seed = 0;
@@ -79,10 +81,26 @@ struct Mesh {
     std::vector<int> boundary;                       // Dirichlet cell flag
     std::vector<double> nodeXY;                      // node coordinates (x, y), for output
     std::vector<int> cellNodes;                      // nodes per cell (2 in 1-D, 3 for triangles)
+    std::vector<double> bndNormal;                   // per cell: unit normal of its ghost face (Cell::UpdateBoundaryNormal)
 };
+
+// Boundary codes of Mesh::boundary: 0 interior, 1 Dirichlet (frozen cell),
+// 2 no-slip wall, 3 shallow-water wall (reflecting ghost states,
+// expliciteuler.cpp:25-58).
+enum BoundaryCode { BC_NONE = 0, BC_DIRICHLET = 1, BC_NOSLIP = 2, BC_SWWALL = 3 };
+
+// SU2 mesh (Mesh2D::LoadSU2MeshFromFile, mesh2d.cpp:68-259): triangles only.
+// Builds the mesh and sets each boundary cell's code from the markers.
+Mesh read_su2_mesh( const std::string& path, const std::vector<std::pair<std::string, int>>& bcs );
 
 Mesh build_mesh_1d( int nCells, double a, double b );
 void tri_jitter_nodes( int nx, int ny, double jitter, uint64_t seed, double* xy, int* bnd, int* tri );
+void set_boundary_normals( Mesh& m );
+inline bool mesh_has_walls( const Mesh& m ) {
+    for( int b : m.boundary )
+        if( b >= BC_NOSLIP ) return true;
+    return false;
+}
 Mesh build_mesh_tri( int nNodes, const double* xy, const int* bnd, int nTri, const int* tri );
 
 }    // namespace uqc

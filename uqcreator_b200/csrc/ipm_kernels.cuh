@@ -76,7 +76,8 @@ struct KParams {
     bool tablesInSmem;
     // geometry
     const double *area, *dx, *center, *unitN, *scaledN;
-    const int *nbr, *boundary;
+    const int *nbr, *boundary;    // boundary: 0 interior, 1 Dirichlet, 2 no-slip wall, 3 shallow-water wall
+    const double* bndNormal;      // unit normal of each wall cell's ghost face (null without walls)
     // state
     double *u, *lam, *uQ, *uOld0;
     unsigned* level;
@@ -910,6 +911,25 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
     if( g.r == 0 && dtMin < 1e300 ) atomic_min_pos_double( &P.ctl->dtBits, dtMin );
 }
 
+// Ghost state of a wall cell at one node (expliciteuler.cpp:24-58): the
+// velocity v = (u1, u2) / u0 loses its component along the boundary normal n,
+// Vb = v - (n.v) n; momentum becomes u0 Vb, and on a no-slip wall the energy
+// changes by u0 (|Vb|^2 - |v|^2) / 2. Euler 2-D states only.
+template <int CL> __device__ __forceinline__ void wall_ghost( const double* a, const double* n, bool noslip, double* gh ) {
+    constexpr int NS = Closure<CL>::NS;
+#pragma unroll
+    for( int s = 0; s < NS; ++s ) gh[s] = a[s];
+    if constexpr( NS >= 4 ) {
+        const double v0 = a[1] / a[0], v1 = a[2] / a[0];
+        const double vn = n[0] * v0 + n[1] * v1;
+        const double b0 = -( vn * n[0] ) + v0, b1 = -( vn * n[1] ) + v1;
+        const double rho = a[0];
+        gh[1]            = rho * b0;
+        gh[2]            = rho * b1;
+        if( noslip ) gh[3] += rho * 0.5 * ( ( b0 * b0 + b1 * b1 ) - ( v0 * v0 + v1 * v1 ) );
+    }
+}
+
 // Flux + explicit Euler update (expliciteuler.cpp:17-74), one warp per cell
 // (grid-stride over cells, many warps per SM), and the residual / time
 // control finished by the last CTA. Per node the kinetic fluxes of the cell's
@@ -939,7 +959,8 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
     const size_t ldc = size_t( NS ) * P.nT;
     double res       = 0.0;
     for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
-        if( P.boundary[cell] ) {
+        const int bc = P.boundary[cell];
+        if( bc == 1 ) {
             // Dirichlet cell: uNew = u (expliciteuler.cpp:21-23)
             if( lane == 0 ) res += fabs( P.u[cell * ldc] - P.uOld0[cell] ) * P.area[cell];
             continue;
@@ -949,10 +970,21 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
         // the faces' neighbours and normals, once per cell (nFaces <= 3)
         const double* ub[3];
         double nu[3][2], ns[3][2];
+        bool ghost[3];
+        // wall cells (Euler 2-D): faces without a neighbour see the cell's own
+        // states reflected at the boundary normal (expliciteuler.cpp:24-70)
+        const bool wall = CL == 1 && bc >= 2;
+        double bn[2]    = {0.0, 0.0};
+        if( wall ) {
+            bn[0] = P.bndNormal[2 * cell];
+            bn[1] = P.bndNormal[2 * cell + 1];
+        }
 #pragma unroll
         for( int f = 0; f < 3; ++f ) {
             if( f < P.nFaces ) {
-                ub[f]    = P.uQ + size_t( P.nbr[cell * P.nFaces + f] ) * NS * P.nQ;
+                const int nb = P.nbr[cell * P.nFaces + f];
+                ghost[f]     = wall && nb == P.nCells;
+                ub[f]        = P.uQ + size_t( nb ) * NS * P.nQ;
                 nu[f][0] = P.unitN[( cell * P.nFaces + f ) * 2];
                 nu[f][1] = P.unitN[( cell * P.nFaces + f ) * 2 + 1];
                 ns[f][0] = P.scaledN[( cell * P.nFaces + f ) * 2];
@@ -960,19 +992,24 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
             }
         }
         for( int k = lane; k < P.nQ; k += 32 ) {
-            double a[NS], gsum[NS];
+            double a[NS], gsum[NS], gh[NS];
 #pragma unroll
             for( int s = 0; s < NS; ++s ) {
                 a[s]    = ua[s * P.nQ + k];
                 gsum[s] = 0.0;
             }
+            if( wall ) wall_ghost<CL>( a, bn, bc == 2, gh );
 #pragma unroll
             for( int f = 0; f < 3; ++f ) {
                 if( f < P.nFaces ) {
                     double b[NS], y[NS];
+                    if( ghost[f] )
+                        Problem<CL>::flux( gh, gh, nu[f], ns[f], y, P.phys );
+                    else {
 #pragma unroll
-                    for( int s = 0; s < NS; ++s ) b[s] = ub[f][s * P.nQ + k];
-                    Problem<CL>::flux( a, b, nu[f], ns[f], y, P.phys );
+                        for( int s = 0; s < NS; ++s ) b[s] = ub[f][s * P.nQ + k];
+                        Problem<CL>::flux( a, b, nu[f], ns[f], y, P.phys );
+                    }
 #pragma unroll
                     for( int s = 0; s < NS; ++s ) gsum[s] += y[s];
                 }

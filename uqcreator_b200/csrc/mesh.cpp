@@ -7,6 +7,11 @@
 
 #include "host.h"
 
+#include <cctype>
+#include <fstream>
+#include <map>
+#include <sstream>
+
 namespace uqc {
 
 // Mesh1D + Line (mesh1d.cpp:5-67, line.cpp:3-44): N cells on [a, b], nodes
@@ -161,6 +166,149 @@ Mesh build_mesh_tri( int nNodes, const double* xy, const int* bnd, int N, const 
         }
     m.nodeXY.assign( xy, xy + 2 * size_t( nNodes ) );
     m.cellNodes.assign( tri, tri + 3 * size_t( N ) );
+    return m;
+}
+
+// Cell::UpdateBoundaryNormal (cell.cpp:57-68): the unit normal of the face
+// with the largest neighbour id (the ghost face), first such face on ties.
+void set_boundary_normals( Mesh& m ) {
+    m.bndNormal.assign( 2 * size_t( m.nCells ), 0.0 );
+    for( int c = 0; c < m.nCells; ++c ) {
+        int id = 0;
+        for( int f = 1; f < m.nFaces; ++f )
+            if( m.nbr[size_t( c ) * m.nFaces + f] > m.nbr[size_t( c ) * m.nFaces + id] ) id = f;
+        m.bndNormal[2 * c]     = m.unitN[( size_t( c ) * m.nFaces + id ) * 2];
+        m.bndNormal[2 * c + 1] = m.unitN[( size_t( c ) * m.nFaces + id ) * 2 + 1];
+    }
+}
+
+namespace {
+// Mesh2D::GetTrailingNumber (mesh2d.cpp:261-263): the number from the first digit on.
+unsigned trailing_number( const std::string& line ) {
+    const size_t p = line.find_first_of( "0123456789" );
+    if( p == std::string::npos ) throw ConfigError( "[mesh2d] no number in '" + line + "'" );
+    return unsigned( std::stoul( line.substr( p ) ) );
+}
+}    // namespace
+
+// The reader follows mesh2d.cpp:68-259: NPOIN lines "x y id" (nodes sorted by
+// id), NMARK markers (MARKER_TAG, MARKER_ELEMS with line elements "3 a b";
+// their nodes are boundary nodes), NELEM lines "5 a b c id" (triangles;
+// quadrangles are refused). A triangle with two boundary nodes is a boundary
+// cell; its code is that of the last marker (in file order) holding one of
+// its nodes as the first or second node of an element, scanning the cell's
+// nodes in order (:197-211). Neighbours come from sorted edge keys
+// (O(N log N), instead of the reference's O(N^2) pair search).
+Mesh read_su2_mesh( const std::string& path, const std::vector<std::pair<std::string, int>>& bcs ) {
+    std::ifstream f( path );
+    if( !f ) throw ConfigError( "[mesh2d] File not found: " + path );
+    std::vector<std::string> lines;
+    for( std::string l; std::getline( f, l ); ) {
+        if( !l.empty() && l.back() == '\r' ) l.pop_back();
+        lines.push_back( l );
+    }
+    auto find = [&]( const char* key ) -> size_t {
+        for( size_t i = 0; i < lines.size(); ++i )
+            if( lines[i].find( key ) != std::string::npos ) return i;
+        throw ConfigError( std::string( "[mesh2d] " ) + key + " not found in " + path );
+    };
+    if( trailing_number( lines[find( "NDIME" )] ) != 2 ) throw ConfigError( "[mesh2d] NDIME must be 2" );
+    // nodes
+    size_t at           = find( "NPOIN" );
+    const unsigned nPts = trailing_number( lines[at] );
+    std::vector<std::pair<unsigned, std::pair<double, double>>> pts( nPts );
+    for( unsigned i = 0; i < nPts; ++i ) {
+        if( at + 1 + i >= lines.size() ) throw ConfigError( "[mesh2d] truncated NPOIN section" );
+        std::stringstream ss( lines[at + 1 + i] );
+        double x = 0, y = 0;
+        unsigned id = i;
+        ss >> x >> y;
+        if( !( ss >> id ) ) id = i;
+        pts[i] = {id, {x, y}};
+    }
+    std::sort( pts.begin(), pts.end(), []( const auto& a, const auto& b ) { return a.first < b.first; } );
+    std::map<unsigned, int> index;
+    std::vector<double> xy( 2 * size_t( nPts ) );
+    for( unsigned i = 0; i < nPts; ++i ) {
+        index[pts[i].first] = int( i );
+        xy[2 * i]           = pts[i].second.first;
+        xy[2 * i + 1]       = pts[i].second.second;
+    }
+    auto node = [&]( unsigned id ) {
+        auto it = index.find( id );
+        if( it == index.end() ) throw ConfigError( "[mesh2d] unknown node id " + std::to_string( id ) );
+        return it->second;
+    };
+    // markers
+    std::vector<int> bnd( nPts, 0 );
+    struct Marker {
+        int code;
+        std::vector<std::pair<int, int>> elems;
+    };
+    std::vector<Marker> markers;
+    at                  = find( "NMARK" );
+    const unsigned nMrk = trailing_number( lines[at] );
+    size_t k            = at + 1;
+    for( unsigned m = 0; m < nMrk; ++m ) {
+        std::string tag;
+        Marker mk{0, {}};
+        for( int part = 0; part < 2; ++part, ++k ) {
+            if( k >= lines.size() ) throw ConfigError( "[mesh2d] truncated NMARK section" );
+            const std::string& l = lines[k];
+            if( l.find( "MARKER_TAG" ) != std::string::npos ) {
+                tag = l.substr( l.find( '=' ) + 1 );
+                tag.erase( std::remove_if( tag.begin(), tag.end(), ::isspace ), tag.end() );
+            }
+            else if( l.find( "MARKER_ELEMS" ) != std::string::npos ) {
+                const unsigned ne = trailing_number( l );
+                for( unsigned e = 0; e < ne; ++e ) {
+                    std::stringstream ss( lines.at( k + 1 + e ) );
+                    unsigned type = 0, a = 0, b = 0;
+                    ss >> type >> a >> b;
+                    const int ia = node( a ), ib = node( b );
+                    bnd[ia] = bnd[ib] = 1;
+                    mk.elems.emplace_back( ia, ib );
+                }
+                k += ne;
+            }
+            else {
+                throw ConfigError( "[mesh2d] expected MARKER_TAG / MARKER_ELEMS at line " + std::to_string( k + 1 ) );
+            }
+        }
+        for( const auto& b : bcs )
+            if( b.first == tag ) mk.code = b.second;
+        if( mk.code == 0 ) throw ConfigError( "[mesh2d] no SU2BC entry for marker '" + tag + "'" );
+        markers.push_back( std::move( mk ) );
+    }
+    // cells
+    at                  = find( "NELEM" );
+    const unsigned nEl  = trailing_number( lines[at] );
+    std::vector<int> tri( 3 * size_t( nEl ) );
+    for( unsigned c = 0; c < nEl; ++c ) {
+        std::stringstream ss( lines.at( at + 1 + c ) );
+        unsigned type = 0, a = 0, b = 0, d = 0;
+        ss >> type;
+        if( type != 5 ) throw ConfigError( "[mesh2d] element type " + std::to_string( type ) + " is not supported (triangles only)" );
+        ss >> a >> b >> d;
+        unsigned id = c;
+        if( ( ss >> id ) && id != c ) throw ConfigError( "[mesh2d] element " + std::to_string( c ) + " carries id " + std::to_string( id ) + "; ids must follow file order" );
+        tri[3 * c]     = node( a );
+        tri[3 * c + 1] = node( b );
+        tri[3 * c + 2] = node( d );
+    }
+    Mesh m = build_mesh_tri( int( nPts ), xy.data(), bnd.data(), int( nEl ), tri.data() );
+    for( int c = 0; c < m.nCells; ++c ) {
+        if( !m.boundary[c] ) continue;
+        int code = BC_DIRICHLET;
+        for( int v = 0; v < 3; ++v ) {
+            const int nid = tri[3 * c + v];
+            for( const Marker& mk : markers )
+                for( const auto& e : mk.elems )
+                    if( e.first == nid || e.second == nid ) code = mk.code;
+        }
+        m.boundary[c] = code;
+    }
+    set_boundary_normals( m );
     return m;
 }
 

@@ -45,6 +45,7 @@ struct uqc_solver {
     double *d_phi = nullptr, *d_phiWf = nullptr, *d_xi = nullptr;
     double *d_area = nullptr, *d_dx = nullptr, *d_center = nullptr, *d_unitN = nullptr, *d_scaledN = nullptr;
     int *d_nbr = nullptr, *d_boundary = nullptr;
+    double* d_bndNormal = nullptr;    // wall meshes only
     double *d_u = nullptr, *d_lam = nullptr, *d_uQ = nullptr, *d_uOld0 = nullptr, *d_blockPartial = nullptr;
     unsigned* d_level = nullptr;
     int *d_status = nullptr, *d_iters = nullptr;
@@ -191,6 +192,7 @@ KParams make_params( const uqc_solver* h ) {
     P.scaledN      = h->d_scaledN;
     P.nbr          = h->d_nbr;
     P.boundary     = h->d_boundary;
+    P.bndNormal    = h->d_bndNormal;
     P.u            = h->d_u;
     P.lam          = h->d_lam;
     P.uQ           = h->d_uQ;
@@ -429,14 +431,19 @@ void read_control( uqc_solver* h ) {
     CK( cudaStreamSynchronize( h->stream ) );
 }
 
-void build( uqc_solver* h, const std::string& text, void* stream ) {
-    h->cfg = parse_config( text );
+void build( uqc_solver* h, const std::string& text, void* stream, const std::string& inputDir ) {
+    h->cfg          = parse_config( text );
+    h->cfg.inputDir = inputDir;
     h->tab = build_tables( h->cfg );
     h->nS  = h->cfg.closure == CL_BOUNDED_BARRIER ? 1 : ( h->cfg.closure == CL_EULER2D ? 4 : 2 );
     h->ld  = ( h->tab.nT % 2 ) ? h->tab.nT : h->tab.nT + 1;    // odd row stride: conflict-free column reads
     h->ldc = size_t( h->nS ) * h->tab.nT;
     if( h->cfg.meshDim == 1 )
         h->mesh = build_mesh_1d( h->cfg.nCells1d, h->cfg.a, h->cfg.b );
+    else if( h->cfg.meshKind == "su2" ) {
+        const std::string& f = h->cfg.su2File;
+        h->mesh              = read_su2_mesh( f[0] == '/' ? f : h->cfg.inputDir + "/" + f, h->cfg.su2BC );
+    }
     else {
         int nn = ( h->cfg.nx + 1 ) * ( h->cfg.ny + 1 ), nt = 2 * h->cfg.nx * h->cfg.ny;
         std::vector<double> xy( 2 * size_t( nn ) );
@@ -496,6 +503,7 @@ void ensure_device( uqc_solver* h ) {
     h->d_scaledN  = dupload( m.scaledN );
     h->d_nbr      = dupload( m.nbr );
     h->d_boundary = dupload( m.boundary );
+    if( mesh_has_walls( m ) ) h->d_bndNormal = dupload( m.bndNormal );
     const size_t N = size_t( m.nCells );
     h->d_u         = dalloc<double>( N * h->ldc );
     h->d_lam       = dalloc<double>( N * h->ldc );
@@ -523,7 +531,7 @@ void release( uqc_solver* h ) {
     h->graphs.clear();
     for( void* p : {(void*)h->d_phi, (void*)h->d_phiWf, (void*)h->d_xi, (void*)h->d_wt, (void*)h->d_area, (void*)h->d_dx, (void*)h->d_center,
                     (void*)h->d_unitN, (void*)h->d_scaledN, (void*)h->d_nbr, (void*)h->d_boundary, (void*)h->d_u, (void*)h->d_lam,
-                    (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
+                    (void*)h->d_bndNormal, (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
                     (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
                     (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_phiF, (void*)h->d_fallbackList,
                     (void*)h->d_factorStore, (void*)h->d_factorLevel} )
@@ -668,7 +676,7 @@ unsigned long long device_bytes_of( const uqc_solver* h ) {
     const unsigned long long tab = ( (unsigned long long)h->tab.nQ * h->ld + 8 ) * ( 8 + 8 + 4 ) + h->tab.xi.size() * 8 + h->tab.nQ * 8;
     const unsigned long long d8  = N * ( 2 * ldc + 1 + 1 + 2 + 4 * F ) + ( N + 1 ) * sq;    // state, uQ, geometry (doubles)
     const unsigned long long d4  = N * ( F + 1 + 1 + 1 + 1 + 1 + 1 );                         // nbr, boundary, level, status, iters, lists
-    return tab + 8 * d8 + 4 * d4 + sizeof( Control ) + 8 * 4096 + ( h->precision == UQC_MIXED && h->chord ? factor_store_bytes( h ) : 0 );
+    return tab + 8 * d8 + 4 * d4 + ( mesh_has_walls( h->mesh ) ? 16 * N : 0 ) + sizeof( Control ) + 8 * 4096 + ( h->precision == UQC_MIXED && h->chord ? factor_store_bytes( h ) : 0 );
 }
 
 void to_layout( const uqc_solver* h, const double* src, double* dst, int layout, bool toDevice ) {
@@ -688,16 +696,15 @@ void to_layout( const uqc_solver* h, const double* src, double* dst, int layout,
 
 }    // namespace
 
-// ========================================================================== C ABI
-
-extern "C" {
-
-int uqc_create_from_string( const char* toml_text, void* cuda_stream, uqc_solver** out, char* err, int err_len ) {
-    if( !out || !toml_text ) return UQC_ERR_ARGUMENT;
+namespace {
+// Files a config names (SU2MeshFile, restartFile) are relative to inputDir:
+// the config file's directory (Settings::_inputDir, settings.cpp:30), or the
+// working directory for a config given as text.
+int create_impl( const char* toml_text, const std::string& inputDir, void* cuda_stream, uqc_solver** out, char* err, int err_len ) {
     *out           = nullptr;
     uqc_solver* h  = new uqc_solver();
     int rc         = guarded( h, [&] {
-        build( h, toml_text, cuda_stream );
+        build( h, toml_text, cuda_stream, inputDir );
         return UQC_OK;
     } );
     if( rc != UQC_OK ) {
@@ -712,6 +719,17 @@ int uqc_create_from_string( const char* toml_text, void* cuda_stream, uqc_solver
     *out = h;
     return UQC_OK;
 }
+}    // namespace
+
+// ========================================================================== C ABI
+
+extern "C" {
+
+
+int uqc_create_from_string( const char* toml_text, void* cuda_stream, uqc_solver** out, char* err, int err_len ) {
+    if( !out || !toml_text ) return UQC_ERR_ARGUMENT;
+    return create_impl( toml_text, ".", cuda_stream, out, err, err_len );
+}
 
 int uqc_create_from_file( const char* toml_path, void* cuda_stream, uqc_solver** out, char* err, int err_len ) {
     if( !toml_path || !out ) return UQC_ERR_ARGUMENT;
@@ -722,13 +740,9 @@ int uqc_create_from_file( const char* toml_path, void* cuda_stream, uqc_solver**
     }
     std::stringstream ss;
     ss << f.rdbuf();
-    const int rc = uqc_create_from_string( ss.str().c_str(), cuda_stream, out, err, err_len );
-    if( rc == UQC_OK ) {
-        const std::string path = toml_path;
-        const size_t slash     = path.find_last_of( '/' );
-        ( *out )->cfg.inputDir = slash == std::string::npos ? "." : path.substr( 0, slash );
-    }
-    return rc;
+    const std::string path = toml_path;
+    const size_t slash     = path.find_last_of( '/' );
+    return create_impl( ss.str().c_str(), slash == std::string::npos ? "." : path.substr( 0, slash ), cuda_stream, out, err, err_len );
 }
 
 void uqc_destroy( uqc_solver* h ) {

@@ -74,7 +74,10 @@ class Solver:
         h = C.c_void_p()
         err = C.create_string_buffer(1024)
         s = None if stream is None else C.c_void_p(int(stream))
-        rc = self.lib.uqc_create_from_string(settings.text.encode(), s, C.byref(h), err, 1024)
+        if settings.path is not None:    # files the config names are relative to its directory
+            rc = self.lib.uqc_create_from_file(os.fsencode(settings.path), s, C.byref(h), err, 1024)
+        else:
+            rc = self.lib.uqc_create_from_string(settings.text.encode(), s, C.byref(h), err, 1024)
         if rc != 0:
             raise UqcError(rc, err.value.decode())
         self.h = h

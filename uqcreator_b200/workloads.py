@@ -33,7 +33,7 @@ numberOfCells = {ncells}
 a = {a}
 b = {b}
 outputFile = "{name}"
-
+{mesh_extra}
 [problem]
 timestepping = "explicitEuler"
 distribution = [[{dists}],[{sigmas}]]
@@ -61,7 +61,7 @@ steps = {steps}
 def make_toml(*, name, problem, closure, dim, ncells=0, a=0.0, b=1.0, sigmas, cfl, tend, degrees,
               nquad, ic, bounds=(3.0, 12.0), mesh="uniform1d", mesh_params=(0, 0, 0.0, 0),
               maxit=1000, eps=1e-10, degtype="totalDegree", precision="fp64", gamma=None,
-              newton="reference", steps=0) -> str:
+              newton="reference", steps=0, mesh_extra="") -> str:
     degrees = list(degrees)
     quads = [nquad] * len(degrees)
     extra = f"gamma = {gamma!r}\n" if gamma is not None else ""
@@ -73,7 +73,7 @@ def make_toml(*, name, problem, closure, dim, ncells=0, a=0.0, b=1.0, sigmas, cf
         maxit=int(maxit), eps=repr(float(eps)), ic=",".join(repr(float(v)) for v in ic),
         bounds=",".join(repr(float(v)) for v in bounds), mesh=mesh,
         mesh_params=",".join(repr(v) if isinstance(v, float) else str(v) for v in mesh_params),
-        precision=precision, newton=newton, steps=int(steps))
+        precision=precision, newton=newton, steps=int(steps), mesh_extra=mesh_extra)
 
 
 def burgers1d(ncells=500, tend=0.11, degree=4, nquad=20, eps=1e-10, x0=0.5, **kw) -> str:
@@ -207,6 +207,50 @@ def tri_jitter_mesh(nx: int, ny: int, jitter: float = 0.2, seed: int = 7) -> dic
     t1 = np.where(flip[:, None], np.stack([b, c, d], 1), np.stack([a, c, d], 1))
     tri = np.stack([t0, t1], axis=1).reshape(-1, 3).astype(np.int32)
     return dict(xy=xy, node_boundary=bnd, tri=tri)
+
+
+def su2_channel(nx: int, ny: int, jitter: float = 0.2, seed: int = 7, slant: float = 0.25, shuffle: int = 5) -> str:
+    """SU2 text (the format Mesh2D::LoadSU2MeshFromFile reads, mesh2d.cpp:68-259)
+    of the tri_jitter mesh mapped to a channel whose right wall leans,
+    x' = x (1 + slant y). Markers "inlet" (x = 0), "outlet" (the leaning
+    wall), "bottom", "top" as line elements "3 a b". Node lines carry their
+    ids in a seeded shuffled order (the reader sorts them)."""
+    import numpy as np
+    m = tri_jitter_mesh(nx, ny, jitter, seed)
+    xy = m["xy"].copy()
+    xy[:, 0] = xy[:, 0] * (1.0 + slant * xy[:, 1])
+    tri = m["tri"]
+    node = lambda i, j: j * (nx + 1) + i
+    out = ["% channel with a leaning right wall", "NDIME= 2", f"NELEM= {len(tri)}"]
+    out += [f"5 {a} {b} {c} {e}" for e, (a, b, c) in enumerate(tri)]
+    order = np.random.default_rng(shuffle).permutation(len(xy)) if shuffle else np.arange(len(xy))
+    out.append(f"NPOIN= {len(xy)}")
+    out += [f"{float(xy[n, 0])!r} {float(xy[n, 1])!r} {n}" for n in order]
+    markers = {
+        "inlet": [(node(0, j), node(0, j + 1)) for j in range(ny)],
+        "outlet": [(node(nx, j), node(nx, j + 1)) for j in range(ny)],
+        "bottom": [(node(i, 0), node(i + 1, 0)) for i in range(nx)],
+        "top": [(node(i, ny), node(i + 1, ny)) for i in range(nx)],
+    }
+    out.append(f"NMARK= {len(markers)}")
+    for tag, elems in markers.items():
+        out += [f"MARKER_TAG= {tag}", f"MARKER_ELEMS= {len(elems)}"]
+        out += [f"3 {a} {b}" for a, b in elems]
+    return "\n".join(out) + "\n"
+
+
+def euler2d_su2(mesh_file: str, bcs=(("inlet", "dirichlet"), ("outlet", "noslip"), ("bottom", "swwall"), ("top", "swwall")),
+                degree=5, nquad=10, dim_xi=2, tend=0.2, cfl=0.5, eps=1e-10, newton="guarded", xs=0.7, **kw) -> str:
+    """2-D Euler (the euler2d problem) on an SU2 mesh: [mesh] format = "SU2",
+    SU2MeshFile (relative to the config's directory) and SU2BC markers
+    (mesh2d.cpp:21-56). Walls reflect the flow through ghost states
+    (expliciteuler.cpp:24-70)."""
+    sig = [0.05, 0.1, 0.1][:dim_xi]
+    bc = ", ".join(f'["{t}", "{k}"]' for t, k in bcs)
+    extra = f'format = "SU2"\nSU2MeshFile = "{mesh_file}"\nSU2BC = [{bc}]\n'
+    return make_toml(name="euler2d_su2", problem="Euler2D", closure="Euler2D", dim=2, ncells=0, sigmas=sig, cfl=cfl,
+                     tend=tend, degrees=[degree], nquad=nquad, ic=[xs, 1.0, 1.0, 0.125, 0.1], eps=eps, gamma=1.4,
+                     newton=newton, mesh_extra=extra, **kw)
 
 
 def mesh_for(toml_text: str):
