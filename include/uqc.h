@@ -287,7 +287,11 @@ int uqc_server_release( uqc_server* s, long long id );
 /* Device time (ms) of the kernels of the last uqc_step call, by phase:
  * [0] closure + reconstruction, [1] flux + update, [2] total. */
 int uqc_last_timing( uqc_solver* h, float* ms3 );
-/* Device pointers of the resident state (for zero-copy callers): u, lambda. */
+/* Device pointers of the resident state (for zero-copy callers): u, lambda.
+ * Between steps u holds the updated moments (as the reference's u after
+ * ExplicitEuler::Advance). A caller that writes through the pointers calls
+ * this function again after writing (it makes the next step test every cell
+ * for convergence instead of the list the last update prepared). */
 int uqc_device_state( uqc_solver* h, double** d_u, double** d_lambda );
 /* Number of kernel launches issued by the last uqc_step / uqc_solve_closure. */
 int uqc_last_launch_count( uqc_solver* h );

@@ -146,3 +146,28 @@ def test_autotune_picks_a_valid_shape_and_keeps_results(tmp_path):
     assert (err <= 1e-10).all(), err
     s2 = Solver(toml); s2.init_state()
     assert autotune(s2, cache=tmp_path / "tune.json")["cached"]
+
+
+@pytest.mark.parametrize("toml,steps", [
+    (W.euler2d(nx=24, ny=8), 6),
+    (W.shallow_water1d(ncells=400), 12),
+    (W.burgers1d(ncells=300), 20),
+])
+def test_update_side_convergence_test_matches_check_kernel(toml, steps):
+    """k_update's test of the next step's convergence (cells that pass keep
+    their moments and skip the closure) against k_check testing every cell:
+    the same Newton work and the same results up to rounding of the
+    re-projection."""
+    a = Solver(toml); a.init_state()
+    b = Solver(toml); b.init_state()
+    b.set_option("update_test", 0)
+    ia = a.step(steps)
+    ib = b.step(steps)
+    assert ia["newton_iterations"] == ib["newton_iterations"]
+    assert ia["failed_cells"] == ib["failed_cells"] == 0
+    ua, la, va = a.download_state()
+    ub, lb, vb = b.download_state()
+    np.testing.assert_array_equal(va, vb)
+    np.testing.assert_allclose(ua, ub, rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(la, lb, rtol=1e-10, atol=1e-12)
+    assert abs(ia["t"] - ib["t"]) <= 1e-14 * ib["t"]

@@ -54,7 +54,9 @@ struct Control {
     int failedCells;
     int activeCells;      // cells with Newton iterations in the running step
     int activeCellsLast;  // ... in the last finished step
-    unsigned int nActive; // length of the active-cell list of the running step
+    unsigned int nActive[2];      // lengths of the two active-cell lists (step parity)
+    int listReady;                // k_update built the running step's list: k_check has nothing to do
+    unsigned long long dtBitsNext;    // min dt of the cells k_update finished for the next step
     unsigned long long newtonIters, lineSearchTrials;
     unsigned long long fallbackCells;    // mixed form: cells handed to the FP64 form
 };
@@ -80,12 +82,16 @@ struct KParams {
     const double* bndNormal;      // unit normal of each wall cell's ghost face (null without walls)
     // state
     double *u, *lam, *uQ, *uOld0;
+    double* uRe;              // step mode: the moments re-projected by the closure epilogue (k_update's input)
     unsigned* level;
     const unsigned* nTotalCell;  // closure-only calls: moments per cell (else from level)
     int *status, *iters;
     double* blockPartial;     // one per CTA of k_update
-    int* activeList;          // step mode: cells that need Newton (filled by k_check), or null
+    int* activeList;          // step mode: cells that need Newton (filled by k_check / k_update), or null
     unsigned* activeCount;
+    int listParity;           // step mode: two lists of nCells, the running step's is (ctl->steps & 1)
+    int finishInUpdate;       // k_update tests the next step's convergence and fills the other list
+    double* cellDt;           // per cell: the CFL step of its nodal states (written by the epilogue)
     unsigned* workCounter;    // work-stealing counter of k_closure (in ctl)
     float* factorStore;       // mixed form, step mode: each cell's last FP32 factor (or null)
     int* factorLevel;         // ... nTj it was formed for, -1 none
@@ -639,7 +645,7 @@ __device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const do
     for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
         int s = idx / P.nT, i = idx - s * P.nT;
         // ugs: the same sums kept from the gradient test (i < nTj), when the caller has them
-        P.u[cell * ldc + idx] = i < nTn ? ( ugs && i < nTj ? ugs[idx] : node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) ) : 0.0;
+        P.uRe[cell * ldc + idx] = i < nTn ? ( ugs && i < nTj ? ugs[idx] : node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) ) : 0.0;
     }
     // [F] the cell's time step (min over its nodes)
     double dloc = 1e300;
@@ -650,7 +656,21 @@ __device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const do
         double d = Problem<CL>::dt( uqk, P.dx[cell], P.phys );
         dloc     = d < dloc ? d : dloc;
     }
-    return group_min<GROUP>( g, dloc, red );
+    dloc = group_min<GROUP>( g, dloc, red );
+    if( g.r == 0 && P.cellDt ) P.cellDt[cell] = dloc;
+    return dloc;
+}
+
+// The active-cell list of the running step (step mode: one of two, by step
+// parity; k_update fills the other one for the next step).
+__device__ __forceinline__ void step_list( const KParams& P, int ahead, int*& list, unsigned*& count ) {
+    list  = P.activeList;
+    count = P.activeCount;
+    if( P.listParity && list ) {
+        const int par = ( P.ctl->steps + ahead ) & 1;
+        list += size_t( par ) * P.nCells;
+        count += par;
+    }
 }
 
 __device__ __forceinline__ void atomic_min_pos_double( unsigned long long* addr, double v ) {
@@ -708,8 +728,11 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
     unsigned long long itSum = 0, lsSum = 0;
     int failSum = 0, activeSum = 0, fbSum = 0;
     double dtMin = 1e300;
-    // work items: all cells, or the cells k_check found unconverged
-    const int nWork = P.activeList ? int( *P.activeCount ) : P.nCells;
+    // work items: all cells, or the cells k_check / k_update found unconverged
+    int* alist;
+    unsigned* acount;
+    step_list( P, 0, alist, acount );
+    const int nWork = alist ? int( *acount ) : P.nCells;
     for( ;; ) {
         int item;
         if( g.r == 0 ) bc[0] = double( atomicAdd( P.workCounter, 1u ) );
@@ -717,7 +740,7 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
         item = int( bc[0] );
         g.sync();
         if( item >= nWork ) break;
-        const int cell = P.activeList ? P.activeList[item] : item;
+        const int cell = alist ? alist[item] : item;
         const int lev = P.level ? int( P.level[cell] ) : P.nLevels - 1;
         const int nTj = P.nTotalCell ? int( P.nTotalCell[cell] ) : P.nTLevel[lev];
         // load duals and moments (state-major, finest stride), checking finiteness on the way
@@ -829,7 +852,10 @@ __host__ __device__ inline size_t check_ws_doubles( int nS, int nT, int nQ ) {
 template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) {
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
-    if( !P.ctl->active ) return;
+    if( !P.ctl->active || P.ctl->listReady ) return;
+    int* alist;
+    unsigned* acount;
+    step_list( P, 0, alist, acount );
     Grp<32> g{int( threadIdx.x & 31 ), 0};
     const int warp = threadIdx.x >> 5, nWarps = blockDim.x >> 5;
     const double *phi = P.phi, *phiWf = P.phiWf;
@@ -903,7 +929,7 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
             CT_END( tep, 19, g.r == 0 );
         }
         else if( g.r == 0 ) {
-            P.activeList[atomicAdd( P.activeCount, 1u )] = cell;
+            alist[atomicAdd( acount, 1u )] = cell;
         }
         __syncwarp();
         CT_END( tcell, 20, g.r == 0 );
@@ -928,6 +954,30 @@ template <int CL> __device__ __forceinline__ void wall_ghost( const double* a, c
         gh[2]            = rho * b1;
         if( noslip ) gh[3] += rho * 0.5 * ( ( b0 * b0 + b1 * b1 ) - ( v0 * v0 + v1 * v1 ) );
     }
+}
+
+// rhs(s, i) = sum_k Gs(s, k) phiWf(k, i) for one i (t = phiWf + i), the NS
+// states as independent chains sharing each table value.
+template <int NS>
+__device__ __forceinline__ void project_lane( const double* Gs, const double* t, int ld, int nQ, double* r ) {
+#pragma unroll
+    for( int s = 0; s < NS; ++s ) r[s] = 0.0;
+    for( int k = 0; k < nQ; ++k, t += ld ) {
+        const double w = *t;
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) r[s] = fma( Gs[s * nQ + k], w, r[s] );
+    }
+}
+
+// A cell whose next closure test k_update found passed: it keeps its duals,
+// nodal states, moments and level; the next step sees it converged with no
+// iterations, its residual reference is u_new(0, 0) and its dt the stored one.
+__device__ __forceinline__ void finish_cell( const KParams& P, int cell, double u00, double& dtNext ) {
+    P.uOld0[cell]  = u00;
+    P.status[cell] = UQC_CELL_CONVERGED;
+    P.iters[cell]  = 0;
+    const double d = P.cellDt[cell];
+    dtNext         = d < dtNext ? d : dtNext;
 }
 
 // Flux + explicit Euler update (expliciteuler.cpp:17-74), one warp per cell
@@ -958,11 +1008,28 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
     const double dt  = __longlong_as_double( (long long)P.ctl->dtBits );
     const size_t ldc = size_t( NS ) * P.nT;
     double res       = 0.0;
+    double dtNext    = 1e300;    // lane 0: min dt of the cells finished for the next step
+    int* nlist       = nullptr;
+    unsigned* ncount = nullptr;
+    if( P.finishInUpdate ) step_list( P, 1, nlist, ncount );
     for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
         const int bc = P.boundary[cell];
         if( bc == 1 ) {
             // Dirichlet cell: uNew = u (expliciteuler.cpp:21-23)
-            if( lane == 0 ) res += fabs( P.u[cell * ldc] - P.uOld0[cell] ) * P.area[cell];
+            for( int idx = lane; idx < int( ldc ); idx += 32 ) P.u[cell * ldc + idx] = P.uRe[cell * ldc + idx];
+            if( lane == 0 ) {
+                const double u0 = P.uRe[cell * ldc];
+                res += fabs( u0 - P.uOld0[cell] ) * P.area[cell];
+                if( P.finishInUpdate ) {
+                    // its moments are the re-projected ones: the next closure
+                    // test passes; with refinement levels the closure kernel
+                    // still runs it for the level update
+                    if( P.nLevels > 1 )
+                        nlist[atomicAdd( ncount, 1u )] = cell;
+                    else
+                        finish_cell( P, cell, u0, dtNext );
+                }
+            }
             continue;
         }
         const int nTj    = P.nTLevel[P.level[cell]];
@@ -1021,26 +1088,58 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
         // projection and update: a lane per basis function i, the NS states as
         // independent chains sharing each table value
         const double c = dt / P.area[cell];
-        for( int i = lane; i < nTj; i += 32 ) {
+        double sq      = 0.0;
+        for( int i = lane; i < P.nT; i += 32 ) {
             double r[NS];
+            if( i < nTj )
+                project_lane<NS>( Gs, phiWf + i, P.ld, P.nQ, r );
+            else {
 #pragma unroll
-            for( int s = 0; s < NS; ++s ) r[s] = 0.0;
-            const double* t = phiWf + i;
-            for( int k = 0; k < P.nQ; ++k, t += P.ld ) {
-                const double w = *t;
-#pragma unroll
-                for( int s = 0; s < NS; ++s ) r[s] = fma( Gs[s * P.nQ + k], w, r[s] );
+                for( int s = 0; s < NS; ++s ) r[s] = 0.0;    // beyond the level: zero, as re-projected
             }
 #pragma unroll
             for( int s = 0; s < NS; ++s ) {
-                double* up      = P.u + cell * ldc + s * P.nT + i;
-                const double nu0 = *up - r[s] * c;
-                *up             = nu0;
-                if( s == 0 && i == 0 ) res += fabs( nu0 - P.uOld0[cell] ) * P.area[cell];
+                const double old = P.uRe[cell * ldc + s * P.nT + i];
+                const double v   = old - r[s] * c;
+                const double gi  = old - v;
+                P.u[cell * ldc + s * P.nT + i] = v;
+                sq                             = fma( gi, gi, sq );
+                if( s == 0 && i == 0 ) res += fabs( v - P.uOld0[cell] ) * P.area[cell];
+            }
+        }
+        if( P.finishInUpdate ) {
+            // The next step's closure test, here: its gradient is
+            // sum_k U(Lambda_k) phiWf(k, i) - u_new = uRe - u_new, because uRe was
+            // re-projected from the same duals' nodal states (which this kernel
+            // just used). A cell that passes (and keeps its level) would only
+            // be re-projected onto uRe again: it skips the closure and keeps
+            // uRe; the others go to the next step's list.
+            for( int o = 16; o > 0; o >>= 1 ) sq += __shfl_xor_sync( 0xffffffffu, sq, o );
+            __syncwarp();
+            if( lane == 0 ) {
+                const double* un = P.u + cell * ldc;    // state 0, written by this warp
+                bool fin         = sqrt( sq ) < P.eps;
+                if( fin && P.nLevels > 1 ) {
+                    // the level rule of the epilogue, on u_new(0, .) in the same order
+                    const int lev = int( P.level[cell] );
+                    double ind    = 0.0;
+                    if( P.dimXi == 1 )
+                        ind = fabs( un[nTj - 1] ) + fabs( un[nTj - 2] );
+                    else {
+                        const int prev = lev == 0 ? 1 : P.nTLevel[lev - 1];
+                        for( int i = prev; i < nTj; ++i ) ind += fabs( un[i] );
+                    }
+                    if( ( ind > 0.02 && lev < P.nLevels - 1 ) || ( ind < 0.004 && lev > 0 ) ) fin = false;
+                }
+                if( fin )
+                    finish_cell( P, cell, un[0], dtNext );
+                else
+                    nlist[atomicAdd( ncount, 1u )] = cell;
             }
         }
         __syncwarp();
     }
+    if( lane == 0 && dtNext < 1e300 ) atomic_min_pos_double( &P.ctl->dtBitsNext, dtNext );
     // deterministic residual: per-thread partials -> CTA sum -> per-CTA slot -> last CTA sums in order
     for( int o = 16; o > 0; o >>= 1 ) res += __shfl_xor_sync( 0xffffffffu, res, o );
     if( ( threadIdx.x & 31 ) == 0 ) blockRes[threadIdx.x >> 5] = res;
@@ -1059,6 +1158,7 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
         double s = 0.0;
         for( unsigned b = 0; b < gridDim.x; ++b ) s += ( (volatile double*)P.blockPartial )[b];
         Control* C    = P.ctl;
+        C->nActive[C->steps & 1] = 0;    // this step's list is consumed (before steps advances)
         C->residual   = s;
         C->dt         = dt;
         C->t          = C->t + dt;
@@ -1066,11 +1166,13 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
         C->active     = ( C->t < C->tEnd && C->residual > C->minResidual && ( C->maxSteps == 0 || C->steps < C->maxSteps ) ) ? 1 : 0;
         C->activeCellsLast = C->activeCells;
         C->activeCells     = 0;
-        C->dtBits     = 0x7FF0000000000000ull;    // +inf for the next step's min
+        // the next step's min starts from the cells finished here (+inf if none)
+        C->dtBits     = P.finishInUpdate ? ( (volatile unsigned long long*)&C->dtBitsNext )[0] : 0x7FF0000000000000ull;
+        C->dtBitsNext = 0x7FF0000000000000ull;
+        C->listReady = P.finishInUpdate ? 1 : 0;
         C->workCounter  = 0;
         C->workCounter2 = 0;
         C->nFallback    = 0;
-        C->nActive      = 0;
         C->doneBlocks  = 0;
     }
 }

@@ -60,7 +60,9 @@ struct uqc_solver {
     int closureBlock = 256, closureGrid = 0, updateBlock = 256, updateGrid = 0, auxGrid = 0, auxBlock = 256;
     size_t closureSmem = 0, updateSmem = 0, initSmem = 0, mvSmem = 0, checkSmem = 0;
     int checkBlock = 256, checkGrid = 0;
-    int* d_activeList = nullptr;    // cells that need Newton in the running step
+    int* d_activeList = nullptr;    // cells that need Newton: two lists (running step, next step)
+    double* d_cellDt  = nullptr;    // per cell: CFL step of its nodal states
+    double* d_uRe     = nullptr;    // moments re-projected by the closure epilogue (input of k_update)
     bool tablesInSmem        = false;    // check / update / init kernels stage the tables in shared memory
     bool closureTablesInSmem = false;    // ... the FP64 closure kernel
     int closureTablesOpt     = -1;       // option closure_tables_smem: -1 automatic, 0 read through L1, 1 stage
@@ -96,6 +98,7 @@ struct uqc_solver {
     std::map<int, std::pair<cudaGraphExec_t, int>> graphs;    // n -> (graph, kernel launches)
     int planGen = 0, graphGen = 0;
     bool useGraphs = true;
+    bool finishInUpdate = true;    // k_update runs the next step's convergence test (option update_test)
     std::vector<double> padPhi, padPhiWf;    // host tables in the device layout
     std::vector<double> padWt;               // w_k / 2^dimXi per node
     double* d_wt = nullptr;
@@ -197,6 +200,8 @@ KParams make_params( const uqc_solver* h ) {
     P.lam          = h->d_lam;
     P.uQ           = h->d_uQ;
     P.uOld0        = h->d_uOld0;
+    P.cellDt       = h->d_cellDt;
+    P.uRe          = h->d_uRe;
     P.level        = h->d_level;
     P.nTotalCell   = nullptr;
     P.status       = h->d_status;
@@ -415,6 +420,7 @@ void reset_control( uqc_solver* h, double t ) {
     c.minResidual     = h->cfg.minResidual;
     c.residual        = h->cfg.minResidual + 1.0;    // momentsolver.cpp:76
     c.dtBits          = 0x7FF0000000000000ull;
+    c.dtBitsNext      = 0x7FF0000000000000ull;
     c.maxSteps        = h->cfg.maxSteps;
     c.active          = t < h->cfg.tEnd ? 1 : 0;
     *h->h_ctl         = c;
@@ -423,6 +429,16 @@ void reset_control( uqc_solver* h, double t ) {
     h->lastFailed     = 0;
     h->lastFallback   = 0;
     CK( cudaMemcpyAsync( h->d_ctl, h->h_ctl, sizeof( Control ), cudaMemcpyHostToDevice, h->stream ) );
+    CK( cudaStreamSynchronize( h->stream ) );
+}
+
+// Drops the next step's active-cell list that k_update built (after a change
+// of the convergence test): the next k_check tests every cell again.
+void invalidate_lists( uqc_solver* h ) {
+    if( !h->deviceReady ) return;
+    static const unsigned long long inf = 0x7FF0000000000000ull;
+    CK( cudaMemsetAsync( &h->d_ctl->nActive[0], 0, 2 * sizeof( unsigned ) + sizeof( int ), h->stream ) );
+    CK( cudaMemcpyAsync( &h->d_ctl->dtBits, &inf, sizeof( inf ), cudaMemcpyHostToDevice, h->stream ) );
     CK( cudaStreamSynchronize( h->stream ) );
 }
 
@@ -513,7 +529,9 @@ void ensure_device( uqc_solver* h ) {
     h->d_level  = dalloc<unsigned>( N );
     h->d_status = dalloc<int>( N );
     h->d_iters  = dalloc<int>( N );
-    h->d_activeList   = dalloc<int>( N );
+    h->d_activeList   = dalloc<int>( 2 * N );
+    h->d_cellDt       = dalloc<double>( N );
+    h->d_uRe          = dalloc<double>( N * h->ldc );
     h->d_fallbackList = dalloc<int>( N );
     h->d_ctl    = dalloc<Control>( 1 );
     CK( cudaMallocHost( &h->h_ctl, sizeof( Control ) ) );
@@ -533,7 +551,7 @@ void release( uqc_solver* h ) {
                     (void*)h->d_unitN, (void*)h->d_scaledN, (void*)h->d_nbr, (void*)h->d_boundary, (void*)h->d_u, (void*)h->d_lam,
                     (void*)h->d_bndNormal, (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
                     (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
-                    (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_phiF, (void*)h->d_fallbackList,
+                    (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_cellDt, (void*)h->d_uRe, (void*)h->d_phiF, (void*)h->d_fallbackList,
                     (void*)h->d_factorStore, (void*)h->d_factorLevel} )
         if( p ) cudaFree( p );
     if( h->h_ctl ) cudaFreeHost( h->h_ctl );
@@ -559,6 +577,7 @@ void launch_closure( uqc_solver* h, KParams& P, int mode ) {
         KParams F     = P;
         F.activeList  = h->d_fallbackList;
         F.activeCount = &h->d_ctl->nFallback;
+        F.listParity  = 0;    // one fallback list
         F.workCounter  = &h->d_ctl->workCounter2;
         F.tablesInSmem = h->closureTablesInSmem;
         void* fargs[]  = {&F, &mode};
@@ -580,20 +599,36 @@ void reset_work( uqc_solver* h ) {
 // Closure half of a time step: k_check (warp per cell) finishes converged
 // cells and lists the others, then k_closure runs Newton on the list. In
 // SolveClosureSafe mode every cell takes a Newton step, so k_closure gets all.
+// The two active-cell lists of step mode (see step_list): k_check fills the
+// running step's list on the first step after a state change, k_update fills
+// the next step's list from its own convergence test, so later k_check
+// launches return at once (Control::listReady).
+void step_lists( uqc_solver* h, KParams& P ) {
+    if( h->cfg.newtonMode == 2 ) return;
+    P.activeList  = h->d_activeList;
+    P.activeCount = h->d_ctl->nActive;
+    P.listParity  = 1;
+}
+
 void enqueue_closure_phase( uqc_solver* h, KParams P ) {
+    step_lists( h, P );
     if( h->cfg.newtonMode != 2 ) {
-        P.activeList  = h->d_activeList;
-        P.activeCount = &h->d_ctl->nActive;
-        void* args[]  = {&P};
+        void* args[] = {&P};
         launch( h, pick_check( h->cfg.closure ), h->checkGrid, h->checkBlock, h->checkSmem, args );
     }
     launch_closure( h, P, 1 );
 }
 
+void enqueue_update( uqc_solver* h, KParams P ) {
+    step_lists( h, P );
+    P.finishInUpdate = h->cfg.newtonMode != 2 && h->finishInUpdate;
+    void* args[]     = {&P};
+    launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
+}
+
 void enqueue_step( uqc_solver* h, KParams& P ) {
     enqueue_closure_phase( h, P );
-    void* args[] = {&P};
-    launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
+    enqueue_update( h, P );
 }
 
 // n time steps on the handle's stream: one launch of a cached CUDA graph of
@@ -674,8 +709,8 @@ unsigned long long device_bytes_of( const uqc_solver* h ) {
     const unsigned long long N = (unsigned long long)h->mesh.nCells, F = (unsigned long long)h->mesh.nFaces;
     const unsigned long long ldc = h->ldc, sq = (unsigned long long)h->nS * h->tab.nQ;
     const unsigned long long tab = ( (unsigned long long)h->tab.nQ * h->ld + 8 ) * ( 8 + 8 + 4 ) + h->tab.xi.size() * 8 + h->tab.nQ * 8;
-    const unsigned long long d8  = N * ( 2 * ldc + 1 + 1 + 2 + 4 * F ) + ( N + 1 ) * sq;    // state, uQ, geometry (doubles)
-    const unsigned long long d4  = N * ( F + 1 + 1 + 1 + 1 + 1 + 1 );                         // nbr, boundary, level, status, iters, lists
+    const unsigned long long d8  = N * ( 3 * ldc + 1 + 1 + 1 + 2 + 4 * F ) + ( N + 1 ) * sq;    // state (u, re-projected u, lambda), uQ, geometry, cell dt
+    const unsigned long long d4  = N * ( F + 1 + 1 + 1 + 1 + 2 + 1 );                         // nbr, boundary, level, status, iters, lists
     return tab + 8 * d8 + 4 * d4 + ( mesh_has_walls( h->mesh ) ? 16 * N : 0 ) + sizeof( Control ) + 8 * 4096 + ( h->precision == UQC_MIXED && h->chord ? factor_store_bytes( h ) : 0 );
 }
 
@@ -846,6 +881,14 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
         ++h->planGen;
         return UQC_OK;
     }
+    if( k == "update_test" ) {
+        h->finishInUpdate = value != 0.0;
+        ++h->planGen;
+        return guarded( h, [&] {
+            invalidate_lists( h );
+            return UQC_OK;
+        } );
+    }
     return fail( h, UQC_ERR_ARGUMENT, "unknown option '" + k + "'" );
 }
 
@@ -855,7 +898,10 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
     h->cfg.epsilon       = epsilon;
     h->cfg.newtonMode    = newton_mode;
     ++h->planGen;
-    return UQC_OK;
+    return guarded( h, [&] {
+        invalidate_lists( h );    // the next step's list was built with the old test
+        return UQC_OK;
+    } );
 }
 
 int uqc_get_tables( const uqc_solver* h, double* phi, double* phi_wf, double* xi, double* w ) {
@@ -1205,8 +1251,7 @@ int uqc_step( uqc_solver* h, int n_steps, uqc_step_info* info ) {
             CK( cudaEventRecord( h->stepEvents[3 * s], h->stream ) );
             enqueue_closure_phase( h, P );
             CK( cudaEventRecord( h->stepEvents[3 * s + 1], h->stream ) );
-            void* args[] = {&P};
-            launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
+            enqueue_update( h, P );
             CK( cudaEventRecord( h->stepEvents[3 * s + 2], h->stream ) );
         }
         CK( cudaGetLastError() );
@@ -1605,6 +1650,7 @@ int uqc_device_state( uqc_solver* h, double** d_u, double** d_lambda ) {
     if( !h ) return UQC_ERR_ARGUMENT;
     int rc = guarded( h, [&] {
         ensure_device( h );
+        invalidate_lists( h );    // the caller may write the state: the next step tests every cell
         return UQC_OK;
     } );
     if( rc != UQC_OK ) return rc;
