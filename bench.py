@@ -249,6 +249,9 @@ def run_b200(args, rank, world, local):
     for form in forms:
         s.set_precision(MIXED if form == "mixed" else FP64)
         s.upload_state(u0, l0, v0, t=warm["t"])
+        # untimed warm-up in this form: an upload drops the mixed form's held
+        # factors and the update kernel's next-step list, as a fresh run has none
+        s.step(args.warmup)
         torch.cuda.synchronize()
         barrier(world)
         torch.cuda.synchronize()

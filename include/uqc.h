@@ -121,8 +121,17 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *                    2 n^2 bytes per cell, n = states x moments) and reuses it
  *                    across iterations and time steps while it contracts;
  *                    0: a new factor at every iteration.
+ *   "mixed_chord_inverse"  1 (default): the held factor is kept as its
+ *                    packed inverse U^-1 (formed at each re-factorisation), so
+ *                    a held-factor direction is two mat-vecs instead of two
+ *                    triangular solves; used when its shared memory costs no
+ *                    cell per SM (else the triangular solves); 0: never.
  *   "mixed_chord_theta"  re-factor after a step with the held factor that
  *                    reduced ||g|| by less than the factor 1/theta (default 0.1).
+ *   "update_test"    1 (default): the update kernel tests the next step's
+ *                    closure convergence per cell and lists only the cells
+ *                    that need Newton; 0: a check kernel tests every cell at
+ *                    the start of each step.
  *   "graphs"         1 (default): uqc_run and uqc_step_async launch cached
  *                    CUDA graphs of whole time steps; 0: direct launches.
  *   "mixed_max_iterations"  UQC_MIXED: Newton iterations of the FP32 pass

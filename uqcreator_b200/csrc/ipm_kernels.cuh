@@ -30,14 +30,19 @@ constexpr int MAXLEV = 16;
 // Phase counters (slots 0-7 of g_phaseCycles, diagnostic builds; rank 0 of
 // each thread group accumulates clock64 deltas): 0 newton, 1 initial
 // gradient, 2 Hessian, 3 Cholesky, 4 back substitution, 5 trial gradients,
-// 6 epilogue, 7 load.
+// 6 epilogue, 7 load; chord Newton of the mixed form: 21 solves with the
+// held factor, 22 initial gradient, 23 whole cell, and counts 25 held-factor
+// directions, 26 refreshed factors, 27 trial gradients.
 #ifdef UQC_PHASE_TIMERS
 #define PT_BEGIN( v ) long long v = clock64();
 #define PT_END( v, id ) \
     if( g.r == 0 ) atomicAdd( &g_phaseCycles[id], (unsigned long long)( clock64() - v ) );
+#define PT_COUNT( id ) \
+    if( g.r == 0 ) atomicAdd( &g_phaseCycles[id], 1ull );
 #else
 #define PT_BEGIN( v )
 #define PT_END( v, id )
+#define PT_COUNT( id )
 #endif
 
 // Grid-wide loop state kept on the device so a step needs no host round trip.
@@ -96,6 +101,7 @@ struct KParams {
     float* factorStore;       // mixed form, step mode: each cell's last FP32 factor (or null)
     int* factorLevel;         // ... nTj it was formed for, -1 none
     int factorStride;         // floats per cell in factorStore
+    int chordInverse;         // the store and the workspace hold the packed inverse X = U^-1 (else the factor)
     double chordTheta;        // re-factor after a held-factor step that reduced ||g|| by less than 1/chordTheta
     int* fallbackList;        // mixed form: cells handed to the FP64 form (non-PD FP32 factor, ...)
     unsigned* fallbackCount;
@@ -113,6 +119,7 @@ struct CellWs {
     double* H;                              // block-packed upper triangle + right-hand side (hess_doubles(n))
     double *D, *I;                          // Cholesky pivots and their inverses (n each)
     double* red;                            // reduction scratch (16) + broadcast (16)
+    float* X;                               // mixed chord form: packed inverse of the factor (or null)
 };
 
 // Layout: [lam uh g LA D I red] then a region shared by the trial data
@@ -121,11 +128,12 @@ struct CellWs {
 // solve), so DU aliases them. Then the block-packed Hessian. Every buffer
 // starts on a 32-byte boundary; D and I are padded to whole tiles.
 struct WsLayout {
-    size_t lam, uh, g, LA, D, I, red, LB, uk, gN, d, lamN, du, H, total;    // offsets in doubles
+    size_t lam, uh, g, LA, D, I, red, LB, uk, gN, d, lamN, du, H, X, total;    // offsets in doubles
 };
 
-// hElem: bytes of a Hessian element (8 FP64 form, 4 mixed form)
-__host__ __device__ inline WsLayout ws_layout( int nS, int nT, int nQ, int NP, int hElem ) {
+// hElem: bytes of a Hessian element (8 FP64 form, 4 mixed form); xFloats:
+// floats of the packed factor inverse (mixed chord form) or 0
+__host__ __device__ inline WsLayout ws_layout( int nS, int nT, int nQ, int NP, int hElem, int xFloats = 0 ) {
     auto a4          = []( size_t x ) { return ( x + 3 ) & ~size_t( 3 ); };
     const size_t n   = size_t( nS ) * nT, n8 = size_t( hnb( int( n ) ) ) * 8, sq = size_t( nS ) * nQ;
     const size_t npp = size_t( ( NP + 1 ) & ~1 );
@@ -149,16 +157,18 @@ __host__ __device__ inline WsLayout ws_layout( int nS, int nT, int nQ, int NP, i
     o       = trialEnd > duEnd ? trialEnd : duEnd;
     L.H     = o;
     o += a4( ( hess_doubles( int( n ) ) * size_t( hElem ) + 7 ) / 8 );
+    L.X = o;
+    o += a4( ( size_t( xFloats ) * 4 + 7 ) / 8 );
     L.total = o;
     return L;
 }
 
-__host__ __device__ inline size_t cell_ws_doubles( int nS, int nT, int nQ, int NP, int hElem = 8 ) {
-    return ws_layout( nS, nT, nQ, NP, hElem ).total;
+__host__ __device__ inline size_t cell_ws_doubles( int nS, int nT, int nQ, int NP, int hElem = 8, int xFloats = 0 ) {
+    return ws_layout( nS, nT, nQ, NP, hElem, xFloats ).total;
 }
 
-__device__ inline CellWs carve( double* p, int nS, int nT, int nQ, int NP, int hElem ) {
-    const WsLayout L = ws_layout( nS, nT, nQ, NP, hElem );
+__device__ inline CellWs carve( double* p, int nS, int nT, int nQ, int NP, int hElem, int xFloats = 0 ) {
+    const WsLayout L = ws_layout( nS, nT, nQ, NP, hElem, xFloats );
     CellWs w;
     w.lam  = p + L.lam;
     w.uh   = p + L.uh;
@@ -174,6 +184,7 @@ __device__ inline CellWs carve( double* p, int nS, int nT, int nQ, int NP, int h
     w.lamN = p + L.lamN;
     w.du   = p + L.du;    // aliases the trial buffers while the Hessian is assembled
     w.H    = p + L.H;
+    w.X    = xFloats ? reinterpret_cast<float*>( p + L.X ) : nullptr;
     return w;
 }
 
@@ -536,16 +547,23 @@ __device__ int newton_cell_chord( const Grp<GROUP>& g, const KParams& P, const d
         for( int idx = g.r; idx < NS * P.nQ; idx += GROUP ) LA[idx] = LB[idx];
     };
     auto trial = [&]( double step ) {
+        PT_BEGIN( tt );
+        PT_COUNT( 27 );
         add_step<GROUP>( g, P, nTj, w.lam, -step, w.d, w.lamN );
         g.sync();
         eval_lambda<NS, GROUP>( g, P, phi, w.lamN, nTj, LB );
         g.sync();
-        return gradient<CL, GROUP>( g, P, phiWf, LB, w.uh, nTj, w.uk, w.gN, w.red );
+        const double r = gradient<CL, GROUP>( g, P, phiWf, LB, w.uh, nTj, w.uk, w.gN, w.red );
+        PT_END( tt, 5 );
+        return r;
     };
     int rc = UQC_CELL_MAX_ITER;
+    PT_BEGIN( tc );
+    PT_BEGIN( t0 );
     eval_lambda<NS, GROUP>( g, P, phi, w.lam, nTj, LA );
     g.sync();
     double gn = gradient<CL, GROUP>( g, P, phiWf, LA, w.uh, nTj, w.uk, w.g, w.red );
+    PT_END( t0, 22 );
     if( gn < eps ) return UQC_CELL_CONVERGED;
     bool refresh = !have;
     double gnN   = 0.0;
@@ -558,14 +576,24 @@ __device__ int newton_cell_chord( const Grp<GROUP>& g, const KParams& P, const d
         bool chord = false;
         for( int attempt = 0; attempt < 2; ++attempt ) {
             if( refresh ) {
+                PT_COUNT( 26 );
                 if( newton_direction<CL, GROUP, float>( g, P, phi, phiH, w, nTj, LA ) ) return UQC_CELL_NOT_PD;
+                if( P.chordInverse ) tri_inverse_packed<GROUP, float>( g, H, I, n, w.X );
                 fresh   = true;
                 refresh = false;
                 chord   = false;
             }
             else {
-                forward_solve_warp<GROUP, float>( g, H, n, I, w.g );
-                back_solve_warp<GROUP, float>( g, H, n, I, w.d );
+                PT_BEGIN( ts );
+                PT_COUNT( 25 );
+                g.sync();    // w.g complete (copied by the whole group)
+                if( P.chordInverse )
+                    chord_direction_packed<GROUP, float>( g, w.X, n, w.g, reinterpret_cast<float*>( w.D ), I, w.d );
+                else {
+                    forward_solve_warp<GROUP, float>( g, H, n, I, w.g );
+                    back_solve_warp<GROUP, float>( g, H, n, I, w.d );
+                }
+                PT_END( ts, 21 );
                 chord = true;
             }
             ++iters;
@@ -602,6 +630,7 @@ __device__ int newton_cell_chord( const Grp<GROUP>& g, const KParams& P, const d
     }
 out:
     g.sync();
+    PT_END( tc, 23 );
     w.LA = LA;
     w.LB = LB;
     return rc;
@@ -722,7 +751,8 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
         }
         __syncthreads();
     }
-    CellWs w = carve( base + gid * cell_ws_doubles( NS, P.nT, P.nQ, NP, sizeof( HT ) ), NS, P.nT, P.nQ, NP, sizeof( HT ) );
+    const int xf = MIXED && P.chordInverse ? xpacked( NS * P.nT ) : 0;
+    CellWs w     = carve( base + gid * cell_ws_doubles( NS, P.nT, P.nQ, NP, sizeof( HT ), xf ), NS, P.nT, P.nQ, NP, sizeof( HT ), xf );
     const size_t ldc = size_t( NS ) * P.nT;
     double* bc       = w.red + 16;    // broadcast slot
     unsigned long long itSum = 0, lsSum = 0;
@@ -768,16 +798,25 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
                     float* H        = reinterpret_cast<float*>( w.H );
                     float* Iv       = reinterpret_cast<float*>( w.I );
                     const bool have = P.factorLevel[cell] == nTj;
+                    const int nX    = xpacked( NS * nTj );
                     if( have ) {
-                        for( int i = g.r; i < nH; i += GROUP ) H[i] = st[i];
-                        for( int i = g.r; i < n8; i += GROUP ) Iv[i] = st[nH + i];
+                        if( P.chordInverse )
+                            for( int i = g.r; i < nX; i += GROUP ) w.X[i] = st[i];
+                        else {
+                            for( int i = g.r; i < nH; i += GROUP ) H[i] = st[i];
+                            for( int i = g.r; i < n8; i += GROUP ) Iv[i] = st[nH + i];
+                        }
                     }
                     g.sync();
                     bool fresh = false;
                     rc         = newton_cell_chord<CL, GROUP>( g, P, phi, phiWf, phiH, w, nTj, have, iters, ls, fresh );
                     if( rc == UQC_CELL_CONVERGED && fresh ) {
-                        for( int i = g.r; i < nH; i += GROUP ) st[i] = H[i];
-                        for( int i = g.r; i < n8; i += GROUP ) st[nH + i] = Iv[i];
+                        if( P.chordInverse )
+                            for( int i = g.r; i < nX; i += GROUP ) st[i] = w.X[i];
+                        else {
+                            for( int i = g.r; i < nH; i += GROUP ) st[i] = H[i];
+                            for( int i = g.r; i < n8; i += GROUP ) st[nH + i] = Iv[i];
+                        }
                     }
                     if( g.r == 0 ) P.factorLevel[cell] = rc == UQC_CELL_CONVERGED ? ( fresh || have ? nTj : -1 ) : -1;
                 }
@@ -958,14 +997,29 @@ template <int CL> __device__ __forceinline__ void wall_ghost( const double* a, c
 
 // rhs(s, i) = sum_k Gs(s, k) phiWf(k, i) for one i (t = phiWf + i), the NS
 // states as independent chains sharing each table value.
+// Gs is node-major (Gs[k NS + s]), so a node's NS values come in 16-byte
+// shared-memory loads.
 template <int NS>
 __device__ __forceinline__ void project_lane( const double* Gs, const double* t, int ld, int nQ, double* r ) {
 #pragma unroll
     for( int s = 0; s < NS; ++s ) r[s] = 0.0;
     for( int k = 0; k < nQ; ++k, t += ld ) {
         const double w = *t;
+        double g[NS];
+        if constexpr( NS % 2 == 0 ) {
 #pragma unroll
-        for( int s = 0; s < NS; ++s ) r[s] = fma( Gs[s * nQ + k], w, r[s] );
+            for( int s = 0; s < NS; s += 2 ) {
+                const double2 v = *reinterpret_cast<const double2*>( Gs + k * NS + s );
+                g[s]            = v.x;
+                g[s + 1]        = v.y;
+            }
+        }
+        else {
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) g[s] = Gs[k * NS + s];
+        }
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) r[s] = fma( g[s], w, r[s] );
     }
 }
 
@@ -1082,7 +1136,7 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
                 }
             }
 #pragma unroll
-            for( int s = 0; s < NS; ++s ) Gs[s * P.nQ + k] = gsum[s];
+            for( int s = 0; s < NS; ++s ) Gs[k * NS + s] = gsum[s];
         }
         __syncwarp();
         // projection and update: a lane per basis function i, the NS states as

@@ -494,4 +494,95 @@ __device__ void back_solve_warp( const Grp<GROUP>& g, const T* H, int n, const T
     g.sync();
 }
 
+// ---- explicit inverse of the factor (chord Newton of the mixed form)
+//
+// X = U^-1 in packed upper-triangular storage, row-major: X(i, j), i <= j,
+// at xrow(i, n) + j - i. With it a held-factor direction H^-1 g = X (X^T g)
+// is two mat-vecs with independent outputs instead of two triangular solves
+// with a dependent chain per tile row.
+__device__ __forceinline__ int xrow( int i, int n ) { return i * n - ( ( i * ( i - 1 ) ) >> 1 ); }
+__host__ __device__ inline int xpacked( int n ) { return ( n * ( n + 1 ) ) >> 1; }
+
+// X from a factor that cholesky_la left: off-diagonal tiles hold U(I, K);
+// a diagonal tile holds U in its upper part and its inverse X_JJ in the lower
+// part (X_JJ(r, c) at tix(c, r)), with the inverse pivots in Iv. A thread per
+// column j (columns are independent): the column's own tile from X_JJ, then
+// tile rows I = J-1 .. 0 by blocks, x_I = -X_II sum_{K > I} U(I, K) x_K. The
+// warp's lanes step through (I, K) together, so the U elements they read are
+// broadcasts.
+template <int GROUP, class T>
+__device__ void tri_inverse_packed( const Grp<GROUP>& g, const T* H, const T* Iv, int n, T* X ) {
+    const int nb = hnb( n );
+    for( int j0 = 0; j0 < n; j0 += GROUP ) {
+        if( j0 + ( g.r & ~31 ) >= n ) continue;    // the warp has no column in this round
+        const int j = j0 + g.r;
+        // the warp's largest tile column (lanes step through the tiles together)
+        const int Jw = min( j0 + ( g.r & ~31 ) + 31, n - 1 ) >> 3;
+        const bool act = j < n;
+        const int J = act ? j >> 3 : -1, c = j & 7;
+        if( act ) {
+            const T* DJ = H + htile( J, J );
+            for( int r = 0; r <= c; ++r ) X[xrow( 8 * J + r, n ) + j - 8 * J - r] = r == c ? Iv[8 * J + c] : DJ[tix( c, r )];
+        }
+        for( int I = Jw - 1; I >= 0; --I ) {
+            T s[8];
+#pragma unroll
+            for( int r = 0; r < 8; ++r ) s[r] = T( 0 );
+            for( int K = I + 1; K <= Jw; ++K ) {
+                const T* A = H + htile( I, K );
+#pragma unroll
+                for( int kk = 0; kk < 8; ++kk ) {
+                    const int k = 8 * K + kk;
+                    if( act && I < J && k <= j ) {
+                        const T xk = X[xrow( k, n ) + j - k];
+#pragma unroll
+                        for( int r = 0; r < 8; ++r ) s[r] = fma( A[tix( r, kk )], xk, s[r] );
+                    }
+                }
+            }
+            if( act && I < J ) {
+                const T* DI = H + htile( I, I );
+#pragma unroll
+                for( int r = 0; r < 8; ++r ) {
+                    T v = Iv[8 * I + r] * s[r];
+#pragma unroll
+                    for( int q = r + 1; q < 8; ++q ) v = fma( DI[tix( q, r )], s[q], v );
+                    X[xrow( 8 * I + r, n ) + j - 8 * I - r] = -v;
+                }
+            }
+        }
+    }
+    g.sync();
+}
+
+// d = X (X^T b) = H^-1 b with the packed inverse; gf, tf: n floats of scratch.
+template <int GROUP, class T>
+__device__ void chord_direction_packed( const Grp<GROUP>& g, const T* X, int n, const double* b, T* gf, T* tf, double* d ) {
+    for( int i = g.r; i < n; i += GROUP ) gf[i] = T( b[i] );
+    g.sync();
+    for( int o = g.r; o < n; o += GROUP ) {    // t = X^T b: column o, rows 0..o
+        T a0 = 0, a1 = 0;
+        int i = 0;
+        for( ; i + 1 <= o; i += 2 ) {
+            a0 = fma( X[xrow( i, n ) + o - i], gf[i], a0 );
+            a1 = fma( X[xrow( i + 1, n ) + o - i - 1], gf[i + 1], a1 );
+        }
+        if( i <= o ) a0 = fma( X[xrow( i, n ) + o - i], gf[i], a0 );
+        tf[o] = a0 + a1;
+    }
+    g.sync();
+    for( int o = g.r; o < n; o += GROUP ) {    // d = X t: row o, columns o..n-1
+        const T* row = X + xrow( o, n ) - o;
+        T a0 = 0, a1 = 0;
+        int j = o;
+        for( ; j + 1 < n; j += 2 ) {
+            a0 = fma( row[j], tf[j], a0 );
+            a1 = fma( row[j + 1], tf[j + 1], a1 );
+        }
+        if( j < n ) a0 = fma( row[j], tf[j], a0 );
+        d[o] = double( a0 + a1 );
+    }
+    g.sync();
+}
+
 }    // namespace uqc

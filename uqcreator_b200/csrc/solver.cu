@@ -78,6 +78,8 @@ struct uqc_solver {
     int* d_factorLevel   = nullptr;
     int factorStride     = 0;
     bool chord           = true;
+    bool chordInverse    = false;    // planned: the mixed workspace holds the packed factor inverse
+    bool chordInverseOpt = true;     // option mixed_chord_inverse
     double chordTheta    = 0.1;
     size_t mixedSmem       = 0;
     bool mixedTablesInSmem = false;
@@ -214,6 +216,7 @@ KParams make_params( const uqc_solver* h ) {
     P.factorStore       = useStore ? h->d_factorStore : nullptr;
     P.factorLevel       = useStore ? h->d_factorLevel : nullptr;
     P.factorStride      = h->factorStride;
+    P.chordInverse      = useStore && h->chordInverse ? 1 : 0;
     P.chordTheta        = h->chordTheta;
     P.fallbackCount = h->d_ctl ? &h->d_ctl->nFallback : nullptr;
     return P;
@@ -289,9 +292,11 @@ void launch( uqc_solver* h, void* fn, int grid, int block, size_t smem, void** a
 
 // Factor store of the mixed form: floats per cell (tiles + pivot inverses of
 // the finest level, padded to 16 bytes) and its total bytes.
+// Floats per cell of the factor store: the factor tiles and inverse pivots,
+// or the packed inverse (whichever is larger, so the planner may switch).
 int factor_stride( const uqc_solver* h ) {
     const int n = h->nS * h->tab.nT;
-    return int( ( hess_doubles( n ) + size_t( hnb( n ) ) * 8 + 3 ) & ~size_t( 3 ) );
+    return int( ( std::max<size_t>( hess_doubles( n ) + size_t( hnb( n ) ) * 8, size_t( xpacked( n ) ) ) + 3 ) & ~size_t( 3 ) );
 }
 unsigned long long factor_store_bytes( const uqc_solver* h ) {
     return (unsigned long long)h->mesh.nCells * ( (unsigned long long)factor_stride( h ) * 4 + 4 );
@@ -314,17 +319,26 @@ void plan_mixed( uqc_solver* h, int maxSmem ) {
     const size_t n       = size_t( nS ) * nT;
     const size_t tn      = size_t( nQ ) * h->ld + 4;
     const size_t tables  = 2 * tn * sizeof( double ) + ( tn + 1 ) / 2 * sizeof( double );
-    const size_t wsCell  = cell_ws_doubles( nS, nT, nQ, closure_np( cl ), 4 ) * sizeof( double );
-    h->mixedTablesInSmem = h->closureTablesOpt != 0 && tables <= 112 * 1024 && tables + 2 * wsCell <= size_t( maxSmem );
+    const size_t ws0     = cell_ws_doubles( nS, nT, nQ, closure_np( cl ), 4 ) * sizeof( double );
+    h->mixedTablesInSmem = h->closureTablesOpt != 0 && tables <= 112 * 1024 && tables + 2 * ws0 <= size_t( maxSmem );
     const size_t avail   = size_t( maxSmem ) - ( h->mixedTablesInSmem ? tables : 0 );
-    const int fit        = int( std::min<size_t>( 8, avail / wsCell ) );
-    if( fit < 1 ) {
+    const int fit0       = int( std::min<size_t>( 8, avail / ws0 ) );
+    if( fit0 < 1 ) {
         h->mixedOk  = false;
-        h->mixedWhy = "mixed-form closure workspace (" + std::to_string( wsCell ) + " B per cell) exceeds shared memory";
+        h->mixedWhy = "mixed-form closure workspace (" + std::to_string( ws0 ) + " B per cell) exceeds shared memory";
         return;
     }
     h->mixedGroup = n <= 32 ? 32 : 64;
-    h->mixedBlock = h->mixedGroup * std::min( h->mixedGroup == 32 ? 8 : 4, fit );
+    // chord directions from the packed inverse of the held factor (two
+    // independent-output mat-vecs instead of two triangular solves), when its
+    // shared memory costs no cell per CTA
+    const int cap         = h->mixedGroup == 32 ? 8 : 4;
+    const size_t wsX      = cell_ws_doubles( nS, nT, nQ, closure_np( cl ), 4, xpacked( int( n ) ) ) * sizeof( double );
+    const int fitX        = int( std::min<size_t>( 8, avail / wsX ) );
+    h->chordInverse       = h->chord && h->chordInverseOpt != 0 && std::min( cap, fitX ) >= std::min( cap, fit0 );
+    const size_t wsCell   = h->chordInverse ? wsX : ws0;
+    const int fit         = h->chordInverse ? fitX : fit0;
+    h->mixedBlock = h->mixedGroup * std::min( cap, fit );
     h->mixedSmem  = wsCell * ( h->mixedBlock / h->mixedGroup ) + ( h->mixedTablesInSmem ? tables : 0 );
     void* k       = pick( cl, h->mixedGroup, 4 );
     allow_dynamic_smem( k );
@@ -858,11 +872,12 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
         ++h->planGen;
         return UQC_OK;
     }
-    if( k == "mixed_chord" ) {
-        h->chord = value != 0.0;
-        if( h->chord && h->precision == UQC_MIXED && h->deviceReady ) {
+    if( k == "mixed_chord" || k == "mixed_chord_inverse" ) {
+        ( k == "mixed_chord" ? h->chord : h->chordInverseOpt ) = value != 0.0;
+        if( h->deviceReady ) {
             int rc = guarded( h, [&] {
-                reset_factor_store( h );
+                plan_launches( h );    // the mixed workspace depends on the chord form
+                if( h->chord && h->precision == UQC_MIXED ) reset_factor_store( h );
                 return UQC_OK;
             } );
             if( rc != UQC_OK ) return rc;
