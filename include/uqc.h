@@ -128,10 +128,11 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *                    cell per SM (else the triangular solves); 0: never.
  *   "mixed_chord_theta"  re-factor after a step with the held factor that
  *                    reduced ||g|| by less than the factor 1/theta (default 0.1).
- *   "update_test"    1 (default): the update kernel tests the next step's
- *                    closure convergence per cell and lists only the cells
- *                    that need Newton; 0: a check kernel tests every cell at
- *                    the start of each step.
+ *   "update_test"    1: the update kernel tests the next step's closure
+ *                    convergence per cell and lists only the cells that need
+ *                    Newton; 0: a check kernel tests every cell at the start
+ *                    of each step; -1 (default): 1 with a single refinement
+ *                    level, 0 with several.
  *   "graphs"         1 (default): uqc_run and uqc_step_async launch cached
  *                    CUDA graphs of whole time steps; 0: direct launches.
  *   "mixed_max_iterations"  UQC_MIXED: Newton iterations of the FP32 pass

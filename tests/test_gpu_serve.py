@@ -160,6 +160,7 @@ def test_update_side_convergence_test_matches_check_kernel(toml, steps):
     re-projection."""
     a = Solver(toml); a.init_state()
     b = Solver(toml); b.init_state()
+    a.set_option("update_test", 1)    # also with refinement levels (automatic: off there)
     b.set_option("update_test", 0)
     ia = a.step(steps)
     ib = b.step(steps)

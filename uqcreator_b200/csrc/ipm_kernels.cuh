@@ -60,7 +60,8 @@ struct Control {
     int activeCells;      // cells with Newton iterations in the running step
     int activeCellsLast;  // ... in the last finished step
     unsigned int nActive[2];      // lengths of the two active-cell lists (step parity)
-    int listReady;                // k_update built the running step's list: k_check has nothing to do
+    int listReady;                // k_update built the running step's lists: k_check runs only the check list
+    unsigned int nCheck[2];       // lengths of the two check lists (cells whose level changes)
     unsigned long long dtBitsNext;    // min dt of the cells k_update finished for the next step
     unsigned long long newtonIters, lineSearchTrials;
     unsigned long long fallbackCells;    // mixed form: cells handed to the FP64 form
@@ -95,7 +96,10 @@ struct KParams {
     int* activeList;          // step mode: cells that need Newton (filled by k_check / k_update), or null
     unsigned* activeCount;
     int listParity;           // step mode: two lists of nCells, the running step's is (ctl->steps & 1)
-    int finishInUpdate;       // k_update tests the next step's convergence and fills the other list
+    int finishInUpdate;       // k_update tests the next step's convergence and fills the other lists
+    int* checkList;           // step mode: converged cells whose level changes (k_check's epilogue), two lists
+    unsigned* checkCount;
+    unsigned char* finFlag;   // per cell: finished by k_update for the next step (no closure there)
     double* cellDt;           // per cell: the CFL step of its nodal states (written by the epilogue)
     unsigned* workCounter;    // work-stealing counter of k_closure (in ctl)
     float* factorStore;       // mixed form, step mode: each cell's last FP32 factor (or null)
@@ -675,6 +679,7 @@ __device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const do
         int s = idx / P.nT, i = idx - s * P.nT;
         // ugs: the same sums kept from the gradient test (i < nTj), when the caller has them
         P.uRe[cell * ldc + idx] = i < nTn ? ( ugs && i < nTj ? ugs[idx] : node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) ) : 0.0;
+        if( i >= nTn ) P.u[cell * ldc + idx] = 0.0;    // the update writes u below the level only
     }
     // [F] the cell's time step (min over its nodes)
     double dloc = 1e300;
@@ -891,7 +896,13 @@ __host__ __device__ inline size_t check_ws_doubles( int nS, int nT, int nQ ) {
 template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) {
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
-    if( !P.ctl->active || P.ctl->listReady ) return;
+    if( !P.ctl->active ) return;
+    // after a state change every cell; otherwise only the check list that
+    // k_update filled (converged cells whose refinement level changes)
+    const bool listMode = P.ctl->listReady != 0;
+    const int par       = P.ctl->steps & 1;
+    const int nItems    = listMode ? int( P.checkCount[par] ) : P.nCells;
+    if( nItems == 0 ) return;
     int* alist;
     unsigned* acount;
     step_list( P, 0, alist, acount );
@@ -917,7 +928,9 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
     double* uk       = ugs + ldc;
     double* red      = uk + size_t( NS ) * P.nQ;
     double dtMin     = 1e300;
-    for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
+    for( int item = blockIdx.x * nWarps + warp; item < nItems; item += gridDim.x * nWarps ) {
+        const int cell = listMode ? P.checkList[size_t( par ) * P.nCells + item] : item;
+        if( !listMode && P.finFlag && g.r == 0 ) P.finFlag[cell] = 0;
         CT_BEGIN( tcell );
         CT_BEGIN( tload );
         const int lev = int( P.level[cell] ), nTj = P.nTLevel[lev];
@@ -1023,13 +1036,33 @@ __device__ __forceinline__ void project_lane( const double* Gs, const double* t,
     }
 }
 
+// Warp-buffered append to a device list (warp-uniform call): lane `cnt` keeps
+// the entry; 32 entries take one atomicAdd on the list length.
+struct WarpListBuf {
+    int cell = 0, cnt = 0;
+    __device__ __forceinline__ void push( int lane, int c, int* list, unsigned* count ) {
+        if( lane == cnt ) cell = c;
+        if( ++cnt == 32 ) flush( lane, list, count );
+    }
+    __device__ __forceinline__ void flush( int lane, int* list, unsigned* count ) {
+        if( cnt == 0 ) return;
+        unsigned base = 0;
+        if( lane == 0 ) base = atomicAdd( count, unsigned( cnt ) );
+        base = __shfl_sync( 0xffffffffu, base, 0 );
+        if( lane < cnt ) list[base + lane] = cell;
+        cnt = 0;
+    }
+};
+
 // A cell whose next closure test k_update found passed: it keeps its duals,
 // nodal states, moments and level; the next step sees it converged with no
 // iterations, its residual reference is u_new(0, 0) and its dt the stored one.
+// Its closure status of that step (converged, 0 iterations) is written by the
+// k_update of that step, so that between steps the status arrays describe the
+// last closure, as without this shortcut.
 __device__ __forceinline__ void finish_cell( const KParams& P, int cell, double u00, double& dtNext ) {
     P.uOld0[cell]  = u00;
-    P.status[cell] = UQC_CELL_CONVERGED;
-    P.iters[cell]  = 0;
+    P.finFlag[cell] = 1;    // its status is written by the next k_update (after the step it skips)
     const double d = P.cellDt[cell];
     dtNext         = d < dtNext ? d : dtNext;
 }
@@ -1042,7 +1075,7 @@ __device__ __forceinline__ void finish_cell( const KParams& P, int cell, double 
 // projection face by face (momentsolver.cpp:413-416); the sums agree up to
 // reassociation. Each lane carries two outputs with two partial sums each.
 template <int CL>
-__global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
+__global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
     __shared__ double blockRes[32];
@@ -1066,24 +1099,32 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
     int* nlist       = nullptr;
     unsigned* ncount = nullptr;
     if( P.finishInUpdate ) step_list( P, 1, nlist, ncount );
+    int* clist        = nullptr;
+    unsigned* ccount  = nullptr;
+    if( P.finishInUpdate ) {
+        clist  = P.checkList + size_t( ( P.ctl->steps + 1 ) & 1 ) * P.nCells;
+        ccount = P.checkCount + ( ( P.ctl->steps + 1 ) & 1 );
+    }
+    WarpListBuf nbuf, cbuf;    // next step's active list and check list
     for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
         const int bc = P.boundary[cell];
+        if( P.finishInUpdate && lane == 0 && P.finFlag[cell] ) {
+            // finished by the previous update: this step's closure status
+            P.status[cell]  = UQC_CELL_CONVERGED;
+            P.iters[cell]   = 0;
+            P.finFlag[cell] = 0;
+        }
         if( bc == 1 ) {
             // Dirichlet cell: uNew = u (expliciteuler.cpp:21-23)
             for( int idx = lane; idx < int( ldc ); idx += 32 ) P.u[cell * ldc + idx] = P.uRe[cell * ldc + idx];
             if( lane == 0 ) {
                 const double u0 = P.uRe[cell * ldc];
                 res += fabs( u0 - P.uOld0[cell] ) * P.area[cell];
-                if( P.finishInUpdate ) {
-                    // its moments are the re-projected ones: the next closure
-                    // test passes; with refinement levels the closure kernel
-                    // still runs it for the level update
-                    if( P.nLevels > 1 )
-                        nlist[atomicAdd( ncount, 1u )] = cell;
-                    else
-                        finish_cell( P, cell, u0, dtNext );
-                }
+                // its moments are the re-projected ones: the next closure test passes
+                if( P.finishInUpdate && P.nLevels == 1 ) finish_cell( P, cell, u0, dtNext );
             }
+            // with refinement levels k_check's epilogue applies the level rule
+            if( P.finishInUpdate && P.nLevels > 1 ) cbuf.push( lane, cell, clist, ccount );
             continue;
         }
         const int nTj    = P.nTLevel[P.level[cell]];
@@ -1143,14 +1184,10 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
         // independent chains sharing each table value
         const double c = dt / P.area[cell];
         double sq      = 0.0;
-        for( int i = lane; i < P.nT; i += 32 ) {
+        double v0a = 0.0, v0b = 0.0;    // u_new(0, lane) and u_new(0, lane + 32), for the level rule
+        for( int i = lane; i < nTj; i += 32 ) {    // beyond the level u stays zero (epilogue)
             double r[NS];
-            if( i < nTj )
-                project_lane<NS>( Gs, phiWf + i, P.ld, P.nQ, r );
-            else {
-#pragma unroll
-                for( int s = 0; s < NS; ++s ) r[s] = 0.0;    // beyond the level: zero, as re-projected
-            }
+            project_lane<NS>( Gs, phiWf + i, P.ld, P.nQ, r );
 #pragma unroll
             for( int s = 0; s < NS; ++s ) {
                 const double old = P.uRe[cell * ldc + s * P.nT + i];
@@ -1158,6 +1195,8 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
                 const double gi  = old - v;
                 P.u[cell * ldc + s * P.nT + i] = v;
                 sq                             = fma( gi, gi, sq );
+                if( s == 0 && i < 32 ) v0a = v;
+                if( s == 0 && i >= 32 && i < 64 ) v0b = v;
                 if( s == 0 && i == 0 ) res += fabs( v - P.uOld0[cell] ) * P.area[cell];
             }
         }
@@ -1169,29 +1208,42 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
             // be re-projected onto uRe again: it skips the closure and keeps
             // uRe; the others go to the next step's list.
             for( int o = 16; o > 0; o >>= 1 ) sq += __shfl_xor_sync( 0xffffffffu, sq, o );
-            __syncwarp();
-            if( lane == 0 ) {
-                const double* un = P.u + cell * ldc;    // state 0, written by this warp
-                bool fin         = sqrt( sq ) < P.eps;
-                if( fin && P.nLevels > 1 ) {
-                    // the level rule of the epilogue, on u_new(0, .) in the same order
-                    const int lev = int( P.level[cell] );
-                    double ind    = 0.0;
-                    if( P.dimXi == 1 )
-                        ind = fabs( un[nTj - 1] ) + fabs( un[nTj - 2] );
-                    else {
-                        const int prev = lev == 0 ? 1 : P.nTLevel[lev - 1];
-                        for( int i = prev; i < nTj; ++i ) ind += fabs( un[i] );
-                    }
-                    if( ( ind > 0.02 && lev < P.nLevels - 1 ) || ( ind < 0.004 && lev > 0 ) ) fin = false;
+            sq              = __shfl_sync( 0xffffffffu, sq, 0 );    // one decision for the warp
+            const bool pass = sqrt( sq ) < P.eps;
+            bool fin        = pass;
+            if( fin && P.nLevels > 1 ) {
+                // the level rule of the epilogue, on u_new(0, .) in the same order
+                // (values from the lanes' registers; beyond 64 moments from memory)
+                __syncwarp();
+                const int lev = int( P.level[cell] );
+                auto at       = [&]( int i ) {
+                    const double r = __shfl_sync( 0xffffffffu, ( i >> 5 ) ? v0b : v0a, i & 31 );
+                    return i < 64 ? r : P.u[cell * ldc + i];
+                };
+                double ind = 0.0;
+                if( P.dimXi == 1 ) {
+                    const double a = at( nTj - 1 ), b = at( nTj - 2 );
+                    ind            = fabs( a ) + fabs( b );
                 }
-                if( fin )
-                    finish_cell( P, cell, un[0], dtNext );
-                else
-                    nlist[atomicAdd( ncount, 1u )] = cell;
+                else {
+                    const int prev = lev == 0 ? 1 : P.nTLevel[lev - 1];
+                    for( int i = prev; i < nTj; ++i ) ind += fabs( at( i ) );
+                }
+                if( ( ind > 0.02 && lev < P.nLevels - 1 ) || ( ind < 0.004 && lev > 0 ) ) fin = false;
             }
+            if( fin ) {
+                if( lane == 0 ) finish_cell( P, cell, v0a, dtNext );
+            }
+            else if( pass )
+                cbuf.push( lane, cell, clist, ccount );    // converged, new level: k_check's epilogue
+            else
+                nbuf.push( lane, cell, nlist, ncount );
         }
         __syncwarp();
+    }
+    if( P.finishInUpdate ) {
+        nbuf.flush( lane, nlist, ncount );
+        cbuf.flush( lane, clist, ccount );
     }
     if( lane == 0 && dtNext < 1e300 ) atomic_min_pos_double( &P.ctl->dtBitsNext, dtNext );
     // deterministic residual: per-thread partials -> CTA sum -> per-CTA slot -> last CTA sums in order
@@ -1212,7 +1264,8 @@ __global__ void __launch_bounds__( 256 ) k_update( KParams P ) {
         double s = 0.0;
         for( unsigned b = 0; b < gridDim.x; ++b ) s += ( (volatile double*)P.blockPartial )[b];
         Control* C    = P.ctl;
-        C->nActive[C->steps & 1] = 0;    // this step's list is consumed (before steps advances)
+        C->nActive[C->steps & 1] = 0;    // this step's lists are consumed (before steps advances)
+        C->nCheck[C->steps & 1]  = 0;
         C->residual   = s;
         C->dt         = dt;
         C->t          = C->t + dt;

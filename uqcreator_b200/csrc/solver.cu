@@ -63,6 +63,8 @@ struct uqc_solver {
     int* d_activeList = nullptr;    // cells that need Newton: two lists (running step, next step)
     double* d_cellDt  = nullptr;    // per cell: CFL step of its nodal states
     double* d_uRe     = nullptr;    // moments re-projected by the closure epilogue (input of k_update)
+    int* d_checkList  = nullptr;    // two lists: converged cells whose level changes (k_check's epilogue)
+    unsigned char* d_finFlag = nullptr;    // per cell: finished by k_update for the next step
     bool tablesInSmem        = false;    // check / update / init kernels stage the tables in shared memory
     bool closureTablesInSmem = false;    // ... the FP64 closure kernel
     int closureTablesOpt     = -1;       // option closure_tables_smem: -1 automatic, 0 read through L1, 1 stage
@@ -100,7 +102,7 @@ struct uqc_solver {
     std::map<int, std::pair<cudaGraphExec_t, int>> graphs;    // n -> (graph, kernel launches)
     int planGen = 0, graphGen = 0;
     bool useGraphs = true;
-    bool finishInUpdate = true;    // k_update runs the next step's convergence test (option update_test)
+    int finishInUpdateOpt = -1;    // option update_test: 1 on, 0 off, -1 automatic
     std::vector<double> padPhi, padPhiWf;    // host tables in the device layout
     std::vector<double> padWt;               // w_k / 2^dimXi per node
     double* d_wt = nullptr;
@@ -160,6 +162,15 @@ template <class T> T* dupload( const std::vector<T>& v, size_t extra = 0 ) {
     return p;
 }
 
+// Whether k_update tests the next step's convergence (option update_test;
+// automatic: with a single refinement level. With several, cells whose level
+// flips every step still need the check kernel's epilogue, which then costs
+// as much as testing every cell there).
+bool update_test_on( const uqc_solver* h ) {
+    const bool on = h->finishInUpdateOpt == -1 ? h->tab.nLevels == 1 : h->finishInUpdateOpt != 0;
+    return h->cfg.newtonMode != 2 && on;
+}
+
 KParams make_params( const uqc_solver* h ) {
     KParams P{};
     P.nS      = h->nS;
@@ -203,7 +214,9 @@ KParams make_params( const uqc_solver* h ) {
     P.uQ           = h->d_uQ;
     P.uOld0        = h->d_uOld0;
     P.cellDt       = h->d_cellDt;
-    P.uRe          = h->d_uRe;
+    // re-projected moments: a buffer of their own when k_update tests the next
+    // step's convergence (it needs them next to u_new), else u itself (in place)
+    P.uRe          = update_test_on( h ) ? h->d_uRe : h->d_u;
     P.level        = h->d_level;
     P.nTotalCell   = nullptr;
     P.status       = h->d_status;
@@ -451,7 +464,7 @@ void reset_control( uqc_solver* h, double t ) {
 void invalidate_lists( uqc_solver* h ) {
     if( !h->deviceReady ) return;
     static const unsigned long long inf = 0x7FF0000000000000ull;
-    CK( cudaMemsetAsync( &h->d_ctl->nActive[0], 0, 2 * sizeof( unsigned ) + sizeof( int ), h->stream ) );
+    CK( cudaMemsetAsync( &h->d_ctl->nActive[0], 0, 4 * sizeof( unsigned ) + sizeof( int ), h->stream ) );    // nActive, listReady, nCheck
     CK( cudaMemcpyAsync( &h->d_ctl->dtBits, &inf, sizeof( inf ), cudaMemcpyHostToDevice, h->stream ) );
     CK( cudaStreamSynchronize( h->stream ) );
 }
@@ -546,6 +559,9 @@ void ensure_device( uqc_solver* h ) {
     h->d_activeList   = dalloc<int>( 2 * N );
     h->d_cellDt       = dalloc<double>( N );
     h->d_uRe          = dalloc<double>( N * h->ldc );
+    h->d_checkList    = dalloc<int>( 2 * N );
+    h->d_finFlag      = dalloc<unsigned char>( N );
+    CK( cudaMemset( h->d_finFlag, 0, N ) );
     h->d_fallbackList = dalloc<int>( N );
     h->d_ctl    = dalloc<Control>( 1 );
     CK( cudaMallocHost( &h->h_ctl, sizeof( Control ) ) );
@@ -565,7 +581,7 @@ void release( uqc_solver* h ) {
                     (void*)h->d_unitN, (void*)h->d_scaledN, (void*)h->d_nbr, (void*)h->d_boundary, (void*)h->d_u, (void*)h->d_lam,
                     (void*)h->d_bndNormal, (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
                     (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
-                    (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_cellDt, (void*)h->d_uRe, (void*)h->d_phiF, (void*)h->d_fallbackList,
+                    (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_cellDt, (void*)h->d_uRe, (void*)h->d_checkList, (void*)h->d_finFlag, (void*)h->d_phiF, (void*)h->d_fallbackList,
                     (void*)h->d_factorStore, (void*)h->d_factorLevel} )
         if( p ) cudaFree( p );
     if( h->h_ctl ) cudaFreeHost( h->h_ctl );
@@ -622,6 +638,9 @@ void step_lists( uqc_solver* h, KParams& P ) {
     P.activeList  = h->d_activeList;
     P.activeCount = h->d_ctl->nActive;
     P.listParity  = 1;
+    P.checkList   = h->d_checkList;
+    P.checkCount  = h->d_ctl->nCheck;
+    P.finFlag     = h->d_finFlag;
 }
 
 void enqueue_closure_phase( uqc_solver* h, KParams P ) {
@@ -635,7 +654,7 @@ void enqueue_closure_phase( uqc_solver* h, KParams P ) {
 
 void enqueue_update( uqc_solver* h, KParams P ) {
     step_lists( h, P );
-    P.finishInUpdate = h->cfg.newtonMode != 2 && h->finishInUpdate;
+    P.finishInUpdate = update_test_on( h );
     void* args[]     = {&P};
     launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
 }
@@ -724,8 +743,8 @@ unsigned long long device_bytes_of( const uqc_solver* h ) {
     const unsigned long long ldc = h->ldc, sq = (unsigned long long)h->nS * h->tab.nQ;
     const unsigned long long tab = ( (unsigned long long)h->tab.nQ * h->ld + 8 ) * ( 8 + 8 + 4 ) + h->tab.xi.size() * 8 + h->tab.nQ * 8;
     const unsigned long long d8  = N * ( 3 * ldc + 1 + 1 + 1 + 2 + 4 * F ) + ( N + 1 ) * sq;    // state (u, re-projected u, lambda), uQ, geometry, cell dt
-    const unsigned long long d4  = N * ( F + 1 + 1 + 1 + 1 + 2 + 1 );                         // nbr, boundary, level, status, iters, lists
-    return tab + 8 * d8 + 4 * d4 + ( mesh_has_walls( h->mesh ) ? 16 * N : 0 ) + sizeof( Control ) + 8 * 4096 + ( h->precision == UQC_MIXED && h->chord ? factor_store_bytes( h ) : 0 );
+    const unsigned long long d4  = N * ( F + 1 + 1 + 1 + 1 + 2 + 2 + 1 );                     // nbr, boundary, level, status, iters, lists
+    return tab + 8 * d8 + 4 * d4 + N + ( mesh_has_walls( h->mesh ) ? 16 * N : 0 ) + sizeof( Control ) + 8 * 4096 + ( h->precision == UQC_MIXED && h->chord ? factor_store_bytes( h ) : 0 );
 }
 
 void to_layout( const uqc_solver* h, const double* src, double* dst, int layout, bool toDevice ) {
@@ -897,7 +916,8 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
         return UQC_OK;
     }
     if( k == "update_test" ) {
-        h->finishInUpdate = value != 0.0;
+        if( value != 0.0 && value != 1.0 && value != -1.0 ) return fail( h, UQC_ERR_ARGUMENT, "update_test must be 1, 0 or -1" );
+        h->finishInUpdateOpt = int( value );
         ++h->planGen;
         return guarded( h, [&] {
             invalidate_lists( h );
