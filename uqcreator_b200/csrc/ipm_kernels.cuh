@@ -1186,13 +1186,17 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         double sq      = 0.0;
         double v0a = 0.0, v0b = 0.0;    // u_new(0, lane) and u_new(0, lane + 32), for the level rule
         for( int i = lane; i < nTj; i += 32 ) {    // beyond the level u stays zero (epilogue)
-            double r[NS];
+            // the re-projected moments first: their loads overlap the
+            // projection (uRe and u may alias, so a load after a store to u
+            // could not be moved ahead of it)
+            double old[NS], r[NS];
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) old[s] = P.uRe[cell * ldc + s * P.nT + i];
             project_lane<NS>( Gs, phiWf + i, P.ld, P.nQ, r );
 #pragma unroll
             for( int s = 0; s < NS; ++s ) {
-                const double old = P.uRe[cell * ldc + s * P.nT + i];
-                const double v   = old - r[s] * c;
-                const double gi  = old - v;
+                const double v   = old[s] - r[s] * c;
+                const double gi  = old[s] - v;
                 P.u[cell * ldc + s * P.nT + i] = v;
                 sq                             = fma( gi, gi, sq );
                 if( s == 0 && i < 32 ) v0a = v;
