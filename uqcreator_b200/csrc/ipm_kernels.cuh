@@ -1074,8 +1074,11 @@ __device__ __forceinline__ void finish_cell( const KParams& P, int cell, double 
 // rhs(s, i) = sum_k Gsum(s, k) phiWf(k, i). The reference accumulates the
 // projection face by face (momentsolver.cpp:413-416); the sums agree up to
 // reassociation. Each lane carries two outputs with two partial sums each.
-template <int CL>
+// FIN: with the next step's convergence test (P.finishInUpdate); the plain
+// instance (adaptive configurations, test off) carries none of its code.
+template <int CL, bool FIN>
 __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
+    const bool finish = FIN && P.finishInUpdate;
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
     __shared__ double blockRes[32];
@@ -1098,17 +1101,17 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
     double dtNext    = 1e300;    // lane 0: min dt of the cells finished for the next step
     int* nlist       = nullptr;
     unsigned* ncount = nullptr;
-    if( P.finishInUpdate ) step_list( P, 1, nlist, ncount );
+    if( finish ) step_list( P, 1, nlist, ncount );
     int* clist        = nullptr;
     unsigned* ccount  = nullptr;
-    if( P.finishInUpdate ) {
+    if( finish ) {
         clist  = P.checkList + size_t( ( P.ctl->steps + 1 ) & 1 ) * P.nCells;
         ccount = P.checkCount + ( ( P.ctl->steps + 1 ) & 1 );
     }
     WarpListBuf nbuf, cbuf;    // next step's active list and check list
     for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
         const int bc = P.boundary[cell];
-        if( P.finishInUpdate && lane == 0 && P.finFlag[cell] ) {
+        if( finish && lane == 0 && P.finFlag[cell] ) {
             // finished by the previous update: this step's closure status
             P.status[cell]  = UQC_CELL_CONVERGED;
             P.iters[cell]   = 0;
@@ -1121,10 +1124,10 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
                 const double u0 = P.uRe[cell * ldc];
                 res += fabs( u0 - P.uOld0[cell] ) * P.area[cell];
                 // its moments are the re-projected ones: the next closure test passes
-                if( P.finishInUpdate && P.nLevels == 1 ) finish_cell( P, cell, u0, dtNext );
+                if( finish && P.nLevels == 1 ) finish_cell( P, cell, u0, dtNext );
             }
             // with refinement levels k_check's epilogue applies the level rule
-            if( P.finishInUpdate && P.nLevels > 1 ) cbuf.push( lane, cell, clist, ccount );
+            if( finish && P.nLevels > 1 ) cbuf.push( lane, cell, clist, ccount );
             continue;
         }
         const int nTj    = P.nTLevel[P.level[cell]];
@@ -1204,7 +1207,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
                 if( s == 0 && i == 0 ) res += fabs( v - P.uOld0[cell] ) * P.area[cell];
             }
         }
-        if( P.finishInUpdate ) {
+        if( finish ) {
             // The next step's closure test, here: its gradient is
             // sum_k U(Lambda_k) phiWf(k, i) - u_new = uRe - u_new, because uRe was
             // re-projected from the same duals' nodal states (which this kernel
@@ -1245,7 +1248,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         }
         __syncwarp();
     }
-    if( P.finishInUpdate ) {
+    if( finish ) {
         nbuf.flush( lane, nlist, ncount );
         cbuf.flush( lane, clist, ccount );
     }
@@ -1278,9 +1281,9 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         C->activeCellsLast = C->activeCells;
         C->activeCells     = 0;
         // the next step's min starts from the cells finished here (+inf if none)
-        C->dtBits     = P.finishInUpdate ? ( (volatile unsigned long long*)&C->dtBitsNext )[0] : 0x7FF0000000000000ull;
+        C->dtBits     = finish ? ( (volatile unsigned long long*)&C->dtBitsNext )[0] : 0x7FF0000000000000ull;
         C->dtBitsNext = 0x7FF0000000000000ull;
-        C->listReady = P.finishInUpdate ? 1 : 0;
+        C->listReady = finish ? 1 : 0;
         C->workCounter  = 0;
         C->workCounter2 = 0;
         C->nFallback    = 0;

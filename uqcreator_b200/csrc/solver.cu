@@ -239,7 +239,8 @@ KParams make_params( const uqc_solver* h ) {
 template <int CL, int GROUP> struct Kern {
     static void* closure() { return (void*)&k_closure<CL, GROUP, double>; }
     static void* closure_mixed() { return (void*)&k_closure<CL, GROUP, float>; }
-    static void* update() { return (void*)&k_update<CL>; }
+    static void* update() { return (void*)&k_update<CL, true>; }
+    static void* update_plain() { return (void*)&k_update<CL, false>; }
     static void* init() { return (void*)&k_init<CL, GROUP>; }
     static void* meanvar() { return (void*)&k_meanvar<CL, GROUP>; }
 };
@@ -250,6 +251,7 @@ void* pick( int cl, int group, int which ) {
         switch( which ) {                                                                                                \
             case 0: return Kern<C, G>::closure();                                                                        \
             case 1: return Kern<C, G>::update();                                                                         \
+            case 5: return Kern<C, G>::update_plain();                                                                   \
             case 2: return Kern<C, G>::init();                                                                           \
             default: return Kern<C, G>::meanvar();                                                                       \
         }                                                                                                                \
@@ -411,6 +413,7 @@ void plan_launches( uqc_solver* h ) {
         h->updateSmem  = uTables + size_t( warps ) * perWarp;
         void* ku       = pick( cl, h->group, 1 );
         allow_dynamic_smem( ku );
+        allow_dynamic_smem( pick( cl, h->group, 5 ) );
         CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ku, h->updateBlock, h->updateSmem ) );
         h->updateGrid = std::max( 1, occ ) * h->numSMs;
         h->updateGrid = std::min( h->updateGrid, std::max( 1, ( h->mesh.nCells + warps - 1 ) / warps ) );
@@ -656,7 +659,7 @@ void enqueue_update( uqc_solver* h, KParams P ) {
     step_lists( h, P );
     P.finishInUpdate = update_test_on( h );
     void* args[]     = {&P};
-    launch( h, pick( h->cfg.closure, h->group, 1 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
+    launch( h, pick( h->cfg.closure, h->group, P.finishInUpdate ? 1 : 5 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
 }
 
 void enqueue_step( uqc_solver* h, KParams& P ) {
