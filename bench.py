@@ -42,17 +42,6 @@ sys.path.insert(0, str(ROOT))
 METRIC = "cell-steps/s mixed vs FP64 GPU at ≤1e-6 moment err; p50/p99 request latency"
 WORKLOAD = dict(nx=400, ny=250, degree=5, nquad=10, dim_xi=2)
 SAMPLE_NY = 10           # CPU sample: a 400 x 10 strip of the same mesh construction (8,000 cells)
-FP64_NOMINAL_TFLOPS = 40.0
-# FP64 FMA throughput measured on this pool's B200s with a register-only
-# micro-benchmark (independent DFMA chains, 16 warps/SM; mma.sync m8n8k4 f64
-# reaches the same rate): the ceiling of an FP64 kernel.
-FP64_MEASURED_TFLOPS = 36.5
-# DRAM bytes (read + write) of one k_closure launch per cell that takes Newton
-# iterations, from an ncu capture of a 12,000-cell step (2.35 MB for 1,532
-# active cells); the launch's traffic is this times its active cells.
-CLOSURE_DRAM_BYTES_PER_ACTIVE_CELL = 2.345472e6 / 1532
-
-
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -73,6 +62,47 @@ def work_per_cell_step(n_states, n_total, n_quad, n_faces=3):
     f_epi = 4 * n_quad * n
     f_flux = n_faces * 2 * n_quad * n
     return f_it, f_grad, f_epi, f_flux
+
+
+# Where each form computes the Newton system's parts: the Hessian assembly
+# (2 nQ n^2 flops per iteration), the factorisation and solves (n^3/3 + 2 n^2)
+# and everything else (ansatz, gradients, line search, epilogue: FP64 in both
+# forms).
+HESSIAN_UNIT = {"fp64": "fp64", "mixed": "fp32"}
+FACTOR_UNIT = {"fp64": "fp64", "mixed": "fp32"}
+# DRAM bytes (read + write) per cell that takes Newton iterations, from the ncu
+# captures of each form's closure kernel on a 12,000-cell step (1,532 active
+# cells): FP64 2.35 MB, mixed 23.6 MB (it reloads each active cell's held factor).
+CLOSURE_DRAM_BYTES_PER_ACTIVE_CELL = {"fp64": 2.345472e6 / 1532, "mixed": 23.6e6 / 1532}
+
+
+def closure_roofline(form, n_states, n_total, n_quad, cells, steps, ref_info, closure_ms, measured, active_cells):
+    """T_bound of the closure phase: max over units of (work on that unit /
+    its measured peak); achieved = algorithmic work / measured time, peak =
+    work / T_bound, frac = T_bound / time. Work uses the FP64 form's Newton
+    iteration and line-search counts (ref_info) for both forms, so the mixed
+    form is not credited for the extra iterations of its inexact Newton."""
+    n = n_states * n_total
+    iters = ref_info["newton_iterations"]
+    grads = iters + ref_info["line_search_trials"] + cells * steps    # + the initial test of every cell
+    work = {"fp64": 0.0, "fp32": 0.0, "tensor": 0.0}
+    work[HESSIAN_UNIT[form]] += iters * 2.0 * n_quad * n * n
+    work[FACTOR_UNIT[form]] += iters * (n ** 3 / 3.0 + 2.0 * n * n)
+    work["fp64"] += grads * 4.0 * n_quad * n + cells * steps * 4.0 * n_quad * n
+    hbm, bf16, src = peaks()
+    peak = {"fp64": measured.get("fp64_tflops"), "fp32": measured.get("fp32_tflops"), "tensor": bf16}
+    t_unit = {u: (w / steps) / (peak[u] * 1e12) * 1e3 for u, w in work.items() if w > 0 and peak[u]}
+    total = sum(work.values()) / steps
+    traffic = CLOSURE_DRAM_BYTES_PER_ACTIVE_CELL[form] * active_cells
+    t_unit["hbm"] = traffic / (hbm * 1e9) * 1e3
+    bound = max(t_unit, key=t_unit.get)
+    t_bound = t_unit[bound]
+    return {"bound": bound, "achieved": total / (closure_ms / 1e3) / 1e12, "peak": total / (t_bound / 1e3) / 1e12,
+            "unit": "TFLOP/s", "frac": t_bound / closure_ms, "traffic": traffic,
+            "traffic_unit": "bytes per closure phase (scaled from the form's ncu capture by its active cells)",
+            "t_bound_ms": t_unit, "closure_ms_per_launch": closure_ms, "flops_per_launch": total,
+            "peaks_tflops": {**peak, "tensor_source": f"bf16 {src} (MEASURED_PEAKS.json)"},
+            "hbm_peak_gbs": hbm, "kernels": "closure phase: k_check + k_closure (+ the mixed form's FP64 fallback pass)"}
 
 
 class Clocks:
@@ -188,6 +218,61 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def oracle_strip_errors(forms, steps=5):
+    """Error of each GPU form against the FP64 oracle (oracle/uqc_oracle.c) on
+    the 400 x 10 x 2 = 8,000-cell strip of the benchmark mesh construction (same
+    x resolution), `steps` steps from the initial state; outside the timed
+    region. Returns {form: {"moment_rel_l1", "mean_var_rel_l1_max"}}."""
+    from oracle.oracle import Oracle
+    from uqcreator_b200 import Solver, workloads as W, FP64, MIXED
+    toml = W.euler2d(nx=WORKLOAD["nx"], ny=SAMPLE_NY)
+    o = Oracle(toml, W.mesh_for(toml))
+    o.init_state()
+    o.step(steps)
+    uo = o.get_state()[0]
+    mvo = o.mean_var()
+    area = o.geometry()["area"][:, None]
+    out = {"sample": f"{WORKLOAD['nx']}x{SAMPLE_NY}x2 = {o.n_cells}-cell strip, {steps} steps from the initial state"}
+    for form in forms:
+        s = Solver(toml)
+        s.set_precision(MIXED if form == "mixed" else FP64)
+        s.init_state()
+        s.step(steps)
+        u = s.download_state()[0]
+        mv = s.mean_var()
+        s.close()
+        mv_err = (np.abs(mv - mvo) * area).sum(0) / (np.abs(mvo) * area).sum(0)
+        out[form] = {"moment_rel_l1": float(np.abs(u - uo).sum() / np.abs(uo).sum()),
+                     "mean_var_rel_l1_max": float(mv_err.max())}
+    return out
+
+
+def measure_peaks(device_index=0):
+    """FP64 and FP32 (no TF32) GEMM throughput of cuBLAS on this GPU (torch.matmul,
+    8192^3, best of 5 after a warm-up, CUDA events): the CUDA-core ceilings of
+    the FP64 and FP32 parts of the closure, measured in the same run."""
+    import torch
+    out = {}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        for name, dt, n in (("fp64_tflops", torch.float64, 8192), ("fp32_tflops", torch.float32, 8192)):
+            a = torch.randn(n, n, dtype=dt, device=f"cuda:{device_index}")
+            b = torch.randn(n, n, dtype=dt, device=f"cuda:{device_index}")
+            torch.matmul(a, b)
+            best = 1e30
+            for _ in range(5):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(); torch.matmul(a, b); e1.record(); torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            out[name] = 2.0 * n ** 3 / (best / 1e3) / 1e12
+            del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    out["how"] = "cuBLAS GEMM 8192^3 via torch.matmul (TF32 off), best of 5, CUDA events"
+    return out
+
+
 def run_serving(args, precision):
     """p50/p99 request latency: the first `serve_requests` requests of the seeded
     serving stream (Poisson arrivals, Burgers 1-D 200-20k cells / Euler 2-D
@@ -298,24 +383,17 @@ def run_b200(args, rank, world, local):
     r = results[chosen]
     value = cells * args.steps * world / (r["ms"] / 1e3)
     fp64_value = cells * args.steps * world / (results["fp64"]["ms"] / 1e3)
-    # roofline of the dominant kernel (the closure kernel): algorithmic flops per launch / mean launch time
-    f_it, f_grad, f_epi, f_flux = work_per_cell_step(s.n_states, s.n_total, s.n_quad)
-    # algorithmic work of the timed steps with the FP64 form's Newton iteration
-    # and line-search counts for both forms (the mixed form is not credited
-    # for the extra, cheaper iterations of its inexact Newton)
+    # roofline of the closure phase (the dominant kernels): algorithmic work
+    # of the timed steps, split by the unit it runs on, over the phase time
     inf = r["info"]
     ref_inf = results["fp64"]["info"]
-    flops = ref_inf["newton_iterations"] * f_it + (ref_inf["line_search_trials"] + cells * args.steps) * f_grad + cells * args.steps * f_epi
     closure_ms = r["phase"][0] / args.steps
-    achieved = flops / args.steps / (closure_ms / 1e3) / 1e12
-    hbm, bf16, src = peaks()
-    roof = {"bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s", "frac": achieved / bf16,
-            "traffic": CLOSURE_DRAM_BYTES_PER_ACTIVE_CELL * inf["active_cells"], "traffic_unit": "bytes per launch (scaled)",
-            "peak_source": src, "kernel": "k_closure (Newton + reconstruction)",
-            "closure_ms_per_launch": closure_ms, "update_ms_per_launch": r["phase"][1] / args.steps,
-            "fp64_nominal_tflops": FP64_NOMINAL_TFLOPS, "frac_of_fp64_nominal": achieved / FP64_NOMINAL_TFLOPS,
-            "fp64_measured_tflops": FP64_MEASURED_TFLOPS, "frac_of_fp64_measured": achieved / FP64_MEASURED_TFLOPS,
-            "flops_per_launch": flops / args.steps}
+    measured = measure_peaks(dev)
+    roof = closure_roofline(chosen, s.n_states, s.n_total, s.n_quad, cells, args.steps, ref_inf, closure_ms, measured,
+                            inf["active_cells"])
+    roof["update_ms_per_launch"] = r["phase"][1] / args.steps
+    roof["fp64_form"] = closure_roofline("fp64", s.n_states, s.n_total, s.n_quad, cells, args.steps, ref_inf,
+                                         results["fp64"]["phase"][0] / args.steps, measured, ref_inf["active_cells"])
     state_bytes = cells * s.n_states * s.n_total * 8
     h2d = 2 * state_bytes + 4 * cells
     d2h = 2 * state_bytes + 4 * cells
@@ -337,6 +415,8 @@ def run_b200(args, rank, world, local):
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
     }
+    if rank == 0 and not args.no_oracle_strip:
+        line["moment_rel_l1_vs_oracle_strip"] = oracle_strip_errors(forms)
     if args.serve_requests > 0:
         line["serving"] = run_serving(args, MIXED if chosen == "mixed" else FP64)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -424,6 +504,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-oracle-strip", action="store_true", help="skip the error against the oracle on the 8,000-cell strip")
     ap.add_argument("--serve-requests", type=int, default=120, help="requests of the serving stream (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=12.0, help="arrivals per second")
     ap.add_argument("--serve-budget-gb", type=float, default=100.0)

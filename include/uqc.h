@@ -205,16 +205,21 @@ int uqc_closure_solve_host( uqc_solver* h, int n, double* lambda, const double* 
 int uqc_closure_solve_device( uqc_solver* h, int n, double* d_lambda, const double* d_u, const unsigned* d_n_total,
                               int* d_status );
 
-/* For callers that must not allocate GPU memory: the same batched closure as
+/* For callers that must not allocate GPU memory: the batched FP64 closure of
  * uqc_closure_solve_device, on caller-owned DEVICE arrays, without any
  * cudaMalloc/cudaFree, not even on its first call. No counterpart in the
  * reference (its closure runs on the host).
  *
  * Who needs it: code that runs inside a framework owning all device memory
- * (its own arena or pool), code enqueued while another thread captures a CUDA
- * graph in global mode, and latency-critical loops that may not hit the
- * allocator. The handle may be freshly created (its own device state is never
- * touched); its configuration and basis tables come from host memory.
+ * (its own arena or pool, where a stray cudaMalloc would fragment or exceed
+ * the budget the framework manages), and latency-critical loops that may not
+ * reach the allocator, whose calls can synchronise the device. The handle may
+ * be freshly created (its own device state is never touched); its
+ * configuration and basis tables come from host memory.
+ *
+ * Precision: always the FP64 form, whatever the handle's precision (the mixed
+ * form keeps a per-cell factor store, which would need an allocation); its
+ * results are those of uqc_closure_solve_device on a UQC_FP64 handle.
  *
  * Scratch lives in one statically allocated device array inside this library
  * (UQC_NOALLOC_SCRATCH_BYTES, held on every GPU that loads the library until
@@ -231,9 +236,11 @@ int uqc_closure_solve_device( uqc_solver* h, int n, double* d_lambda, const doub
  * per cell or NULL (finest level); d_status: n uqc_cell_code values (required);
  * cuda_stream: the stream to enqueue on (NULL = the legacy default stream).
  * Asynchronous: results are valid once the stream has reached this point.
- * The first call on each device looks up the array's device address and sets
- * the kernel's shared-memory limit; make that first call before any stream
- * capture begins. */
+ * The first call on each device (with that device current) looks up the
+ * array's device address and sets the kernel's shared-memory limit; make that
+ * first call before any stream capture begins. The address is kept for the
+ * life of the process: do not call cudaDeviceReset on a device while this
+ * library is in use there. */
 #define UQC_NOALLOC_MAX_CELLS 65536
 #define UQC_NOALLOC_MAX_TABLE 8192
 #define UQC_NOALLOC_SCRATCH_BYTES ( 256 + 4 * UQC_NOALLOC_MAX_CELLS + 16 * UQC_NOALLOC_MAX_TABLE )

@@ -21,7 +21,7 @@ BUILD = PKG / "_build"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_SRCS = ["config.cpp", "tables.cpp", "mesh.cpp"]
-CUDA_SRCS = ["solver.cu"]
+CUDA_SRCS = ["solver.cu", "kernels_bb.cu", "kernels_euler2d.cu", "kernels_sw.cu"]
 
 
 def _sources():
@@ -41,18 +41,20 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         return LIB
     BUILD.mkdir(exist_ok=True)
     common = ["-std=c++17", "-O3", "-Xcompiler", "-fPIC", "-I" + str(ROOT / "include"), "-I" + str(CSRC)]
-    objs = []
+    jobs = []
     for s in HOST_SRCS:
         o = BUILD / (Path(s).stem + ".o")
-        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-I" + str(ROOT / "include"), "-I" + str(CSRC),
-               "-c", str(CSRC / s), "-o", str(o)]
-        _run(cmd, verbose)
-        objs.append(o)
+        jobs.append((["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-I" + str(ROOT / "include"), "-I" + str(CSRC),
+                      "-c", str(CSRC / s), "-o", str(o)], o))
     for s in CUDA_SRCS:
         o = BUILD / (Path(s).stem + ".o")
-        cmd = [NVCC, *ARCH, "-lineinfo", *common, "-Xptxas", "-v" if verbose else "-O3", "-c", str(CSRC / s), "-o", str(o)]
-        _run(cmd, verbose)
-        objs.append(o)
+        jobs.append(([NVCC, *ARCH, "-lineinfo", *common, "-Xptxas", "-v" if verbose else "-O3", "-c", str(CSRC / s), "-o", str(o)], o))
+    # the translation units compile in parallel (the kernel units dominate)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
+        for f in [ex.submit(_run, cmd, verbose) for cmd, _ in jobs]:
+            f.result()
+    objs = [o for _, o in jobs]
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [NVCC, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"]
     _run(cmd, verbose)

@@ -1,0 +1,25 @@
+// Kernel addresses per closure kind. The kernels are instantiated in one
+// translation unit per closure kind (kernels_bb.cu, kernels_euler2d.cu,
+// kernels_sw.cu); the host code launches them through these addresses.
+#pragma once
+
+namespace uqc {
+
+// `which`: the kernel; `group`: threads per cell where the kernel has variants.
+enum KernelId {
+    KERNEL_CLOSURE       = 0,    // k_closure, FP64 (group 32, 64 or 256)
+    KERNEL_UPDATE        = 1,    // k_update with the next step's convergence test
+    KERNEL_INIT          = 2,    // k_init (group 32 or 256)
+    KERNEL_MEANVAR       = 3,    // k_meanvar (group 32 or 256)
+    KERNEL_CLOSURE_MIXED = 4,    // k_closure, mixed form (group 32 or 64)
+    KERNEL_UPDATE_PLAIN  = 5,    // k_update without it
+    KERNEL_CHECK         = 6,    // k_check
+    KERNEL_PHASE_COUNTERS = 7    // device address of this unit's phase counters (diagnostic builds), else nullptr
+};
+
+// nullptr when there is no such variant
+void* kernel_bounded_barrier( int group, int which );
+void* kernel_euler2d( int group, int which );
+void* kernel_shallow_water( int group, int which );
+
+}    // namespace uqc

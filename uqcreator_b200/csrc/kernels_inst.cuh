@@ -1,0 +1,43 @@
+// Instantiation of every kernel of one closure kind (included once per kind
+// by kernels_<kind>.cu) and the table of their addresses.
+#pragma once
+#include "ipm_kernels.cuh"
+#include "kernels.h"
+
+namespace uqc {
+
+template <int CL> void* kernel_of( int group, int which ) {
+    switch( which ) {
+        case KERNEL_CLOSURE:
+            if( group == 32 ) return (void*)&k_closure<CL, 32, double>;
+            if( group == 64 ) return (void*)&k_closure<CL, 64, double>;
+            if( group == 256 ) return (void*)&k_closure<CL, 256, double>;
+            return nullptr;
+        case KERNEL_CLOSURE_MIXED:
+            if( group == 32 ) return (void*)&k_closure<CL, 32, float>;
+            if( group == 64 ) return (void*)&k_closure<CL, 64, float>;
+            return nullptr;
+        case KERNEL_UPDATE: return (void*)&k_update<CL, true>;
+        case KERNEL_UPDATE_PLAIN: return (void*)&k_update<CL, false>;
+        case KERNEL_INIT:
+            if( group == 32 ) return (void*)&k_init<CL, 32>;
+            if( group == 256 ) return (void*)&k_init<CL, 256>;
+            return nullptr;
+        case KERNEL_MEANVAR:
+            if( group == 32 ) return (void*)&k_meanvar<CL, 32>;
+            if( group == 256 ) return (void*)&k_meanvar<CL, 256>;
+            return nullptr;
+        case KERNEL_CHECK: return (void*)&k_check<CL>;
+        case KERNEL_PHASE_COUNTERS: {
+#ifdef UQC_PHASE_TIMERS
+            void* p = nullptr;
+            return cudaGetSymbolAddress( &p, g_phaseCycles ) == cudaSuccess ? p : nullptr;
+#else
+            return nullptr;
+#endif
+        }
+        default: return nullptr;
+    }
+}
+
+}    // namespace uqc

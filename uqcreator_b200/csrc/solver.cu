@@ -26,6 +26,7 @@
 
 #include "host.h"
 #include "ipm_kernels.cuh"
+#include "kernels.h"
 #include "uqc.h"
 
 using namespace uqc;
@@ -236,54 +237,18 @@ KParams make_params( const uqc_solver* h ) {
 }
 
 // ---- kernel dispatch on (closure kind, group size) ------------------------
-template <int CL, int GROUP> struct Kern {
-    static void* closure() { return (void*)&k_closure<CL, GROUP, double>; }
-    static void* closure_mixed() { return (void*)&k_closure<CL, GROUP, float>; }
-    static void* update() { return (void*)&k_update<CL, true>; }
-    static void* update_plain() { return (void*)&k_update<CL, false>; }
-    static void* init() { return (void*)&k_init<CL, GROUP>; }
-    static void* meanvar() { return (void*)&k_meanvar<CL, GROUP>; }
-};
-
+// The kernels are instantiated per closure kind in kernels_<kind>.cu (three
+// translation units compiled in parallel); each exports its kernel addresses.
 void* pick( int cl, int group, int which ) {
-#define PICK( C, G )                                                                                                     \
-    if( cl == C && group == G ) {                                                                                        \
-        switch( which ) {                                                                                                \
-            case 0: return Kern<C, G>::closure();                                                                        \
-            case 1: return Kern<C, G>::update();                                                                         \
-            case 5: return Kern<C, G>::update_plain();                                                                   \
-            case 2: return Kern<C, G>::init();                                                                           \
-            default: return Kern<C, G>::meanvar();                                                                       \
-        }                                                                                                                \
-    }
-    if( which == 0 && group == 64 ) {    // two warps per cell: closure kernel only
-        if( cl == 0 ) return Kern<0, 64>::closure();
-        if( cl == 1 ) return Kern<1, 64>::closure();
-        if( cl == 2 ) return Kern<2, 64>::closure();
-    }
-    if( which == 4 ) {    // mixed-form closure kernel, warp or two-warp groups
-        if( group == 32 ) {
-            if( cl == 0 ) return Kern<0, 32>::closure_mixed();
-            if( cl == 1 ) return Kern<1, 32>::closure_mixed();
-            if( cl == 2 ) return Kern<2, 32>::closure_mixed();
-        }
-        if( group == 64 ) {
-            if( cl == 0 ) return Kern<0, 64>::closure_mixed();
-            if( cl == 1 ) return Kern<1, 64>::closure_mixed();
-            if( cl == 2 ) return Kern<2, 64>::closure_mixed();
-        }
-    }
-    PICK( 0, 32 ) PICK( 0, 256 ) PICK( 1, 32 ) PICK( 1, 256 ) PICK( 2, 32 ) PICK( 2, 256 )
-#undef PICK
-    throw ConfigError( "no kernel for this closure" );
+    void* fn = nullptr;
+    if( cl == 0 ) fn = kernel_bounded_barrier( group, which );
+    if( cl == 1 ) fn = kernel_euler2d( group, which );
+    if( cl == 2 ) fn = kernel_shallow_water( group, which );
+    if( !fn ) throw ConfigError( "no kernel for this closure" );
+    return fn;
 }
 
-void* pick_check( int cl ) {
-    if( cl == 0 ) return (void*)&k_check<0>;
-    if( cl == 1 ) return (void*)&k_check<1>;
-    if( cl == 2 ) return (void*)&k_check<2>;
-    throw ConfigError( "no kernel for this closure" );
-}
+void* pick_check( int cl ) { return pick( cl, 32, KERNEL_CHECK ); }
 
 int closure_np( int cl ) { return cl == 0 ? 1 : ( cl == 1 ? 10 : 3 ); }
 
@@ -364,6 +329,45 @@ void plan_mixed( uqc_solver* h, int maxSmem ) {
     h->mixedWhy.clear();
 }
 
+// Launch shape of the FP64 closure kernel k_closure for a handle's
+// configuration: threads per cell (group), threads per CTA, dynamic shared
+// memory and whether the basis tables are staged in it. Shared by the
+// allocating entry points (plan_launches) and the no-alloc closure.
+struct ClosureShape {
+    int group = 32, block = 256;
+    size_t smem       = 0;
+    bool tablesInSmem = false;
+};
+
+ClosureShape fp64_closure_shape( const uqc_solver* h, int maxSmem ) {
+    const int cl = h->cfg.closure, nT = h->tab.nT, nQ = h->tab.nQ, nS = h->nS;
+    const size_t n      = size_t( nS ) * nT;
+    const size_t tables = 2 * ( size_t( nQ ) * h->ld + 4 ) * sizeof( double );
+    const size_t wsCell = cell_ws_doubles( nS, nT, nQ, closure_np( cl ) ) * sizeof( double );
+    const bool canStage = tables <= 96 * 1024 && tables + wsCell <= size_t( maxSmem );
+    ClosureShape s;
+    {
+        // automatic: read the tables through L1 when that lets more cells share a CTA
+        const int cap     = n <= 32 ? 8 : 4;
+        const int staged  = canStage ? int( std::min<size_t>( cap, ( size_t( maxSmem ) - tables ) / wsCell ) ) : 0;
+        const int through = int( std::min<size_t>( cap, size_t( maxSmem ) / wsCell ) );
+        s.tablesInSmem    = canStage && ( h->closureTablesOpt == 1 || ( h->closureTablesOpt == -1 && staged >= through ) );
+    }
+    const size_t avail = size_t( maxSmem ) - ( s.tablesInSmem ? tables : 0 );
+    // small systems: a warp per cell, up to 8 per CTA; larger: two warps per
+    // cell (named barriers), up to 4 per CTA; a whole CTA per cell otherwise
+    const int fit = int( std::min<size_t>( 8, avail / wsCell ) );
+    s.group       = h->closureGroupOverride ? h->closureGroupOverride : ( n <= 32 ? 32 : 64 );
+    if( s.group == 32 && fit < 1 ) s.group = 256;
+    if( s.group == 64 && fit < ( h->closureGroupOverride ? 1 : 2 ) ) s.group = 256;
+    s.block                = s.group == 32 ? 32 * fit : ( s.group == 64 ? 64 * std::min( 4, fit ) : 256 );
+    const int groupsPerCta = s.block / s.group;
+    s.smem                 = wsCell * groupsPerCta + ( s.tablesInSmem ? tables : 0 );
+    if( s.smem > size_t( maxSmem ) )
+        throw ConfigError( "closure workspace (" + std::to_string( s.smem ) + " B) exceeds shared memory; reduce moments or nodes" );
+    return s;
+}
+
 void plan_launches( uqc_solver* h ) {
     ++h->planGen;
     int dev;
@@ -378,26 +382,11 @@ void plan_launches( uqc_solver* h ) {
     const size_t tables  = 2 * ( size_t( nQ ) * h->ld + 4 ) * sizeof( double );
     const size_t wsCell  = cell_ws_doubles( nS, nT, nQ, closure_np( cl ) ) * sizeof( double );
     h->tablesInSmem = tables <= 96 * 1024 && tables + wsCell <= size_t( maxSmem );
-    {
-        // automatic: read the tables through L1 when that lets more cells share a CTA
-        const int cap     = n <= 32 ? 8 : 4;
-        const int staged  = int( std::min<size_t>( cap, ( size_t( maxSmem ) - tables ) / wsCell ) );
-        const int through = int( std::min<size_t>( cap, size_t( maxSmem ) / wsCell ) );
-        h->closureTablesInSmem =
-            h->tablesInSmem && ( h->closureTablesOpt == 1 || ( h->closureTablesOpt == -1 && staged >= through ) );
-    }
-    const size_t avail = size_t( maxSmem ) - ( h->closureTablesInSmem ? tables : 0 );
-    // small systems: a warp per cell, up to 8 per CTA; larger: two warps per
-    // cell (named barriers), up to 4 per CTA; a whole CTA per cell otherwise
-    const int fit        = int( std::min<size_t>( 8, avail / wsCell ) );
-    h->closureGroup      = h->closureGroupOverride ? h->closureGroupOverride : ( n <= 32 ? 32 : 64 );
-    if( h->closureGroup == 32 && fit < 1 ) h->closureGroup = 256;
-    if( h->closureGroup == 64 && fit < ( h->closureGroupOverride ? 1 : 2 ) ) h->closureGroup = 256;
-    h->closureBlock        = h->closureGroup == 32 ? 32 * fit : ( h->closureGroup == 64 ? 64 * std::min( 4, fit ) : 256 );
-    const int groupsPerCta = h->closureBlock / h->closureGroup;
-    h->closureSmem         = wsCell * groupsPerCta + ( h->closureTablesInSmem ? tables : 0 );
-    if( h->closureSmem > size_t( maxSmem ) )
-        throw ConfigError( "closure workspace (" + std::to_string( h->closureSmem ) + " B) exceeds shared memory; reduce moments or nodes" );
+    const ClosureShape cs  = fp64_closure_shape( h, maxSmem );
+    h->closureTablesInSmem = cs.tablesInSmem;
+    h->closureGroup        = cs.group;
+    h->closureBlock        = cs.block;
+    h->closureSmem         = cs.smem;
     void* kc = pick( cl, h->closureGroup, 0 );
     allow_dynamic_smem( kc );
     int occ = 0;
@@ -1720,11 +1709,21 @@ int uqc_mesh_tri_jitter( int nx, int ny, double jitter, unsigned long long seed,
 // Diagnostic builds only: the per-phase cycle counters of k_closure (summed
 // over CTAs since the last call), then reset.
 extern "C" int uqc_debug_phase_cycles( double* out32 ) {
-    unsigned long long v[32];
-    if( cudaMemcpyFromSymbol( v, g_phaseCycles, sizeof( v ) ) != cudaSuccess ) return UQC_ERR_CUDA;
-    for( int i = 0; i < 32; ++i ) out32[i] = double( v[i] );
-    std::memset( v, 0, sizeof( v ) );
-    return cudaMemcpyToSymbol( g_phaseCycles, v, sizeof( v ) ) == cudaSuccess ? UQC_OK : UQC_ERR_CUDA;
+    for( int i = 0; i < 32; ++i ) out32[i] = 0.0;
+    for( int cl = 0; cl < 3; ++cl ) {    // one counter array per kernel translation unit
+        void* addr = nullptr;
+        try {
+            addr = pick( cl, 32, KERNEL_PHASE_COUNTERS );
+        } catch( ... ) {
+            return UQC_ERR_CUDA;
+        }
+        unsigned long long v[32];
+        if( cudaMemcpy( v, addr, sizeof( v ), cudaMemcpyDeviceToHost ) != cudaSuccess ) return UQC_ERR_CUDA;
+        for( int i = 0; i < 32; ++i ) out32[i] += double( v[i] );
+        std::memset( v, 0, sizeof( v ) );
+        if( cudaMemcpy( addr, v, sizeof( v ), cudaMemcpyHostToDevice ) != cudaSuccess ) return UQC_ERR_CUDA;
+    }
+    return UQC_OK;
 }
 #endif
 
@@ -1798,24 +1797,19 @@ extern "C" int uqc_closure_solve_device_noalloc( uqc_solver* h, int n, double* d
         P.workCounter  = &ctl->workCounter;
         P.activeList   = nullptr;
         P.fallbackList = nullptr;
-        // launch shape of k_closure, as plan_launches chooses it
+        // the FP64 kernel in the launch shape that the allocating entry point uses
         int dev = 0, maxSmem = 0, sms = 0, occ = 0;
         CK( cudaGetDevice( &dev ) );
         CK( cudaDeviceGetAttribute( &maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev ) );
         CK( cudaDeviceGetAttribute( &sms, cudaDevAttrMultiProcessorCount, dev ) );
-        const int nS = h->nS, nT = h->tab.nT, nQ = h->tab.nQ, cl = h->cfg.closure;
-        const int group = size_t( nS ) * nT <= 32 ? 32 : 256, block = 256;
-        const size_t tables = 2 * ( size_t( nQ ) * h->ld + 4 ) * sizeof( double );
-        const size_t ws     = cell_ws_doubles( nS, nT, nQ, closure_np( cl ) ) * sizeof( double ) * ( block / group );
-        P.tablesInSmem      = tables + ws <= size_t( maxSmem ) && tables <= 96 * 1024;
-        const size_t smem   = ws + ( P.tablesInSmem ? tables : 0 );
-        if( smem > size_t( maxSmem ) ) throw ConfigError( "closure workspace exceeds shared memory" );
-        void* fn = pick( cl, group, 0 );
+        const ClosureShape cs = fp64_closure_shape( h, maxSmem );
+        P.tablesInSmem        = cs.tablesInSmem;
+        void* fn              = pick( h->cfg.closure, cs.group, 0 );
         allow_dynamic_smem( fn );
-        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, fn, block, smem ) );
+        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, fn, cs.block, cs.smem ) );
         int mode     = 0;
         void* args[] = {&P, &mode};
-        CK( cudaLaunchKernel( fn, dim3( std::max( 1, occ ) * sms ), dim3( block ), args, smem, st ) );
+        CK( cudaLaunchKernel( fn, dim3( std::max( 1, occ ) * sms ), dim3( cs.block ), args, cs.smem, st ) );
         return UQC_OK;
     } );
 }
