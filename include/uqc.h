@@ -71,6 +71,11 @@ typedef struct uqc_info {
     int newton_mode;       /* 0 reference SolveClosure, 1 guarded, 2 SolveClosureSafe */
     double t;              /* simulated time */
     long long steps;       /* time steps taken */
+    int mixed_form;        /* how UQC_MIXED time steps run the closure: 0 one kernel (FP32 Hessian on
+                              CUDA cores), 1 rounds of chord / Hessian / inverse kernels with the Hessian
+                              on CUDA cores, 2 the same with the Hessian on the tensor cores; -1 before
+                              the device side is set up (option "mixed_hessian") */
+    int mixed_rounds;      /* re-factorisation rounds per time step of forms 1 and 2 */
 } uqc_info;
 
 typedef struct uqc_step_info {
@@ -138,6 +143,19 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *   "mixed_max_iterations"  UQC_MIXED: Newton iterations of the FP32 pass
  *                    after which a cell continues in the FP64 form (>= 2;
  *                    0 = the configured maxIterations).
+ *   "mixed_hessian"  UQC_MIXED time steps of the 2-D Euler closure (one
+ *                    refinement level): -1 (default) rounds with the Hessian
+ *                    on the tensor cores where its basis-pair table fits one
+ *                    MMA (at most 256 pairs, i.e. total degree <= 5 in two
+ *                    uncertainties), else on CUDA cores; 0 the single-kernel
+ *                    form; 1 rounds with the CUDA-core Hessian; 2 rounds with
+ *                    the tensor-core Hessian (UQC_ERR_CONFIG where it does
+ *                    not fit). Rounds: a chord kernel (a warp per cell, held
+ *                    inverse H0^-1 in FP32, FP64 gradients and tests), then
+ *                    per round the Hessians and inverses of the cells whose
+ *                    held inverse stopped contracting, and the chord kernel
+ *                    again; cells left after the last round finish in FP64.
+ *   "mixed_rounds"   re-factorisation rounds per step of the forms above (1-3, default 3).
  * Unknown keys return UQC_ERR_ARGUMENT. */
 int uqc_set_option( uqc_solver* h, const char* key, double value );
 
@@ -310,6 +328,13 @@ int uqc_last_timing( uqc_solver* h, float* ms3 );
  * this function again after writing (it makes the next step test every cell
  * for convergence instead of the list the last update prepared). */
 int uqc_device_state( uqc_solver* h, double** d_u, double** d_lambda );
+/* Inverse Hessians H^-1 of the mixed form's re-factorisation (FP32) for n
+ * cells of the resident state (cells: host array of cell ids), with the
+ * Hessian assembled on CUDA cores (form 1) or on the tensor cores (form 2);
+ * out: n x (nS nT)^2 floats, each cell's H^-1 row-major. Clears the handle's
+ * held inverses. 2-D Euler with one refinement level (uqc_info.mixed_form >= 1).
+ * No reference counterpart: a diagnostic of the tensor-core Hessian. */
+int uqc_debug_mixed_inverse( uqc_solver* h, int n, const int* cells, int form, float* out );
 /* Number of kernel launches issued by the last uqc_step / uqc_solve_closure. */
 int uqc_last_launch_count( uqc_solver* h );
 /* CUDA stream of the handle (cudaStream_t). */

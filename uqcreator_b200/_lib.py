@@ -30,6 +30,7 @@ EXPORTS = [
     "uqc_set_option", "uqc_step_async", "uqc_step_query", "uqc_device_bytes", "uqc_server_create",
     "uqc_server_destroy", "uqc_server_last_error", "uqc_server_submit", "uqc_server_progress",
     "uqc_server_request", "uqc_server_release", "uqc_server_request_error", "uqc_export_state", "uqc_write_vtk",
+    "uqc_debug_mixed_inverse",
 ]
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
 NOALLOC_MAX_CELLS = 65536
@@ -45,7 +46,7 @@ class Info(C.Structure):
     _fields_ = [("n_cells", C.c_int), ("n_states", C.c_int), ("n_total", C.c_int), ("n_quad", C.c_int),
                 ("n_levels", C.c_int), ("dim_xi", C.c_int), ("n_faces", C.c_int), ("mesh_dim", C.c_int),
                 ("n_total_level", C.c_int * 16), ("precision", C.c_int), ("newton_mode", C.c_int),
-                ("t", C.c_double), ("steps", C.c_longlong)]
+                ("t", C.c_double), ("steps", C.c_longlong), ("mixed_form", C.c_int), ("mixed_rounds", C.c_int)]
 
 
 class StepInfo(C.Structure):
@@ -123,6 +124,7 @@ def lib() -> C.CDLL:
         "uqc_server_request_error": ([_vp, C.c_longlong], C.c_char_p),
         "uqc_export_state": ([_vp, C.c_char_p], C.c_int),
         "uqc_write_vtk": ([_vp, C.c_char_p], C.c_int),
+        "uqc_debug_mixed_inverse": ([_vp, C.c_int, _ip, C.c_int, C.POINTER(C.c_float)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -1,0 +1,674 @@
+// Mixed-form closure of the time step, split by what bounds each part.
+//
+// The damped Newton of Closure::SolveClosure (closure.cpp:133-193) spends
+// most of its iterations on directions and line-search trials; the Hessian
+// and its factorisation are needed only when a cell's held inverse stops
+// contracting (an inexact, chord Newton). The three kernels below split the
+// work accordingly, and a time step runs them in rounds:
+//
+//   k_chord   a warp per cell, about 8 KB of shared memory per cell (duals,
+//             moments, gradients and nodal states; no Hessian), so that many
+//             cells share an SM and hide each other's FP64 latency. Newton
+//             directions d = H0^-1 g from the cell's held inverse (FP32, read
+//             from HBM/L2 as one coalesced mat-vec), FP64 trial gradients,
+//             line search and convergence test, then the epilogue of a
+//             converged cell. A cell without a usable inverse is appended to
+//             the round's re-factor list and leaves.
+//   k_hess_tc the Hessians of the listed cells on the tensor cores: every
+//             block (l, m) of a cell's Hessian is sum_k phi_kj phi_ki wt_k
+//             DU_lm(Lambda_k) (closure.cpp:255-271, the pair-product table
+//             _hPartial of :69-72), i.e. the product of a constant table Q
+//             (pairs j <= i x nodes) with the cell's nodal DU (nodes x blocks).
+//             Twelve cells' DU rows form the A operand (M = 128) and Q the B
+//             operand (N = pairs), both BF16 split into a high and a low part
+//             (three products: FP32-level accuracy), accumulated in FP32 in
+//             tensor memory by tcgen05.mma and written out per cell.
+//   k_invert  per cell (two warps): the Hessian (from k_hess_tc, or assembled
+//             on CUDA cores), Cholesky factor (FP32), inverse H^-1 = U^-1
+//             U^-T written to the cell's store slot for the next k_chord round.
+//
+// The gradient, the line-search and convergence tests, the duals and the
+// moments stay FP64, so a converged cell meets the FP64 tolerance. Cells that
+// the mixed form cannot finish (iteration or refinement limit, FP32 factor
+// not positive definite, more re-factorisations than rounds) go to the FP64
+// kernel's fallback list with their last accepted duals.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "ipm_kernels.cuh"
+
+namespace uqc {
+
+// ---------------------------------------------------------------- chord kernel
+
+// Per-warp workspace of k_chord (doubles): duals, trial duals and moments at
+// the finest stride nT; gradient, trial gradient and direction (compact, n =
+// NS nTj); nodal states uk (NS x nQ); reduction scratch; the gradient in FP32.
+struct ChordWs {
+    double *lam, *lamN, *uh, *g, *gN, *d, *uk, *red;
+    float* gf;
+};
+
+__host__ __device__ inline size_t chord_ws_doubles( int nS, int nT, int nQ ) {
+    auto a4          = []( size_t x ) { return ( x + 3 ) & ~size_t( 3 ); };
+    const size_t ldc = size_t( nS ) * nT;
+    return 6 * a4( ldc ) + a4( size_t( nS ) * nQ ) + 32 + a4( ( ldc + 1 ) / 2 );
+}
+
+__device__ inline ChordWs chord_carve( double* p, int nS, int nT, int nQ ) {
+    auto a4          = []( size_t x ) { return ( x + 3 ) & ~size_t( 3 ); };
+    const size_t ldc = a4( size_t( nS ) * nT );
+    ChordWs w;
+    w.lam  = p;
+    w.lamN = p + ldc;
+    w.uh   = p + 2 * ldc;
+    w.g    = p + 3 * ldc;
+    w.gN   = p + 4 * ldc;
+    w.d    = p + 5 * ldc;
+    w.uk   = p + 6 * ldc;
+    w.red  = w.uk + a4( size_t( nS ) * nQ );
+    w.gf   = reinterpret_cast<float*>( w.red + 32 );
+    return w;
+}
+
+// Lists of the mixed form's rounds: round r's re-factor list is the input of
+// k_hess_tc / k_invert round r and of k_chord round r + 1.
+__device__ __forceinline__ int* refactor_list( const KParams& P, int r ) { return P.v2Lists + size_t( r ) * P.nCells; }
+
+// gStore slot of a cell: the gradient at its accepted duals (compact, n values)
+// and its norm at index ldc.
+__device__ __forceinline__ double* gslot( const KParams& P, int cell ) { return P.gStore + size_t( cell ) * P.gStride; }
+
+// d = H0^-1 g with the cell's held inverse (FP32, n x n, symmetric, row-major):
+// lane o sums column o, d_o = sum_j Hinv(j, o) g_j; each step j reads a row of
+// the inverse with consecutive lanes on consecutive addresses.
+__device__ __forceinline__ void chord_direction( const float* __restrict__ Hinv, int n, const float* gf, double* d, int lane ) {
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    const int o0 = lane, o1 = lane + 32, o2 = lane + 64, o3 = lane + 96;
+    for( int j = 0; j < n; ++j ) {
+        const float gj  = gf[j];
+        const float* rj = Hinv + size_t( j ) * n;
+        if( o0 < n ) a0 = fmaf( __ldg( rj + o0 ), gj, a0 );
+        if( o1 < n ) a1 = fmaf( __ldg( rj + o1 ), gj, a1 );
+        if( o2 < n ) a2 = fmaf( __ldg( rj + o2 ), gj, a2 );
+        if( o3 < n ) a3 = fmaf( __ldg( rj + o3 ), gj, a3 );
+    }
+    if( o0 < n ) d[o0] = double( a0 );
+    if( o1 < n ) d[o1] = double( a1 );
+    if( o2 < n ) d[o2] = double( a2 );
+    if( o3 < n ) d[o3] = double( a3 );
+    for( int o = lane + 128; o < n; o += 32 ) {    // systems beyond 128 duals
+        float a = 0.f;
+        for( int j = 0; j < n; ++j ) a = fmaf( __ldg( Hinv + size_t( j ) * n + o ), gf[j], a );
+        d[o] = double( a );
+    }
+}
+
+// Chord Newton rounds of the mixed form, step mode. round 0 takes the step's
+// active list (cells k_check or the previous k_update found unconverged);
+// round r > 0 takes the cells re-factored in round r - 1. A cell whose held
+// inverse is missing or stops contracting goes to the re-factor list of this
+// round (the last round: to the FP64 fallback list).
+template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_chord( KParams P, int round ) {
+    constexpr int NS = Closure<CL>::NS;
+    extern __shared__ __align__( 16 ) double smem[];
+    if( !P.ctl->active ) return;
+    const int* inList;
+    int nIn;
+    if( round == 0 ) {
+        int* al;
+        unsigned* ac;
+        step_list( P, 0, al, ac );
+        inList = al;
+        nIn    = int( *ac );
+    }
+    else {
+        inList = refactor_list( P, round - 1 );
+        nIn    = int( P.ctl->v2Count[round - 1] );
+    }
+    if( nIn == 0 ) return;
+    const bool last = round >= P.v2Rounds;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Grp<32> g{lane, 0};
+    const double *phi = P.phi, *phiWf = P.phiWf;
+    double* base = smem;
+    if( P.tablesInSmem ) {
+        const size_t tn = size_t( P.nQ ) * P.ld + 4;
+        for( size_t i = threadIdx.x; i < tn; i += blockDim.x ) {
+            base[i]      = i < size_t( P.nQ ) * P.ld ? P.phi[i] : 0.0;
+            base[tn + i] = i < size_t( P.nQ ) * P.ld ? P.phiWf[i] : 0.0;
+        }
+        phi   = base;
+        phiWf = base + tn;
+        base += 2 * tn;
+        __syncthreads();
+    }
+    ChordWs w        = chord_carve( base + warp * chord_ws_doubles( NS, P.nT, P.nQ ), NS, P.nT, P.nQ );
+    const size_t ldc = size_t( NS ) * P.nT;
+    const double eps = P.eps;
+    const bool guard = P.newtonMode != 0;
+    unsigned long long itSum = 0, lsSum = 0;
+    int activeSum = 0, fbSum = 0;
+    double dtMin = 1e300;
+    int* outList      = last ? P.fallbackList : refactor_list( P, round );
+    unsigned* outCnt  = last ? P.fallbackCount : &P.ctl->v2Count[round];
+    unsigned* counter = &P.ctl->v2Work[round];
+    for( ;; ) {
+        int item = 0;
+        if( lane == 0 ) item = int( atomicAdd( counter, 1u ) );
+        item = __shfl_sync( 0xffffffffu, item, 0 );
+        if( item >= nIn ) break;
+        const int cell = inList[item];
+        if( round > 0 && P.factorLevel[cell] == -2 ) continue;    // not positive definite: in the FP64 list already
+        const int lev = int( P.level[cell] ), nTj = P.nTLevel[lev], n = NS * nTj;
+        bool bad = false;
+        for( int idx = lane; idx < int( ldc ); idx += 32 ) {
+            const double a = P.lam[cell * ldc + idx], b = P.u[cell * ldc + idx];
+            w.lam[idx]  = a;
+            w.lamN[idx] = a;    // trial duals beyond the cell's level stay the accepted ones
+            w.uh[idx]   = b;
+            bad         = bad || !isfinite( a ) || !isfinite( b );
+        }
+        const double* gs = gslot( P, cell );
+        for( int idx = lane; idx < n; idx += 32 ) w.g[idx] = gs[idx];
+        double gn = gs[ldc];
+        bad       = __any_sync( 0xffffffffu, bad );
+        int iters = round == 0 ? 0 : P.chordIters[cell];
+        const int iters0 = iters;    // iterations of earlier rounds of this step
+        int ls = 0, rc = -1;         // rc: uqc_cell_code once decided
+        bool refactor = !bad && P.factorLevel[cell] != nTj;
+        bool fresh    = round > 0;    // the inverse was formed at the current duals
+        const float* Hinv = P.factorStore + size_t( cell ) * P.factorStride;
+        __syncwarp();
+        // lamN <- lam + c d (closure.cpp:273-279), Lambda and U at the nodes,
+        // the trial gradient (closure.cpp:234-253) and its norm
+        auto trial = [&]( double c ) {
+            for( int idx = lane; idx < NS * nTj; idx += 32 ) {
+                const int s = idx / nTj, i = idx - s * nTj;
+                w.lamN[s * P.nT + i] = w.lam[s * P.nT + i] + c * w.d[idx];
+            }
+            __syncwarp();
+            for( int k = lane; k < P.nQ; k += 32 ) {
+                const double* row = phi + size_t( k ) * P.ld;
+                double Lk[NS], y[NS];
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) Lk[s] = 0.0;
+                for( int i = 0; i < nTj; ++i ) {
+                    const double r = row[i];
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) Lk[s] = fma( w.lamN[s * P.nT + i], r, Lk[s] );
+                }
+                Closure<CL>::U( Lk, y, true, P.phys );
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) w.uk[s * P.nQ + k] = y[s];
+            }
+            __syncwarp();
+            const double sq = gradient_sums<NS, 32>( g, P, phiWf, w.uk, w.uh, nTj, w.gN, nullptr );
+            return sqrt( group_sum<32>( g, sq, w.red ) );
+        };
+        if( bad ) {
+            rc = UQC_CELL_NONFINITE;    // the FP64 form reports it
+        }
+        else {
+            while( !refactor && rc < 0 ) {
+                if( iters >= P.maxIter ) {
+                    rc = UQC_CELL_MAX_ITER;
+                    break;
+                }
+                for( int j = lane; j < n; j += 32 ) w.gf[j] = float( w.g[j] );
+                __syncwarp();
+                chord_direction( Hinv, n, w.gf, w.d, lane );
+                __syncwarp();
+                ++iters;
+                double gnN = trial( -1.0 );
+                if( !fresh && !( gnN < gn ) ) {    // no decrease with a held inverse: a new one, same duals
+                    refactor = true;
+                    break;
+                }
+                double step = 1.0;
+                int refine  = 0;
+                bool done   = false;
+                while( gn < gnN || ( guard && !isfinite( gnN ) ) ) {
+                    step *= 0.5;
+                    ++ls;
+                    gnN = trial( -step );
+                    if( gnN < eps ) {
+                        done = true;
+                        break;
+                    }
+                    if( ++refine > 1000 ) {
+                        rc = UQC_CELL_LINE_SEARCH;
+                        break;
+                    }
+                }
+                if( rc >= 0 ) break;
+                // accept: lam <- lamN, g <- gN (the gradient at the accepted duals)
+                for( int idx = lane; idx < int( ldc ); idx += 32 ) w.lam[idx] = w.lamN[idx];
+                for( int idx = lane; idx < n; idx += 32 ) w.g[idx] = w.gN[idx];
+                __syncwarp();
+                if( done || gnN < eps ) {
+                    rc = UQC_CELL_CONVERGED;
+                    break;
+                }
+                const bool held = !fresh;
+                const double gPrev = gn;
+                gn    = gnN;
+                fresh = false;
+                if( held && gnN > P.chordTheta * gPrev ) refactor = true;    // contracts too slowly: re-factor
+            }
+        }
+        for( int idx = lane; idx < int( ldc ); idx += 32 ) P.lam[cell * ldc + idx] = w.lam[idx];
+        if( rc == UQC_CELL_CONVERGED ) {
+            if( lane == 0 ) {
+                P.status[cell] = rc;
+                P.iters[cell]  = iters;
+                ++activeSum;
+            }
+            itSum += iters - iters0;
+            lsSum += ls;
+            // uk holds U at the accepted duals (the last trial evaluated)
+            const double dloc = cell_epilogue<CL, 32>( g, P, phiWf, w.uh, w.uk, cell, lev, nTj, w.red );
+            dtMin             = dloc < dtMin ? dloc : dtMin;
+        }
+        else if( refactor && !last ) {
+            double* gsw = gslot( P, cell );
+            for( int idx = lane; idx < n; idx += 32 ) gsw[idx] = w.g[idx];
+            if( lane == 0 ) {
+                gsw[ldc]              = gn;
+                P.chordIters[cell]    = iters;
+                outList[atomicAdd( outCnt, 1u )] = cell;
+            }
+            itSum += iters - iters0;
+            lsSum += ls;
+        }
+        else {
+            // the FP64 form continues from the last accepted duals
+            if( lane == 0 ) {
+                P.fallbackList[atomicAdd( P.fallbackCount, 1u )] = cell;
+                ++fbSum;
+            }
+            itSum += iters - iters0;
+            lsSum += ls;
+        }
+        __syncwarp();
+    }
+    if( lane == 0 ) {
+        if( itSum ) atomicAdd( &P.ctl->newtonIters, itSum );
+        if( lsSum ) atomicAdd( &P.ctl->lineSearchTrials, lsSum );
+        if( activeSum ) atomicAdd( &P.ctl->activeCells, activeSum );
+        if( fbSum ) atomicAdd( &P.ctl->fallbackCells, (unsigned long long)fbSum );
+        if( dtMin < 1e300 ) atomic_min_pos_double( &P.ctl->dtBits, dtMin );
+    }
+}
+
+// ---------------------------------------------------------------- tcgen05 helpers
+
+__device__ __forceinline__ unsigned smem_u32( const void* p ) { return unsigned( __cvta_generic_to_shared( p ) ); }
+
+// Shared-memory matrix descriptor of tcgen05.mma, K-major operand without
+// swizzle: core matrices of 8 rows x 16 bytes stored contiguously; lbo = byte
+// distance of core matrices adjacent along K, sbo = along M/N; version 1
+// (bits 46-47) as the sm_100 format requires.
+__device__ __forceinline__ unsigned long long umma_desc( unsigned addr, unsigned lbo, unsigned sbo ) {
+    unsigned long long d = 0;
+    d |= (unsigned long long)( ( addr >> 4 ) & 0x3FFF );
+    d |= (unsigned long long)( ( lbo >> 4 ) & 0x3FFF ) << 16;
+    d |= (unsigned long long)( ( sbo >> 4 ) & 0x3FFF ) << 32;
+    d |= 1ull << 46;
+    return d;
+}
+
+// Instruction descriptor, kind::f16: BF16 A and B (K-major), FP32 accumulator, M x N.
+__host__ __device__ constexpr unsigned umma_idesc_bf16( int M, int N ) {
+    return ( 1u << 4 ) | ( 1u << 7 ) | ( 1u << 10 ) | ( unsigned( N >> 3 ) << 17 ) | ( unsigned( M >> 4 ) << 24 );
+}
+
+__device__ __forceinline__ void umma_bf16( unsigned tmem_d, unsigned long long da, unsigned long long db, unsigned idesc, int accumulate ) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"( tmem_d ),
+        "l"( da ), "l"( db ), "r"( idesc ), "r"( accumulate ) );
+}
+
+__device__ __forceinline__ void umma_commit( unsigned long long* bar ) {
+    asm volatile( "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"( smem_u32( bar ) ) : "memory" );
+}
+
+__device__ __forceinline__ void mbar_init( unsigned long long* bar, unsigned count ) {
+    asm volatile( "mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"( smem_u32( bar ) ), "r"( count ) : "memory" );
+}
+
+// Waits until the barrier's phase `parity` has completed; gives up after about
+// `limitCycles` SM cycles and returns false.
+__device__ __forceinline__ bool mbar_wait( unsigned long long* bar, unsigned parity, long long limitCycles ) {
+    const unsigned a  = smem_u32( bar );
+    const long long t0 = clock64();
+    for( ;; ) {
+        unsigned ok = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"( ok )
+            : "r"( a ), "r"( parity )
+            : "memory" );
+        if( ok ) return true;
+        if( clock64() - t0 > limitCycles ) return false;
+    }
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile( "tcgen05.fence::before_thread_sync;" ::: "memory" ); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile( "tcgen05.fence::after_thread_sync;" ::: "memory" ); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile( "fence.proxy.async.shared::cta;" ::: "memory" ); }
+
+// 16 consecutive 32-bit columns of this thread's TMEM lane (warp w reads lanes
+// 32 (w % 4) .. + 31 at taddr's column).
+__device__ __forceinline__ void tmem_ld16( unsigned taddr, float* v ) {
+    unsigned r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"( r[0] ), "=r"( r[1] ), "=r"( r[2] ), "=r"( r[3] ), "=r"( r[4] ), "=r"( r[5] ), "=r"( r[6] ), "=r"( r[7] ), "=r"( r[8] ),
+          "=r"( r[9] ), "=r"( r[10] ), "=r"( r[11] ), "=r"( r[12] ), "=r"( r[13] ), "=r"( r[14] ), "=r"( r[15] )
+        : "r"( taddr ) );
+    asm volatile( "tcgen05.wait::ld.sync.aligned;" ::: "memory" );
+#pragma unroll
+    for( int i = 0; i < 16; ++i ) v[i] = __uint_as_float( r[i] );
+}
+
+// Byte offset of element (row, k) of a K-major operand tile without swizzle,
+// stored as [K/8 core columns][rows/8 core rows][8 rows][8 BF16 values].
+__host__ __device__ inline unsigned umma_kmajor_offset( int row, int k, int rows ) {
+    return unsigned( ( ( k >> 3 ) * ( rows >> 3 ) + ( row >> 3 ) ) * 128 + ( row & 7 ) * 16 + ( k & 7 ) * 2 );
+}
+
+// ---------------------------------------------------------------- Hessians on the tensor cores
+
+// Shape of the tensor-core Hessian for a configuration (host and device).
+struct TcShape {
+    int pairs, nPad, kPad, cellsPerTile, tmemCols;
+    size_t qBytes, aBytes;    // one BF16 part (high or low) of B = Q and of A = DU
+};
+__host__ __device__ inline TcShape tc_shape( int nS, int NP, int nT, int nQ ) {
+    TcShape s;
+    s.pairs        = nT * ( nT + 1 ) / 2;
+    s.nPad         = ( s.pairs + 15 ) & ~15;
+    s.kPad         = ( nQ + 15 ) & ~15;
+    s.cellsPerTile = 128 / NP;
+    s.tmemCols     = 32;
+    while( s.tmemCols < s.nPad ) s.tmemCols <<= 1;
+    s.qBytes = size_t( s.nPad ) * s.kPad * 2;
+    s.aBytes = size_t( 128 ) * s.kPad * 2;
+    (void)nS;
+    return s;
+}
+
+// Bytes of dynamic shared memory of k_hess_tc.
+__host__ __device__ inline size_t hess_tc_smem( int nS, int NP, int nT, int nQ, int ld ) {
+    const TcShape s = tc_shape( nS, NP, nT, nQ );
+    return 1024 + 2 * s.qBytes + 2 * s.aBytes + size_t( nQ ) * ld * 8 + size_t( s.cellsPerTile ) * nS * nT * 8 + 64;
+}
+
+// Hessians of the cells of re-factor list `round` on the tensor cores:
+// persistent CTAs of 256 threads, tiles of cellsPerTile cells. Per tile the
+// threads evaluate Lambda and DU at every node of every cell (FP64) and store
+// DU in BF16 high and low parts as A rows (cell, block); one thread issues
+// Dh Qh + Dh Ql + Dl Qh (three tcgen05.mma per K step of 16 nodes) into the
+// FP32 accumulator in tensor memory; the eight warps read it back (warp w:
+// lanes 32 (w % 4).., column half w / 4) and write each cell's values as
+// raw[p NP + b] (pair p, block b) at the start of the cell's store slot.
+// Q (P.qTiles): the two BF16 parts of the constant table in the operand layout.
+template <int CL> __global__ void __launch_bounds__( 256, 1 ) k_hess_tc( KParams P, int round ) {
+    constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP;
+    extern __shared__ __align__( 1024 ) unsigned char sm[];
+    if( !P.ctl->active ) return;
+    const int nIn = int( P.ctl->v2Count[round] );
+    if( nIn == 0 ) return;
+    const TcShape S  = tc_shape( NS, NP, P.nT, P.nQ );
+    unsigned char* b = reinterpret_cast<unsigned char*>( ( reinterpret_cast<size_t>( sm ) + 1023 ) & ~size_t( 1023 ) );
+    unsigned char* qh = b;
+    unsigned char* ql = qh + S.qBytes;
+    unsigned char* ah = ql + S.qBytes;
+    unsigned char* al = ah + S.aBytes;
+    double* phiS      = reinterpret_cast<double*>( al + S.aBytes );
+    double* lamS      = phiS + size_t( P.nQ ) * P.ld;
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>( lamS + size_t( S.cellsPerTile ) * NS * P.nT );
+    unsigned* tmemBase      = reinterpret_cast<unsigned*>( bar + 1 );
+    int* tileInfo           = reinterpret_cast<int*>( tmemBase + 1 );    // [0] tile index, [1] error
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // stage Q (both parts) and phi; zero the A operand (its padding rows and
+    // K columns stay zero)
+    {
+        const uint4* src = reinterpret_cast<const uint4*>( P.qTiles );
+        uint4* dst       = reinterpret_cast<uint4*>( qh );
+        for( size_t i = threadIdx.x; i < 2 * S.qBytes / 16; i += blockDim.x ) dst[i] = src[i];
+        uint4* a = reinterpret_cast<uint4*>( ah );
+        for( size_t i = threadIdx.x; i < 2 * S.aBytes / 16; i += blockDim.x ) a[i] = make_uint4( 0, 0, 0, 0 );
+        for( size_t i = threadIdx.x; i < size_t( P.nQ ) * P.ld; i += blockDim.x ) phiS[i] = P.phi[i];
+    }
+    if( threadIdx.x == 0 ) {
+        mbar_init( bar, 1 );
+        asm volatile( "fence.mbarrier_init.release.cluster;" ::: "memory" );
+    }
+    if( warp == 0 ) {
+        asm volatile( "tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"( smem_u32( tmemBase ) ), "r"( S.tmemCols ) );
+        asm volatile( "tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" );
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem  = *tmemBase;
+    const unsigned idesc = umma_idesc_bf16( 128, S.nPad );
+    const unsigned lboA = 16 * 128, lboB = unsigned( S.nPad / 8 ) * 128;
+    const int kSteps    = S.kPad / 16;
+    const size_t ldc    = size_t( NS ) * P.nT;
+    const int nTiles    = ( nIn + S.cellsPerTile - 1 ) / S.cellsPerTile;
+    const int* list     = refactor_list( P, round );
+    unsigned phase      = 0;
+    for( ;; ) {
+        if( threadIdx.x == 0 ) tileInfo[0] = int( atomicAdd( &P.ctl->v2Work[4 + round], 1u ) );
+        __syncthreads();
+        const int tile = tileInfo[0];
+        if( tile >= nTiles ) break;
+        const int c0 = tile * S.cellsPerTile, nc = min( S.cellsPerTile, nIn - c0 );
+        for( int idx = threadIdx.x; idx < nc * int( ldc ); idx += blockDim.x ) {
+            const int c = idx / int( ldc ), e = idx - c * int( ldc );
+            lamS[idx]   = P.lam[size_t( list[c0 + c] ) * ldc + e];
+        }
+        __syncthreads();
+        // A rows (cell c, block b) = DU_b(Lambda_k) at node k, as high + low BF16
+        for( int it = threadIdx.x; it < S.cellsPerTile * P.nQ; it += blockDim.x ) {
+            const int c = it / P.nQ, k = it - c * P.nQ;
+            double y[NP];
+            if( c < nc ) {
+                const double* lam = lamS + size_t( c ) * ldc;
+                const double* row = phiS + size_t( k ) * P.ld;
+                double Lk[NS];
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) Lk[s] = 0.0;
+                for( int i = 0; i < P.nT; ++i ) {
+                    const double r = row[i];
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) Lk[s] = fma( lam[s * P.nT + i], r, Lk[s] );
+                }
+                Closure<CL>::DU( Lk, y, P.phys );
+            }
+            else {
+#pragma unroll
+                for( int p = 0; p < NP; ++p ) y[p] = 0.0;
+            }
+#pragma unroll
+            for( int p = 0; p < NP; ++p ) {
+                const __nv_bfloat16 hi = __double2bfloat16( y[p] );
+                const __nv_bfloat16 lo = __double2bfloat16( y[p] - double( __bfloat162float( hi ) ) );
+                const unsigned off     = umma_kmajor_offset( c * NP + p, k, 128 );
+                *reinterpret_cast<__nv_bfloat16*>( ah + off ) = hi;
+                *reinterpret_cast<__nv_bfloat16*>( al + off ) = lo;
+            }
+        }
+        fence_async_smem();
+        __syncthreads();
+        if( threadIdx.x == 0 ) {
+            tc_fence_after();
+            const unsigned aH = smem_u32( ah ), aL = smem_u32( al ), bH = smem_u32( qh ), bL = smem_u32( ql );
+            for( int ks = 0; ks < kSteps; ++ks ) {
+                const unsigned oa = unsigned( ks ) * 2 * lboA, ob = unsigned( ks ) * 2 * lboB;
+                umma_bf16( tmem, umma_desc( aH + oa, lboA, 128 ), umma_desc( bH + ob, lboB, 128 ), idesc, ks > 0 );
+                umma_bf16( tmem, umma_desc( aH + oa, lboA, 128 ), umma_desc( bL + ob, lboB, 128 ), idesc, 1 );
+                umma_bf16( tmem, umma_desc( aL + oa, lboA, 128 ), umma_desc( bH + ob, lboB, 128 ), idesc, 1 );
+            }
+            umma_commit( bar );
+        }
+        __syncwarp();
+        // about a second at the SM clock: far beyond the microseconds a tile takes
+        const bool ok = mbar_wait( bar, phase, 2000000000ll );
+        phase ^= 1u;
+        if( __syncthreads_or( !ok ) ) {
+            // the tensor cores did not finish in time: flag the error, give the
+            // MMAs in flight another bounded wait, then free tensor memory
+            if( threadIdx.x == 0 ) {
+                P.ctl->v2Error = 1;
+                mbar_wait( bar, phase ^ 1u, 2000000000ll );
+            }
+            __syncthreads();
+            break;
+        }
+        tc_fence_after();
+        // read the accumulator back: thread row m = 32 (warp % 4) + lane = (cell, block)
+        const int q = warp & 3, half = warp >> 2;
+        const int m = 32 * q + lane, c = m / NP, bk = m - c * NP;
+        const int cell = c < nc ? list[c0 + c] : -1;
+        float* raw     = cell >= 0 ? P.factorStore + size_t( cell ) * P.factorStride : nullptr;
+        const int colBeg = half * ( S.nPad / 2 ) & ~15, colEnd = half ? S.nPad : ( ( S.nPad / 2 ) & ~15 );
+        for( int col = colBeg; col < colEnd; col += 16 ) {
+            float v[16];
+            tmem_ld16( tmem + ( unsigned( 32 * q ) << 16 ) + unsigned( col ), v );
+            if( raw ) {
+#pragma unroll
+                for( int t = 0; t < 16; ++t )
+                    if( col + t < S.pairs ) raw[size_t( col + t ) * NP + bk] = v[t];
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+    __syncthreads();
+    if( warp == 0 ) asm volatile( "tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"( tmem ), "r"( S.tmemCols ) );
+}
+
+// ---------------------------------------------------------------- inverse of each listed cell's Hessian
+
+__host__ __device__ inline size_t invert_ws_bytes( int n, int nQ, int NP, bool raw ) {
+    auto a16       = []( size_t x ) { return ( x + 15 ) & ~size_t( 15 ); };
+    const size_t n8 = size_t( hnb( n ) ) * 8;
+    size_t b       = a16( hess_doubles( n ) * 4 ) + 2 * a16( n8 * 4 ) + a16( size_t( xpacked( n ) ) * 4 ) + 64;
+    if( !raw ) b += a16( size_t( ( NP + 1 ) & ~1 ) * nQ * 4 ) + a16( size_t( 4 ) * nQ * 8 );
+    return b;
+}
+
+// Per cell (two warps): the Hessian in FP32 block-packed tiles, either from
+// the raw pair values k_hess_tc left in the store slot (RAW) or assembled on
+// the CUDA cores (hessian_sym, FP32); Cholesky (cholesky_la); the packed
+// inverse X = U^-1 (tri_inverse_packed); H^-1 = X X^T written over the slot
+// (n x n, row-major, symmetric). A factor that is not positive definite sends
+// the cell to the FP64 fallback list (factorLevel -2).
+template <int CL, bool RAW> __global__ void __launch_bounds__( 256, 1 ) k_invert( KParams P, int round ) {
+    constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP;
+    extern __shared__ __align__( 16 ) double smem[];
+    if( !P.ctl->active ) return;
+    const int nIn = int( P.ctl->v2Count[round] );
+    if( nIn == 0 ) return;
+    const int gid = threadIdx.x >> 6, groups = blockDim.x >> 6;
+    Grp<64> g{int( threadIdx.x & 63 ), 1 + gid};
+    const int* list  = refactor_list( P, round );
+    const size_t ldc = size_t( NS ) * P.nT;
+    const int nMax   = NS * P.nT;
+    unsigned char* ws = reinterpret_cast<unsigned char*>( smem ) + size_t( gid ) * invert_ws_bytes( nMax, P.nQ, NP, RAW );
+    auto a16          = []( size_t x ) { return ( x + 15 ) & ~size_t( 15 ); };
+    float* H          = reinterpret_cast<float*>( ws );
+    float* D          = reinterpret_cast<float*>( ws + a16( hess_doubles( nMax ) * 4 ) );
+    float* Iv         = D + a16( size_t( hnb( nMax ) ) * 8 * 4 ) / 4;
+    float* X          = Iv + a16( size_t( hnb( nMax ) ) * 8 * 4 ) / 4;
+    int* flag         = reinterpret_cast<int*>( X + a16( size_t( xpacked( nMax ) ) * 4 ) / 4 );
+    int* itemS        = flag + 1;
+    float* du         = reinterpret_cast<float*>( flag + 16 );
+    double* LA        = reinterpret_cast<double*>( reinterpret_cast<unsigned char*>( du ) + a16( size_t( ( NP + 1 ) & ~1 ) * P.nQ * 4 ) );
+    for( ;; ) {
+        if( g.r == 0 ) *itemS = int( atomicAdd( &P.ctl->v2Work[8 + round], 1u ) );
+        g.sync();
+        const int item = *itemS;
+        g.sync();
+        if( item >= nIn ) break;
+        const int cell = list[item];
+        const int nTj = P.nTLevel[P.level[cell]], n = NS * nTj, nb = hnb( n );
+        float* slot   = P.factorStore + size_t( cell ) * P.factorStride;
+        if constexpr( RAW ) {
+            const int pairs = nTj * ( nTj + 1 ) / 2;
+            for( int e = g.r; e < pairs * NP; e += 64 ) {
+                const int p = e / NP, bk = e - p * NP;
+                int j, i;
+                unpack_pair( p, j, i );
+                int m = 0, l = 0, q = bk;    // block bk -> (m, l), m <= l, in DU's packed order
+                while( q >= NS - m ) {
+                    q -= NS - m;
+                    ++m;
+                }
+                l             = m + q;
+                const float a = slot[e];
+                H[hblk( m * nTj + j, l * nTj + i )] = a;
+                if( m < l && j != i ) H[hblk( m * nTj + i, l * nTj + j )] = a;
+            }
+            if( n & 7 ) {
+                const int C = nb - 1;
+                for( int e = g.r; e < nb * 64; e += 64 ) {
+                    const int R = e >> 6, col = C * 8 + ( ( e >> 3 ) & 7 ), row = R * 8 + ( e & 7 );
+                    if( col >= n && row <= col ) H[hblk( row, col )] = row == col ? 1.f : 0.f;
+                }
+            }
+        }
+        else {
+            for( int idx = g.r; idx < NS * P.nQ; idx += 64 ) {
+                const int s = idx / P.nQ, k = idx - s * P.nQ;
+                const double* row = P.phi + size_t( k ) * P.ld;
+                double a          = 0.0;
+                for( int i = 0; i < nTj; ++i ) a = fma( P.lam[cell * ldc + s * P.nT + i], row[i], a );
+                LA[idx] = a;
+            }
+            g.sync();
+            hessian_sym<NS, NP, 64, float>( g, P.nQ, P.ld, P.phiF, P.wt, LA, nTj, du, H,
+                                           [&]( const double* L, double* y ) { Closure<CL>::DU( L, y, P.phys ); } );
+        }
+        for( int r = g.r; r < nb * 8; r += 64 ) H[hrhs( nb ) + r] = 0.f;
+        g.sync();
+        if( cholesky_la<64, float>( g, H, n, D, Iv, flag ) ) {
+            if( g.r == 0 ) {
+                P.factorLevel[cell] = -2;
+                P.fallbackList[atomicAdd( P.fallbackCount, 1u )] = cell;
+                atomicAdd( &P.ctl->fallbackCells, 1ull );
+            }
+            g.sync();
+            continue;
+        }
+        tri_inverse_packed<64, float>( g, H, Iv, n, X );
+        // H^-1 (a, b) = sum_{k >= max(a, b)} X(a, k) X(b, k), full rows
+        for( int a = 0; a < n; ++a ) {
+            const float* xa = X + xrow( a, n ) - a;
+            for( int bcol = g.r; bcol < n; bcol += 64 ) {
+                const float* xb = X + xrow( bcol, n ) - bcol;
+                float s0 = 0.f, s1 = 0.f;
+                int k    = a > bcol ? a : bcol;
+                for( ; k + 1 < n; k += 2 ) {
+                    s0 = fmaf( xa[k], xb[k], s0 );
+                    s1 = fmaf( xa[k + 1], xb[k + 1], s1 );
+                }
+                if( k < n ) s0 = fmaf( xa[k], xb[k], s0 );
+                slot[size_t( a ) * n + bcol] = s0 + s1;
+            }
+        }
+        if( g.r == 0 ) P.factorLevel[cell] = nTj;
+        g.sync();
+    }
+}
+
+}    // namespace uqc

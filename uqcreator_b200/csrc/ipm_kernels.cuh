@@ -65,6 +65,12 @@ struct Control {
     unsigned long long dtBitsNext;    // min dt of the cells k_update finished for the next step
     unsigned long long newtonIters, lineSearchTrials;
     unsigned long long fallbackCells;    // mixed form: cells handed to the FP64 form
+    // mixed form in rounds (chord.cuh): work-stealing counters (0-3 k_chord
+    // rounds, 4-7 k_hess_tc, 8-11 k_invert), re-factor list lengths, and an
+    // error flag (tensor-core wait timed out)
+    unsigned int v2Work[16];
+    unsigned int v2Count[4];
+    int v2Error;
 };
 
 struct KParams {
@@ -109,6 +115,13 @@ struct KParams {
     double chordTheta;        // re-factor after a held-factor step that reduced ||g|| by less than 1/chordTheta
     int* fallbackList;        // mixed form: cells handed to the FP64 form (non-PD FP32 factor, ...)
     unsigned* fallbackCount;
+    // mixed form in rounds (chord.cuh)
+    double* gStore;           // per cell: gradient at the accepted duals (compact) and its norm at [nS nT]; or null
+    int gStride;              // doubles per cell in gStore
+    int* v2Lists;             // re-factor lists, one of nCells per round
+    int v2Rounds;             // re-factor rounds per step
+    int* chordIters;          // per cell: Newton iterations of the step so far
+    const unsigned short* qTiles;    // tensor-core Hessian: the BF16 high and low parts of Q in the operand layout
     Control* ctl;
 };
 
@@ -966,7 +979,17 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
             CT_END( tlu, 17, g.r == 0 );
             CT_BEGIN( tgr );
             const double sq = gradient_sums<NS, 32>( g, P, phiWf, uk, uh, nTj, nullptr, ugs );
-            converged = sqrt( group_sum<32>( g, sq, red ) ) < P.eps;
+            const double gn = sqrt( group_sum<32>( g, sq, red ) );
+            converged       = gn < P.eps;
+            if( !converged && P.gStore ) {
+                // the gradient the mixed form's Newton starts from: g = sum_k U phiWf - u
+                double* gs = P.gStore + size_t( cell ) * P.gStride;
+                for( int idx = g.r; idx < NS * nTj; idx += 32 ) {
+                    const int s = idx / nTj, i = idx - s * nTj;
+                    gs[idx]     = ugs[s * P.nT + i] - uh[s * P.nT + i];
+                }
+                if( g.r == 0 ) gs[ldc] = gn;
+            }
             CT_END( tgr, 18, g.r == 0 );
         }
         if( converged ) {
@@ -1188,6 +1211,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         const double c = dt / P.area[cell];
         double sq      = 0.0;
         double v0a = 0.0, v0b = 0.0;    // u_new(0, lane) and u_new(0, lane + 32), for the level rule
+        double ga[NS], gb[NS];          // the next step's gradient uRe - u_new at i = lane, lane + 32
         for( int i = lane; i < nTj; i += 32 ) {    // beyond the level u stays zero (epilogue)
             // the re-projected moments first: their loads overlap the
             // projection (uRe and u may alias, so a load after a store to u
@@ -1202,6 +1226,9 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
                 const double gi  = old[s] - v;
                 P.u[cell * ldc + s * P.nT + i] = v;
                 sq                             = fma( gi, gi, sq );
+                if( i < 32 ) ga[s] = gi;
+                else if( i < 64 ) gb[s] = gi;
+                else if( P.gStore ) P.gStore[size_t( cell ) * P.gStride + s * nTj + i] = gi;
                 if( s == 0 && i < 32 ) v0a = v;
                 if( s == 0 && i >= 32 && i < 64 ) v0b = v;
                 if( s == 0 && i == 0 ) res += fabs( v - P.uOld0[cell] ) * P.area[cell];
@@ -1243,8 +1270,18 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
             }
             else if( pass )
                 cbuf.push( lane, cell, clist, ccount );    // converged, new level: k_check's epilogue
-            else
+            else {
+                if( P.gStore ) {    // the gradient the mixed form's Newton starts from
+                    double* gs = P.gStore + size_t( cell ) * P.gStride;
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) {
+                        if( lane < nTj ) gs[s * nTj + lane] = ga[s];
+                        if( lane + 32 < nTj && lane + 32 < 64 ) gs[s * nTj + lane + 32] = gb[s];
+                    }
+                    if( lane == 0 ) gs[ldc] = sqrt( sq );
+                }
                 nbuf.push( lane, cell, nlist, ncount );
+            }
         }
         __syncwarp();
     }
@@ -1287,6 +1324,8 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         C->workCounter  = 0;
         C->workCounter2 = 0;
         C->nFallback    = 0;
+        for( int r = 0; r < 16; ++r ) C->v2Work[r] = 0;
+        for( int r = 0; r < 4; ++r ) C->v2Count[r] = 0;
         C->doneBlocks  = 0;
     }
 }

@@ -14,7 +14,11 @@ enum KernelId {
     KERNEL_CLOSURE_MIXED = 4,    // k_closure, mixed form (group 32 or 64)
     KERNEL_UPDATE_PLAIN  = 5,    // k_update without it
     KERNEL_CHECK         = 6,    // k_check
-    KERNEL_PHASE_COUNTERS = 7    // device address of this unit's phase counters (diagnostic builds), else nullptr
+    KERNEL_PHASE_COUNTERS = 7,   // device address of this unit's phase counters (diagnostic builds), else nullptr
+    KERNEL_CHORD         = 8,    // k_chord (mixed form in rounds; 2-D Euler only)
+    KERNEL_HESS_TC       = 9,    // k_hess_tc
+    KERNEL_INVERT_RAW    = 10,   // k_invert from k_hess_tc's values
+    KERNEL_INVERT        = 11    // k_invert with the Hessian on CUDA cores
 };
 
 // nullptr when there is no such variant

@@ -1,6 +1,7 @@
 // Instantiation of every kernel of one closure kind (included once per kind
 // by kernels_<kind>.cu) and the table of their addresses.
 #pragma once
+#include "chord.cuh"
 #include "ipm_kernels.cuh"
 #include "kernels.h"
 
@@ -36,6 +37,17 @@ template <int CL> void* kernel_of( int group, int which ) {
             return nullptr;
 #endif
         }
+        case KERNEL_CHORD:
+        case KERNEL_HESS_TC:
+        case KERNEL_INVERT_RAW:
+        case KERNEL_INVERT:
+            if constexpr( Closure<CL>::NS == 4 ) {    // the mixed form in rounds serves the 2-D Euler closure
+                if( which == KERNEL_CHORD ) return (void*)&k_chord<CL>;
+                if( which == KERNEL_HESS_TC ) return (void*)&k_hess_tc<CL>;
+                if( which == KERNEL_INVERT_RAW ) return (void*)&k_invert<CL, true>;
+                return (void*)&k_invert<CL, false>;
+            }
+            return nullptr;
         default: return nullptr;
     }
 }

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "host.h"
+#include "chord.cuh"
 #include "ipm_kernels.cuh"
 #include "kernels.h"
 #include "uqc.h"
@@ -86,6 +87,20 @@ struct uqc_solver {
     double chordTheta    = 0.1;
     size_t mixedSmem       = 0;
     bool mixedTablesInSmem = false;
+    // mixed form in rounds (chord.cuh; 2-D Euler with one refinement level):
+    // k_chord, then per round k_hess_tc / k_invert and k_chord again
+    int roundsOpt   = -1;    // option mixed_hessian: -1 automatic, 0 single kernel, 1 CUDA-core Hessian, 2 tensor cores
+    int v2Mode      = 0;     // planned: 0 off, 1 rounds with the CUDA-core Hessian, 2 with the tensor-core Hessian
+    int v2Rounds    = 3;     // option mixed_rounds
+    std::string v2Why;       // why the rounds (or the tensor cores) are not used
+    double* d_gStore        = nullptr;
+    int gStride             = 0;
+    int* d_v2Lists          = nullptr;
+    int* d_chordIters       = nullptr;
+    unsigned short* d_qTiles = nullptr;
+    int chordBlock = 512, chordGrid = 0, hessGrid = 0, invBlock = 256, invGrid = 0;
+    size_t chordSmem = 0, hessSmem = 0, invSmem = 0;
+    bool chordTablesInSmem = false;
     // bookkeeping
     bool stateReady = false;
     int precision   = 0;
@@ -232,6 +247,15 @@ KParams make_params( const uqc_solver* h ) {
     P.factorStride      = h->factorStride;
     P.chordInverse      = useStore && h->chordInverse ? 1 : 0;
     P.chordTheta        = h->chordTheta;
+    // the mixed form in rounds: k_check / k_update store the gradient of the
+    // cells they list (gStore non-null) only when the rounds run
+    const bool rounds = useStore && h->v2Mode && h->d_gStore;
+    P.gStore          = rounds ? h->d_gStore : nullptr;
+    P.gStride         = h->gStride;
+    P.v2Lists         = rounds ? h->d_v2Lists : nullptr;
+    P.v2Rounds        = h->v2Rounds;
+    P.chordIters      = rounds ? h->d_chordIters : nullptr;
+    P.qTiles          = h->d_qTiles;
     P.fallbackCount = h->d_ctl ? &h->d_ctl->nFallback : nullptr;
     return P;
 }
@@ -276,19 +300,131 @@ void launch( uqc_solver* h, void* fn, int grid, int block, size_t smem, void** a
 // or the packed inverse (whichever is larger, so the planner may switch).
 int factor_stride( const uqc_solver* h ) {
     const int n = h->nS * h->tab.nT;
-    return int( ( std::max<size_t>( hess_doubles( n ) + size_t( hnb( n ) ) * 8, size_t( xpacked( n ) ) ) + 3 ) & ~size_t( 3 ) );
+    size_t f    = std::max<size_t>( hess_doubles( n ) + size_t( hnb( n ) ) * 8, size_t( xpacked( n ) ) );
+    if( h->cfg.closure == 1 ) {    // the rounds' inverse (n x n) and tensor-core values (pairs x blocks)
+        const size_t pairs = size_t( h->tab.nT ) * ( h->tab.nT + 1 ) / 2;
+        f                  = std::max( f, std::max( size_t( n ) * n, pairs * size_t( closure_np( 1 ) ) ) );
+    }
+    return int( ( f + 3 ) & ~size_t( 3 ) );
 }
 unsigned long long factor_store_bytes( const uqc_solver* h ) {
-    return (unsigned long long)h->mesh.nCells * ( (unsigned long long)factor_stride( h ) * 4 + 4 );
+    const unsigned long long N = (unsigned long long)h->mesh.nCells;
+    // the rounds' gradient store, lists and iteration counts (2-D Euler)
+    const unsigned long long rounds = h->cfg.closure == 1 ? N * ( ( h->ldc + 2 + 3 ) / 4 * 4 * 8 + 4 * 4 ) : 0;
+    return N * ( (unsigned long long)factor_stride( h ) * 4 + 4 ) + rounds;
 }
 // Allocates the store on first use; marks every stored factor invalid.
 void reset_factor_store( uqc_solver* h ) {
+    const size_t N = size_t( h->mesh.nCells );
     if( !h->d_factorStore ) {
         h->factorStride  = factor_stride( h );
-        h->d_factorStore = dalloc<float>( size_t( h->mesh.nCells ) * h->factorStride );
-        h->d_factorLevel = dalloc<int>( size_t( h->mesh.nCells ) );
+        h->d_factorStore = dalloc<float>( N * h->factorStride );
+        h->d_factorLevel = dalloc<int>( N );
     }
-    CK( cudaMemsetAsync( h->d_factorLevel, 0xFF, size_t( h->mesh.nCells ) * sizeof( int ), h->stream ) );
+    if( h->v2Mode && !h->d_gStore ) {
+        h->gStride      = int( ( h->ldc + 2 + 3 ) & ~size_t( 3 ) );
+        h->d_gStore     = dalloc<double>( N * h->gStride );
+        h->d_v2Lists    = dalloc<int>( 3 * N );
+        h->d_chordIters = dalloc<int>( N );
+    }
+    CK( cudaMemsetAsync( h->d_factorLevel, 0xFF, N * sizeof( int ), h->stream ) );
+}
+
+// Round-to-nearest-even BF16 bits of a float.
+unsigned short bf16_bits( float f ) {
+    unsigned u;
+    std::memcpy( &u, &f, 4 );
+    if( ( u & 0x7F800000u ) == 0x7F800000u ) return (unsigned short)( u >> 16 );    // inf / nan
+    u += 0x7FFFu + ( ( u >> 16 ) & 1u );
+    return (unsigned short)( u >> 16 );
+}
+float bf16_value( unsigned short b ) {
+    unsigned u = unsigned( b ) << 16;
+    float f;
+    std::memcpy( &f, &u, 4 );
+    return f;
+}
+
+// Mixed form in rounds: eligibility, launch shapes, and the tensor-core
+// table Q (pairs j <= i x nodes, Q = phi_kj phi_ki wt_k, high and low BF16
+// parts in the K-major operand layout of k_hess_tc).
+void plan_rounds( uqc_solver* h, int maxSmem ) {
+    h->v2Mode = 0;
+    const int cl = h->cfg.closure, nT = h->tab.nT, nQ = h->tab.nQ, nS = h->nS;
+    if( h->roundsOpt == 0 ) {
+        h->v2Why = "option mixed_hessian = 0";
+        return;
+    }
+    if( cl != 1 || h->tab.nLevels != 1 || h->cfg.newtonMode == 2 || h->cfg.maxIterations < 2 || !h->chord ) {
+        h->v2Why = "rounds serve the 2-D Euler closure with one refinement level, SolveClosure Newton, maxIterations > 1 and the chord form";
+        return;
+    }
+    const int NP = closure_np( cl );
+    // chord kernel: tables in shared memory when that leaves room for 8 cells
+    const size_t tables = 2 * ( size_t( nQ ) * h->ld + 4 ) * sizeof( double );
+    const size_t ws     = chord_ws_doubles( nS, nT, nQ ) * sizeof( double );
+    h->chordTablesInSmem = tables <= 96 * 1024 && tables + 8 * ws <= size_t( maxSmem );
+    const size_t avail   = size_t( maxSmem ) - ( h->chordTablesInSmem ? tables : 0 );
+    const int warps      = int( std::min<size_t>( 16, avail / ws ) );
+    if( warps < 1 ) {
+        h->v2Why = "chord workspace exceeds shared memory";
+        return;
+    }
+    h->chordBlock = 32 * warps;
+    h->chordSmem  = ( h->chordTablesInSmem ? tables : 0 ) + size_t( warps ) * ws;
+    int occ       = 0;
+    void* kc      = pick( cl, 32, KERNEL_CHORD );
+    allow_dynamic_smem( kc );
+    CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kc, h->chordBlock, h->chordSmem ) );
+    h->chordGrid = std::max( 1, occ ) * h->numSMs;
+    // tensor cores when the table fits one MMA's N (256) and shared memory
+    const TcShape ts    = tc_shape( nS, NP, nT, nQ );
+    const size_t hsmem  = hess_tc_smem( nS, NP, nT, nQ, h->ld );
+    const bool tcFits   = ts.nPad <= 256 && ts.cellsPerTile >= 1 && hsmem <= size_t( maxSmem );
+    int mode            = h->roundsOpt == 1 ? 1 : ( tcFits ? 2 : 1 );
+    if( h->roundsOpt == 2 && !tcFits ) {
+        h->v2Why = "tensor-core Hessian: " + std::to_string( ts.pairs ) + " basis pairs or " + std::to_string( hsmem ) +
+                   " B of shared memory exceed one MMA (256 pairs)";
+        return;
+    }
+    // inverse kernel: two warps per cell, as many cells per CTA (up to 4) as fit
+    const size_t iws = invert_ws_bytes( nS * nT, nQ, NP, mode == 2 );
+    const int groups = int( std::min<size_t>( 4, size_t( maxSmem ) / iws ) );
+    if( groups < 1 ) {
+        h->v2Why = "inverse workspace exceeds shared memory";
+        return;
+    }
+    h->invBlock = 64 * groups;
+    h->invSmem  = iws * groups;
+    void* ki    = pick( cl, 32, mode == 2 ? KERNEL_INVERT_RAW : KERNEL_INVERT );
+    allow_dynamic_smem( ki );
+    CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ki, h->invBlock, h->invSmem ) );
+    h->invGrid = std::max( 1, occ ) * h->numSMs;
+    if( mode == 2 ) {
+        h->hessSmem = hsmem;
+        void* kh    = pick( cl, 32, KERNEL_HESS_TC );
+        allow_dynamic_smem( kh );
+        h->hessGrid = h->numSMs;
+        if( !h->d_qTiles ) {
+            std::vector<unsigned short> q( 2 * ts.qBytes / 2, 0 );
+            for( int i = 0; i < nT; ++i )
+                for( int j = 0; j <= i; ++j ) {
+                    const int pr = i * ( i + 1 ) / 2 + j;
+                    for( int k = 0; k < nQ; ++k ) {
+                        const double v =
+                            h->tab.phi[size_t( k ) * nT + j] * h->tab.phi[size_t( k ) * nT + i] * h->padWt[k];
+                        const unsigned short hi = bf16_bits( float( v ) );
+                        const unsigned short lo = bf16_bits( float( v - double( bf16_value( hi ) ) ) );
+                        const size_t off        = umma_kmajor_offset( pr, k, ts.nPad ) / 2;
+                        q[off]                  = hi;
+                        q[ts.qBytes / 2 + off]  = lo;
+                    }
+                }
+            h->d_qTiles = dupload( q );
+        }
+    }
+    h->v2Mode = mode;
+    h->v2Why.clear();
 }
 
 // Mixed-form closure: the FP32 Hessian halves the per-cell shared memory, so
@@ -430,6 +566,7 @@ void plan_launches( uqc_solver* h ) {
         h->checkGrid = std::min( std::max( 1, occ ) * h->numSMs, std::max( 1, ( h->mesh.nCells + warps - 1 ) / warps ) );
     }
     plan_mixed( h, maxSmem );
+    plan_rounds( h, maxSmem );
 }
 
 void reset_control( uqc_solver* h, double t ) {
@@ -574,7 +711,8 @@ void release( uqc_solver* h ) {
                     (void*)h->d_bndNormal, (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
                     (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
                     (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_cellDt, (void*)h->d_uRe, (void*)h->d_checkList, (void*)h->d_finFlag, (void*)h->d_phiF, (void*)h->d_fallbackList,
-                    (void*)h->d_factorStore, (void*)h->d_factorLevel} )
+                    (void*)h->d_factorStore, (void*)h->d_factorLevel, (void*)h->d_gStore, (void*)h->d_v2Lists,
+                    (void*)h->d_chordIters, (void*)h->d_qTiles} )
         if( p ) cudaFree( p );
     if( h->h_ctl ) cudaFreeHost( h->h_ctl );
     for( auto& e : h->ev )
@@ -590,6 +728,36 @@ void release( uqc_solver* h ) {
 // an empty list returns at once). The work counters and the fallback list
 // length must be zero on entry (k_update resets them after every step).
 void launch_closure( uqc_solver* h, KParams& P, int mode ) {
+    if( mode == 1 && P.gStore ) {
+        // the mixed form in rounds: k_chord, then per round the Hessians of
+        // the listed cells (tensor cores or CUDA cores) and their inverses,
+        // and k_chord again; then the FP64 pass over the fallback list
+        const int cl = h->cfg.closure;
+        KParams C    = P;
+        C.tablesInSmem = h->chordTablesInSmem;
+        if( h->mixedMaxIter > 1 && P.maxIter > 1 ) C.maxIter = std::min( P.maxIter, h->mixedMaxIter );
+        for( int r = 0; r <= h->v2Rounds; ++r ) {
+            if( r > 0 ) {
+                int rr        = r - 1;
+                void* hargs[] = {&C, &rr};
+                if( h->v2Mode == 2 ) launch( h, pick( cl, 32, KERNEL_HESS_TC ), h->hessGrid, 256, h->hessSmem, hargs );
+                launch( h, pick( cl, 32, h->v2Mode == 2 ? KERNEL_INVERT_RAW : KERNEL_INVERT ), h->invGrid, h->invBlock, h->invSmem, hargs );
+            }
+            int rr       = r;
+            void* args[] = {&C, &rr};
+            launch( h, pick( cl, 32, KERNEL_CHORD ), h->chordGrid, h->chordBlock, h->chordSmem, args );
+        }
+        KParams F      = P;
+        F.activeList   = h->d_fallbackList;
+        F.activeCount  = &h->d_ctl->nFallback;
+        F.listParity   = 0;
+        F.workCounter  = &h->d_ctl->workCounter2;
+        F.tablesInSmem = h->closureTablesInSmem;
+        F.gStore       = nullptr;
+        void* fargs[]  = {&F, &mode};
+        launch( h, pick( cl, h->closureGroup, 0 ), h->closureGrid, h->closureBlock, h->closureSmem, fargs );
+        return;
+    }
     if( h->precision == UQC_MIXED && h->mixedOk ) {
         KParams M      = P;
         M.tablesInSmem = h->mixedTablesInSmem;
@@ -724,6 +892,7 @@ int fill_info_host( uqc_solver* h, uqc_step_info* info, int stepsBefore ) {
 
 int fill_info( uqc_solver* h, uqc_step_info* info, int stepsBefore ) {
     read_control( h );
+    if( h->h_ctl->v2Error ) throw CudaError( "k_hess_tc: the tensor cores did not complete a tile within the wait limit" );
     return fill_info_host( h, info, stepsBefore );
 }
 
@@ -830,6 +999,8 @@ int uqc_get_info( const uqc_solver* h, uqc_info* o ) {
     o->newton_mode = h->cfg.newtonMode;
     o->t           = h->h_ctl ? h->h_ctl->t : 0.0;
     o->steps       = h->h_ctl ? h->h_ctl->steps : 0;
+    o->mixed_form  = h->deviceReady ? h->v2Mode : -1;
+    o->mixed_rounds = h->v2Rounds;
     return UQC_OK;
 }
 
@@ -848,8 +1019,15 @@ int uqc_set_precision( uqc_solver* h, int precision ) {
         } );
         if( rc != UQC_OK ) return rc;
     }
-    h->precision = precision;
+    const bool changed = h->precision != precision;
+    h->precision       = precision;
     ++h->planGen;
+    // the next step's list was built by the other form's update kernel (the
+    // mixed form's rounds also need the listed cells' gradients): test every cell
+    if( changed ) return guarded( h, [&] {
+            invalidate_lists( h );
+            return UQC_OK;
+        } );
     return UQC_OK;
 }
 
@@ -892,6 +1070,24 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
                 return UQC_OK;
             } );
             if( rc != UQC_OK ) return rc;
+        }
+        ++h->planGen;
+        return UQC_OK;
+    }
+    if( k == "mixed_hessian" || k == "mixed_rounds" ) {
+        const int v = int( value );
+        if( k == "mixed_hessian" && ( v < -1 || v > 2 ) ) return fail( h, UQC_ERR_ARGUMENT, "mixed_hessian must be -1, 0, 1 or 2" );
+        if( k == "mixed_rounds" && ( v < 1 || v > 3 ) ) return fail( h, UQC_ERR_ARGUMENT, "mixed_rounds must be 1, 2 or 3" );
+        ( k == "mixed_hessian" ? h->roundsOpt : h->v2Rounds ) = v;
+        if( h->deviceReady ) {
+            int rc = guarded( h, [&] {
+                plan_launches( h );
+                if( h->chord && h->precision == UQC_MIXED ) reset_factor_store( h );    // the store's format depends on the form
+                invalidate_lists( h );    // the next step's list carries no stored gradients yet
+                return UQC_OK;
+            } );
+            if( rc != UQC_OK ) return rc;
+            if( k == "mixed_hessian" && v == 2 && h->v2Mode != 2 ) return fail( h, UQC_ERR_CONFIG, "tensor-core Hessian not available: " + h->v2Why );
         }
         ++h->planGen;
         return UQC_OK;
@@ -1687,6 +1883,65 @@ int uqc_device_state( uqc_solver* h, double** d_u, double** d_lambda ) {
 }
 
 int uqc_last_launch_count( uqc_solver* h ) { return h ? h->launches : 0; }
+
+int uqc_debug_mixed_inverse( uqc_solver* h, int n, const int* cells, int form, float* out ) {
+    if( !h || n < 1 || !cells || !out || ( form != 1 && form != 2 ) ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
+    for( int i = 0; i < n; ++i )
+        if( cells[i] < 0 || cells[i] >= h->mesh.nCells ) return fail( h, UQC_ERR_ARGUMENT, "cell id out of range" );
+    return guarded_dev( h, [&] {
+        if( !h->v2Mode ) throw ConfigError( "the mixed form's rounds are not available: " + h->v2Why );
+        if( form == 2 && h->v2Mode != 2 ) throw ConfigError( "tensor-core Hessian not available: " + h->v2Why );
+        if( n > h->mesh.nCells ) throw ConfigError( "too many cells" );
+        if( !h->d_gStore ) {
+            const int v = h->v2Mode;
+            reset_factor_store( h );
+            h->v2Mode = v;
+        }
+        read_control( h );
+        const Control saved = *h->h_ctl;
+        Control c           = saved;
+        c.active            = 1;
+        c.v2Error           = 0;
+        for( int r = 0; r < 16; ++r ) c.v2Work[r] = 0;
+        for( int r = 0; r < 4; ++r ) c.v2Count[r] = 0;
+        c.v2Count[0] = unsigned( n );
+        *h->h_ctl    = c;
+        CK( cudaMemcpyAsync( h->d_ctl, h->h_ctl, sizeof( Control ), cudaMemcpyHostToDevice, h->stream ) );
+        CK( cudaMemcpyAsync( h->d_v2Lists, cells, size_t( n ) * sizeof( int ), cudaMemcpyHostToDevice, h->stream ) );
+        KParams P          = make_params( h );
+        P.factorStore      = h->d_factorStore;
+        P.factorLevel      = h->d_factorLevel;
+        P.factorStride     = h->factorStride;
+        P.v2Lists          = h->d_v2Lists;
+        P.fallbackList     = h->d_fallbackList;
+        int r0             = 0;
+        void* args[]       = {&P, &r0};
+        const int cl       = h->cfg.closure;
+        int dev = 0, maxSmem = 0, occ = 0;
+        CK( cudaGetDevice( &dev ) );
+        CK( cudaDeviceGetAttribute( &maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev ) );
+        if( form == 2 ) launch( h, pick( cl, 32, KERNEL_HESS_TC ), h->hessGrid, 256, h->hessSmem, args );
+        const size_t iws = invert_ws_bytes( h->nS * h->tab.nT, h->tab.nQ, closure_np( cl ), form == 2 );
+        const int groups = int( std::min<size_t>( 4, size_t( maxSmem ) / iws ) );
+        void* ki         = pick( cl, 32, form == 2 ? KERNEL_INVERT_RAW : KERNEL_INVERT );
+        allow_dynamic_smem( ki );
+        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ki, 64 * groups, iws * groups ) );
+        launch( h, ki, std::max( 1, occ ) * h->numSMs, 64 * groups, iws * groups, args );
+        const size_t nn = size_t( h->nS ) * h->tab.nT * h->nS * h->tab.nT;
+        for( int i = 0; i < n; ++i )
+            CK( cudaMemcpyAsync( out + i * nn, h->d_factorStore + size_t( cells[i] ) * h->factorStride, nn * sizeof( float ),
+                                 cudaMemcpyDeviceToHost, h->stream ) );
+        read_control( h );
+        const int err = h->h_ctl->v2Error;
+        *h->h_ctl     = saved;
+        CK( cudaMemcpyAsync( h->d_ctl, h->h_ctl, sizeof( Control ), cudaMemcpyHostToDevice, h->stream ) );
+        CK( cudaMemsetAsync( h->d_factorLevel, 0xFF, size_t( h->mesh.nCells ) * sizeof( int ), h->stream ) );
+        CK( cudaStreamSynchronize( h->stream ) );
+        if( err ) throw CudaError( "k_hess_tc: the tensor cores did not complete a tile within the wait limit" );
+        return UQC_OK;
+    } );
+}
 
 void* uqc_stream( uqc_solver* h ) {
     if( !h || guarded( h, [&] {

@@ -87,6 +87,24 @@ class Solver:
         self.n_levels, self.dim_xi, self.n_faces = info.n_levels, info.dim_xi, info.n_faces
         self.n_total_levels = list(info.n_total_level)[: info.n_levels]
 
+    def form(self):
+        """Precision in use and how UQC_MIXED steps run the closure (uqc_info:
+        mixed_form 0 single kernel, 1 rounds with the CUDA-core Hessian, 2 with
+        the tensor-core Hessian; -1 before the device side is set up)."""
+        info = Info()
+        check(self.h, self.lib.uqc_get_info(self.h, C.byref(info)))
+        return dict(precision=info.precision, mixed_form=info.mixed_form, mixed_rounds=info.mixed_rounds)
+
+    def debug_mixed_inverse(self, cells, form):
+        """H^-1 (FP32) of the mixed form's re-factorisation for the given cells of
+        the resident state; form 1: Hessian on CUDA cores, 2: on the tensor cores."""
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        n = self.n_states * self.n_total
+        out = np.zeros((len(cells), n, n), dtype=np.float32)
+        check(self.h, self.lib.uqc_debug_mixed_inverse(self.h, len(cells), ptr(cells, L._ip), form,
+                                                       out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.uqc_destroy(self.h)
