@@ -65,10 +65,14 @@ def work_per_cell_step(n_states, n_total, n_quad, n_faces=3):
 
 
 # Where each form computes the Newton system's parts: the Hessian assembly
-# (2 nQ n^2 flops per iteration), the factorisation and solves (n^3/3 + 2 n^2)
-# and everything else (ansatz, gradients, line search, epilogue: FP64 in both
-# forms).
-HESSIAN_UNIT = {"fp64": "fp64", "mixed": "fp32"}
+# (2 nQ n^2 flops per iteration: FP64 form on FP64 units, the mixed form on the
+# tensor cores when uqc_info.mixed_form == 2, else FP32 CUDA cores), the
+# factorisation and solves (n^3/3 + 2 n^2: FP64, or FP32 in the mixed form) and
+# everything else (ansatz, gradients, line search, epilogue: FP64 in both forms).
+def hessian_unit(form, mixed_form):
+    return "fp64" if form == "fp64" else ("tensor" if mixed_form == 2 else "fp32")
+
+
 FACTOR_UNIT = {"fp64": "fp64", "mixed": "fp32"}
 # DRAM bytes (read + write) per cell that takes Newton iterations, from the ncu
 # captures of each form's closure kernel on a 12,000-cell step (1,532 active
@@ -76,7 +80,7 @@ FACTOR_UNIT = {"fp64": "fp64", "mixed": "fp32"}
 CLOSURE_DRAM_BYTES_PER_ACTIVE_CELL = {"fp64": 2.345472e6 / 1532, "mixed": 23.6e6 / 1532}
 
 
-def closure_roofline(form, n_states, n_total, n_quad, cells, steps, ref_info, closure_ms, measured, active_cells):
+def closure_roofline(form, n_states, n_total, n_quad, cells, steps, ref_info, closure_ms, measured, active_cells, mixed_form=0):
     """T_bound of the closure phase: max over units of (work on that unit /
     its measured peak); achieved = algorithmic work / measured time, peak =
     work / T_bound, frac = T_bound / time. Work uses the FP64 form's Newton
@@ -86,7 +90,7 @@ def closure_roofline(form, n_states, n_total, n_quad, cells, steps, ref_info, cl
     iters = ref_info["newton_iterations"]
     grads = iters + ref_info["line_search_trials"] + cells * steps    # + the initial test of every cell
     work = {"fp64": 0.0, "fp32": 0.0, "tensor": 0.0}
-    work[HESSIAN_UNIT[form]] += iters * 2.0 * n_quad * n * n
+    work[hessian_unit(form, mixed_form)] += iters * 2.0 * n_quad * n * n
     work[FACTOR_UNIT[form]] += iters * (n ** 3 / 3.0 + 2.0 * n * n)
     work["fp64"] += grads * 4.0 * n_quad * n + cells * steps * 4.0 * n_quad * n
     hbm, bf16, src = peaks()
@@ -389,8 +393,11 @@ def run_b200(args, rank, world, local):
     ref_inf = results["fp64"]["info"]
     closure_ms = r["phase"][0] / args.steps
     measured = measure_peaks(dev)
+    s.set_precision(MIXED if chosen == "mixed" else FP64)
+    mixed_form = s.form()["mixed_form"]
     roof = closure_roofline(chosen, s.n_states, s.n_total, s.n_quad, cells, args.steps, ref_inf, closure_ms, measured,
-                            inf["active_cells"])
+                            inf["active_cells"], mixed_form)
+    roof["mixed_form"] = mixed_form
     roof["update_ms_per_launch"] = r["phase"][1] / args.steps
     roof["fp64_form"] = closure_roofline("fp64", s.n_states, s.n_total, s.n_quad, cells, args.steps, ref_inf,
                                          results["fp64"]["phase"][0] / args.steps, measured, ref_inf["active_cells"])

@@ -132,7 +132,7 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *                    triangular solves; used when its shared memory costs no
  *                    cell per SM (else the triangular solves); 0: never.
  *   "mixed_chord_theta"  re-factor after a step with the held factor that
- *                    reduced ||g|| by less than the factor 1/theta (default 0.1).
+ *                    reduced ||g|| by less than the factor 1/theta (default 0.2, the autotuner's choice for the 2-D Euler workload).
  *   "update_test"    1: the update kernel tests the next step's closure
  *                    convergence per cell and lists only the cells that need
  *                    Newton; 0: a check kernel tests every cell at the start
@@ -155,7 +155,7 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *                    per round the Hessians and inverses of the cells whose
  *                    held inverse stopped contracting, and the chord kernel
  *                    again; cells left after the last round finish in FP64.
- *   "mixed_rounds"   re-factorisation rounds per step of the forms above (1-3, default 3).
+ *   "mixed_rounds"   re-factorisation rounds per step of the forms above (1-3, default 2).
  * Unknown keys return UQC_ERR_ARGUMENT. */
 int uqc_set_option( uqc_solver* h, const char* key, double value );
 

@@ -25,7 +25,9 @@ _up = C.POINTER(C.c_uint)
 
 
 def lib_path(variant: str = "exact") -> Path:
-    name = "libuqcref.so" if variant == "exact" else "libuqcref_omp.so"
+    """exact: the parity build; omp: the timed OpenMP build; gpu: the parity
+    build with GpuClosure (oracle/ref/gpuclosure.cpp) selected by Closure::Create."""
+    name = {"exact": "libuqcref.so", "omp": "libuqcref_omp.so", "gpu": "libuqcref_gpu.so"}[variant]
     return _HERE / "_ref" / name
 
 

@@ -1,14 +1,21 @@
-"""Autotuner of the closure kernel's launch shape.
+"""Autotuner of the closure's launch shapes and schedule.
 
-The closure kernel can run a cell on one warp, two warps (several cells per
-CTA, named barriers) or a whole CTA, and can stage the basis tables in shared
-memory or read them through L1 (which leaves room for more cells per SM).
-Which is fastest depends on the moments per cell, the node count and the
-precision. `autotune(solver)` times every candidate on a few time steps of the
-solver's own state, restores the state, applies the fastest through
-uqc_set_option and returns the timings. Results are cached per configuration
-shape (states, moments, nodes, levels, uncertain dimensions, precision) in a
-JSON file, so a shape is tuned once per machine.
+FP64 form: the closure kernel can run a cell on one warp, two warps (several
+cells per CTA, named barriers) or a whole CTA, and can stage the basis tables
+in shared memory or read them through L1 (which leaves room for more cells per
+SM). Mixed form in rounds (2-D Euler): the chord schedule decides how often a
+cell's held inverse is re-formed (re-factor after a step with the held
+inverse that reduced ||g|| by less than 1/theta; more re-factorisations mean
+fewer, dearer iterations) and how many re-factorisation rounds a step runs
+before the FP64 form takes the remaining cells.
+
+Which is fastest depends on the moments per cell, the node count, the
+precision and the state. `autotune(solver)` times every candidate on a few
+time steps of the solver's own state (after untimed warm-up steps, so held
+inverses are in their steady state), restores the state, applies the fastest
+through uqc_set_option and returns the timings. Results are cached per
+configuration shape (states, moments, nodes, levels, uncertain dimensions,
+precision, mixed form) in a JSON file, so a shape is tuned once per machine.
 
     s = Solver(toml); s.init_state(); s.step(3)     # tune on a representative state
     best = autotune(s)
@@ -27,23 +34,43 @@ __all__ = ["autotune", "candidates", "DEFAULT_CACHE"]
 DEFAULT_CACHE = Path(os.environ.get("UQC_AUTOTUNE_CACHE", Path.home() / ".cache" / "uqcreator_b200" / "autotune.json"))
 
 
-def candidates(n_per_cell: int):
-    """Launch shapes worth timing for n = states x moments duals per cell."""
+THETAS = (0.05, 0.1, 0.2, 0.35, 0.5)
+ROUNDS = (2, 3)
+
+
+def candidates(n_per_cell: int, mixed_form: int = 0):
+    """Options worth timing: launch shapes of the FP64 closure kernel for
+    n = states x moments duals per cell, or (mixed form in rounds) the chord
+    schedule: theta x re-factorisation rounds."""
+    if mixed_form >= 1:
+        return [{"mixed_chord_theta": t, "mixed_rounds": r} for t in THETAS for r in ROUNDS]
     groups = [32, 64, 256] if n_per_cell <= 64 else [64, 256]
     return [{"closure_group": g, "closure_tables_smem": t} for g in groups for t in (1, 0)]
 
 
-def _key(solver, precision):
-    return f"s{solver.n_states}_t{solver.n_total}_q{solver.n_quad}_l{solver.n_levels}_d{solver.dim_xi}_p{precision}"
+def _key(solver, precision, mixed_form):
+    return (f"s{solver.n_states}_t{solver.n_total}_q{solver.n_quad}_l{solver.n_levels}_d{solver.dim_xi}_p{precision}"
+            f"_m{mixed_form if precision else 0}")
 
 
-def autotune(solver, steps: int = 2, repeats: int = 2, cache: Path | None = DEFAULT_CACHE, verbose: bool = False) -> dict:
-    """Times each candidate for `steps` steps (best of `repeats`) from the
-    solver's current state, restores that state and applies the fastest.
+def _parse(name):
+    out = {}
+    for kv in name.split(","):
+        k, v = kv.split("=")
+        out[k] = float(v) if "." in v else int(v)
+    return out
+
+
+def autotune(solver, steps: int = 2, repeats: int = 2, cache: Path | None = DEFAULT_CACHE, verbose: bool = False,
+             warmup: int = 2) -> dict:
+    """Times each candidate for `steps` steps (best of `repeats`, each after
+    `warmup` untimed steps) from the solver's current state, restores that
+    state and applies the fastest.
     Returns {"best": options, "ms_per_step": {name: ms or None}, "cached": bool}."""
     info = Info()
     check(solver.h, lib().uqc_get_info(solver.h, C.byref(info)))
-    key = _key(solver, info.precision)
+    mixed_form = info.mixed_form if info.precision == 1 else 0
+    key = _key(solver, info.precision, mixed_form)
     table = {}
     if cache is not None and Path(cache).exists():
         try:
@@ -58,7 +85,7 @@ def autotune(solver, steps: int = 2, repeats: int = 2, cache: Path | None = DEFA
     u0, l0, v0 = solver.download_state()
     t0 = info.t
     timings = {}
-    for opts in candidates(solver.n_states * solver.n_total):
+    for opts in candidates(solver.n_states * solver.n_total, mixed_form):
         name = ",".join(f"{k}={v}" for k, v in opts.items())
         try:
             for k, v in opts.items():
@@ -66,6 +93,8 @@ def autotune(solver, steps: int = 2, repeats: int = 2, cache: Path | None = DEFA
             best_ms = None
             for _ in range(repeats):
                 solver.upload_state(u0, l0, v0, t=t0)
+                if warmup:
+                    solver.step(warmup)
                 solver.step(steps)
                 ms = solver.last_timing()[2] / steps
                 best_ms = ms if best_ms is None or ms < best_ms else best_ms
@@ -80,7 +109,7 @@ def autotune(solver, steps: int = 2, repeats: int = 2, cache: Path | None = DEFA
     if not valid:
         raise UqcError(-2, "no launch shape fits this configuration")
     best_name = min(valid, key=valid.get)
-    best = {kv.split("=")[0]: int(kv.split("=")[1]) for kv in best_name.split(",")}
+    best = _parse(best_name)
     for k, v in best.items():
         solver.set_option(k, v)
     solver.upload_state(u0, l0, v0, t=t0)

@@ -42,18 +42,21 @@ namespace uqc {
 
 // ---------------------------------------------------------------- chord kernel
 
-// Per-warp workspace of k_chord (doubles): duals, trial duals and moments at
-// the finest stride nT; gradient, trial gradient and direction (compact, n =
-// NS nTj); nodal states uk (NS x nQ); reduction scratch; the gradient in FP32.
+// Per-warp workspace of k_chord (doubles): duals and moments at the finest
+// stride nT (state-major, as in HBM); trial duals basis-major (lamI[i NS + s],
+// so a basis function's NS values are 16-byte loads); the trial's moment sums
+// m(s, i) = sum_k U phiWf (kept for the epilogue's re-projection); gradient,
+// trial gradient and direction (compact, n = NS nTj); nodal states uk
+// node-major (uk[k NS + s]); reduction scratch; the gradient in FP32.
 struct ChordWs {
-    double *lam, *lamN, *uh, *g, *gN, *d, *uk, *red;
+    double *lam, *lamI, *uh, *m, *g, *gN, *d, *uk, *red;
     float* gf;
 };
 
 __host__ __device__ inline size_t chord_ws_doubles( int nS, int nT, int nQ ) {
     auto a4          = []( size_t x ) { return ( x + 3 ) & ~size_t( 3 ); };
     const size_t ldc = size_t( nS ) * nT;
-    return 6 * a4( ldc ) + a4( size_t( nS ) * nQ ) + 32 + a4( ( ldc + 1 ) / 2 );
+    return 7 * a4( ldc ) + a4( size_t( nS ) * nQ ) + 32 + a4( ( ldc + 1 ) / 2 );
 }
 
 __device__ inline ChordWs chord_carve( double* p, int nS, int nT, int nQ ) {
@@ -61,12 +64,13 @@ __device__ inline ChordWs chord_carve( double* p, int nS, int nT, int nQ ) {
     const size_t ldc = a4( size_t( nS ) * nT );
     ChordWs w;
     w.lam  = p;
-    w.lamN = p + ldc;
+    w.lamI = p + ldc;
     w.uh   = p + 2 * ldc;
-    w.g    = p + 3 * ldc;
-    w.gN   = p + 4 * ldc;
-    w.d    = p + 5 * ldc;
-    w.uk   = p + 6 * ldc;
+    w.m    = p + 3 * ldc;
+    w.g    = p + 4 * ldc;
+    w.gN   = p + 5 * ldc;
+    w.d    = p + 6 * ldc;
+    w.uk   = p + 7 * ldc;
     w.red  = w.uk + a4( size_t( nS ) * nQ );
     w.gf   = reinterpret_cast<float*>( w.red + 32 );
     return w;
@@ -82,27 +86,99 @@ __device__ __forceinline__ double* gslot( const KParams& P, int cell ) { return 
 
 // d = H0^-1 g with the cell's held inverse (FP32, n x n, symmetric, row-major):
 // lane o sums column o, d_o = sum_j Hinv(j, o) g_j; each step j reads a row of
-// the inverse with consecutive lanes on consecutive addresses.
+// the inverse with consecutive lanes on consecutive addresses. The rows are
+// loaded in batches of CHORD_JB before their FMAs, so that a batch's loads
+// are in flight together (the inverse comes from L2 or HBM).
+constexpr int CHORD_JB = 14;
 __device__ __forceinline__ void chord_direction( const float* __restrict__ Hinv, int n, const float* gf, double* d, int lane ) {
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-    const int o0 = lane, o1 = lane + 32, o2 = lane + 64, o3 = lane + 96;
-    for( int j = 0; j < n; ++j ) {
-        const float gj  = gf[j];
-        const float* rj = Hinv + size_t( j ) * n;
-        if( o0 < n ) a0 = fmaf( __ldg( rj + o0 ), gj, a0 );
-        if( o1 < n ) a1 = fmaf( __ldg( rj + o1 ), gj, a1 );
-        if( o2 < n ) a2 = fmaf( __ldg( rj + o2 ), gj, a2 );
-        if( o3 < n ) a3 = fmaf( __ldg( rj + o3 ), gj, a3 );
+    const int o0 = lane, o1 = lane + 32, o2 = lane + 64;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for( int j0 = 0; j0 < n; j0 += CHORD_JB ) {
+        float h0[CHORD_JB], h1[CHORD_JB], h2[CHORD_JB];
+#pragma unroll
+        for( int t = 0; t < CHORD_JB; ++t ) {
+            const int j     = j0 + t;
+            const float* rj = Hinv + size_t( j ) * n;
+            h0[t]           = ( j < n && o0 < n ) ? __ldg( rj + o0 ) : 0.f;
+            h1[t]           = ( j < n && o1 < n ) ? __ldg( rj + o1 ) : 0.f;
+            h2[t]           = ( j < n && o2 < n ) ? __ldg( rj + o2 ) : 0.f;
+        }
+#pragma unroll
+        for( int t = 0; t < CHORD_JB; ++t ) {
+            const float gj = j0 + t < n ? gf[j0 + t] : 0.f;
+            a0             = fmaf( h0[t], gj, a0 );
+            a1             = fmaf( h1[t], gj, a1 );
+            a2             = fmaf( h2[t], gj, a2 );
+        }
     }
     if( o0 < n ) d[o0] = double( a0 );
     if( o1 < n ) d[o1] = double( a1 );
     if( o2 < n ) d[o2] = double( a2 );
-    if( o3 < n ) d[o3] = double( a3 );
-    for( int o = lane + 128; o < n; o += 32 ) {    // systems beyond 128 duals
+    for( int o = lane + 96; o < n; o += 32 ) {    // systems beyond 96 duals
         float a = 0.f;
         for( int j = 0; j < n; ++j ) a = fmaf( __ldg( Hinv + size_t( j ) * n + o ), gf[j], a );
         d[o] = double( a );
     }
+}
+
+// NS values of node k of a node-major array (16-byte loads for even NS).
+template <int NS> __device__ __forceinline__ void load_node( const double* a, int k, double* v ) {
+    if constexpr( NS % 2 == 0 ) {
+#pragma unroll
+        for( int s = 0; s < NS; s += 2 ) {
+            const double2 t = *reinterpret_cast<const double2*>( a + k * NS + s );
+            v[s]            = t.x;
+            v[s + 1]        = t.y;
+        }
+    }
+    else {
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) v[s] = a[k * NS + s];
+    }
+}
+
+// Trial gradient of the chord kernel (closure.cpp:234-253): lane i sums
+// m(s, i) = sum_k uk(s, k) phiWf(k, i) over even and odd nodes as separate
+// chains (half the dependent FMA chain of one sum), uk node-major;
+// gout[s nTj + i] = m - uh, ms[s nT + i] = m; returns this lane's share of ||gout||^2.
+template <int NS>
+__device__ __forceinline__ double chord_gradient( const KParams& P, const double* phiWf, const double* uk, const double* uh, int nTj,
+                                                  double* gout, double* ms, int lane ) {
+    double sq = 0.0;
+    for( int i = lane; i < nTj; i += 32 ) {
+        double a0[NS], a1[NS];
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) a0[s] = a1[s] = 0.0;
+        const double* t = phiWf + i;
+        int k           = 0;
+        for( ; k + 1 < P.nQ; k += 2, t += 2 * P.ld ) {
+            const double w0 = t[0], w1 = t[P.ld];
+            double v0[NS], v1[NS];
+            load_node<NS>( uk, k, v0 );
+            load_node<NS>( uk, k + 1, v1 );
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) {
+                a0[s] = fma( v0[s], w0, a0[s] );
+                a1[s] = fma( v1[s], w1, a1[s] );
+            }
+        }
+        if( k < P.nQ ) {
+            const double w0 = t[0];
+            double v0[NS];
+            load_node<NS>( uk, k, v0 );
+#pragma unroll
+            for( int s = 0; s < NS; ++s ) a0[s] = fma( v0[s], w0, a0[s] );
+        }
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) {
+            const double mm   = a0[s] + a1[s];
+            const double d    = mm - uh[s * P.nT + i];
+            ms[s * P.nT + i]  = mm;
+            gout[s * nTj + i] = d;
+            sq += d * d;
+        }
+    }
+    return sq;
 }
 
 // Chord Newton rounds of the mixed form, step mode. round 0 takes the step's
@@ -165,9 +241,8 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_chord( KParams P
         bool bad = false;
         for( int idx = lane; idx < int( ldc ); idx += 32 ) {
             const double a = P.lam[cell * ldc + idx], b = P.u[cell * ldc + idx];
-            w.lam[idx]  = a;
-            w.lamN[idx] = a;    // trial duals beyond the cell's level stay the accepted ones
-            w.uh[idx]   = b;
+            w.lam[idx] = a;
+            w.uh[idx]  = b;
             bad         = bad || !isfinite( a ) || !isfinite( b );
         }
         const double* gs = gslot( P, cell );
@@ -186,7 +261,7 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_chord( KParams P
         auto trial = [&]( double c ) {
             for( int idx = lane; idx < NS * nTj; idx += 32 ) {
                 const int s = idx / nTj, i = idx - s * nTj;
-                w.lamN[s * P.nT + i] = w.lam[s * P.nT + i] + c * w.d[idx];
+                w.lamI[i * NS + s] = w.lam[s * P.nT + i] + c * w.d[idx];
             }
             __syncwarp();
             for( int k = lane; k < P.nQ; k += 32 ) {
@@ -196,15 +271,17 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_chord( KParams P
                 for( int s = 0; s < NS; ++s ) Lk[s] = 0.0;
                 for( int i = 0; i < nTj; ++i ) {
                     const double r = row[i];
+                    double li[NS];
+                    load_node<NS>( w.lamI, i, li );
 #pragma unroll
-                    for( int s = 0; s < NS; ++s ) Lk[s] = fma( w.lamN[s * P.nT + i], r, Lk[s] );
+                    for( int s = 0; s < NS; ++s ) Lk[s] = fma( li[s], r, Lk[s] );
                 }
                 Closure<CL>::U( Lk, y, true, P.phys );
 #pragma unroll
-                for( int s = 0; s < NS; ++s ) w.uk[s * P.nQ + k] = y[s];
+                for( int s = 0; s < NS; ++s ) w.uk[k * NS + s] = y[s];
             }
             __syncwarp();
-            const double sq = gradient_sums<NS, 32>( g, P, phiWf, w.uk, w.uh, nTj, w.gN, nullptr );
+            const double sq = chord_gradient<NS>( P, phiWf, w.uk, w.uh, nTj, w.gN, w.m, lane );
             return sqrt( group_sum<32>( g, sq, w.red ) );
         };
         if( bad ) {
@@ -243,8 +320,11 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_chord( KParams P
                     }
                 }
                 if( rc >= 0 ) break;
-                // accept: lam <- lamN, g <- gN (the gradient at the accepted duals)
-                for( int idx = lane; idx < int( ldc ); idx += 32 ) w.lam[idx] = w.lamN[idx];
+                // accept: lam <- the trial duals, g <- gN (the gradient at the accepted duals)
+                for( int idx = lane; idx < NS * nTj; idx += 32 ) {
+                    const int s = idx / nTj, i = idx - s * nTj;
+                    w.lam[s * P.nT + i] = w.lamI[i * NS + s];
+                }
                 for( int idx = lane; idx < n; idx += 32 ) w.g[idx] = w.gN[idx];
                 __syncwarp();
                 if( done || gnN < eps ) {
@@ -267,8 +347,9 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_chord( KParams P
             }
             itSum += iters - iters0;
             lsSum += ls;
-            // uk holds U at the accepted duals (the last trial evaluated)
-            const double dloc = cell_epilogue<CL, 32>( g, P, phiWf, w.uh, w.uk, cell, lev, nTj, w.red );
+            // uk holds U at the accepted duals (the last trial evaluated) and w.m
+            // its moment sums, the re-projected moments of momentsolver.cpp:120-124
+            const double dloc = cell_epilogue<CL, 32, true>( g, P, phiWf, w.uh, w.uk, cell, lev, nTj, w.red, w.m );
             dtMin             = dloc < dtMin ? dloc : dtMin;
         }
         else if( refactor && !last ) {
@@ -668,6 +749,152 @@ template <int CL, bool RAW> __global__ void __launch_bounds__( 256, 1 ) k_invert
         }
         if( g.r == 0 ) P.factorLevel[cell] = nTj;
         g.sync();
+    }
+}
+
+// ---------------------------------------------------------------- inverse by symmetric sweeps
+
+// Rows of a cell's matrix per warp and columns per lane of k_invert_sweep:
+// four warps per cell hold the n x n matrix (n <= 4 SWEEP_RG) in registers,
+// warp g rows [SWEEP_RG g, SWEEP_RG (g + 1)), lane l columns l, l + 32, l + 64.
+constexpr int SWEEP_RG = 21, SWEEP_CW = 3;
+
+// floats per cell of k_invert_sweep's shared memory: the raw values (rounded
+// up to 16 bytes), two pivot-row buffers, two ints; a multiple of 4 floats
+__host__ __device__ inline size_t sweep_raw_floats( int pairs, int NP ) { return ( size_t( pairs ) * NP + 3 ) & ~size_t( 3 ); }
+// a pivot-row buffer: 32 SWEEP_CW columns (those beyond the matrix hold
+// zeros) and the pivot itself at index 32 SWEEP_CW
+constexpr int SWEEP_PR = 32 * SWEEP_CW + 4;
+__host__ __device__ inline size_t sweep_ws_floats( int pairs, int NP ) { return sweep_raw_floats( pairs, NP ) + 2 * SWEEP_PR + 8; }
+
+// H^-1 of the cells of re-factor list `round` from the raw values k_hess_tc
+// left in their store slots, by the sweep operator (Gauss-Jordan on a
+// symmetric matrix: sweeping pivot k maps a_kk -> -1/a_kk, a_ik -> a_ik / a_kk,
+// a_ij -> a_ij - a_ik a_kj / a_kk; after all n pivots the matrix is -H^-1).
+// The matrix stays symmetric, so column k is row k: one warp publishes the
+// pivot row in shared memory, one named barrier per pivot, and every thread
+// updates its 21 x 3 register block with one FMA per element. No pivoting:
+// H is symmetric positive definite, and a pivot that is not positive (FP32
+// factor not positive definite) sends the cell to the FP64 fallback list.
+template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_invert_sweep( KParams P, int round ) {
+    constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP;
+    constexpr int RG = SWEEP_RG, CW = SWEEP_CW;
+    extern __shared__ __align__( 16 ) float fsm[];
+    if( !P.ctl->active ) return;
+    const int nIn = int( P.ctl->v2Count[round] );
+    if( nIn == 0 ) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cg = warp >> 2, g = warp & 3;    // cell group of the CTA, row group of the warp
+    const int nT = P.nT, n = NS * nT, pairs = nT * ( nT + 1 ) / 2;
+    float* raw  = fsm + size_t( cg ) * sweep_ws_floats( pairs, NP );
+    float* prow = raw + sweep_raw_floats( pairs, NP );    // two pivot-row buffers of SWEEP_PR floats
+    int* misc   = reinterpret_cast<int*>( prow + 2 * SWEEP_PR );    // [0] item, [1] not positive definite
+    const int bar = 1 + cg, tid = threadIdx.x & 127;
+    auto sync = [&]() { asm volatile( "bar.sync %0, 128;" ::"r"( bar ) : "memory" ); };
+    const int* list = refactor_list( P, round );
+    // decomposition of this thread's columns: c = l nT + i
+    int cm[CW], ci[CW];
+#pragma unroll
+    for( int q = 0; q < CW; ++q ) {
+        const int c = lane + 32 * q;
+        cm[q]       = c / nT;
+        ci[q]       = c - cm[q] * nT;
+    }
+    for( ;; ) {
+        if( tid == 0 ) misc[0] = int( atomicAdd( &P.ctl->v2Work[8 + round], 1u ) );
+        sync();
+        const int item = misc[0];
+        if( item >= nIn ) break;
+        const int cell = list[item];
+        float* slot    = P.factorStore + size_t( cell ) * P.factorStride;
+        for( int e = tid; e < pairs * NP; e += 128 ) raw[e] = slot[e];
+        if( tid == 0 ) misc[1] = 0;
+        sync();
+        // gather: element (r, c), r = m nT + j, c = l nT + i, is block (min, max)
+        // of (m, l) at pair (min, max) of (j, i); identity beyond n
+        float a[RG][CW];
+#pragma unroll
+        for( int rr = 0; rr < RG; ++rr ) {
+            const int r = RG * g + rr, rm = r / nT, rj = r - rm * nT;
+#pragma unroll
+            for( int q = 0; q < CW; ++q ) {
+                const int c = lane + 32 * q;
+                float v     = r == c ? 1.f : 0.f;
+                if( r < n && c < n ) {
+                    const int lo = min( rm, cm[q] ), hi = max( rm, cm[q] );
+                    const int b  = lo * NS - ( lo * ( lo - 1 ) ) / 2 + ( hi - lo );
+                    const int pl = min( rj, ci[q] ), ph = max( rj, ci[q] );
+                    v            = raw[( ( ph * ( ph + 1 ) ) / 2 + pl ) * NP + b];
+                }
+                a[rr][q] = v;
+            }
+        }
+        bool bad = false;
+        for( int gg = 0; gg < 4; ++gg ) {
+#pragma unroll
+            for( int rr = 0; rr < RG; ++rr ) {
+                const int k = RG * gg + rr;
+                if( k >= n ) break;
+                float* pr = prow + ( k & 1 ) * SWEEP_PR;
+                const int kl = k & 31, kq = k >> 5;
+                if( g == gg ) {
+                    // the pivot row; at the pivot p - 1 (so that pr[k] / p = 1 - 1/p,
+                    // the factor that turns column k into a_ik / p), p itself at the end
+#pragma unroll
+                    for( int q = 0; q < CW; ++q ) {
+                        float v = a[rr][q];
+                        if( lane == kl && q == kq ) {
+                            pr[32 * CW] = v;
+                            v -= 1.f;
+                        }
+                        pr[lane + 32 * q] = v;
+                    }
+                }
+                sync();
+                const float p    = pr[32 * CW];
+                bad              = bad || !( p > 0.f );
+                const float pinv = __frcp_rn( p );
+                // a_ij -= a_ik a_kj / p (column k: a_ik / p)
+                float sv[CW];
+#pragma unroll
+                for( int q = 0; q < CW; ++q ) sv[q] = pr[lane + 32 * q] * pinv;
+#pragma unroll
+                for( int rr2 = 0; rr2 < RG; ++rr2 ) {
+                    const float f = pr[RG * g + rr2];    // a_ik (column k = row k)
+#pragma unroll
+                    for( int q = 0; q < CW; ++q ) a[rr2][q] = fmaf( -f, sv[q], a[rr2][q] );
+                }
+                if( g == gg ) {    // the pivot row: a_kj / p, and -1/p at the pivot
+#pragma unroll
+                    for( int q = 0; q < CW; ++q ) a[rr][q] = ( lane == kl && q == kq ) ? sv[q] - 1.f : sv[q];
+                }
+            }
+        }
+        if( bad ) misc[1] = 1;
+        sync();
+        if( misc[1] ) {
+            if( tid == 0 ) {
+                P.factorLevel[cell] = -2;
+                P.fallbackList[atomicAdd( P.fallbackCount, 1u )] = cell;
+                atomicAdd( &P.ctl->fallbackCells, 1ull );
+            }
+        }
+        else {
+            // H^-1 = -(the swept matrix), row-major n x n
+#pragma unroll
+            for( int rr = 0; rr < RG; ++rr ) {
+                const int r = RG * g + rr;
+                if( r < n ) {
+#pragma unroll
+                    for( int q = 0; q < CW; ++q ) {
+                        const int c = lane + 32 * q;
+                        if( c < n ) slot[size_t( r ) * n + c] = -a[rr][q];
+                    }
+                }
+            }
+            if( tid == 0 ) P.factorLevel[cell] = nT;
+        }
+        sync();
     }
 }
 

@@ -660,11 +660,13 @@ out:
 // the nodes, uh the moments before re-projection. Writes uQ, the new
 // refinement level (indicator of :271-289, thresholds of :104-112) and the
 // re-projected moments, and returns the cell's CFL time step.
-template <int CL, int GROUP>
+// NM: uk node-major (uk[k NS + s]) instead of state-major (uk[s nQ + k]).
+template <int CL, int GROUP, bool NM = false>
 __device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* uh, const double* uk, int cell,
                                  int lev, int nTj, double* red,
                                  const double* ugs = nullptr ) {
     constexpr int NS = Closure<CL>::NS;
+    auto ukAt = [&]( int s, int k ) { return NM ? uk[k * NS + s] : uk[s * P.nQ + k]; };
     const size_t ldc = size_t( NS ) * P.nT;
     int newLev       = lev;
     if( P.nLevels > 1 ) {
@@ -686,12 +688,24 @@ __device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const do
         P.level[cell] = unsigned( newLev );
     }
     double* uq = P.uQ + size_t( cell ) * NS * P.nQ;
-    for( int idx = g.r; idx < NS * P.nQ; idx += GROUP ) uq[idx] = uk[idx];
+    for( int idx = g.r; idx < NS * P.nQ; idx += GROUP ) {
+        const int s = idx / P.nQ, k = idx - s * P.nQ;
+        uq[idx]     = ukAt( s, k );
+    }
     // [E] u(s, i) = sum_k uQ(s, k) phiWf(k, i) for i < nT(new level), 0 beyond
     for( int idx = g.r; idx < int( ldc ); idx += GROUP ) {
         int s = idx / P.nT, i = idx - s * P.nT;
         // ugs: the same sums kept from the gradient test (i < nTj), when the caller has them
-        P.uRe[cell * ldc + idx] = i < nTn ? ( ugs && i < nTj ? ugs[idx] : node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ ) ) : 0.0;
+        double m = 0.0;
+        if( i < nTn ) {
+            if( ugs && i < nTj )
+                m = ugs[idx];
+            else if( !NM )
+                m = node_dot( uk + s * P.nQ, phiWf, P.ld, i, P.nQ );
+            else
+                for( int k = 0; k < P.nQ; ++k ) m = fma( uk[k * NS + s], phiWf[size_t( k ) * P.ld + i], m );
+        }
+        P.uRe[cell * ldc + idx] = m;
         if( i >= nTn ) P.u[cell * ldc + idx] = 0.0;    // the update writes u below the level only
     }
     // [F] the cell's time step (min over its nodes)
@@ -699,7 +713,7 @@ __device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const do
     for( int k = g.r; k < P.nQ; k += GROUP ) {
         double uqk[NS];
 #pragma unroll
-        for( int s = 0; s < NS; ++s ) uqk[s] = uk[s * P.nQ + k];
+        for( int s = 0; s < NS; ++s ) uqk[s] = ukAt( s, k );
         double d = Problem<CL>::dt( uqk, P.dx[cell], P.phys );
         dloc     = d < dloc ? d : dloc;
     }
@@ -1157,7 +1171,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         const double* ua = P.uQ + size_t( cell ) * NS * P.nQ;
         // the faces' neighbours and normals, once per cell (nFaces <= 3)
         const double* ub[3];
-        double nu[3][2], ns[3][2];
+        double nu[3][2], ns[3][2], nlen[3];
         bool ghost[3];
         // wall cells (Euler 2-D): faces without a neighbour see the cell's own
         // states reflected at the boundary normal (expliciteuler.cpp:24-70)
@@ -1177,6 +1191,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
                 nu[f][1] = P.unitN[( cell * P.nFaces + f ) * 2 + 1];
                 ns[f][0] = P.scaledN[( cell * P.nFaces + f ) * 2];
                 ns[f][1] = P.scaledN[( cell * P.nFaces + f ) * 2 + 1];
+                nlen[f]  = sqrt( ns[f][0] * ns[f][0] + ns[f][1] * ns[f][1] );    // euler2d.cpp:84, once per face
             }
         }
         for( int k = lane; k < P.nQ; k += 32 ) {
@@ -1192,11 +1207,11 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
                 if( f < P.nFaces ) {
                     double b[NS], y[NS];
                     if( ghost[f] )
-                        Problem<CL>::flux( gh, gh, nu[f], ns[f], y, P.phys );
+                        Problem<CL>::flux( gh, gh, nu[f], ns[f], nlen[f], y, P.phys );
                     else {
 #pragma unroll
                         for( int s = 0; s < NS; ++s ) b[s] = ub[f][s * P.nQ + k];
-                        Problem<CL>::flux( a, b, nu[f], ns[f], y, P.phys );
+                        Problem<CL>::flux( a, b, nu[f], ns[f], nlen[f], y, P.phys );
                     }
 #pragma unroll
                     for( int s = 0; s < NS; ++s ) gsum[s] += y[s];

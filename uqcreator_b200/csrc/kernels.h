@@ -18,7 +18,8 @@ enum KernelId {
     KERNEL_CHORD         = 8,    // k_chord (mixed form in rounds; 2-D Euler only)
     KERNEL_HESS_TC       = 9,    // k_hess_tc
     KERNEL_INVERT_RAW    = 10,   // k_invert from k_hess_tc's values
-    KERNEL_INVERT        = 11    // k_invert with the Hessian on CUDA cores
+    KERNEL_INVERT        = 11,   // k_invert with the Hessian on CUDA cores
+    KERNEL_INVERT_SWEEP  = 12    // k_invert_sweep (from k_hess_tc's values, n <= 84)
 };
 
 // nullptr when there is no such variant

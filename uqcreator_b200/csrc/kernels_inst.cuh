@@ -41,8 +41,10 @@ template <int CL> void* kernel_of( int group, int which ) {
         case KERNEL_HESS_TC:
         case KERNEL_INVERT_RAW:
         case KERNEL_INVERT:
+        case KERNEL_INVERT_SWEEP:
             if constexpr( Closure<CL>::NS == 4 ) {    // the mixed form in rounds serves the 2-D Euler closure
                 if( which == KERNEL_CHORD ) return (void*)&k_chord<CL>;
+                if( which == KERNEL_INVERT_SWEEP ) return (void*)&k_invert_sweep<CL>;
                 if( which == KERNEL_HESS_TC ) return (void*)&k_hess_tc<CL>;
                 if( which == KERNEL_INVERT_RAW ) return (void*)&k_invert<CL, true>;
                 return (void*)&k_invert<CL, false>;

@@ -128,13 +128,14 @@ template <int NS> __device__ __forceinline__ int pair_index( int a, int b ) {
 }
 
 // ---------------------------------------------------------------- problems
-// Numerical flux g(u, v) for face unit normal nu and scaled normal n.
+// Numerical flux g(u, v) for face unit normal nu, scaled normal n and face
+// length nn = |n| (computed once per face by the caller).
 template <int CL> struct Problem;
 
 // Burgers with the local Lax-Friedrichs flux (julia/Tensorization/IPMSolver.jl:38-42)
 // and CFL rule of burgers.cpp:114-122; ramp initial state (burgers.cpp:48-68).
 template <> struct Problem<0> {
-    __device__ static void flux( const double* u, const double* v, const double*, const double* n, double* y, const PhysParams& ) {
+    __device__ static void flux( const double* u, const double* v, const double*, const double* n, double, double* y, const PhysParams& ) {
         double beta = fabs( u[0] ) < fabs( v[0] ) ? fabs( v[0] ) : fabs( u[0] );
         y[0]        = 0.5 * ( 0.5 * u[0] * u[0] + 0.5 * v[0] * v[0] ) * n[0] - 0.5 * beta * ( v[0] - u[0] ) * fabs( n[0] );
     }
@@ -161,7 +162,8 @@ template <> struct Problem<1> {
         out[2]   = ( u[1] * v2 ) * n[0] + ( u[2] * v2 + p ) * n[1];
         out[3]   = ( ( u[3] + p ) * v1 ) * n[0] + ( ( u[3] + p ) * v2 ) * n[1];
     }
-    __device__ static void flux( const double* u, const double* v, const double* nu, const double* n, double* y, const PhysParams& P ) {
+    __device__ static void flux( const double* u, const double* v, const double* nu, const double* n, double nn, double* y,
+                                 const PhysParams& P ) {
         const double gm = P.gamma;
         double rhoInv = 1.0 / u[0], uU = u[1] * rhoInv, vU = u[2] * rhoInv;
         double p  = ( gm - 1.0 ) * ( u[3] - 0.5 * u[0] * ( uU * uU + vU * vU ) );
@@ -180,7 +182,7 @@ template <> struct Problem<1> {
             double fu[4], fv[4];
             Fn( gm, u, n, fu );
             Fn( gm, v, n, fv );
-            double nn = sqrt( n[0] * n[0] + n[1] * n[1] ), ll = lmax * lmin, inv = 1.0 / ( lmax - lmin );
+            double ll = lmax * lmin, inv = 1.0 / ( lmax - lmin );
             for( int i = 0; i < 4; ++i ) y[i] = inv * ( ( lmax * fu[i] - lmin * fv[i] ) + ll * ( v[i] - u[i] ) * nn );
         }
     }
@@ -215,7 +217,8 @@ template <> struct Problem<1> {
 // Shallow water 1-D: Lax-Friedrichs with dx/dt = 12 / CFL (shallowwater.cpp:21-35);
 // time step Settings::GetDT (problem.cpp:44); dam-break initial state.
 template <> struct Problem<2> {
-    __device__ static void flux( const double* u, const double* v, const double*, const double* n, double* y, const PhysParams& P ) {
+    __device__ static void flux( const double* u, const double* v, const double*, const double* n, double, double* y,
+                                 const PhysParams& P ) {
         const double gr = 9.81;
         double s        = 0.5 / ( P.cfl / 12.0 );
         double fl1 = ( u[1] * u[1] ) / u[0] + 0.5 * gr * ( u[0] * u[0] );

@@ -84,14 +84,14 @@ struct uqc_solver {
     bool chord           = true;
     bool chordInverse    = false;    // planned: the mixed workspace holds the packed factor inverse
     bool chordInverseOpt = true;     // option mixed_chord_inverse
-    double chordTheta    = 0.1;
+    double chordTheta    = 0.2;
     size_t mixedSmem       = 0;
     bool mixedTablesInSmem = false;
     // mixed form in rounds (chord.cuh; 2-D Euler with one refinement level):
     // k_chord, then per round k_hess_tc / k_invert and k_chord again
     int roundsOpt   = -1;    // option mixed_hessian: -1 automatic, 0 single kernel, 1 CUDA-core Hessian, 2 tensor cores
     int v2Mode      = 0;     // planned: 0 off, 1 rounds with the CUDA-core Hessian, 2 with the tensor-core Hessian
-    int v2Rounds    = 3;     // option mixed_rounds
+    int v2Rounds    = 2;     // option mixed_rounds
     std::string v2Why;       // why the rounds (or the tensor cores) are not used
     double* d_gStore        = nullptr;
     int gStride             = 0;
@@ -101,6 +101,7 @@ struct uqc_solver {
     int chordBlock = 512, chordGrid = 0, hessGrid = 0, invBlock = 256, invGrid = 0;
     size_t chordSmem = 0, hessSmem = 0, invSmem = 0;
     bool chordTablesInSmem = false;
+    bool invSweep          = false;    // the inverse kernel is k_invert_sweep
     // bookkeeping
     bool stateReady = false;
     int precision   = 0;
@@ -387,16 +388,27 @@ void plan_rounds( uqc_solver* h, int maxSmem ) {
                    " B of shared memory exceed one MMA (256 pairs)";
         return;
     }
-    // inverse kernel: two warps per cell, as many cells per CTA (up to 4) as fit
-    const size_t iws = invert_ws_bytes( nS * nT, nQ, NP, mode == 2 );
-    const int groups = int( std::min<size_t>( 4, size_t( maxSmem ) / iws ) );
-    if( groups < 1 ) {
-        h->v2Why = "inverse workspace exceeds shared memory";
-        return;
+    // inverse kernel: by sweeps in registers (four warps per cell, four cells
+    // per CTA) for n <= 84 after the tensor-core Hessian; else Cholesky and
+    // triangular inverse, two warps per cell, as many cells (up to 4) as fit
+    h->invSweep = mode == 2 && nS * nT <= 4 * SWEEP_RG && nS * nT <= 32 * SWEEP_CW;
+    void* ki    = nullptr;
+    if( h->invSweep ) {
+        h->invBlock = 512;
+        h->invSmem  = 4 * sweep_ws_floats( nT * ( nT + 1 ) / 2, NP ) * sizeof( float );
+        ki          = pick( cl, 32, KERNEL_INVERT_SWEEP );
     }
-    h->invBlock = 64 * groups;
-    h->invSmem  = iws * groups;
-    void* ki    = pick( cl, 32, mode == 2 ? KERNEL_INVERT_RAW : KERNEL_INVERT );
+    else {
+        const size_t iws = invert_ws_bytes( nS * nT, nQ, NP, mode == 2 );
+        const int groups = int( std::min<size_t>( 4, size_t( maxSmem ) / iws ) );
+        if( groups < 1 ) {
+            h->v2Why = "inverse workspace exceeds shared memory";
+            return;
+        }
+        h->invBlock = 64 * groups;
+        h->invSmem  = iws * groups;
+        ki          = pick( cl, 32, mode == 2 ? KERNEL_INVERT_RAW : KERNEL_INVERT );
+    }
     allow_dynamic_smem( ki );
     CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ki, h->invBlock, h->invSmem ) );
     h->invGrid = std::max( 1, occ ) * h->numSMs;
@@ -741,7 +753,8 @@ void launch_closure( uqc_solver* h, KParams& P, int mode ) {
                 int rr        = r - 1;
                 void* hargs[] = {&C, &rr};
                 if( h->v2Mode == 2 ) launch( h, pick( cl, 32, KERNEL_HESS_TC ), h->hessGrid, 256, h->hessSmem, hargs );
-                launch( h, pick( cl, 32, h->v2Mode == 2 ? KERNEL_INVERT_RAW : KERNEL_INVERT ), h->invGrid, h->invBlock, h->invSmem, hargs );
+                const int ik = h->invSweep ? KERNEL_INVERT_SWEEP : ( h->v2Mode == 2 ? KERNEL_INVERT_RAW : KERNEL_INVERT );
+                launch( h, pick( cl, 32, ik ), h->invGrid, h->invBlock, h->invSmem, hargs );
             }
             int rr       = r;
             void* args[] = {&C, &rr};
@@ -1922,12 +1935,17 @@ int uqc_debug_mixed_inverse( uqc_solver* h, int n, const int* cells, int form, f
         CK( cudaGetDevice( &dev ) );
         CK( cudaDeviceGetAttribute( &maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev ) );
         if( form == 2 ) launch( h, pick( cl, 32, KERNEL_HESS_TC ), h->hessGrid, 256, h->hessSmem, args );
-        const size_t iws = invert_ws_bytes( h->nS * h->tab.nT, h->tab.nQ, closure_np( cl ), form == 2 );
-        const int groups = int( std::min<size_t>( 4, size_t( maxSmem ) / iws ) );
-        void* ki         = pick( cl, 32, form == 2 ? KERNEL_INVERT_RAW : KERNEL_INVERT );
-        allow_dynamic_smem( ki );
-        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ki, 64 * groups, iws * groups ) );
-        launch( h, ki, std::max( 1, occ ) * h->numSMs, 64 * groups, iws * groups, args );
+        if( form == 2 && h->invSweep ) {
+            launch( h, pick( cl, 32, KERNEL_INVERT_SWEEP ), h->invGrid, h->invBlock, h->invSmem, args );
+        }
+        else {
+            const size_t iws = invert_ws_bytes( h->nS * h->tab.nT, h->tab.nQ, closure_np( cl ), form == 2 );
+            const int groups = int( std::min<size_t>( 4, size_t( maxSmem ) / iws ) );
+            void* ki         = pick( cl, 32, form == 2 ? KERNEL_INVERT_RAW : KERNEL_INVERT );
+            allow_dynamic_smem( ki );
+            CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ki, 64 * groups, iws * groups ) );
+            launch( h, ki, std::max( 1, occ ) * h->numSMs, 64 * groups, iws * groups, args );
+        }
         const size_t nn = size_t( h->nS ) * h->tab.nT * h->nS * h->tab.nT;
         for( int i = 0; i < n; ++i )
             CK( cudaMemcpyAsync( out + i * nn, h->d_factorStore + size_t( cells[i] ) * h->factorStride, nn * sizeof( float ),
