@@ -132,7 +132,8 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *                    triangular solves; used when its shared memory costs no
  *                    cell per SM (else the triangular solves); 0: never.
  *   "mixed_chord_theta"  re-factor after a step with the held factor that
- *                    reduced ||g|| by less than the factor 1/theta (default 0.2, the autotuner's choice for the 2-D Euler workload).
+ *                    reduced ||g|| by less than the factor 1/theta (default: 0.2 in the
+ *                    rounds form, 0.1 in the single kernel; the autotuner's choices).
  *   "update_test"    1: the update kernel tests the next step's closure
  *                    convergence per cell and lists only the cells that need
  *                    Newton; 0: a check kernel tests every cell at the start

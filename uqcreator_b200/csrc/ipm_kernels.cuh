@@ -1073,6 +1073,9 @@ __device__ __forceinline__ void project_lane( const double* Gs, const double* t,
     }
 }
 
+// doubles per warp of k_update's shared memory: the nodal flux sums and 16 of face data
+__host__ __device__ inline size_t update_warp_doubles( int nS, int nQ ) { return ( ( size_t( nS ) * nQ + 3 ) & ~size_t( 3 ) ) + 16; }
+
 // Warp-buffered append to a device list (warp-uniform call): lane `cnt` keeps
 // the entry; 32 entries take one atomicAdd on the list length.
 struct WarpListBuf {
@@ -1113,7 +1116,10 @@ __device__ __forceinline__ void finish_cell( const KParams& P, int cell, double 
 // reassociation. Each lane carries two outputs with two partial sums each.
 // FIN: with the next step's convergence test (P.finishInUpdate); the plain
 // instance (adaptive configurations, test off) carries none of its code.
-template <int CL, bool FIN>
+// WALL: the mesh has wall cells (ghost states at their boundary faces); the
+// instance without walls evaluates two nodes per lane at a time (independent
+// flux chains for the scheduler) with no ghost-state code.
+template <int CL, bool FIN, bool WALL>
 __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
     const bool finish = FIN && P.finishInUpdate;
     constexpr int NS = Closure<CL>::NS;
@@ -1131,7 +1137,10 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         base += ( tn + 4 ) & ~size_t( 3 );
         __syncthreads();
     }
-    double* Gs       = base + size_t( warp ) * ( ( size_t( NS ) * P.nQ + 3 ) & ~size_t( 3 ) );
+    // per warp: the summed nodal fluxes (NS x nQ, node-major), then the cell's
+    // face data: unit normal (2), scaled normal (2) and length of each face
+    double* Gs       = base + size_t( warp ) * update_warp_doubles( NS, P.nQ );
+    double* fd       = Gs + ( ( size_t( NS ) * P.nQ + 3 ) & ~size_t( 3 ) );
     const double dt  = __longlong_as_double( (long long)P.ctl->dtBits );
     const size_t ldc = size_t( NS ) * P.nT;
     double res       = 0.0;
@@ -1171,11 +1180,10 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         const double* ua = P.uQ + size_t( cell ) * NS * P.nQ;
         // the faces' neighbours and normals, once per cell (nFaces <= 3)
         const double* ub[3];
-        double nu[3][2], ns[3][2], nlen[3];
         bool ghost[3];
         // wall cells (Euler 2-D): faces without a neighbour see the cell's own
         // states reflected at the boundary normal (expliciteuler.cpp:24-70)
-        const bool wall = CL == 1 && bc >= 2;
+        const bool wall = WALL && CL == 1 && bc >= 2;
         double bn[2]    = {0.0, 0.0};
         if( wall ) {
             bn[0] = P.bndNormal[2 * cell];
@@ -1187,38 +1195,84 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
                 const int nb = P.nbr[cell * P.nFaces + f];
                 ghost[f]     = wall && nb == P.nCells;
                 ub[f]        = P.uQ + size_t( nb ) * NS * P.nQ;
-                nu[f][0] = P.unitN[( cell * P.nFaces + f ) * 2];
-                nu[f][1] = P.unitN[( cell * P.nFaces + f ) * 2 + 1];
-                ns[f][0] = P.scaledN[( cell * P.nFaces + f ) * 2];
-                ns[f][1] = P.scaledN[( cell * P.nFaces + f ) * 2 + 1];
-                nlen[f]  = sqrt( ns[f][0] * ns[f][0] + ns[f][1] * ns[f][1] );    // euler2d.cpp:84, once per face
             }
         }
-        for( int k = lane; k < P.nQ; k += 32 ) {
-            double a[NS], gsum[NS], gh[NS];
+        __syncwarp();    // the previous cell's face data is read
+        if( lane < P.nFaces ) {
+            const int f    = lane;
+            const double a = P.scaledN[( cell * P.nFaces + f ) * 2], b = P.scaledN[( cell * P.nFaces + f ) * 2 + 1];
+            fd[5 * f]      = P.unitN[( cell * P.nFaces + f ) * 2];
+            fd[5 * f + 1]  = P.unitN[( cell * P.nFaces + f ) * 2 + 1];
+            fd[5 * f + 2]  = a;
+            fd[5 * f + 3]  = b;
+            fd[5 * f + 4]  = sqrt( a * a + b * b );    // |n| of euler2d.cpp:84, once per face
+        }
+        __syncwarp();
+        if constexpr( WALL ) {
+            for( int k = lane; k < P.nQ; k += 32 ) {
+                double a[NS], gsum[NS], gh[NS];
 #pragma unroll
-            for( int s = 0; s < NS; ++s ) {
-                a[s]    = ua[s * P.nQ + k];
-                gsum[s] = 0.0;
-            }
-            if( wall ) wall_ghost<CL>( a, bn, bc == 2, gh );
+                for( int s = 0; s < NS; ++s ) {
+                    a[s]    = ua[s * P.nQ + k];
+                    gsum[s] = 0.0;
+                }
+                if( wall ) wall_ghost<CL>( a, bn, bc == 2, gh );
 #pragma unroll
-            for( int f = 0; f < 3; ++f ) {
-                if( f < P.nFaces ) {
-                    double b[NS], y[NS];
-                    if( ghost[f] )
-                        Problem<CL>::flux( gh, gh, nu[f], ns[f], nlen[f], y, P.phys );
-                    else {
+                for( int f = 0; f < 3; ++f ) {
+                    if( f < P.nFaces ) {
+                        double b[NS], y[NS];
+                        if( ghost[f] )
+                            Problem<CL>::flux( gh, gh, fd + 5 * f, fd + 5 * f + 2, fd[5 * f + 4], y, P.phys );
+                        else {
 #pragma unroll
-                        for( int s = 0; s < NS; ++s ) b[s] = ub[f][s * P.nQ + k];
-                        Problem<CL>::flux( a, b, nu[f], ns[f], nlen[f], y, P.phys );
+                            for( int s = 0; s < NS; ++s ) b[s] = ub[f][s * P.nQ + k];
+                            Problem<CL>::flux( a, b, fd + 5 * f, fd + 5 * f + 2, fd[5 * f + 4], y, P.phys );
+                        }
+#pragma unroll
+                        for( int s = 0; s < NS; ++s ) gsum[s] += y[s];
                     }
+                }
 #pragma unroll
-                    for( int s = 0; s < NS; ++s ) gsum[s] += y[s];
+                for( int s = 0; s < NS; ++s ) Gs[k * NS + s] = gsum[s];
+            }
+        }
+        else {
+            // nodes k and k + 32 together; a lane without a second node repeats its first
+            for( int k0 = lane; k0 < P.nQ; k0 += 64 ) {
+                const bool two = k0 + 32 < P.nQ;
+                const int k1   = two ? k0 + 32 : k0;
+                double a0[NS], a1[NS], g0[NS], g1[NS];
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) {
+                    a0[s] = ua[s * P.nQ + k0];
+                    a1[s] = ua[s * P.nQ + k1];
+                    g0[s] = g1[s] = 0.0;
+                }
+#pragma unroll
+                for( int f = 0; f < 3; ++f ) {
+                    if( f < P.nFaces ) {
+                        double b0[NS], b1[NS], y0[NS], y1[NS];
+#pragma unroll
+                        for( int s = 0; s < NS; ++s ) {
+                            b0[s] = ub[f][s * P.nQ + k0];
+                            b1[s] = ub[f][s * P.nQ + k1];
+                        }
+                        Problem<CL>::flux( a0, b0, fd + 5 * f, fd + 5 * f + 2, fd[5 * f + 4], y0, P.phys );
+                        Problem<CL>::flux( a1, b1, fd + 5 * f, fd + 5 * f + 2, fd[5 * f + 4], y1, P.phys );
+#pragma unroll
+                        for( int s = 0; s < NS; ++s ) {
+                            g0[s] += y0[s];
+                            g1[s] += y1[s];
+                        }
+                    }
+                }
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) Gs[k0 * NS + s] = g0[s];
+                if( two ) {
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) Gs[k1 * NS + s] = g1[s];
                 }
             }
-#pragma unroll
-            for( int s = 0; s < NS; ++s ) Gs[k * NS + s] = gsum[s];
         }
         __syncwarp();
         // projection and update: a lane per basis function i, the NS states as
@@ -1226,7 +1280,6 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         const double c = dt / P.area[cell];
         double sq      = 0.0;
         double v0a = 0.0, v0b = 0.0;    // u_new(0, lane) and u_new(0, lane + 32), for the level rule
-        double ga[NS], gb[NS];          // the next step's gradient uRe - u_new at i = lane, lane + 32
         for( int i = lane; i < nTj; i += 32 ) {    // beyond the level u stays zero (epilogue)
             // the re-projected moments first: their loads overlap the
             // projection (uRe and u may alias, so a load after a store to u
@@ -1241,9 +1294,6 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
                 const double gi  = old[s] - v;
                 P.u[cell * ldc + s * P.nT + i] = v;
                 sq                             = fma( gi, gi, sq );
-                if( i < 32 ) ga[s] = gi;
-                else if( i < 64 ) gb[s] = gi;
-                else if( P.gStore ) P.gStore[size_t( cell ) * P.gStride + s * nTj + i] = gi;
                 if( s == 0 && i < 32 ) v0a = v;
                 if( s == 0 && i >= 32 && i < 64 ) v0b = v;
                 if( s == 0 && i == 0 ) res += fabs( v - P.uOld0[cell] ) * P.area[cell];
@@ -1286,12 +1336,14 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
             else if( pass )
                 cbuf.push( lane, cell, clist, ccount );    // converged, new level: k_check's epilogue
             else {
-                if( P.gStore ) {    // the gradient the mixed form's Newton starts from
+                if( P.gStore ) {
+                    // the gradient the mixed form's Newton starts from: uRe - u_new,
+                    // the same differences as gi above (from the values just stored)
+                    __syncwarp();
                     double* gs = P.gStore + size_t( cell ) * P.gStride;
-#pragma unroll
-                    for( int s = 0; s < NS; ++s ) {
-                        if( lane < nTj ) gs[s * nTj + lane] = ga[s];
-                        if( lane + 32 < nTj && lane + 32 < 64 ) gs[s * nTj + lane + 32] = gb[s];
+                    for( int idx = lane; idx < NS * nTj; idx += 32 ) {
+                        const int s = idx / nTj, i = idx - s * nTj;
+                        gs[idx]     = P.uRe[cell * ldc + s * P.nT + i] - P.u[cell * ldc + s * P.nT + i];
                     }
                     if( lane == 0 ) gs[ldc] = sqrt( sq );
                 }

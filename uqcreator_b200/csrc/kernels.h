@@ -19,7 +19,9 @@ enum KernelId {
     KERNEL_HESS_TC       = 9,    // k_hess_tc
     KERNEL_INVERT_RAW    = 10,   // k_invert from k_hess_tc's values
     KERNEL_INVERT        = 11,   // k_invert with the Hessian on CUDA cores
-    KERNEL_INVERT_SWEEP  = 12    // k_invert_sweep (from k_hess_tc's values, n <= 84)
+    KERNEL_INVERT_SWEEP  = 12,   // k_invert_sweep (from k_hess_tc's values, n <= 84)
+    KERNEL_UPDATE_WALL   = 13,   // k_update for meshes with wall cells (2-D Euler)
+    KERNEL_UPDATE_PLAIN_WALL = 14
 };
 
 // nullptr when there is no such variant

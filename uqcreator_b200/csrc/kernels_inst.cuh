@@ -18,8 +18,10 @@ template <int CL> void* kernel_of( int group, int which ) {
             if( group == 32 ) return (void*)&k_closure<CL, 32, float>;
             if( group == 64 ) return (void*)&k_closure<CL, 64, float>;
             return nullptr;
-        case KERNEL_UPDATE: return (void*)&k_update<CL, true>;
-        case KERNEL_UPDATE_PLAIN: return (void*)&k_update<CL, false>;
+        case KERNEL_UPDATE: return (void*)&k_update<CL, true, false>;
+        case KERNEL_UPDATE_PLAIN: return (void*)&k_update<CL, false, false>;
+        case KERNEL_UPDATE_WALL: return CL == 1 ? (void*)&k_update<CL, true, true> : nullptr;
+        case KERNEL_UPDATE_PLAIN_WALL: return CL == 1 ? (void*)&k_update<CL, false, true> : nullptr;
         case KERNEL_INIT:
             if( group == 32 ) return (void*)&k_init<CL, 32>;
             if( group == 256 ) return (void*)&k_init<CL, 256>;

@@ -84,7 +84,7 @@ struct uqc_solver {
     bool chord           = true;
     bool chordInverse    = false;    // planned: the mixed workspace holds the packed factor inverse
     bool chordInverseOpt = true;     // option mixed_chord_inverse
-    double chordTheta    = 0.2;
+    double chordTheta    = 0.0;      // option mixed_chord_theta; 0: automatic (0.2 with rounds, 0.1 in the single kernel)
     size_t mixedSmem       = 0;
     bool mixedTablesInSmem = false;
     // mixed form in rounds (chord.cuh; 2-D Euler with one refinement level):
@@ -247,7 +247,7 @@ KParams make_params( const uqc_solver* h ) {
     P.factorLevel       = useStore ? h->d_factorLevel : nullptr;
     P.factorStride      = h->factorStride;
     P.chordInverse      = useStore && h->chordInverse ? 1 : 0;
-    P.chordTheta        = h->chordTheta;
+    P.chordTheta        = h->chordTheta > 0.0 ? h->chordTheta : ( h->v2Mode ? 0.2 : 0.1 );
     // the mixed form in rounds: k_check / k_update store the gradient of the
     // cells they list (gStore non-null) only when the rounds run
     const bool rounds = useStore && h->v2Mode && h->d_gStore;
@@ -543,14 +543,15 @@ void plan_launches( uqc_solver* h ) {
     // update kernel: a warp per cell; phiWf + one node-flux buffer per warp
     {
         const size_t uTables = h->tablesInSmem ? ( ( size_t( nQ ) * h->ld + 4 + 3 ) & ~size_t( 3 ) ) * sizeof( double ) : 0;
-        const size_t perWarp = ( ( size_t( nS ) * nQ + 3 ) & ~size_t( 3 ) ) * sizeof( double );
+        const size_t perWarp = update_warp_doubles( nS, nQ ) * sizeof( double );
         const int warps      = int( std::min<size_t>( 8, ( size_t( maxSmem ) - uTables ) / perWarp ) );
         if( warps < 1 ) throw ConfigError( "update workspace exceeds shared memory" );
         h->updateBlock = 32 * warps;
         h->updateSmem  = uTables + size_t( warps ) * perWarp;
-        void* ku       = pick( cl, h->group, 1 );
+        const bool walls = h->d_bndNormal != nullptr;
+        void* ku         = pick( cl, h->group, walls ? KERNEL_UPDATE_WALL : KERNEL_UPDATE );
         allow_dynamic_smem( ku );
-        allow_dynamic_smem( pick( cl, h->group, 5 ) );
+        allow_dynamic_smem( pick( cl, h->group, walls ? KERNEL_UPDATE_PLAIN_WALL : KERNEL_UPDATE_PLAIN ) );
         CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ku, h->updateBlock, h->updateSmem ) );
         h->updateGrid = std::max( 1, occ ) * h->numSMs;
         h->updateGrid = std::min( h->updateGrid, std::max( 1, ( h->mesh.nCells + warps - 1 ) / warps ) );
@@ -829,7 +830,10 @@ void enqueue_update( uqc_solver* h, KParams P ) {
     step_lists( h, P );
     P.finishInUpdate = update_test_on( h );
     void* args[]     = {&P};
-    launch( h, pick( h->cfg.closure, h->group, P.finishInUpdate ? 1 : 5 ), h->updateGrid, h->updateBlock, h->updateSmem, args );
+    const bool walls = h->d_bndNormal != nullptr;
+    const int which  = walls ? ( P.finishInUpdate ? KERNEL_UPDATE_WALL : KERNEL_UPDATE_PLAIN_WALL )
+                             : ( P.finishInUpdate ? KERNEL_UPDATE : KERNEL_UPDATE_PLAIN );
+    launch( h, pick( h->cfg.closure, h->group, which ), h->updateGrid, h->updateBlock, h->updateSmem, args );
 }
 
 void enqueue_step( uqc_solver* h, KParams& P ) {
