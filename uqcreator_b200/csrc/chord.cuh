@@ -93,6 +93,31 @@ constexpr int CHORD_JB = 14;
 __device__ __forceinline__ void chord_direction( const float* __restrict__ Hinv, int n, const float* gf, double* d, int lane ) {
     const int o0 = lane, o1 = lane + 32, o2 = lane + 64;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    if( n % CHORD_JB == 0 && n > 64 && n <= 96 ) {
+        // whole batches, two full column blocks: only the third needs a bound
+        const bool in2 = o2 < n;
+        for( int j0 = 0; j0 < n; j0 += CHORD_JB ) {
+            float h0[CHORD_JB], h1[CHORD_JB], h2[CHORD_JB];
+            const float* rj = Hinv + size_t( j0 ) * n;
+#pragma unroll
+            for( int t = 0; t < CHORD_JB; ++t ) {
+                h0[t] = __ldg( rj + t * n + o0 );
+                h1[t] = __ldg( rj + t * n + o1 );
+                h2[t] = in2 ? __ldg( rj + t * n + o2 ) : 0.f;
+            }
+#pragma unroll
+            for( int t = 0; t < CHORD_JB; ++t ) {
+                const float gj = gf[j0 + t];
+                a0             = fmaf( h0[t], gj, a0 );
+                a1             = fmaf( h1[t], gj, a1 );
+                a2             = fmaf( h2[t], gj, a2 );
+            }
+        }
+        d[o0] = double( a0 );
+        d[o1] = double( a1 );
+        if( in2 ) d[o2] = double( a2 );
+        return;
+    }
     for( int j0 = 0; j0 < n; j0 += CHORD_JB ) {
         float h0[CHORD_JB], h1[CHORD_JB], h2[CHORD_JB];
 #pragma unroll
@@ -259,26 +284,38 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_chord( KParams P
         // lamN <- lam + c d (closure.cpp:273-279), Lambda and U at the nodes,
         // the trial gradient (closure.cpp:234-253) and its norm
         auto trial = [&]( double c ) {
-            for( int idx = lane; idx < NS * nTj; idx += 32 ) {
-                const int s = idx / nTj, i = idx - s * nTj;
-                w.lamI[i * NS + s] = w.lam[s * P.nT + i] + c * w.d[idx];
-            }
-            __syncwarp();
-            for( int k = lane; k < P.nQ; k += 32 ) {
-                const double* row = phi + size_t( k ) * P.ld;
-                double Lk[NS], y[NS];
 #pragma unroll
-                for( int s = 0; s < NS; ++s ) Lk[s] = 0.0;
+            for( int s = 0; s < NS; ++s )
+                for( int i = lane; i < nTj; i += 32 ) w.lamI[i * NS + s] = w.lam[s * P.nT + i] + c * w.d[s * nTj + i];
+            __syncwarp();
+            // nodes k0 and k0 + 32 together (a basis function's duals loaded once
+            // for both); a lane without a second node repeats its first
+            for( int k0 = lane; k0 < P.nQ; k0 += 64 ) {
+                const bool two     = k0 + 32 < P.nQ;
+                const int k1       = two ? k0 + 32 : k0;
+                const double* row0 = phi + size_t( k0 ) * P.ld;
+                const double* row1 = phi + size_t( k1 ) * P.ld;
+                double L0[NS], L1[NS], y0[NS], y1[NS];
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) L0[s] = L1[s] = 0.0;
                 for( int i = 0; i < nTj; ++i ) {
-                    const double r = row[i];
+                    const double r0 = row0[i], r1 = row1[i];
                     double li[NS];
                     load_node<NS>( w.lamI, i, li );
 #pragma unroll
-                    for( int s = 0; s < NS; ++s ) Lk[s] = fma( li[s], r, Lk[s] );
+                    for( int s = 0; s < NS; ++s ) {
+                        L0[s] = fma( li[s], r0, L0[s] );
+                        L1[s] = fma( li[s], r1, L1[s] );
+                    }
                 }
-                Closure<CL>::U( Lk, y, true, P.phys );
+                Closure<CL>::U( L0, y0, true, P.phys );
+                Closure<CL>::U( L1, y1, true, P.phys );
 #pragma unroll
-                for( int s = 0; s < NS; ++s ) w.uk[k * NS + s] = y[s];
+                for( int s = 0; s < NS; ++s ) w.uk[k0 * NS + s] = y0[s];
+                if( two ) {
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) w.uk[k1 * NS + s] = y1[s];
+                }
             }
             __syncwarp();
             const double sq = chord_gradient<NS>( P, phiWf, w.uk, w.uh, nTj, w.gN, w.m, lane );
@@ -321,10 +358,9 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_chord( KParams P
                 }
                 if( rc >= 0 ) break;
                 // accept: lam <- the trial duals, g <- gN (the gradient at the accepted duals)
-                for( int idx = lane; idx < NS * nTj; idx += 32 ) {
-                    const int s = idx / nTj, i = idx - s * nTj;
-                    w.lam[s * P.nT + i] = w.lamI[i * NS + s];
-                }
+#pragma unroll
+                for( int s = 0; s < NS; ++s )
+                    for( int i = lane; i < nTj; i += 32 ) w.lam[s * P.nT + i] = w.lamI[i * NS + s];
                 for( int idx = lane; idx < n; idx += 32 ) w.g[idx] = w.gN[idx];
                 __syncwarp();
                 if( done || gnN < eps ) {
