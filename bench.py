@@ -74,10 +74,13 @@ def hessian_unit(form, mixed_form):
 
 
 FACTOR_UNIT = {"fp64": "fp64", "mixed": "fp32"}
-# DRAM bytes (read + write) per cell that takes Newton iterations, from the ncu
-# captures of each form's closure kernel on a 12,000-cell step (1,532 active
-# cells): FP64 2.35 MB, mixed 23.6 MB (it reloads each active cell's held factor).
-CLOSURE_DRAM_BYTES_PER_ACTIVE_CELL = {"fp64": 2.345472e6 / 1532, "mixed": 23.6e6 / 1532}
+# DRAM bytes (read + write) of the closure phase per cell that takes Newton
+# iterations, from ncu captures of the 5th step of a 60,000-cell case of the
+# same workload (6,457 active cells; profiles/closure_rounds_euler2d.md):
+# FP64 form k_closure 9.58 MB; mixed form (rounds) k_chord rounds 0-1, k_hess_tc
+# and k_invert_sweep round 0: 358.9 MB, mostly each active cell's held FP32
+# inverse (28 KB) read by the chord kernel.
+CLOSURE_DRAM_BYTES_PER_ACTIVE_CELL = {"fp64": 9.576e6 / 6457, "mixed": 358.9e6 / 6457}
 
 
 def closure_roofline(form, n_states, n_total, n_quad, cells, steps, ref_info, closure_ms, measured, active_cells, mixed_form=0):
@@ -106,7 +109,7 @@ def closure_roofline(form, n_states, n_total, n_quad, cells, steps, ref_info, cl
             "traffic_unit": "bytes per closure phase (scaled from the form's ncu capture by its active cells)",
             "t_bound_ms": t_unit, "closure_ms_per_launch": closure_ms, "flops_per_launch": total,
             "peaks_tflops": {**peak, "tensor_source": f"bf16 {src} (MEASURED_PEAKS.json)"},
-            "hbm_peak_gbs": hbm, "kernels": "closure phase: k_check + k_closure (+ the mixed form's FP64 fallback pass)"}
+            "hbm_peak_gbs": hbm, "kernels": "closure phase: k_check + k_closure (FP64 form); k_check + k_chord / k_hess_tc / k_invert_sweep rounds + the FP64 fallback pass (mixed form)"}
 
 
 class Clocks:
@@ -285,7 +288,8 @@ def run_serving(args, precision):
     from uqcreator_b200 import workloads as W
     from uqcreator_b200.serve import Server, latency_percentiles
     stream = W.serving_stream(args.serve_requests, args.serve_rate, seed=11)
-    srv = Server(budget_bytes=int(args.serve_budget_gb * (1 << 30)), max_active=16, steps_per_slice=4)
+    srv = Server(budget_bytes=int(args.serve_budget_gb * (1 << 30)), max_active=16, steps_per_slice=4,
+                 policy=args.serve_policy, max_stepping=args.serve_max_stepping)
     t0 = time.perf_counter()
     i, ids = 0, []
     while True:
@@ -301,12 +305,18 @@ def run_serving(args, precision):
     srv.close()
     ok = [x for x in res if x["state"] == "done"]
     lat = [x["latency_ms"] for x in ok]
+    queue = [x["queue_ms"] for x in ok]
+    service = [x["service_ms"] for x in ok]
     out = {"requests": len(res), "failed": len(res) - len(ok), "arrival_rate_per_s": args.serve_rate,
            "elapsed_s": el, "cell_steps_per_s": sum(x["n_cells"] * x["steps"] for x in ok) / el,
            "stream": "seeded serving stream (seed 11): Poisson arrivals, Burgers1D 200-20k cells deg 2-9, "
                      "Euler2D 10k-200k cells deg 2-5, offsets U[0.05,0.3], 5-40 steps per request",
-           "budget_gb": args.serve_budget_gb, "max_active": 16, "steps_per_slice": 4}
+           "budget_gb": args.serve_budget_gb, "max_active": 16, "steps_per_slice": 4,
+           "policy": "shortest remaining work first" if args.serve_policy == 1 else "round robin",
+           "max_stepping": args.serve_max_stepping}
     out.update(latency_percentiles(lat))
+    out["queue"] = latency_percentiles(queue)
+    out["service"] = latency_percentiles(service)
     for kind in ("burgers1d", "euler2d"):
         lk = [x["latency_ms"] for x, (_, k) in zip(res, ids) if k == kind and x["state"] == "done"]
         out[kind] = dict(n=len(lk), **latency_percentiles(lk))
@@ -515,10 +525,20 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=120, help="requests of the serving stream (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=12.0, help="arrivals per second")
     ap.add_argument("--serve-budget-gb", type=float, default=100.0)
+    ap.add_argument("--serve-policy", type=int, default=1, help="0 round robin, 1 shortest remaining work first")
+    ap.add_argument("--serve-max-stepping", type=int, default=4, help="requests stepping at a time (policy 1)")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="only the serving section (e.g. the whole stream: --serve-requests 2000)")
     ap.add_argument("--configs", action="store_true", help="one line per configuration (C1, C2, C3, C5) instead of the bench line")
     args = ap.parse_args()
     rank, world, local = dist_init()
-    if args.configs:
+    if args.serving_only:
+        if rank == 0:
+            import torch
+            from uqcreator_b200 import MIXED
+            torch.cuda.set_device(local)
+            print(json.dumps({"serving": run_serving(args, MIXED)}))
+    elif args.configs:
         if rank == 0:
             run_configs(args)
     elif args.impl == "reference":

@@ -284,11 +284,11 @@ int uqc_device_bytes( const uqc_solver* h, unsigned long long* bytes );
  * TOML configuration run to its tEnd). Requests wait in submission order and
  * are admitted, first fit, while their device memory fits the budget and
  * fewer than max_active run; each admitted request owns a stream and its
- * state stays on the device; every progress call advances each running
- * request by one slice of steps_per_slice time steps (its kernels overlap on
- * the device with the other requests'), retires finished ones (mean and
- * variance are computed and the device memory freed) and admits waiting
- * ones. A request's result does not depend on what else runs. Times are ms
+ * state stays on the device; every progress call advances running requests by
+ * slices of steps_per_slice time steps (their kernels overlap on the device),
+ * retires finished ones (mean and variance are computed and the device memory
+ * freed) and admits waiting ones; the order of admission and slices follows
+ * the scheduling policy (uqc_server_set_option). A request's result does not depend on what else runs. Times are ms
  * since the server was created. Not thread safe: one thread drives a server. */
 typedef struct uqc_server uqc_server;
 enum uqc_request_state { UQC_REQ_QUEUED = 0, UQC_REQ_RUNNING = 1, UQC_REQ_DONE = 2, UQC_REQ_FAILED = 3 };
@@ -317,6 +317,18 @@ int uqc_server_request( const uqc_server* s, long long id, uqc_request_info* inf
 const char* uqc_server_request_error( const uqc_server* s, long long id );
 /* Forgets a finished request and its result. */
 int uqc_server_release( uqc_server* s, long long id );
+/* Scheduling options:
+ *   "policy"        0: every running request advances by a slice per progress
+ *                   call, admission in submission order; 1 (default): shortest
+ *                   remaining work first, for admission and for slices, with
+ *                   at most "max_stepping" requests stepping at a time (the
+ *                   others stay resident and idle). Remaining work = cells x
+ *                   duals x nodes x the steps left ([uqc] steps; 1000 when
+ *                   only tEnd bounds the run), minus the request's waiting
+ *                   time in units of "aging_ms" steps of its own work.
+ *   "max_stepping"  requests with a slice in flight under policy 1 (default 4).
+ *   "aging_ms"      waiting time worth one step of remaining work (default 1000). */
+int uqc_server_set_option( uqc_server* s, const char* key, double value );
 
 /* ---- introspection ----------------------------------------------------- */
 

@@ -172,3 +172,34 @@ def test_update_side_convergence_test_matches_check_kernel(toml, steps):
     np.testing.assert_allclose(ua, ub, rtol=1e-12, atol=1e-14)
     np.testing.assert_allclose(la, lb, rtol=1e-10, atol=1e-12)
     assert abs(ia["t"] - ib["t"]) <= 1e-14 * ib["t"]
+
+
+@pytest.mark.parametrize("policy", [0, 1])
+def test_scheduling_policies_give_the_same_results(policy):
+    """Round robin and shortest-remaining-work-first order the slices
+    differently; each request's result is still the one it has alone."""
+    reqs = _requests()
+    alone = [_alone(t)[0] for t in reqs]
+    srv = Server(budget_bytes=8 << 30, max_active=len(reqs), steps_per_slice=2, policy=policy, max_stepping=2)
+    ids = [srv.submit(t) for t in reqs]
+    srv.drain()
+    for rid, ref in zip(ids, alone):
+        r = srv.result(rid)
+        assert r["state"] == "done", r
+        assert r["queue_ms"] >= 0 and r["service_ms"] >= 0
+        np.testing.assert_array_equal(r["mean_var"], ref)
+
+
+def test_shortest_remaining_work_goes_first():
+    """With one request stepping at a time, a short request submitted after a
+    long one finishes first; under round robin the long one is not held back."""
+    long_req = W.euler2d(nx=40, ny=20, degree=4, nquad=8, tend=10.0, steps=30)
+    short_req = W.burgers1d(ncells=300, degree=3, nquad=16, tend=10.0, steps=4)
+    srv = Server(budget_bytes=8 << 30, max_active=4, steps_per_slice=2, policy=1, max_stepping=1)
+    a = srv.submit(long_req)
+    b = srv.submit(short_req)
+    srv.drain()
+    ra, rb = srv.result(a, mean_var=False), srv.result(b, mean_var=False)
+    assert ra["state"] == rb["state"] == "done"
+    assert ra["steps"] == 30 and rb["steps"] == 4
+    assert rb["done_ms"] < ra["done_ms"]

@@ -1694,7 +1694,10 @@ struct uqc_request {
     long long iters    = 0;
     unsigned long long bytes = 0;
     bool admitted            = false;    // its bytes count against the budget
+    bool stepping            = false;    // a slice of steps is in flight
     double submitMs = 0, admitMs = 0, doneMs = 0;
+    double workPerStep = 0;    // estimated device work of one time step (cells x duals x nodes)
+    int horizon        = 0;    // time steps to the end, when known ([uqc] steps), else 0
     std::vector<double> meanVar;
     std::string err;
 };
@@ -1702,6 +1705,9 @@ struct uqc_request {
 struct uqc_server {
     unsigned long long budget = 0, used = 0;
     int maxActive = 1, slice = 1;
+    int policy      = 1;        // 0: every running request steps (round robin); 1: shortest remaining work first
+    int maxStepping = 4;        // policy 1: requests with a slice in flight at a time
+    double agingMs  = 1000.0;   // policy 1: waiting time that counts as much as a step of remaining work
     long long nextId = 1;
     std::map<long long, uqc_request> reqs;
     std::deque<long long> queue;      // waiting, in submission order
@@ -1767,42 +1773,80 @@ int uqc_server_submit( uqc_server* s, const char* toml_text, int precision, long
     r.nStates   = r.h->nS;
     r.bytes     = device_bytes_of( r.h ) + ( precision == UQC_MIXED && r.h->chord ? factor_store_bytes( r.h ) : 0 );
     r.submitMs  = s->now();
+    r.workPerStep = double( r.nCells ) * double( r.h->ldc ) * double( r.h->tab.nQ );
+    r.horizon     = r.h->cfg.maxSteps;
     *id         = r.id;
     s->queue.push_back( r.id );
     s->reqs.emplace( r.id, std::move( r ) );
     return UQC_OK;
 }
 
-int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_done ) {
-    if( !s ) return UQC_ERR_ARGUMENT;
-    // running requests: collect finished slices, retire finished solves, queue the next slice
-    for( size_t k = 0; k < s->running.size(); ) {
-        uqc_request& r = s->reqs[s->running[k]];
-        uqc_step_info info{};
-        const int q = uqc_step_query( r.h, &info );
-        if( q == 0 ) {
-            ++k;
+namespace {
+// Priority of a request under the shortest-remaining-work policy (smaller
+// first): its estimated remaining device work, in steps of work, minus its
+// waiting time in units of agingMs (so that no request waits forever).
+double priority( const uqc_server* s, const uqc_request& r, double now ) {
+    const int left  = r.horizon > 0 ? std::max( 0, r.horizon - r.steps ) : 1000;
+    const double ms = now - r.submitMs;
+    return r.workPerStep * double( left ) - r.workPerStep * ms / s->agingMs;
+}
+
+// Queues the next slice of steps of idle running requests: all of them
+// (policy 0), or in priority order while fewer than maxStepping have a slice
+// in flight (policy 1). A request whose slice cannot be queued is retired.
+void launch_slices( uqc_server* s ) {
+    const double now = s->now();
+    int inFlight     = 0;
+    std::vector<std::pair<double, long long>> idle;
+    for( long long id : s->running ) {
+        const uqc_request& r = s->reqs[id];
+        if( r.stepping )
+            ++inFlight;
+        else
+            idle.emplace_back( s->policy == 1 ? priority( s, r, now ) : 0.0, id );
+    }
+    if( s->policy == 1 ) std::stable_sort( idle.begin(), idle.end() );
+    for( auto& pr : idle ) {
+        if( s->policy == 1 && inFlight >= s->maxStepping ) break;
+        uqc_request& r = s->reqs[pr.second];
+        const int rc   = uqc_step_async( r.h, s->slice );
+        if( rc != UQC_OK ) {
+            retire( s, r, rc, uqc_last_error( r.h ) );
+            s->running.erase( std::find( s->running.begin(), s->running.end(), pr.second ) );
             continue;
         }
-        bool finished = false;
-        if( q < 0 ) {
-            retire( s, r, q, uqc_last_error( r.h ) );
-            finished = true;
-        }
-        else {
-            r.steps += info.steps;
-            r.iters += info.newton_iterations;
-            r.t = info.t;
-            if( !info.running ) {
-                r.meanVar.assign( size_t( r.nCells ) * 2 * r.nStates, 0.0 );
-                const int rc = uqc_mean_var( r.h, r.meanVar.data() );
-                retire( s, r, rc, rc == UQC_OK ? "" : uqc_last_error( r.h ) );
+        r.stepping = true;
+        ++inFlight;
+    }
+}
+}    // namespace
+
+int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_done ) {
+    if( !s ) return UQC_ERR_ARGUMENT;
+    // running requests: collect finished slices, retire finished solves
+    for( size_t k = 0; k < s->running.size(); ) {
+        uqc_request& r = s->reqs[s->running[k]];
+        bool finished  = false;
+        if( r.stepping ) {
+            uqc_step_info info{};
+            const int q = uqc_step_query( r.h, &info );
+            if( q == 0 ) {
+                ++k;
+                continue;
+            }
+            r.stepping = false;
+            if( q < 0 ) {
+                retire( s, r, q, uqc_last_error( r.h ) );
                 finished = true;
             }
             else {
-                const int rc = uqc_step_async( r.h, s->slice );
-                if( rc != UQC_OK ) {
-                    retire( s, r, rc, uqc_last_error( r.h ) );
+                r.steps += info.steps;
+                r.iters += info.newton_iterations;
+                r.t = info.t;
+                if( !info.running ) {
+                    r.meanVar.assign( size_t( r.nCells ) * 2 * r.nStates, 0.0 );
+                    const int rc = uqc_mean_var( r.h, r.meanVar.data() );
+                    retire( s, r, rc, rc == UQC_OK ? "" : uqc_last_error( r.h ) );
                     finished = true;
                 }
             }
@@ -1812,7 +1856,16 @@ int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_do
         else
             ++k;
     }
-    // admission, first fit in submission order
+    // next slices: every idle running request (round robin), or the idle ones
+    // with the least remaining work while fewer than maxStepping are in flight
+    launch_slices( s );
+    // admission, first fit: in submission order (round robin) or by priority
+    if( s->policy == 1 && s->queue.size() > 1 ) {
+        const double now = s->now();
+        std::stable_sort( s->queue.begin(), s->queue.end(), [&]( long long a, long long b ) {
+            return priority( s, s->reqs[a], now ) < priority( s, s->reqs[b], now );
+        } );
+    }
     for( auto it = s->queue.begin(); it != s->queue.end() && int( s->running.size() ) < s->maxActive; ) {
         uqc_request& r = s->reqs[*it];
         if( r.bytes > s->budget ) {
@@ -1831,17 +1884,39 @@ int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_do
         r.admitMs = s->now();
         int rc    = uqc_init_state( r.h );
         if( rc == UQC_OK && r.precision == UQC_MIXED ) rc = uqc_set_precision( r.h, UQC_MIXED );
-        if( rc == UQC_OK ) rc = uqc_step_async( r.h, s->slice );
         if( rc != UQC_OK )
             retire( s, r, rc, uqc_last_error( r.h ) );
         else
-            s->running.push_back( r.id );
+            s->running.push_back( r.id );    // its first slice goes out with the next pass's slices
         it = s->queue.erase( it );
     }
+    // first slices of the requests admitted in this pass
+    launch_slices( s );
     if( n_queued ) *n_queued = int( s->queue.size() );
     if( n_running ) *n_running = int( s->running.size() );
     if( n_done ) *n_done = s->done;
     return UQC_OK;
+}
+
+int uqc_server_set_option( uqc_server* s, const char* key, double value ) {
+    if( !s || !key ) return UQC_ERR_ARGUMENT;
+    const std::string k = key;
+    if( k == "policy" ) {
+        if( value != 0.0 && value != 1.0 ) return sfail( s, UQC_ERR_ARGUMENT, "policy must be 0 or 1" );
+        s->policy = int( value );
+        return UQC_OK;
+    }
+    if( k == "max_stepping" ) {
+        if( value < 1 ) return sfail( s, UQC_ERR_ARGUMENT, "max_stepping must be >= 1" );
+        s->maxStepping = int( value );
+        return UQC_OK;
+    }
+    if( k == "aging_ms" ) {
+        if( !( value > 0 ) ) return sfail( s, UQC_ERR_ARGUMENT, "aging_ms must be > 0" );
+        s->agingMs = value;
+        return UQC_OK;
+    }
+    return sfail( s, UQC_ERR_ARGUMENT, "unknown server option '" + k + "'" );
 }
 
 int uqc_server_request( const uqc_server* s, long long id, uqc_request_info* info, double* mean_var ) {

@@ -26,13 +26,23 @@ __all__ = ["Server", "latency_percentiles"]
 
 
 class Server:
-    def __init__(self, budget_bytes: int, max_active: int = 8, steps_per_slice: int = 4):
+    def __init__(self, budget_bytes: int, max_active: int = 8, steps_per_slice: int = 4, policy: int | None = None,
+                 max_stepping: int | None = None):
         self.lib = L.lib()
         h = C.c_void_p()
         rc = self.lib.uqc_server_create(int(budget_bytes), int(max_active), int(steps_per_slice), C.byref(h))
         if rc != 0:
             raise UqcError(rc, "server create")
         self.h = h
+        if policy is not None:
+            self.set_option("policy", policy)
+        if max_stepping is not None:
+            self.set_option("max_stepping", max_stepping)
+
+    def set_option(self, key: str, value: float):
+        """Scheduling options of uqc_server_set_option: "policy" (0 round robin,
+        1 shortest remaining work first), "max_stepping", "aging_ms"."""
+        self._check(self.lib.uqc_server_set_option(self.h, key.encode(), float(value)))
 
     def close(self):
         if getattr(self, "h", None):
@@ -73,6 +83,8 @@ class Server:
             self._check(self.lib.uqc_server_request(self.h, int(rid), C.byref(inf), ptr(mv)))
             d["mean_var"] = mv
         d["latency_ms"] = d["done_ms"] - d["submit_ms"] if d["state"] in ("done", "failed") else None
+        d["queue_ms"] = d["admit_ms"] - d["submit_ms"] if d["state"] in ("running", "done", "failed") else None
+        d["service_ms"] = d["done_ms"] - d["admit_ms"] if d["state"] in ("done", "failed") else None
         d["error"] = self.lib.uqc_server_request_error(self.h, int(rid)).decode()
         return d
 
