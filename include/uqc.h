@@ -148,7 +148,7 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *                    refinement level): -1 (default) rounds with the Hessian
  *                    on the tensor cores where its basis-pair table fits one
  *                    MMA (at most 256 pairs, i.e. total degree <= 5 in two
- *                    uncertainties), else on CUDA cores; 0 the single-kernel
+ *                    uncertainties), else the single kernel; 0 the single-kernel
  *                    form; 1 rounds with the CUDA-core Hessian; 2 rounds with
  *                    the tensor-core Hessian (UQC_ERR_CONFIG where it does
  *                    not fit). Rounds: a chord kernel (a warp per cell, held

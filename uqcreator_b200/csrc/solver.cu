@@ -383,7 +383,9 @@ void plan_rounds( uqc_solver* h, int maxSmem ) {
     const size_t hsmem  = hess_tc_smem( nS, NP, nT, nQ, h->ld );
     const bool tcFits   = ts.nPad <= 256 && ts.cellsPerTile >= 1 && hsmem <= size_t( maxSmem );
     int mode            = h->roundsOpt == 1 ? 1 : ( tcFits ? 2 : 1 );
-    if( h->roundsOpt == 2 && !tcFits ) {
+    if( !tcFits && h->roundsOpt != 1 ) {
+        // automatic: without the tensor-core Hessian the single kernel is faster
+        // (measured on the three-uncertainty workload: 41 vs 50 ms per step)
         h->v2Why = "tensor-core Hessian: " + std::to_string( ts.pairs ) + " basis pairs or " + std::to_string( hsmem ) +
                    " B of shared memory exceed one MMA (256 pairs)";
         return;
