@@ -195,6 +195,12 @@ int uqc_export_state( uqc_solver* h, const char* path_prefix );
 /* Batched Closure::SolveClosure (closure.cpp:133-193) on the resident state:
  * every cell's duals solved in place for its current refinement level. */
 int uqc_solve_closure( uqc_solver* h, uqc_step_info* info );
+/* The same on a subset of the resident cells (cells: n_cells host cell ids,
+ * or NULL for all cells), with this call's tolerance and iteration limit
+ * (tol > 0 and max_iter > 0 override the configured epsilon and
+ * maxIterations of settings.cpp:314; 0 keeps them): the closure loop of
+ * momentsolver.cpp:83-89 restricted to the cells a caller lists. */
+int uqc_solve_closure_cells( uqc_solver* h, const unsigned* cells, int n_cells, double tol, int max_iter, uqc_step_info* info );
 /* Closure status and Newton iterations per cell from the last closure solve. */
 int uqc_cell_status( uqc_solver* h, int* status, int* iterations );
 /* n_steps time steps: the body of MomentSolver::Solve (momentsolver.cpp:79-152)
@@ -206,6 +212,8 @@ int uqc_run( uqc_solver* h, double t_end, uqc_step_info* info );
 /* Mean and variance per cell and state (MomentSolver::WriteMeanAndVar,
  * momentsolver.cpp:302-328): out[j * 2 nS + s] = E, out[j * 2 nS + nS + s] = Var. */
 int uqc_mean_var( uqc_solver* h, double* out );
+/* The same entry point under the name of the drop-in boundary's plan. */
+int uqc_moments_mean_var( uqc_solver* h, double* out );
 /* Mesh1D::Export / Mesh2D::Export (mesh1d.cpp:90-220, mesh2d.cpp:399-501):
  * legacy VTK unstructured grid (ASCII) at `path` (".vtk" appended when
  * missing) with the reference's arrays E(.) and Var(.) per state as cell data

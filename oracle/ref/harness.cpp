@@ -11,6 +11,7 @@
 // CPU-baseline leg of bench.py call through ctypes. Nothing in the product
 // links or calls this file.
 #include <cmath>
+#include <fstream>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -735,6 +736,57 @@ int uqcref_full_solve( uqcref* h, double* meanVar, double* lambda15, char* err, 
                     lambda15[j * n + i * nS + s] = std::stod( cell );
                 }
         }
+        return 0;
+    } catch( const std::exception& e ) {
+        set_err( err, errlen, e.what() );
+        return -1;
+    }
+}
+
+// MomentSolver::Solve() as full_solve, also writing what a run of the
+// reference leaves for a restart: <prefix>_moments and <prefix>_duals (the
+// lines MomentSolver::Export writes to its "moments"/"duals" loggers,
+// momentsolver.cpp:565-588, whose file sinks use the pattern "%v"), and the log
+// <prefix> with the configuration echo of main.cpp's PrintInit (:160-180) in
+// the file sink's pattern "%Y-%m-%d %H:%M:%S.%f | %v" (restated here: main.cpp
+// is not compiled into the harness).
+int uqcref_full_solve_export( uqcref* h, const char* prefix, double* meanVar, char* err, int errlen ) {
+    try {
+        auto momentLog = spdlog::get( "moments" );
+        auto dualLog   = spdlog::get( "duals" );
+        momentLog->capture_enabled = dualLog->capture_enabled = true;
+        momentLog->lines.clear();
+        dualLog->lines.clear();
+        h->mesh->exported.clear();
+        {
+            MomentSolver solver( h->settings.get(), h->mesh.get(), h->problem.get() );
+            solver.Solve();
+        }
+        momentLog->capture_enabled = dualLog->capture_enabled = false;
+        auto it = h->mesh->exported.find( "" );
+        if( it == h->mesh->exported.end() ) throw uqc_ref_error( "Solve exported no mean/variance" );
+        const Matrix& mv = it->second;
+        for( unsigned j = 0; j < h->nCells; ++j )
+            for( unsigned r = 0; r < 2 * h->nStates; ++r ) meanVar[size_t( j ) * 2 * h->nStates + r] = mv( r, j );
+        const std::string base = prefix;
+        for( int which = 0; which < 2; ++which ) {
+            std::ofstream f( base + ( which == 0 ? "_moments" : "_duals" ) );
+            for( const auto& line : ( which == 0 ? momentLog : dualLog )->lines ) f << line << "\n";
+            if( !f ) throw uqc_ref_error( "cannot write " + base );
+        }
+        std::ofstream log( base );
+        const std::string stamp = "2000-01-01 00:00:00.000000 | ", rule = "================================================================";
+        log << stamp << "UQCreator\n" << stamp << rule << "\n" << stamp << "Git commit hash:\tharness\n";
+        log << stamp << "Config file:\t" << h->settings->GetInputFile() << "\n";
+        log << stamp << "MPI Threads:\t1\n" << stamp << "OMP Threads:\t1\n" << stamp << rule << "\n";
+        std::ifstream ifs( h->settings->GetInputFile() );
+        std::string line;
+        while( !ifs.eof() ) {
+            std::getline( ifs, line );
+            if( line[0] != '#' ) log << stamp << " " << line << "\n";
+        }
+        log << stamp << rule << "\n" << stamp << "\n";
+        if( !log ) throw uqc_ref_error( "cannot write " + base );
         return 0;
     } catch( const std::exception& e ) {
         set_err( err, errlen, e.what() );

@@ -61,6 +61,8 @@ def _lib(variant: str = "exact") -> C.CDLL:
     lib.uqcref_mean_var.argtypes = [C.c_void_p, _dp]
     lib.uqcref_full_solve.restype = C.c_int
     lib.uqcref_full_solve.argtypes = [C.c_void_p, _dp, _dp, C.c_char_p, C.c_int]
+    lib.uqcref_full_solve_export.restype = C.c_int
+    lib.uqcref_full_solve_export.argtypes = [C.c_void_p, C.c_char_p, _dp, C.c_char_p, C.c_int]
     _LIBS[variant] = lib
     return lib
 
@@ -171,6 +173,17 @@ class RefSolver:
         out = np.zeros(self.n_cells * 2 * self.n_states)
         self.lib.uqcref_mean_var(self.h, _p(out))
         return out.reshape(self.n_cells, 2 * self.n_states)
+
+    def full_solve_export(self, prefix):
+        """MomentSolver::Solve(), writing <prefix>_moments / <prefix>_duals (the
+        reference's Export) and the log <prefix> with its configuration echo;
+        returns the final meanVar (cells, 2 nS)."""
+        mv = np.zeros(self.n_cells * 2 * self.n_states)
+        err = C.create_string_buffer(512)
+        rc = self.lib.uqcref_full_solve_export(self.h, os.fsencode(prefix), _p(mv), err, 512)
+        if rc != 0:
+            raise RuntimeError("reference Solve: " + err.value.decode())
+        return mv.reshape(self.n_cells, 2 * self.n_states)
 
     def full_solve(self):
         """Runs MomentSolver::Solve(); returns (meanVar (cells, 2nS), lambda at 15 digits)."""

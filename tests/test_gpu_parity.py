@@ -158,3 +158,33 @@ def test_closure_group_sizes_agree(group):
     assert a["failed_cells"] == 0
     err = rel_l1(s.mean_var(), o.mean_var(), o.geometry()["area"])
     assert np.all(err <= TOL_MV), err
+
+
+def test_closure_on_a_subset_with_its_own_tolerance():
+    """uqc_solve_closure_cells: the listed cells are solved as the batched host
+    closure solves them; the other cells keep their duals; a looser tolerance
+    takes fewer iterations."""
+    toml = W.euler2d(nx=16, ny=4)
+    s = Solver(toml)
+    s.init_state()
+    s.step(2)
+    u, lam, lev = s.download_state()
+    rng = np.random.default_rng(9)
+    lam_p = lam * (1 + 1e-3 * rng.standard_normal(lam.shape))
+    cells = np.sort(rng.choice(s.n_cells, size=40, replace=False)).astype(np.uint32)
+    s.upload_state(u, lam_p, lev)
+    info = s.solve_closure_cells(cells)
+    assert info["failed_cells"] == 0
+    _, lam_s, _ = s.download_state()
+    lam_h, st = s.closure_solve_host(lam_p[cells], u[cells])
+    assert np.all(st == 0)
+    np.testing.assert_allclose(lam_s[cells], lam_h, rtol=1e-12, atol=1e-14)
+    rest = np.setdiff1d(np.arange(s.n_cells), cells)
+    np.testing.assert_array_equal(lam_s[rest], lam_p[rest])
+    s.upload_state(u, lam_p, lev)
+    loose = s.solve_closure_cells(cells, tol=1e-6)
+    assert loose["newton_iterations"] < info["newton_iterations"]
+    mv = np.zeros((s.n_cells, 2 * s.n_states))
+    from uqcreator_b200._lib import lib, ptr
+    assert lib().uqc_moments_mean_var(s.h, ptr(mv)) == 0
+    np.testing.assert_array_equal(mv, s.mean_var())

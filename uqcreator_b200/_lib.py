@@ -30,7 +30,7 @@ EXPORTS = [
     "uqc_set_option", "uqc_step_async", "uqc_step_query", "uqc_device_bytes", "uqc_server_create",
     "uqc_server_destroy", "uqc_server_last_error", "uqc_server_submit", "uqc_server_progress",
     "uqc_server_request", "uqc_server_release", "uqc_server_request_error", "uqc_export_state", "uqc_write_vtk",
-    "uqc_debug_mixed_inverse", "uqc_server_set_option",
+    "uqc_debug_mixed_inverse", "uqc_server_set_option", "uqc_solve_closure_cells", "uqc_moments_mean_var",
 ]
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
 NOALLOC_MAX_CELLS = 65536
@@ -126,6 +126,8 @@ def lib() -> C.CDLL:
         "uqc_write_vtk": ([_vp, C.c_char_p], C.c_int),
         "uqc_debug_mixed_inverse": ([_vp, C.c_int, _ip, C.c_int, C.POINTER(C.c_float)], C.c_int),
         "uqc_server_set_option": ([_vp, C.c_char_p, C.c_double], C.c_int),
+        "uqc_solve_closure_cells": ([_vp, _up, C.c_int, C.c_double, C.c_int, C.POINTER(StepInfo)], C.c_int),
+        "uqc_moments_mean_var": ([_vp, _dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

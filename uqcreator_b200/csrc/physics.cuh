@@ -24,7 +24,7 @@ template <int CL> struct Closure;
 // U and DU of BoundedBarrier (boundedbarrier.cpp:19-31, 67-80), one state.
 template <> struct Closure<0> {
     static constexpr int NS = 1, NP = 1;
-    __device__ static void U( const double* L, double* u, bool, const PhysParams& p ) {
+    __host__ __device__ static void U( const double* L, double* u, bool, const PhysParams& p ) {
         double ePos = exp( L[0] ), eNeg = 1.0 / ePos;
         if( L[0] > 0.0 )
             u[0] = p.bbPlus / ( eNeg + 1.0 ) + p.bbMinus * eNeg / ( 1.0 + eNeg );
@@ -32,7 +32,7 @@ template <> struct Closure<0> {
             u[0] = p.bbMinus / ( ePos + 1.0 ) + p.bbPlus * ePos / ( 1.0 + ePos );
     }
     // packed symmetric DU: du[0] = DU(0,0)
-    __device__ static void DU( const double* L, double* du, const PhysParams& p ) {
+    __host__ __device__ static void DU( const double* L, double* du, const PhysParams& p ) {
         double ePos = exp( L[0] ), eNeg = 1 / ePos;
         if( L[0] > 0 )
             du[0] = eNeg * ( p.bbPlus - p.bbMinus ) / ( exp( -2.0 * L[0] ) + 2.0 * eNeg + 1.0 );
@@ -40,7 +40,7 @@ template <> struct Closure<0> {
             du[0] = ePos * ( p.bbPlus - p.bbMinus ) / ( 1.0 + 2.0 * ePos + exp( 2.0 * L[0] ) );
     }
     // Closure::DS of the base class leaves the guess unchanged (zero)
-    __device__ static void DS( const double*, double* ds, const PhysParams& ) { ds[0] = 0.0; }
+    __host__ __device__ static void DS( const double*, double* ds, const PhysParams& ) { ds[0] = 0.0; }
 };
 
 // ---------------------------------------------------------------- Euler 2-D
@@ -54,7 +54,7 @@ template <> struct Closure<1> {
     // one logarithm instead of exp and pow, and one division (1/v4); the
     // results agree with the reference's to a few ulps of the exponent.
     // vecForm is kept for the interface.
-    __device__ static void U( const double* L, double* u, bool /*vecForm*/, const PhysParams& p ) {
+    __host__ __device__ static void U( const double* L, double* u, bool /*vecForm*/, const PhysParams& p ) {
         const double g = -p.gamma;
         const double v1 = L[0], v2 = L[1], v3 = L[2], v4 = L[3];
         const double i4 = 1.0 / v4;
@@ -68,7 +68,7 @@ template <> struct Closure<1> {
     }
     // packed upper DU (:54-88): order (0,0)(0,1)(0,2)(0,3)(1,1)(1,2)(1,3)(2,2)(2,3)(3,3)
     // Same rewriting as U: rho' = A exp(A (q + log(-v4))), powers of 1/v4 from one division.
-    __device__ static void DU( const double* L, double* y, const PhysParams& p ) {
+    __host__ __device__ static void DU( const double* L, double* y, const PhysParams& p ) {
         const double g = -p.gamma;
         double v1 = L[0], v2 = L[1], v3 = L[2], v4 = L[3];
         double i4 = 1.0 / v4, v4i2 = i4 * i4, v3p2 = v3 * v3, v2p2 = v2 * v2, v4p2 = v4 * v4;
@@ -87,7 +87,7 @@ template <> struct Closure<1> {
         y[9] = -( e * ( v2p2 * v2p2 + v3p2 * v3p2 + 4.0 * v3p2 * v4 * g - 4.0 * v4p2 * g + 2.0 * v2p2 * ( v3p2 + 2.0 * v4 * g ) ) ) * ( 0.25 * v4i2 * v4i2 );
     }
     // EulerClosure2D::DS (:90-106)
-    __device__ static void DS( const double* u, double* ds, const PhysParams& p ) {
+    __host__ __device__ static void DS( const double* u, double* ds, const PhysParams& p ) {
         const double gamma = -p.gamma;
         double rho = u[0], rhoU = u[1], rhoV = u[2], rhoE = u[3];
         double rhoV2 = rhoV * rhoV, rhoU2 = rhoU * rhoU;
@@ -103,18 +103,18 @@ template <> struct Closure<1> {
 // ShallowWaterClosure (shallowwaterclosure.cpp:10-42), g = 9.81.
 template <> struct Closure<2> {
     static constexpr int NS = 2, NP = 3;
-    __device__ static void U( const double* L, double* u, bool, const PhysParams& ) {
+    __host__ __device__ static void U( const double* L, double* u, bool, const PhysParams& ) {
         const double gr = 9.81;
         u[0] = ( 0.5 * ( 2 * L[0] + L[1] * L[1] ) ) / gr;
         u[1] = ( 0.5 * ( 2 * L[0] * L[1] + L[1] * L[1] * L[1] ) ) / gr;
     }
-    __device__ static void DU( const double* L, double* y, const PhysParams& ) {
+    __host__ __device__ static void DU( const double* L, double* y, const PhysParams& ) {
         const double gr = 9.81;
         y[0] = 1.0 / gr;
         y[1] = L[1] / gr;
         y[2] = ( L[0] + 1.5 * ( L[1] * L[1] ) ) / gr;
     }
-    __device__ static void DS( const double* u, double* ds, const PhysParams& ) {
+    __host__ __device__ static void DS( const double* u, double* ds, const PhysParams& ) {
         const double gr = 9.81;
         ds[0] = ( gr * ( u[0] * u[0] * u[0] ) - 0.5 * ( u[1] * u[1] ) ) / ( u[0] * u[0] );
         ds[1] = u[1] / u[0];

@@ -123,6 +123,8 @@ struct uqc_solver {
     std::vector<double> padPhi, padPhiWf;    // host tables in the device layout
     std::vector<double> padWt;               // w_k / 2^dimXi per node
     double* d_wt = nullptr;
+    std::string cfgText;                     // the input file's text (echoed by uqc_export_state)
+    std::string cfgName = "uqcreator_b200";  // the input file's path, when created from a file
     std::string err;
 };
 
@@ -619,6 +621,7 @@ void read_control( uqc_solver* h ) {
 }
 
 void build( uqc_solver* h, const std::string& text, void* stream, const std::string& inputDir ) {
+    h->cfgText      = text;
     h->cfg          = parse_config( text );
     h->cfg.inputDir = inputDir;
     h->tab = build_tables( h->cfg );
@@ -990,7 +993,9 @@ int uqc_create_from_file( const char* toml_path, void* cuda_stream, uqc_solver**
     ss << f.rdbuf();
     const std::string path = toml_path;
     const size_t slash     = path.find_last_of( '/' );
-    return create_impl( ss.str().c_str(), slash == std::string::npos ? "." : path.substr( 0, slash ), cuda_stream, out, err, err_len );
+    const int rc = create_impl( ss.str().c_str(), slash == std::string::npos ? "." : path.substr( 0, slash ), cuda_stream, out, err, err_len );
+    if( rc == UQC_OK ) ( *out )->cfgName = path;
+    return rc;
 }
 
 void uqc_destroy( uqc_solver* h ) {
@@ -1172,6 +1177,57 @@ int uqc_get_geometry( const uqc_solver* h, double* area, double* max_edge, doubl
 // Reads one of the reference's state files (MomentSolver::Export,
 // momentsolver.cpp:565-588): a line per cell, nS x nT values in state-major
 // order, each followed by a comma (ImportPrevMoments/Duals, :614-650).
+// The configuration a previous run echoed into its log file <restartFile>
+// (main.cpp:160-180 writes it, MomentSolver::ImportPrevSettings reads it back,
+// momentsolver.cpp:590-612): the lines after "Config file" (the fourth line
+// after it is the first one kept) up to the next "====" line, each stripped
+// up to and including the first '|'. Empty when the file has no echo.
+static std::string read_config_echo( const std::string& path ) {
+    std::ifstream f( path );
+    if( !f ) return "";
+    std::string line, out;
+    bool section = false;
+    while( std::getline( f, line ) ) {
+        if( line.find( "Config file" ) != std::string::npos ) {
+            section = true;
+            for( int i = 0; i < 4; ++i ) std::getline( f, line );
+        }
+        else if( section && line.find( "==================================" ) != std::string::npos ) {
+            break;
+        }
+        if( section ) {
+            line.erase( 0, line.find_first_of( '|' ) + 1 );
+            out += line + "\n";
+        }
+    }
+    return out;
+}
+
+// The log a restart reads (main.cpp:160-180's PrintInit in spdlog's file
+// pattern "%Y-%m-%d %H:%M:%S.%f | %v"): header, the input file's lines that do
+// not start with '#', closing rule.
+static void write_config_echo( const std::string& path, const std::string& cfgName, const std::string& text ) {
+    std::ofstream f( path );
+    if( !f ) throw ConfigError( "cannot write " + path );
+    const auto now  = std::chrono::system_clock::now();
+    const time_t tt = std::chrono::system_clock::to_time_t( now );
+    const long us   = long( std::chrono::duration_cast<std::chrono::microseconds>( now.time_since_epoch() ).count() % 1000000 );
+    char ts[64];
+    std::strftime( ts, sizeof( ts ), "%Y-%m-%d %H:%M:%S", std::localtime( &tt ) );
+    char stamp[80];
+    std::snprintf( stamp, sizeof( stamp ), "%s.%06ld | ", ts, us );
+    const std::string rule = "================================================================";
+    f << stamp << "UQCreator\n" << stamp << rule << "\n" << stamp << "Git commit hash:\tuqcreator_b200\n";
+    f << stamp << "Config file:\t" << cfgName << "\n" << stamp << "MPI Threads:\t1\n" << stamp << "OMP Threads:\t1\n";
+    f << stamp << rule << "\n";
+    std::istringstream in( text );
+    std::string line;
+    while( std::getline( in, line ) )
+        if( line.empty() || line[0] != '#' ) f << stamp << " " << line << "\n";
+    f << stamp << rule << "\n" << stamp << "\n";
+    if( !f ) throw ConfigError( "cannot write " + path );
+}
+
 static void read_state_file( const std::string& path, size_t nCells, size_t perCell, std::vector<double>& out ) {
     std::ifstream f( path );
     if( !f ) throw ConfigError( "cannot open restart file " + path );
@@ -1190,16 +1246,157 @@ static void read_state_file( const std::string& path, size_t nCells, size_t perC
     }
 }
 
+// FP64 closure of every resident cell in SolveClosureSafe mode with maxIter
+// iterations (the initial duals of a restart, momentsolver.cpp:486-521).
+static void safe_closure_all( uqc_solver* h, int maxIter ) {
+    KParams P      = make_params( h );
+    P.newtonMode   = 2;
+    P.maxIter      = maxIter;
+    P.tablesInSmem = h->closureTablesInSmem;
+    int mode       = 0;
+    reset_work( h );
+    void* args[] = {&P, &mode};
+    launch( h, pick( h->cfg.closure, h->closureGroup, 0 ), h->closureGrid, h->closureBlock, h->closureSmem, args );
+    CK( cudaStreamSynchronize( h->stream ) );
+    read_control( h );
+    if( h->h_ctl->failedCells ) throw ConfigError( "restart: " + std::to_string( h->h_ctl->failedCells ) + " cells' initial duals did not converge" );
+}
+
+// Restart onto another number of moments (MomentSolver::DetermineMoments and
+// SetDuals, momentsolver.cpp:418-435, 463-523): the previous run's moments
+// (its own number nPrev), Dirichlet cells from the initial state of the new
+// order; the previous duals (imported, or DS of the moments solved with the
+// previous basis and quadrature, SolveClosureSafe, 10000 iterations); the
+// solution U(Lambda) at the new quadrature nodes from the previous basis there,
+// projected onto the new basis; the duals padded with zeros and solved again.
+static void restart_new_order( uqc_solver* h, const std::string& base, const std::string& echo, const Config& prev ) {
+    const size_t N = size_t( h->mesh.nCells );
+    const int nS = h->nS, nT = h->tab.nT, nQ = h->tab.nQ;
+    const Tables pt = build_tables( prev );
+    const int nP    = pt.nT;
+    std::vector<double> u, lam;
+    read_state_file( base + "_moments", N, size_t( nS ) * nP, u );
+    // the new order's initial moments, for the Dirichlet cells
+    {
+        KParams P    = make_params( h );
+        int keep     = 0;
+        void* args[] = {&P, &keep};
+        launch( h, pick( h->cfg.closure, h->group, 2 ), h->auxGrid, h->auxBlock, h->initSmem, args );
+    }
+    std::vector<double> uic( N * h->ldc );
+    CK( cudaMemcpyAsync( uic.data(), h->d_u, uic.size() * sizeof( double ), cudaMemcpyDeviceToHost, h->stream ) );
+    CK( cudaStreamSynchronize( h->stream ) );
+    for( size_t j = 0; j < N; ++j )
+        if( h->mesh.boundary[j] == BC_DIRICHLET )
+            for( int s = 0; s < nS; ++s )
+                for( int i = 0; i < nP; ++i ) u[( j * nS + s ) * nP + i] = uic[j * h->ldc + size_t( s ) * nT + i];
+    // the previous order's duals
+    if( h->cfg.importDualState ) {
+        read_state_file( base + "_duals", N, size_t( nS ) * nP, lam );
+    }
+    else {
+        uqc_solver* ph = nullptr;
+        char err[512]  = {0};
+        if( create_impl( echo.c_str(), h->cfg.inputDir, h->userStream, &ph, err, int( sizeof err ) ) != UQC_OK )
+            throw ConfigError( std::string( "restart: the echoed configuration: " ) + err );
+        ph->precision = UQC_FP64;
+        std::vector<int> st( N );
+        lam.assign( N * nS * nP, 0.0 );
+        int rc = UQC_OK;
+        try {
+            // DS of the mean moments as the first guess (momentsolver.cpp:471-483), on the device
+            ph->cfg.newtonMode    = 2;
+            ph->cfg.maxIterations = 10000;
+            std::vector<double> ds( nS );
+            PhysParams pp = make_params( ph ).phys;
+            for( size_t j = 0; j < N; ++j ) {
+                double u0[4] = {0, 0, 0, 0}, d[4] = {0, 0, 0, 0};
+                for( int s = 0; s < nS; ++s ) u0[s] = u[( j * nS + s ) * nP];
+                if( h->cfg.closure == CL_BOUNDED_BARRIER )
+                    Closure<0>::DS( u0, d, pp );
+                else if( h->cfg.closure == CL_EULER2D )
+                    Closure<1>::DS( u0, d, pp );
+                else
+                    Closure<2>::DS( u0, d, pp );
+                for( int s = 0; s < nS; ++s ) lam[( j * nS + s ) * nP] = d[s];
+            }
+            rc = uqc_closure_solve_host( ph, int( N ), lam.data(), u.data(), nullptr, UQC_LAYOUT_STATE_MAJOR, st.data() );
+            if( rc != UQC_OK ) throw ConfigError( std::string( "restart: previous-order duals: " ) + uqc_last_error( ph ) );
+        } catch( ... ) {
+            uqc_destroy( ph );
+            throw;
+        }
+        uqc_destroy( ph );
+    }
+    // U(Lambda) at the new nodes from the previous basis there, projected onto the new basis
+    Config mid = prev;
+    mid.nQuad  = h->cfg.nQuad;
+    const Tables it = build_tables( mid );
+    if( it.nQ != nQ ) throw ConfigError( "restart: quadrature mismatch" );
+    const PhysParams pp = make_params( h ).phys;
+    std::vector<double> un( N * h->ldc, 0.0 ), ln( N * h->ldc, 0.0 ), uq( size_t( nS ) * nQ );
+    for( size_t j = 0; j < N; ++j ) {
+        for( int k = 0; k < nQ; ++k ) {
+            double L[4] = {0, 0, 0, 0}, y[4] = {0, 0, 0, 0};
+            for( int s = 0; s < nS; ++s ) {
+                double a = 0.0;
+                for( int i = 0; i < nP; ++i ) a += lam[( j * nS + s ) * nP + i] * it.phi[size_t( k ) * nP + i];
+                L[s] = a;
+            }
+            if( h->cfg.closure == CL_BOUNDED_BARRIER )
+                Closure<0>::U( L, y, false, pp );
+            else if( h->cfg.closure == CL_EULER2D )
+                Closure<1>::U( L, y, false, pp );
+            else
+                Closure<2>::U( L, y, false, pp );
+            for( int s = 0; s < nS; ++s ) uq[size_t( s ) * nQ + k] = y[s];
+        }
+        for( int s = 0; s < nS; ++s ) {
+            for( int i = 0; i < nT; ++i ) {
+                double a = 0.0;
+                for( int k = 0; k < nQ; ++k ) a += uq[size_t( s ) * nQ + k] * h->tab.phiWf[size_t( k ) * nT + i];
+                un[j * h->ldc + size_t( s ) * nT + i] = a;
+            }
+            for( int i = 0; i < nP && i < nT; ++i ) ln[j * h->ldc + size_t( s ) * nT + i] = lam[( j * nS + s ) * nP + i];
+        }
+    }
+    CK( cudaMemcpyAsync( h->d_u, un.data(), un.size() * sizeof( double ), cudaMemcpyHostToDevice, h->stream ) );
+    CK( cudaMemcpyAsync( h->d_lam, ln.data(), ln.size() * sizeof( double ), cudaMemcpyHostToDevice, h->stream ) );
+    std::vector<unsigned> lv( N, unsigned( h->tab.nLevels - 1 ) );
+    CK( cudaMemcpyAsync( h->d_level, lv.data(), N * sizeof( unsigned ), cudaMemcpyHostToDevice, h->stream ) );
+    CK( cudaStreamSynchronize( h->stream ) );
+    reset_control( h, 0.0 );
+    safe_closure_all( h, h->cfg.maxIterations == 1 ? 10000 : h->cfg.maxIterations );
+}
+
 int uqc_init_state( uqc_solver* h ) {
     if( !h ) return UQC_ERR_ARGUMENT;
     return guarded_dev( h, [&] {
         h->launches  = 0;
         KParams P    = make_params( h );
         int keep     = 0;
+        double t0    = 0.0;
+        bool oneShotSolve = false;
         if( !h->cfg.restartFile.empty() ) {
-            // restart (MomentSolver::DetermineMoments / SetDuals, momentsolver.cpp:418-485)
+            // restart (MomentSolver::DetermineMoments / SetDuals, momentsolver.cpp:418-523)
             const std::string base = h->cfg.restartFile[0] == '/' ? h->cfg.restartFile : h->cfg.inputDir + "/" + h->cfg.restartFile;
             const size_t N = size_t( h->mesh.nCells );
+            // the previous run's settings from its log (DeterminePreviousSettings, :437-450); the
+            // time continues from their tEnd (momentsolver.cpp:47)
+            const std::string echo = read_config_echo( base );
+            Config prev            = h->cfg;
+            if( !echo.empty() ) {
+                prev = parse_config( echo );
+                t0   = prev.tEnd;
+            }
+            const int nPrev = echo.empty() ? h->tab.nT : build_tables( prev ).nT;
+            if( nPrev != h->tab.nT ) {
+                restart_new_order( h, base, echo, prev );
+                if( h->d_factorLevel ) reset_factor_store( h );
+                reset_control( h, t0 );
+                h->stateReady = true;
+                return UQC_OK;
+            }
             std::vector<double> u, lam;
             read_state_file( base + "_moments", N, h->ldc, u );
             CK( cudaMemcpyAsync( h->d_u, u.data(), u.size() * sizeof( double ), cudaMemcpyHostToDevice, h->stream ) );
@@ -1215,13 +1412,20 @@ int uqc_init_state( uqc_solver* h ) {
                 keep = 1;
             }
         }
+        // One-Shot IPM (maxIterations 1): SetDuals converges the initial duals
+        // (SolveClosureSafe, 10000 iterations, momentsolver.cpp:486-492) unless they are imported
+        oneShotSolve = h->cfg.maxIterations == 1 && keep >= 0;
         if( keep >= 0 ) {
             void* args[] = {&P, &keep};
             launch( h, pick( h->cfg.closure, h->group, 2 ), h->auxGrid, h->auxBlock, h->initSmem, args );
         }
         CK( cudaGetLastError() );
+        if( oneShotSolve ) {
+            reset_control( h, t0 );
+            safe_closure_all( h, 10000 );
+        }
         if( h->d_factorLevel ) reset_factor_store( h );
-        reset_control( h, 0.0 );
+        reset_control( h, t0 );
         h->stateReady = true;
         return UQC_OK;
     } );
@@ -1380,6 +1584,8 @@ int uqc_export_state( uqc_solver* h, const char* path_prefix ) {
             }
             if( std::fclose( f ) != 0 ) throw ConfigError( "cannot write " + path );
         }
+        // the log a restart reads the previous settings from (main.cpp:160-180)
+        write_config_echo( path_prefix, h->cfgName, h->cfgText );
         return UQC_OK;
     } );
 }
@@ -1463,6 +1669,43 @@ int uqc_solve_closure( uqc_solver* h, uqc_step_info* info ) {
         return failed ? fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( failed ) + " cells did not converge" ) : UQC_OK;
     } );
 }
+
+void ensure_scratch( uqc_solver* h, size_t n );
+int uqc_solve_closure_cells( uqc_solver* h, const unsigned* cells, int n_cells, double tol, int max_iter, uqc_step_info* info ) {
+    if( !h || n_cells < 0 || ( cells && n_cells == 0 ) || tol < 0.0 || max_iter < 0 ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
+    if( cells )
+        for( int i = 0; i < n_cells; ++i )
+            if( cells[i] >= unsigned( h->mesh.nCells ) ) return fail( h, UQC_ERR_ARGUMENT, "cell id out of range" );
+    return guarded_dev( h, [&] {
+        h->launches = 0;
+        read_control( h );
+        int stepsBefore = h->h_ctl->steps;
+        reset_work( h );
+        KParams P = make_params( h );
+        if( tol > 0.0 ) P.eps = tol;
+        if( max_iter > 0 ) P.maxIter = max_iter;
+        if( cells ) {
+            // the subset as the kernel's work list (scratch: ids, then their count)
+            ensure_scratch( h, size_t( n_cells ) + 1 );
+            int* list      = reinterpret_cast<int*>( h->d_xStatus );
+            unsigned* cnt  = reinterpret_cast<unsigned*>( h->d_xIters );
+            const unsigned n = unsigned( n_cells );
+            CK( cudaMemcpyAsync( list, cells, size_t( n_cells ) * sizeof( int ), cudaMemcpyHostToDevice, h->stream ) );
+            CK( cudaMemcpyAsync( cnt, &n, sizeof( n ), cudaMemcpyHostToDevice, h->stream ) );
+            CK( cudaStreamSynchronize( h->stream ) );    // n lives on this stack frame
+            P.activeList  = list;
+            P.activeCount = cnt;
+            P.listParity  = 0;
+        }
+        launch_closure( h, P, 0 );
+        CK( cudaGetLastError() );
+        int failed = fill_info( h, info, stepsBefore );
+        return failed ? fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( failed ) + " cells did not converge" ) : UQC_OK;
+    } );
+}
+
+int uqc_moments_mean_var( uqc_solver* h, double* out ) { return uqc_mean_var( h, out ); }
 
 int uqc_cell_status( uqc_solver* h, int* status, int* iterations ) {
     if( !h ) return UQC_ERR_ARGUMENT;
@@ -1555,7 +1798,7 @@ int uqc_mean_var( uqc_solver* h, double* out ) {
     } );
 }
 
-static void ensure_scratch( uqc_solver* h, size_t n ) {
+void ensure_scratch( uqc_solver* h, size_t n ) {
     if( n <= h->xCap ) return;
     for( void* p : {(void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus, (void*)h->d_xIters} )
         if( p ) cudaFree( p );

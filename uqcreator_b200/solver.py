@@ -179,6 +179,19 @@ class Solver:
             check(self.h, rc)
         return info.as_dict()
 
+    def solve_closure_cells(self, cells=None, tol=0.0, max_iter=0, raise_on_failure=True):
+        """Closure on a subset of the resident cells (None: all) with this call's
+        tolerance and iteration limit (0: the configured ones)."""
+        info = StepInfo()
+        if cells is None:
+            rc = self.lib.uqc_solve_closure_cells(self.h, None, 0, float(tol), int(max_iter), C.byref(info))
+        else:
+            c = np.ascontiguousarray(cells, dtype=np.uint32)
+            rc = self.lib.uqc_solve_closure_cells(self.h, ptr(c, L._up), len(c), float(tol), int(max_iter), C.byref(info))
+        if rc != 0 and (raise_on_failure or rc != -4):
+            check(self.h, rc)
+        return info.as_dict()
+
     def cell_status(self):
         st = np.zeros(self.n_cells, dtype=np.int32); it = np.zeros(self.n_cells, dtype=np.int32)
         check(self.h, self.lib.uqc_cell_status(self.h, ptr(st, L._ip), ptr(it, L._ip)))
