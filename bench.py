@@ -20,8 +20,13 @@ state, and the chosen form's moments are compared with it after the K steps.
 server (continuous batching) on the first requests of the seeded serving
 stream, submitted at their Poisson arrival times.
 
-N > 1 (torchrun): replicas only. Each rank runs its own copy of the workload
-on its GPU; there is no data-path collective; time = max over ranks.
+N > 1 (torchrun): spatial sharding, weak scaling. The mesh grows with N (400 N x
+250 rectangles x 2 = N x 200,000 cells) and is split into N blocks of about
+200,000 cells (recursive coordinate bisection: stripes along x), a rank per GPU
+(uqcreator_b200.shard.ShardedSolver). A step is the closure of the rank's
+cells, an NCCL all-reduce MIN of the step size (8 bytes), the halo exchange of
+the nodal states of the cells next to the stripe boundaries (NCCL send/recv on
+the solver's stream) and the update; time = max over ranks.
 """
 from __future__ import annotations
 
@@ -164,7 +169,8 @@ def dist_init():
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         import datetime
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        # host scalars over gloo, device buffers (the step, the halos) over NCCL
+        dist.init_process_group("cpu:gloo,cuda:nccl", timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
@@ -290,6 +296,8 @@ def run_serving(args, precision):
     stream = W.serving_stream(args.serve_requests, args.serve_rate, seed=11)
     srv = Server(budget_bytes=int(args.serve_budget_gb * (1 << 30)), max_active=16, steps_per_slice=4,
                  policy=args.serve_policy, max_stepping=args.serve_max_stepping)
+    if args.serve_policy == 1:
+        srv.set_option("aging", args.serve_aging)
     t0 = time.perf_counter()
     i, ids = 0, []
     while True:
@@ -312,8 +320,8 @@ def run_serving(args, precision):
            "stream": "seeded serving stream (seed 11): Poisson arrivals, Burgers1D 200-20k cells deg 2-9, "
                      "Euler2D 10k-200k cells deg 2-5, offsets U[0.05,0.3], 5-40 steps per request",
            "budget_gb": args.serve_budget_gb, "max_active": 16, "steps_per_slice": 4,
-           "policy": "shortest remaining work first" if args.serve_policy == 1 else "round robin",
-           "max_stepping": args.serve_max_stepping}
+           "policy": "shortest remaining time first" if args.serve_policy == 1 else "round robin",
+           "max_stepping": args.serve_max_stepping, "aging": args.serve_aging if args.serve_policy == 1 else None}
     out.update(latency_percentiles(lat))
     out["queue"] = latency_percentiles(queue)
     out["service"] = latency_percentiles(service)
@@ -323,7 +331,107 @@ def run_serving(args, precision):
     return out
 
 
+def run_b200_sharded(args, rank, world, local):
+    """The bench line at N > 1: the 2-D Euler workload on an N-times wider mesh,
+    one stripe of cells per rank, halo exchange and step all-reduce over NCCL."""
+    import torch
+    import torch.distributed as dist
+    from uqcreator_b200 import workloads as W, FP64, MIXED
+    from uqcreator_b200.shard import ShardedSolver
+
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+    toml = W.euler2d(**dict(WORKLOAD, nx=WORKLOAD["nx"] * world))
+    ss = ShardedSolver(toml)
+    ss.init_state()
+    sh = ss.shard
+    s = sh.solver
+    forms = ["fp64"]
+    try:
+        s.set_precision(MIXED)
+        s.set_precision(FP64)
+        forms.append("mixed")
+    except Exception:
+        pass
+    chosen = "mixed" if "mixed" in forms else "fp64"
+    warm = ss.step(args.warmup, with_info=True)
+    u0, l0, v0 = s.download_state()
+    results = {}
+    for form in forms:
+        s.set_precision(MIXED if form == "mixed" else FP64)
+        s.upload_state(u0, l0, v0, t=warm["t"])
+        ss.step(args.warmup)
+        torch.cuda.synchronize()
+        barrier(world)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(dev) as ck:
+            ev0.record(sh.stream)
+            info = ss.step(args.steps, with_info=True)
+            ev1.record(sh.stream)
+            torch.cuda.synchronize()
+        barrier(world)
+        results[form] = dict(ms=max_over_ranks(ev0.elapsed_time(ev1), world), info=info, clocks=ck.summary(),
+                             launches=s.last_launch_count() * args.steps, state=s.download_state())
+    no = sh.n_owned
+    err = None
+    if chosen != "fp64":
+        uf, ub = results["fp64"]["state"][0][:no], results[chosen]["state"][0][:no]
+        area = s.geometry()["area"][:no, None, None]
+        num = torch.tensor((np.abs(ub - uf) * area).sum(axis=(0, 2)))
+        den = torch.tensor((np.abs(uf) * area).sum(axis=(0, 2)))
+        dist.all_reduce(num)
+        dist.all_reduce(den)
+        err = float((num / den).max())
+    # end to end through the public API: the rank's state from and to pinned host memory every step
+    s.set_precision(MIXED if chosen == "mixed" else FP64)
+    s.upload_state(u0, l0, v0, t=warm["t"])
+    hu = torch.empty(u0.shape, dtype=torch.float64, pin_memory=True).numpy()
+    hl = torch.empty(l0.shape, dtype=torch.float64, pin_memory=True).numpy()
+    hv = torch.empty(v0.shape, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    hu[...] = u0; hl[...] = l0; hv[...] = v0
+    e2e_steps = max(1, min(args.steps, 10))
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    tcur = warm["t"]
+    for _ in range(e2e_steps):
+        s.upload_state(hu, hl, hv, t=tcur)
+        tcur = ss.step(1, with_info=True)["t"]
+        s.download_state(out=(hu, hl, hv))
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(1e3 * (time.perf_counter() - t0), world)
+    cells = sh.plan["n_global"]
+    r = results[chosen]
+    value = cells * args.steps / (r["ms"] / 1e3)
+    fp64_value = cells * args.steps / (results["fp64"]["ms"] / 1e3)
+    local_bytes = s.n_cells * s.n_states * s.n_total * 8
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if chosen == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": f"euler2d_sod_2u_deg5_q10x10 on a {WORKLOAD['nx'] * world}x{WORKLOAD['ny']} mesh",
+                   "cells": cells, "cells_per_rank": no, "halo_rows_per_step": sh.plan["n_send"],
+                   "duals_per_cell": s.n_states * s.n_total, "nodes": s.n_quad, "form": chosen,
+                   "parallelism": f"spatial{world} (stripes, NCCL halo exchange + all-reduce MIN)",
+                   "l2": "inputs larger than L2"},
+        "fp64": {"value": fp64_value, "ms_per_step": results["fp64"]["ms"] / args.steps},
+        "chosen_over_fp64": value / fp64_value,
+        "moment_rel_l1_vs_fp64": err,
+        "roofline": None,
+        "e2e": {"value": cells * e2e_steps / (e2e_ms / 1e3), "unit": "cell-steps/s",
+                "h2d_bytes_per_step": world * (2 * local_bytes + 4 * s.n_cells),
+                "d2h_bytes_per_step": world * (2 * local_bytes + 4 * s.n_cells), "steps": e2e_steps},
+        "gpu_launches": r["launches"],
+        "clocks": r["clocks"],
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    ss.close()
+
+
 def run_b200(args, rank, world, local):
+    if world > 1:
+        return run_b200_sharded(args, rank, world, local)
     import torch
     from uqcreator_b200 import Solver, workloads as W, FP64, MIXED
 
@@ -419,7 +527,7 @@ def run_b200(args, rank, world, local):
         "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if chosen == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": "euler2d_sod_2u_deg5_q10x10", "cells": cells, "duals_per_cell": s.n_states * s.n_total,
-                   "nodes": s.n_quad, "form": chosen, "parallelism": f"replicas{world}",
+                   "nodes": s.n_quad, "form": chosen, "parallelism": "single GPU",
                    "l2": f"inputs larger than L2 (resident state {cells * (2 * s.n_states * s.n_total + s.n_states * s.n_quad) * 8 / 1e9:.2f} GB)"},
         "fp64": {"value": fp64_value, "ms_per_step": results["fp64"]["ms"] / args.steps},
         "chosen_over_fp64": value / fp64_value,
@@ -525,8 +633,9 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=120, help="requests of the serving stream (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=12.0, help="arrivals per second")
     ap.add_argument("--serve-budget-gb", type=float, default=100.0)
-    ap.add_argument("--serve-policy", type=int, default=1, help="0 round robin, 1 shortest remaining work first")
-    ap.add_argument("--serve-max-stepping", type=int, default=4, help="requests stepping at a time (policy 1)")
+    ap.add_argument("--serve-policy", type=int, default=0, help="0 round robin, 1 shortest remaining time first")
+    ap.add_argument("--serve-max-stepping", type=int, default=0, help="requests stepping at a time (policy 1; 0: no limit)")
+    ap.add_argument("--serve-aging", type=float, default=1.0, help="policy 1: ms of remaining time one ms of waiting offsets")
     ap.add_argument("--serving-only", action="store_true",
                     help="only the serving section (e.g. the whole stream: --serve-requests 2000)")
     ap.add_argument("--configs", action="store_true", help="one line per configuration (C1, C2, C3, C5) instead of the bench line")

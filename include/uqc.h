@@ -288,6 +288,63 @@ int uqc_step_query( uqc_solver* h, uqc_step_info* info );
 /* Device memory (bytes) the handle holds once its device side is set up. */
 int uqc_device_bytes( const uqc_solver* h, unsigned long long* bytes );
 
+/* Spatial sharding, one process (one handle) per GPU. Replaces the MPI work
+ * split of MomentSolver::Solve (code/src/momentsolver.cpp:83-152): there every
+ * rank keeps all cells, solves the duals of its round-robin cells
+ * (_cellIndexPE, :83-89), broadcasts every cell's duals (MPI_Bcast, :92-95),
+ * reduces the moments of its quadrature-node slice onto the owner
+ * (MPI_Reduce, :144-146) and takes the step as MPI_Allreduce MIN (:133), the
+ * residual as MPI_Allreduce SUM (:152). Here a rank keeps its own block of
+ * cells and a one-ring halo; one time step is
+ *   uqc_step_phase(h, 0)  closure of the owned cells (their nodal states and
+ *                         the rank's smallest CFL step, as double bits, at
+ *                         *d_dt_bits);
+ *   caller: all-reduce MIN of the 8 bytes at *d_dt_bits (as uint64: positive
+ *           doubles order as their bits), and the halo exchange: uqc_halo_pack
+ *           gathers the rows the peers need (row_doubles each, peers in
+ *           ascending order, send_counts[p] rows to peers[p]); the rows
+ *           received from peers[p] (recv_counts[p] of them, in the same peer
+ *           order) are written contiguously from *d_halo_rows;
+ *   uqc_step_phase(h, 1)  flux and update of the owned cells.
+ * All on the handle's stream (uqc_stream), so the caller's collectives go on
+ * that stream too. A shard's residual (*d_residual after phase 1, the
+ * reference's per-rank sum) is its owned cells' part: the caller all-reduces it
+ * (SUM) when it applies the minResidual stopping rule; the device loop
+ * condition of a sharded handle tests only tEnd and [uqc] steps. */
+typedef struct uqc_shard_info {
+    int rank, n_ranks;
+    int n_global;       /* cells of the whole mesh */
+    int n_owned;        /* local cells 0 .. n_owned-1 are owned (in global order) */
+    int n_halo;         /* local cells n_owned .. n_owned+n_halo-1: halo, grouped by owner rank */
+    int n_peers;        /* ranks this one exchanges with */
+    int n_send;         /* rows sent per step (sum of send_counts) */
+    int row_doubles;    /* nodal states per cell: n_states x n_quad */
+} uqc_shard_info;
+/* Makes the handle rank `rank` of n_ranks: the mesh is split by recursive
+ * coordinate bisection of the cell centres and the handle keeps its owned
+ * cells and their halo (uqc_info.n_cells = n_owned + n_halo; state arrays of
+ * every other call are per local cell). Call before any call that uses the
+ * device. A sharded handle refuses uqc_step, uqc_run, uqc_step_async,
+ * uqc_export_state, uqc_write_vtk and a restart. */
+int uqc_partition( uqc_solver* h, int rank, int n_ranks );
+/* The shard plan (host only): info, and when non-null: global_ids[n_owned +
+ * n_halo] (global cell id of each local cell), peers / send_counts /
+ * recv_counts [n_peers], send_cells[n_send] (local ids, grouped by peer). An
+ * unsharded handle reports itself as rank 0 of 1. */
+int uqc_get_shard( const uqc_solver* h, uqc_shard_info* info, int* global_ids, int* peers, int* send_counts, int* recv_counts,
+                   int* send_cells );
+/* Device pointers of the exchange: the first halo row of the nodal states,
+ * the step's min dt (uint64 bits) and the residual (double). */
+int uqc_shard_buffers( uqc_solver* h, double** d_halo_rows, unsigned long long** d_dt_bits, double** d_residual );
+/* Gathers the rows the peers need into d_send (n_send x row_doubles doubles,
+ * device memory) on the handle's stream. */
+int uqc_halo_pack( uqc_solver* h, double* d_send );
+/* Half of a time step on the handle's stream: phase 0 the closure, phase 1
+ * the flux and update (info, when non-null, is filled as by uqc_step, which
+ * waits for the stream). Also valid on an unsharded handle (phase 0 then
+ * phase 1 is one uqc_step without the graph). */
+int uqc_step_phase( uqc_solver* h, int phase, uqc_step_info* info );
+
 /* Request server: continuous batching of whole UQ solves (each request is a
  * TOML configuration run to its tEnd). Requests wait in submission order and
  * are admitted, first fit, while their device memory fits the budget and
@@ -326,16 +383,17 @@ const char* uqc_server_request_error( const uqc_server* s, long long id );
 /* Forgets a finished request and its result. */
 int uqc_server_release( uqc_server* s, long long id );
 /* Scheduling options:
- *   "policy"        0: every running request advances by a slice per progress
- *                   call, admission in submission order; 1 (default): shortest
- *                   remaining work first, for admission and for slices, with
- *                   at most "max_stepping" requests stepping at a time (the
- *                   others stay resident and idle). Remaining work = cells x
- *                   duals x nodes x the steps left ([uqc] steps; 1000 when
- *                   only tEnd bounds the run), minus the request's waiting
- *                   time in units of "aging_ms" steps of its own work.
- *   "max_stepping"  requests with a slice in flight under policy 1 (default 4).
- *   "aging_ms"      waiting time worth one step of remaining work (default 1000). */
+ *   "policy"        0 (default): every running request advances by a slice
+ *                   per progress call, admission in submission order; 1:
+ *                   shortest remaining time first, for admission and for
+ *                   slices, with at most "max_stepping" requests stepping at a
+ *                   time (the others stay resident and idle). Remaining time =
+ *                   cells x duals x nodes x the steps left ([uqc] steps; 1000
+ *                   when only tEnd bounds the run) over the server's measured
+ *                   rate, minus "aging" x the request's waiting time.
+ *   "max_stepping"  requests with a slice in flight under policy 1 (default 0:
+ *                   no limit).
+ *   "aging"         ms of remaining time one ms of waiting offsets (default 1). */
 int uqc_server_set_option( uqc_server* s, const char* key, double value );
 
 /* ---- introspection ----------------------------------------------------- */

@@ -30,7 +30,9 @@ class Config(C.Structure):
                 ("n_levels", C.c_int), ("degree", C.c_int * 16), ("n_quad", C.c_int), ("sigma", C.c_double * 4),
                 ("cfl", C.c_double), ("epsilon", C.c_double), ("max_iterations", C.c_int), ("newton_mode", C.c_int), ("gamma", C.c_double),
                 ("bb_minus", C.c_double), ("bb_plus", C.c_double), ("ic", C.c_double * 8), ("mesh_dim", C.c_int),
-                ("n_cells_1d", C.c_int), ("a", C.c_double), ("b", C.c_double)]
+                ("n_cells_1d", C.c_int), ("a", C.c_double), ("b", C.c_double),
+                ("ref_indicator", C.c_int), ("ref_down", C.c_double), ("ref_up", C.c_double),
+                ("n_ret_levels", C.c_int), ("ret_res", C.c_double * 8), ("ret_lev", C.c_int * 9)]
 
 
 def build():
@@ -98,6 +100,15 @@ def config_from_toml(toml_text: str) -> Config:
     c.n_cells_1d = int(me.get("numberOfCells", 0))
     c.a = float(me.get("a", 0.0))
     c.b = float(me.get("b", 0.0))
+    c.ref_indicator = {"moments": 0, "energy": 1}[uq.get("refinementIndicator", "moments")]
+    c.ref_down, c.ref_up = (float(v) for v in uq.get("refinementBounds", [0.004, 0.02]))
+    lev = uq.get("retardationLevels", [])
+    res = uq.get("retardationResiduals", [])
+    c.n_ret_levels = len(lev)
+    for i, v in enumerate(lev):
+        c.ret_lev[i] = int(v)
+    for i, v in enumerate(res):
+        c.ret_res[i] = float(v)
     return c
 
 

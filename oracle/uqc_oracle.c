@@ -29,7 +29,10 @@ struct uqco {
     double *u, *lam, *uQ, *uNew, *uOld;
     unsigned* level;
     double t;
+    int levelCap, retIndex; /* retardation: highest level allowed, thresholds passed */
 };
+
+static void reset_retardation( uqco* h );
 
 /* ------------------------------------------------------------------ tables */
 
@@ -865,6 +868,7 @@ void uqco_geometry( const uqco* h, double* area, double* max_edge, double* cente
  * restart (:463-485). */
 void uqco_init_state( uqco* h ) {
     int nS = h->nS, nT = h->nT, nQ = h->nQ, d = h->dimXi;
+    reset_retardation( h );
     double* uIC = malloc( sizeof( double ) * nS * nQ );
     double ds[MAXS] = {0, 0, 0, 0}, u0[MAXS];
     for( int j = 0; j < h->nCells; ++j ) {
@@ -905,6 +909,7 @@ void uqco_set_state( uqco* h, const double* u, const double* lambda, const unsig
     if( lambda ) memcpy( h->lam, lambda, n * sizeof( double ) );
     if( level ) memcpy( h->level, level, h->nCells * sizeof( unsigned ) );
     h->t = t;
+    reset_retardation( h );
 }
 
 int uqco_solve_closure( const uqco* h, int n, double* lambda, const double* u, const unsigned* n_total_cell, int* status, int* iters ) {
@@ -920,9 +925,28 @@ int uqco_solve_closure( const uqco* h, int n, double* lambda, const double* u, c
     return nFail;
 }
 
-/* Refinement indicator (momentsolver.cpp:271-289). */
+/* The retardation schedule from its start (no threshold passed). */
+static void reset_retardation( uqco* h ) {
+    h->levelCap = h->cfg.n_ret_levels > 0 ? h->cfg.ret_lev[0] : 1 << 30;
+    h->retIndex = 0;
+}
+
+/* Refinement indicator (momentsolver.cpp:271-289), or the paper's
+ * S_l = <(u_l - u_{l-1})^2> / <u_l^2> (Paper1/adaptivity.tex:12-14) of the first
+ * state, written with the coefficients (the basis is orthonormal under the
+ * quadrature): the added moments' squares over all squares, level 0 against
+ * the mean alone. */
 static double ref_indicator( const uqco* h, const double* u, unsigned lev ) {
     double ind = 0.0;
+    if( h->cfg.ref_indicator == 1 ) {
+        int prev = lev == 0 ? 1 : h->nTLevel[lev - 1];
+        double num = 0.0, den = 0.0;
+        for( int i = 0; i < h->nTLevel[lev]; ++i ) {
+            den += u[i] * u[i];
+            if( i >= prev ) num += u[i] * u[i];
+        }
+        return den > 0.0 ? num / den : 0.0;
+    }
     if( h->dimXi == 1 ) {
         ind += fabs( u[h->nTLevel[lev] - 1] ) + fabs( u[h->nTLevel[lev] - 2] );
     }
@@ -957,9 +981,12 @@ int uqco_step( uqco* h, int n_steps, double* out ) {
         if( h->nLevels > 1 )
             for( int j = 0; j < N; ++j ) {
                 double ind = ref_indicator( h, h->u + j * m, h->level[j] );
-                if( ind > 0.02 && h->level[j] < (unsigned)h->nLevels - 1 )
+                int cap    = h->levelCap < h->nLevels - 1 ? h->levelCap : h->nLevels - 1;
+                if( (int)h->level[j] > cap )
+                    h->level[j] = (unsigned)cap;
+                else if( ind > h->cfg.ref_up && (int)h->level[j] < cap )
                     h->level[j] += 1;
-                else if( ind < 0.004 && h->level[j] > 0 )
+                else if( ind < h->cfg.ref_down && h->level[j] > 0 )
                     h->level[j] -= 1;
             }
         for( int j = 0; j < N; ++j ) {
@@ -1025,6 +1052,10 @@ int uqco_step( uqco* h, int n_steps, double* out ) {
         }
         memcpy( h->u, h->uNew, sizeof( double ) * N * m );
         for( int j = 0; j < N; ++j ) residual += fabs( h->u[j * m] - h->uOld[j * m] ) * h->area[j];
+        if( h->cfg.n_ret_levels > 0 ) {
+            while( h->retIndex < h->cfg.n_ret_levels - 1 && residual < h->cfg.ret_res[h->retIndex] ) ++h->retIndex;
+            h->levelCap = h->cfg.ret_lev[h->retIndex];
+        }
     }
     free( G );
     free( rhs );

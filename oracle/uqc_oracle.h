@@ -39,6 +39,17 @@ typedef struct uqco_config {
     int mesh_dim;       /* 1 or 2 */
     int n_cells_1d;     /* 1-D: cells, interval [a, b] */
     double a, b;
+    /* level rule: 0 the code's indicator (momentsolver.cpp:271-289), 1 the
+     * paper's S_l (Paper1/adaptivity.tex:12-14); bounds (0.004, 0.02 in the
+     * code, momentsolver.cpp:104-112); retardation schedule: the highest level
+     * is ret_lev[k] once the residual has fallen below ret_res[0..k-1]
+     * (Paper1/results.tex:179,241); n_ret_levels entries of ret_lev (0: no
+     * schedule), one fewer of ret_res */
+    int ref_indicator;
+    double ref_down, ref_up;
+    int n_ret_levels;
+    double ret_res[8];
+    int ret_lev[9];
 } uqco_config;
 
 typedef struct uqco uqco;

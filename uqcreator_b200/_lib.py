@@ -31,6 +31,7 @@ EXPORTS = [
     "uqc_server_destroy", "uqc_server_last_error", "uqc_server_submit", "uqc_server_progress",
     "uqc_server_request", "uqc_server_release", "uqc_server_request_error", "uqc_export_state", "uqc_write_vtk",
     "uqc_debug_mixed_inverse", "uqc_server_set_option", "uqc_solve_closure_cells", "uqc_moments_mean_var",
+    "uqc_partition", "uqc_get_shard", "uqc_shard_buffers", "uqc_halo_pack", "uqc_step_phase",
 ]
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
 NOALLOC_MAX_CELLS = 65536
@@ -47,6 +48,14 @@ class Info(C.Structure):
                 ("n_levels", C.c_int), ("dim_xi", C.c_int), ("n_faces", C.c_int), ("mesh_dim", C.c_int),
                 ("n_total_level", C.c_int * 16), ("precision", C.c_int), ("newton_mode", C.c_int),
                 ("t", C.c_double), ("steps", C.c_longlong), ("mixed_form", C.c_int), ("mixed_rounds", C.c_int)]
+
+
+class ShardInfo(C.Structure):
+    _fields_ = [("rank", C.c_int), ("n_ranks", C.c_int), ("n_global", C.c_int), ("n_owned", C.c_int),
+                ("n_halo", C.c_int), ("n_peers", C.c_int), ("n_send", C.c_int), ("row_doubles", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class StepInfo(C.Structure):
@@ -128,6 +137,11 @@ def lib() -> C.CDLL:
         "uqc_server_set_option": ([_vp, C.c_char_p, C.c_double], C.c_int),
         "uqc_solve_closure_cells": ([_vp, _up, C.c_int, C.c_double, C.c_int, C.POINTER(StepInfo)], C.c_int),
         "uqc_moments_mean_var": ([_vp, _dp], C.c_int),
+        "uqc_partition": ([_vp, C.c_int, C.c_int], C.c_int),
+        "uqc_get_shard": ([_vp, C.POINTER(ShardInfo), _ip, _ip, _ip, _ip, _ip], C.c_int),
+        "uqc_shard_buffers": ([_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)], C.c_int),
+        "uqc_halo_pack": ([_vp, _vp], C.c_int),
+        "uqc_step_phase": ([_vp, C.c_int, C.POINTER(StepInfo)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

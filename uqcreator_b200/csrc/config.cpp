@@ -271,6 +271,34 @@ Config parse_config( const std::string& text ) {
         c.maxSteps = int( v->num() );
         if( c.maxSteps < 0 ) throw ConfigError( "[uqc] 'steps' must be >= 0" );
     }
+    if( const Value* v = find( d, "uqc", "refinementIndicator" ) ) {
+        const std::string p = str( *v, "[uqc] refinementIndicator" );
+        if( p == "moments" )
+            c.refIndicator = 0;
+        else if( p == "energy" )
+            c.refIndicator = 1;
+        else
+            throw ConfigError( "[uqc] 'refinementIndicator' must be moments or energy" );
+    }
+    if( const Value* v = find( d, "uqc", "refinementBounds" ) ) {
+        if( v->kind != Value::ARR || v->items.size() != 2 ) throw ConfigError( "[uqc] 'refinementBounds' must be [lower, upper]" );
+        c.refDown = v->items[0].num();
+        c.refUp   = v->items[1].num();
+        if( !( c.refDown < c.refUp ) ) throw ConfigError( "[uqc] 'refinementBounds' needs lower < upper" );
+    }
+    if( const Value* v = find( d, "uqc", "retardationLevels" ) ) {
+        for( auto& x : v->items ) c.retLevels.push_back( int( x.num() ) );
+        if( const Value* r = find( d, "uqc", "retardationResiduals" ) )
+            for( auto& x : r->items ) c.retResiduals.push_back( x.num() );
+        if( c.retLevels.empty() || c.retLevels.size() > 9 || c.retResiduals.size() + 1 != c.retLevels.size() )
+            throw ConfigError( "[uqc] retardation: 1 to 9 'retardationLevels' and one fewer 'retardationResiduals'" );
+        for( size_t k = 0; k < c.retLevels.size(); ++k ) {
+            if( c.retLevels[k] < 0 || ( k && c.retLevels[k] < c.retLevels[k - 1] ) )
+                throw ConfigError( "[uqc] 'retardationLevels' must be non-negative and non-decreasing" );
+            if( k && k < c.retResiduals.size() && !( c.retResiduals[k] < c.retResiduals[k - 1] ) )
+                throw ConfigError( "[uqc] 'retardationResiduals' must be decreasing" );
+        }
+    }
     size_t needIc = c.problem == PR_BURGERS ? 4 : ( c.problem == PR_EULER2D ? 5 : 3 );
     if( c.ic.size() < needIc ) throw ConfigError( "[uqc] 'ic' needs " + std::to_string( needIc ) + " values for " + c.problemName );
     if( c.meshDim == 1 ) {

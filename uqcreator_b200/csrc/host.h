@@ -52,6 +52,11 @@ struct Config {
     int precision = 0;     // uqc_precision
     int newtonMode = 0;    // 0 reference, 1 guarded, 2 safe
     int maxSteps   = 0;    // [uqc] steps: stop after this many time steps (0: no limit)
+    // refinement levels: indicator and bounds of the level rule, retardation
+    int refIndicator = 0;              // 0: sum of |u(0, i)| (momentsolver.cpp:271-289); 1: S_l (Paper1/adaptivity.tex:12-14)
+    double refDown = 0.004, refUp = 0.02;    // level - 1 below refDown, + 1 above refUp (momentsolver.cpp:104-112)
+    std::vector<int> retLevels;        // highest level allowed, raised as the residual falls below ...
+    std::vector<double> retResiduals;  // ... each of these (one fewer than retLevels)
     std::string restartFile;       // [general] restartFile (settings.cpp:74-79), relative to the input file's directory
     bool importDualState = false;  // [general] importDualState: duals from <restartFile>_duals too
     std::string inputDir = ".";    // directory of the input file (uqc_create_from_file), else "."
@@ -102,5 +107,32 @@ inline bool mesh_has_walls( const Mesh& m ) {
     return false;
 }
 Mesh build_mesh_tri( int nNodes, const double* xy, const int* bnd, int nTri, const int* tri );
+
+// Spatial sharding: one rank's part of a mesh. The reference splits the dual
+// solves round-robin over MPI ranks and replicates every cell's duals and
+// moments on every rank (PEforCell, _cellIndexPE; momentsolver.cpp:83-146).
+// Here a rank owns a compact block of cells and keeps only those plus a
+// one-ring halo: local cells 0..nOwned-1 are the owned ones in global order,
+// then the halo cells grouped by owning rank (ascending), each group in global
+// order. A rank sends to each peer the nodal states of its cells that lie in
+// the peer's halo, in global order, which is the order the peer stores them in.
+struct ShardPlan {
+    int rank = 0, nRanks = 1, nGlobal = 0, nOwned = 0;
+    std::vector<int> globalId;     // per local cell
+    std::vector<int> peers;        // ranks exchanged with, ascending
+    std::vector<int> sendCount;    // per peer
+    std::vector<int> recvCount;    // per peer: halo cells it owns (contiguous, in peer order)
+    std::vector<int> sendCells;    // local ids, grouped by peer
+};
+
+// Owner rank of every cell: recursive coordinate bisection of the cell
+// centres (split across the wider extent, cells ordered by coordinate then id,
+// rank counts split as evenly as possible, cell counts in proportion).
+std::vector<int> partition_cells( const Mesh& m, int nRanks );
+
+// The rank's local mesh (owned cells, then the halo) and its exchange plan.
+// Neighbours outside the local cells, and the global mesh's ghost index, map
+// to the local ghost index (the local cell count).
+Mesh shard_mesh( const Mesh& g, const std::vector<int>& owner, int rank, int nRanks, ShardPlan& plan );
 
 }    // namespace uqc

@@ -71,13 +71,25 @@ struct Control {
     unsigned int v2Work[16];
     unsigned int v2Count[4];
     int v2Error;
+    // refinement retardation: the highest level the level rule may reach, and
+    // how many of the residual thresholds the residual has fallen below
+    int levelCap;
+    int retIndex;
 };
 
 struct KParams {
     int nS, nT, nQ, ld;       // ld: row stride of the tables (odd, >= nT)
     int nLevels;
     int nTLevel[MAXLEV];
+    // level rule: indicator (0 sum of |u(0, i)| over the level's own moments,
+    // 1 the share of their energy S_l), bounds, retardation schedule
+    int refIndicator;
+    double refDown, refUp;
+    int nRet;                 // residual thresholds of the retardation schedule (0: none)
+    double retRes[8];
+    int retLev[9];
     int nCells, nFaces, dimXi;
+    int nWork;                // cells a time step works on: the first nWork (a shard's owned cells), else nCells
     double eps;
     int maxIter, newtonMode;
     PhysParams phys;
@@ -655,6 +667,44 @@ out:
 
 // ------------------------------------------------------------------ kernels
 
+// Refinement indicator of a cell at level lev (nTj moments) from its first
+// state's moments at(i): the sum of |u(0, i)| over the moments the level adds
+// (the last two in one uncertain dimension) of MomentSolver::ComputeRefIndicator
+// (momentsolver.cpp:271-289), or S_l = <(u_l - u_{l-1})^2> / <u_l^2> of
+// Paper1/adaptivity.tex:12-14, which for the orthonormal basis tables is the
+// sum of the added moments' squares over the sum of all squares (level 0
+// measures against the mean alone, as the code's indicator does).
+template <class AT> __device__ __forceinline__ double level_indicator( const KParams& P, AT at, int lev, int nTj ) {
+    double ind = 0.0;
+    if( P.refIndicator == 1 ) {
+        const int prev = lev == 0 ? 1 : P.nTLevel[lev - 1];
+        double num = 0.0, den = 0.0;
+        for( int i = 0; i < nTj; ++i ) {
+            const double v = at( i );
+            den += v * v;
+            if( i >= prev ) num += v * v;
+        }
+        return den > 0.0 ? num / den : 0.0;
+    }
+    if( P.dimXi == 1 )
+        ind = fabs( at( nTj - 1 ) ) + fabs( at( nTj - 2 ) );
+    else {
+        const int prev = lev == 0 ? 1 : P.nTLevel[lev - 1];
+        for( int i = prev; i < nTj; ++i ) ind += fabs( at( i ) );
+    }
+    return ind;
+}
+
+// The level rule of momentsolver.cpp:104-112 with configurable bounds, capped
+// by the retardation schedule (a level above the cap drops to it).
+__device__ __forceinline__ int level_rule( const KParams& P, double ind, int lev ) {
+    const int cap = min( P.nLevels - 1, P.ctl->levelCap );
+    if( lev > cap ) return cap;
+    if( ind > P.refUp && lev < cap ) return lev + 1;
+    if( ind < P.refDown && lev > 0 ) return lev - 1;
+    return lev;
+}
+
 // Epilogue of a cell whose closure is done, phases [C]-[F] of
 // MomentSolver::Solve (momentsolver.cpp:99-133): uk holds U(Lambda(lam)) at
 // the nodes, uh the moments before re-projection. Writes uQ, the new
@@ -669,19 +719,7 @@ __device__ double cell_epilogue( const Grp<GROUP>& g, const KParams& P, const do
     auto ukAt = [&]( int s, int k ) { return NM ? uk[k * NS + s] : uk[s * P.nQ + k]; };
     const size_t ldc = size_t( NS ) * P.nT;
     int newLev       = lev;
-    if( P.nLevels > 1 ) {
-        double ind = 0.0;
-        if( P.dimXi == 1 )
-            ind = fabs( uh[nTj - 1] ) + fabs( uh[nTj - 2] );
-        else {
-            int prev = lev == 0 ? 1 : P.nTLevel[lev - 1];
-            for( int i = prev; i < nTj; ++i ) ind += fabs( uh[i] );
-        }
-        if( ind > 0.02 && lev < P.nLevels - 1 )
-            newLev = lev + 1;
-        else if( ind < 0.004 && lev > 0 )
-            newLev = lev - 1;
-    }
+    if( P.nLevels > 1 ) newLev = level_rule( P, level_indicator( P, [&]( int i ) { return uh[i]; }, lev, nTj ), lev );
     const int nTn = P.nTLevel[newLev];
     if( g.r == 0 ) {
         P.uOld0[cell] = uh[0];
@@ -794,7 +832,7 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
     int* alist;
     unsigned* acount;
     step_list( P, 0, alist, acount );
-    const int nWork = alist ? int( *acount ) : P.nCells;
+    const int nWork = alist ? int( *acount ) : P.nWork;
     for( ;; ) {
         int item;
         if( g.r == 0 ) bc[0] = double( atomicAdd( P.workCounter, 1u ) );
@@ -928,7 +966,7 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
     // k_update filled (converged cells whose refinement level changes)
     const bool listMode = P.ctl->listReady != 0;
     const int par       = P.ctl->steps & 1;
-    const int nItems    = listMode ? int( P.checkCount[par] ) : P.nCells;
+    const int nItems    = listMode ? int( P.checkCount[par] ) : P.nWork;
     if( nItems == 0 ) return;
     int* alist;
     unsigned* acount;
@@ -1155,7 +1193,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         ccount = P.checkCount + ( ( P.ctl->steps + 1 ) & 1 );
     }
     WarpListBuf nbuf, cbuf;    // next step's active list and check list
-    for( int cell = blockIdx.x * nWarps + warp; cell < P.nCells; cell += gridDim.x * nWarps ) {
+    for( int cell = blockIdx.x * nWarps + warp; cell < P.nWork; cell += gridDim.x * nWarps ) {
         const int bc = P.boundary[cell];
         if( finish && lane == 0 && P.finFlag[cell] ) {
             // finished by the previous update: this step's closure status
@@ -1319,16 +1357,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
                     const double r = __shfl_sync( 0xffffffffu, ( i >> 5 ) ? v0b : v0a, i & 31 );
                     return i < 64 ? r : P.u[cell * ldc + i];
                 };
-                double ind = 0.0;
-                if( P.dimXi == 1 ) {
-                    const double a = at( nTj - 1 ), b = at( nTj - 2 );
-                    ind            = fabs( a ) + fabs( b );
-                }
-                else {
-                    const int prev = lev == 0 ? 1 : P.nTLevel[lev - 1];
-                    for( int i = prev; i < nTj; ++i ) ind += fabs( at( i ) );
-                }
-                if( ( ind > 0.02 && lev < P.nLevels - 1 ) || ( ind < 0.004 && lev > 0 ) ) fin = false;
+                if( level_rule( P, level_indicator( P, at, lev, nTj ), lev ) != lev ) fin = false;
             }
             if( fin ) {
                 if( lane == 0 ) finish_cell( P, cell, v0a, dtNext );
@@ -1384,6 +1413,13 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         C->active     = ( C->t < C->tEnd && C->residual > C->minResidual && ( C->maxSteps == 0 || C->steps < C->maxSteps ) ) ? 1 : 0;
         C->activeCellsLast = C->activeCells;
         C->activeCells     = 0;
+        // retardation: raise the level cap as the residual falls below the thresholds
+        if( P.nRet > 0 ) {
+            int k = C->retIndex;
+            while( k < P.nRet && s < P.retRes[k] ) ++k;
+            C->retIndex = k;
+            C->levelCap = P.retLev[k];
+        }
         // the next step's min starts from the cells finished here (+inf if none)
         C->dtBits     = finish ? ( (volatile unsigned long long*)&C->dtBitsNext )[0] : 0x7FF0000000000000ull;
         C->dtBitsNext = 0x7FF0000000000000ull;

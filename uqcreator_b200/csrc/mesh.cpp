@@ -312,4 +312,125 @@ Mesh read_su2_mesh( const std::string& path, const std::vector<std::pair<std::st
     return m;
 }
 
+namespace {
+void bisect( const Mesh& m, std::vector<int>& cells, size_t lo, size_t hi, int r0, int r1, std::vector<int>& owner ) {
+    if( r1 - r0 <= 1 ) {
+        for( size_t i = lo; i < hi; ++i ) owner[cells[i]] = r0;
+        return;
+    }
+    double ext[2];
+    for( int d = 0; d < 2; ++d ) {
+        double a = 1e300, b = -1e300;
+        for( size_t i = lo; i < hi; ++i ) {
+            const double x = m.center[2 * size_t( cells[i] ) + d];
+            a              = std::min( a, x );
+            b              = std::max( b, x );
+        }
+        ext[d] = hi > lo ? b - a : 0.0;
+    }
+    const int d = ext[1] > ext[0] ? 1 : 0;
+    std::sort( cells.begin() + lo, cells.begin() + hi, [&]( int p, int q ) {
+        const double a = m.center[2 * size_t( p ) + d], b = m.center[2 * size_t( q ) + d];
+        return a < b || ( a == b && p < q );
+    } );
+    const int nl     = ( r1 - r0 ) / 2;
+    const size_t mid = lo + size_t( ( (long long)( hi - lo ) * nl ) / ( r1 - r0 ) );
+    bisect( m, cells, lo, mid, r0, r0 + nl, owner );
+    bisect( m, cells, mid, hi, r0 + nl, r1, owner );
+}
+}    // namespace
+
+std::vector<int> partition_cells( const Mesh& m, int nRanks ) {
+    std::vector<int> owner( m.nCells, 0 ), cells( m.nCells );
+    for( int c = 0; c < m.nCells; ++c ) cells[c] = c;
+    bisect( m, cells, 0, cells.size(), 0, std::max( nRanks, 1 ), owner );
+    return owner;
+}
+
+Mesh shard_mesh( const Mesh& g, const std::vector<int>& owner, int rank, int nRanks, ShardPlan& plan ) {
+    const int N = g.nCells, F = g.nFaces;
+    plan           = ShardPlan{};
+    plan.rank      = rank;
+    plan.nRanks    = nRanks;
+    plan.nGlobal   = N;
+    std::vector<int>& gid = plan.globalId;
+    for( int c = 0; c < N; ++c )
+        if( owner[c] == rank ) gid.push_back( c );
+    plan.nOwned = int( gid.size() );
+    // halo: neighbours of owned cells owned elsewhere, by (owner, global id)
+    std::vector<std::pair<int, int>> halo;
+    for( int i = 0; i < plan.nOwned; ++i )
+        for( int f = 0; f < F; ++f ) {
+            const int nb = g.nbr[size_t( gid[i] ) * F + f];
+            if( nb < N && owner[nb] != rank ) halo.push_back( {owner[nb], nb} );
+        }
+    std::sort( halo.begin(), halo.end() );
+    halo.erase( std::unique( halo.begin(), halo.end() ), halo.end() );
+    for( const auto& h : halo ) gid.push_back( h.second );
+    const int L = int( gid.size() );
+    std::vector<int> local( N, -1 );
+    for( int i = 0; i < L; ++i ) local[gid[i]] = i;
+    // sends: owned cells that neighbour a cell of peer p, in global order
+    std::map<int, std::vector<int>> send;
+    for( int c = 0; c < N; ++c ) {
+        const int p = owner[c];
+        if( p == rank ) continue;
+        for( int f = 0; f < F; ++f ) {
+            const int nb = g.nbr[size_t( c ) * F + f];
+            if( nb < N && owner[nb] == rank ) send[p].push_back( nb );
+        }
+    }
+    std::map<int, int> recv;
+    for( const auto& h : halo ) ++recv[h.first];
+    std::vector<int> peers;
+    for( const auto& kv : send ) peers.push_back( kv.first );
+    for( const auto& kv : recv ) peers.push_back( kv.first );
+    std::sort( peers.begin(), peers.end() );
+    peers.erase( std::unique( peers.begin(), peers.end() ), peers.end() );
+    for( int p : peers ) {
+        std::vector<int>& s = send[p];
+        std::sort( s.begin(), s.end() );
+        s.erase( std::unique( s.begin(), s.end() ), s.end() );
+        plan.peers.push_back( p );
+        plan.sendCount.push_back( int( s.size() ) );
+        plan.recvCount.push_back( recv.count( p ) ? recv[p] : 0 );
+        for( int c : s ) plan.sendCells.push_back( local[c] );
+    }
+    // the local mesh: per-cell data copied, neighbours renumbered
+    Mesh m;
+    m.dim    = g.dim;
+    m.nCells = L;
+    m.nFaces = F;
+    m.area.resize( L );
+    m.maxEdge.resize( L );
+    m.center.resize( 2 * size_t( L ) );
+    m.unitN.resize( 2 * size_t( L ) * F );
+    m.scaledN.resize( 2 * size_t( L ) * F );
+    m.nbr.resize( size_t( L ) * F );
+    m.boundary.resize( L );
+    if( !g.bndNormal.empty() ) m.bndNormal.resize( 2 * size_t( L ) );
+    for( int i = 0; i < L; ++i ) {
+        const size_t c = size_t( gid[i] );
+        m.area[i]         = g.area[c];
+        m.maxEdge[i]      = g.maxEdge[c];
+        m.center[2 * i]   = g.center[2 * c];
+        m.center[2 * i + 1] = g.center[2 * c + 1];
+        m.boundary[i]     = g.boundary[c];
+        for( int f = 0; f < F; ++f ) {
+            const size_t a = size_t( i ) * F + f, b = c * F + f;
+            const int nb   = g.nbr[b];
+            m.nbr[a]       = nb < N && local[nb] >= 0 ? local[nb] : L;
+            for( int k = 0; k < 2; ++k ) {
+                m.unitN[2 * a + k]   = g.unitN[2 * b + k];
+                m.scaledN[2 * a + k] = g.scaledN[2 * b + k];
+            }
+        }
+        if( !g.bndNormal.empty() ) {
+            m.bndNormal[2 * i]     = g.bndNormal[2 * c];
+            m.bndNormal[2 * i + 1] = g.bndNormal[2 * c + 1];
+        }
+    }
+    return m;
+}
+
 }    // namespace uqc

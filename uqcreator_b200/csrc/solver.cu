@@ -125,6 +125,11 @@ struct uqc_solver {
     double* d_wt = nullptr;
     std::string cfgText;                     // the input file's text (echoed by uqc_export_state)
     std::string cfgName = "uqcreator_b200";  // the input file's path, when created from a file
+    double area0 = 0.0;                      // area of the global mesh's first cell (TimeSolver's fixed dt)
+    // spatial sharding (uqc_partition): the mesh is this rank's owned cells and halo
+    bool sharded = false;
+    ShardPlan shard;
+    int* d_sendCells = nullptr;
     std::string err;
 };
 
@@ -198,7 +203,14 @@ KParams make_params( const uqc_solver* h ) {
     P.ld      = h->ld;
     P.nLevels = h->tab.nLevels;
     for( int l = 0; l < h->tab.nLevels; ++l ) P.nTLevel[l] = h->tab.nTLevel[l];
+    P.refIndicator = h->cfg.refIndicator;
+    P.refDown      = h->cfg.refDown;
+    P.refUp        = h->cfg.refUp;
+    P.nRet         = int( h->cfg.retResiduals.size() );
+    for( int k = 0; k < P.nRet; ++k ) P.retRes[k] = h->cfg.retResiduals[k];
+    for( int k = 0; k < int( h->cfg.retLevels.size() ); ++k ) P.retLev[k] = h->cfg.retLevels[k];
     P.nCells     = h->mesh.nCells;
+    P.nWork      = h->mesh.nCells;    // a time step works on the owned cells only (step_lists)
     P.nFaces     = h->mesh.nFaces;
     P.dimXi      = h->tab.dimXi;
     P.eps        = h->cfg.epsilon;
@@ -213,7 +225,7 @@ KParams make_params( const uqc_solver* h ) {
     for( size_t i = 0; i < h->cfg.ic.size() && i < 8; ++i ) ph.ic[i] = h->cfg.ic[i];
     for( size_t i = 0; i < h->cfg.sigma.size() && i < 4; ++i ) ph.sigma[i] = h->cfg.sigma[i];
     ph.dimXi   = h->tab.dimXi;
-    ph.dtFixed = h->mesh.area[0] * h->cfg.cfl / 12.0;    // TimeSolver (timesolver.cpp:4-9)
+    ph.dtFixed = h->area0 * h->cfg.cfl / 12.0;    // TimeSolver (timesolver.cpp:4-9)
     P.phi          = h->d_phi;
     P.phiWf        = h->d_phiWf;
     P.xi           = h->d_xi;
@@ -592,10 +604,18 @@ void reset_control( uqc_solver* h, double t ) {
     c.tEnd            = h->cfg.tEnd;
     c.minResidual     = h->cfg.minResidual;
     c.residual        = h->cfg.minResidual + 1.0;    // momentsolver.cpp:76
+    if( h->sharded ) {
+        // a shard's residual is its own cells' part: the stopping rule on the
+        // summed residual is the caller's (after its all-reduce)
+        c.minResidual = -1.0;
+        c.residual    = 0.0;
+    }
     c.dtBits          = 0x7FF0000000000000ull;
     c.dtBitsNext      = 0x7FF0000000000000ull;
     c.maxSteps        = h->cfg.maxSteps;
     c.active          = t < h->cfg.tEnd ? 1 : 0;
+    c.levelCap        = h->cfg.retLevels.empty() ? ( 1 << 30 ) : h->cfg.retLevels[0];
+    c.retIndex        = 0;
     *h->h_ctl         = c;
     h->lastIters      = 0;    // device counters restart from zero
     h->lastLs         = 0;
@@ -641,6 +661,7 @@ void build( uqc_solver* h, const std::string& text, void* stream, const std::str
         tri_jitter_nodes( h->cfg.nx, h->cfg.ny, h->cfg.jitter, h->cfg.seed, xy.data(), bnd.data(), tri.data() );
         h->mesh = build_mesh_tri( nn, xy.data(), bnd.data(), nt, tri.data() );
     }
+    h->area0     = h->mesh.area.empty() ? 0.0 : h->mesh.area[0];
     h->precision = h->cfg.precision;
     h->userStream = (cudaStream_t)stream;
     // host copies of the tables in the device layout (row stride ld, 8 spare
@@ -710,6 +731,7 @@ void ensure_device( uqc_solver* h ) {
     h->d_finFlag      = dalloc<unsigned char>( N );
     CK( cudaMemset( h->d_finFlag, 0, N ) );
     h->d_fallbackList = dalloc<int>( N );
+    if( h->sharded && !h->shard.sendCells.empty() ) h->d_sendCells = dupload( h->shard.sendCells );
     h->d_ctl    = dalloc<Control>( 1 );
     CK( cudaMallocHost( &h->h_ctl, sizeof( Control ) ) );
     for( auto& e : h->ev ) CK( cudaEventCreate( &e ) );
@@ -730,7 +752,7 @@ void release( uqc_solver* h ) {
                     (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
                     (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_cellDt, (void*)h->d_uRe, (void*)h->d_checkList, (void*)h->d_finFlag, (void*)h->d_phiF, (void*)h->d_fallbackList,
                     (void*)h->d_factorStore, (void*)h->d_factorLevel, (void*)h->d_gStore, (void*)h->d_v2Lists,
-                    (void*)h->d_chordIters, (void*)h->d_qTiles} )
+                    (void*)h->d_chordIters, (void*)h->d_qTiles, (void*)h->d_sendCells} )
         if( p ) cudaFree( p );
     if( h->h_ctl ) cudaFreeHost( h->h_ctl );
     for( auto& e : h->ev )
@@ -813,6 +835,7 @@ void reset_work( uqc_solver* h ) {
 // the next step's list from its own convergence test, so later k_check
 // launches return at once (Control::listReady).
 void step_lists( uqc_solver* h, KParams& P ) {
+    if( h->sharded ) P.nWork = h->shard.nOwned;
     if( h->cfg.newtonMode == 2 ) return;
     P.activeList  = h->d_activeList;
     P.activeCount = h->d_ctl->nActive;
@@ -1377,6 +1400,7 @@ int uqc_init_state( uqc_solver* h ) {
         int keep     = 0;
         double t0    = 0.0;
         bool oneShotSolve = false;
+        if( !h->cfg.restartFile.empty() && h->sharded ) throw ConfigError( "a restart of a sharded handle is not supported" );
         if( !h->cfg.restartFile.empty() ) {
             // restart (MomentSolver::DetermineMoments / SetDuals, momentsolver.cpp:418-523)
             const std::string base = h->cfg.restartFile[0] == '/' ? h->cfg.restartFile : h->cfg.inputDir + "/" + h->cfg.restartFile;
@@ -1439,6 +1463,7 @@ int uqc_init_state( uqc_solver* h ) {
 // and averaged to the points (vtkCellDataToPointData with PassCellData).
 int uqc_write_vtk( uqc_solver* h, const char* path ) {
     if( !h || !path ) return UQC_ERR_ARGUMENT;
+    if( h->sharded ) return fail( h, UQC_ERR_STATE, "VTK output of a sharded handle: gather the owned cells (uqc_download_state) instead" );
     if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
     return guarded_dev( h, [&] {
         const Mesh& m = h->mesh;
@@ -1558,6 +1583,7 @@ int uqc_write_vtk( uqc_solver* h, const char* path ) {
 
 int uqc_export_state( uqc_solver* h, const char* path_prefix ) {
     if( !h || !path_prefix ) return UQC_ERR_ARGUMENT;
+    if( h->sharded ) return fail( h, UQC_ERR_STATE, "export of a sharded handle: gather the owned cells (uqc_download_state) instead" );
     if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
     return guarded_dev( h, [&] {
         const size_t N = size_t( h->mesh.nCells ), per = h->ldc;
@@ -1720,6 +1746,7 @@ int uqc_cell_status( uqc_solver* h, int* status, int* iterations ) {
 
 int uqc_step( uqc_solver* h, int n_steps, uqc_step_info* info ) {
     if( !h || n_steps < 0 ) return UQC_ERR_ARGUMENT;
+    if( h->sharded ) return fail( h, UQC_ERR_STATE, "a sharded handle steps through uqc_step_phase" );
     if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state (call uqc_init_state or uqc_upload_state)" );
     return guarded_dev( h, [&] {
         h->launches     = 0;
@@ -1756,6 +1783,7 @@ int uqc_step( uqc_solver* h, int n_steps, uqc_step_info* info ) {
 
 int uqc_run( uqc_solver* h, double t_end, uqc_step_info* info ) {
     if( !h ) return UQC_ERR_ARGUMENT;
+    if( h->sharded ) return fail( h, UQC_ERR_STATE, "a sharded handle steps through uqc_step_phase" );
     if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
     return guarded_dev( h, [&] {
         if( t_end > 0 ) {
@@ -1813,6 +1841,7 @@ void ensure_scratch( uqc_solver* h, size_t n ) {
 static void closure_on( uqc_solver* h, int n, double* d_lam, const double* d_u, const unsigned* d_nt, int* d_status, int* d_iters ) {
     KParams P     = make_params( h );
     P.nCells      = n;
+    P.nWork       = n;
     P.lam         = d_lam;
     P.u           = const_cast<double*>( d_u );
     P.level       = nullptr;
@@ -1891,6 +1920,7 @@ int uqc_closure_solve_device( uqc_solver* h, int n, double* d_lambda, const doub
 
 int uqc_step_async( uqc_solver* h, int n_steps ) {
     if( !h || n_steps < 0 ) return UQC_ERR_ARGUMENT;
+    if( h->sharded ) return fail( h, UQC_ERR_STATE, "a sharded handle steps through uqc_step_phase" );
     if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state (call uqc_init_state or uqc_upload_state)" );
     if( h->asyncPending ) return fail( h, UQC_ERR_STATE, "the previous uqc_step_async has not been queried to completion" );
     return guarded_dev( h, [&] {
@@ -1926,6 +1956,100 @@ int uqc_device_bytes( const uqc_solver* h, unsigned long long* bytes ) {
     return UQC_OK;
 }
 
+// ===================================================== spatial sharding
+
+int uqc_partition( uqc_solver* h, int rank, int n_ranks ) {
+    if( !h || n_ranks < 1 || rank < 0 || rank >= n_ranks ) return UQC_ERR_ARGUMENT;
+    if( h->deviceReady ) return fail( h, UQC_ERR_STATE, "uqc_partition must precede the first call that uses the device" );
+    if( h->sharded ) return fail( h, UQC_ERR_STATE, "the handle is already sharded" );
+    return guarded( h, [&] {
+        if( n_ranks > h->mesh.nCells ) throw ConfigError( "more ranks than cells" );
+        const std::vector<int> owner = partition_cells( h->mesh, n_ranks );
+        h->mesh    = shard_mesh( h->mesh, owner, rank, n_ranks, h->shard );
+        h->sharded = true;
+        return UQC_OK;
+    } );
+}
+
+int uqc_get_shard( const uqc_solver* h, uqc_shard_info* info, int* global_ids, int* peers, int* send_counts, int* recv_counts,
+                   int* send_cells ) {
+    if( !h || !info ) return UQC_ERR_ARGUMENT;
+    const ShardPlan& s = h->shard;
+    const bool on      = h->sharded;
+    info->rank         = on ? s.rank : 0;
+    info->n_ranks      = on ? s.nRanks : 1;
+    info->n_global     = on ? s.nGlobal : h->mesh.nCells;
+    info->n_owned      = on ? s.nOwned : h->mesh.nCells;
+    info->n_halo       = h->mesh.nCells - info->n_owned;
+    info->n_peers      = on ? int( s.peers.size() ) : 0;
+    info->n_send       = on ? int( s.sendCells.size() ) : 0;
+    info->row_doubles  = h->nS * h->tab.nQ;
+    for( int i = 0; i < h->mesh.nCells && global_ids; ++i ) global_ids[i] = on ? s.globalId[i] : i;
+    for( int p = 0; p < info->n_peers; ++p ) {
+        if( peers ) peers[p] = s.peers[p];
+        if( send_counts ) send_counts[p] = s.sendCount[p];
+        if( recv_counts ) recv_counts[p] = s.recvCount[p];
+    }
+    for( int i = 0; i < info->n_send && send_cells; ++i ) send_cells[i] = s.sendCells[i];
+    return UQC_OK;
+}
+
+int uqc_shard_buffers( uqc_solver* h, double** d_halo_rows, unsigned long long** d_dt_bits, double** d_residual ) {
+    if( !h ) return UQC_ERR_ARGUMENT;
+    return guarded_dev( h, [&] {
+        const size_t row = size_t( h->nS ) * h->tab.nQ;
+        const size_t own = size_t( h->sharded ? h->shard.nOwned : h->mesh.nCells );
+        if( d_halo_rows ) *d_halo_rows = h->d_uQ + own * row;
+        if( d_dt_bits ) *d_dt_bits = &h->d_ctl->dtBits;
+        if( d_residual ) *d_residual = &h->d_ctl->residual;
+        return UQC_OK;
+    } );
+}
+
+__global__ void k_halo_pack( const double* __restrict__ uQ, const int* __restrict__ cells, int n, int row, double* __restrict__ out ) {
+    for( int r = blockIdx.x; r < n; r += gridDim.x ) {
+        const double* src = uQ + size_t( cells[r] ) * row;
+        double* dst       = out + size_t( r ) * row;
+        for( int i = threadIdx.x; i < row; i += blockDim.x ) dst[i] = src[i];
+    }
+}
+
+int uqc_halo_pack( uqc_solver* h, double* d_send ) {
+    if( !h ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state" );
+    const int n = h->sharded ? int( h->shard.sendCells.size() ) : 0;
+    if( n == 0 ) return UQC_OK;
+    if( !d_send ) return UQC_ERR_ARGUMENT;
+    return guarded_dev( h, [&] {
+        const int row = h->nS * h->tab.nQ, grid = std::min( n, 4 * h->numSMs );
+        k_halo_pack<<<grid, 128, 0, h->stream>>>( h->d_uQ, h->d_sendCells, n, row, d_send );
+        ++h->launches;
+        CK( cudaGetLastError() );
+        return UQC_OK;
+    } );
+}
+
+int uqc_step_phase( uqc_solver* h, int phase, uqc_step_info* info ) {
+    if( !h || phase < 0 || phase > 1 ) return UQC_ERR_ARGUMENT;
+    if( !h->stateReady ) return fail( h, UQC_ERR_STATE, "no state (call uqc_init_state or uqc_upload_state)" );
+    if( h->asyncPending ) return fail( h, UQC_ERR_STATE, "a uqc_step_async is in flight" );
+    return guarded_dev( h, [&] {
+        if( phase == 0 ) h->launches = 0;
+        const int stepsBefore = h->h_ctl->steps;
+        KParams P             = make_params( h );
+        if( phase == 0 )
+            enqueue_closure_phase( h, P );
+        else
+            enqueue_update( h, P );
+        CK( cudaGetLastError() );
+        if( phase == 1 && info ) {
+            const int failed = fill_info( h, info, stepsBefore );
+            if( failed ) return fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( failed ) + " cells did not converge" );
+        }
+        return int( UQC_OK );
+    } );
+}
+
 // ===================================================== request server
 
 struct uqc_request {
@@ -1950,9 +2074,12 @@ struct uqc_request {
 struct uqc_server {
     unsigned long long budget = 0, used = 0;
     int maxActive = 1, slice = 1;
-    int policy      = 1;        // 0: every running request steps (round robin); 1: shortest remaining work first
-    int maxStepping = 4;        // policy 1: requests with a slice in flight at a time
-    double agingMs  = 1000.0;   // policy 1: waiting time that counts as much as a step of remaining work
+    int policy      = 0;        // 0: every running request steps (round robin); 1: shortest remaining time first
+    int maxStepping = 0;        // policy 1: requests with a slice in flight at a time (0: no limit)
+    double aging    = 1.0;      // policy 1: ms of remaining service time that one ms of waiting offsets
+    double workDone = 0.0;      // work of the finished slices (units of uqc_request::workPerStep)
+    double busyMs   = 0.0;      // time with requests running (between progress calls)
+    double lastPassMs = -1.0;
     long long nextId = 1;
     std::map<long long, uqc_request> reqs;
     std::deque<long long> queue;      // waiting, in submission order
@@ -2027,13 +2154,15 @@ int uqc_server_submit( uqc_server* s, const char* toml_text, int precision, long
 }
 
 namespace {
-// Priority of a request under the shortest-remaining-work policy (smaller
-// first): its estimated remaining device work, in steps of work, minus its
-// waiting time in units of agingMs (so that no request waits forever).
+// Priority of a request under the shortest-remaining-time policy (smaller
+// first), in ms: its remaining work over the server's measured rate (work of
+// finished slices per ms with requests running), minus its waiting time
+// times the aging factor, so that a request that has waited as long as its
+// remaining service time ranks with one that is about to finish.
 double priority( const uqc_server* s, const uqc_request& r, double now ) {
-    const int left  = r.horizon > 0 ? std::max( 0, r.horizon - r.steps ) : 1000;
-    const double ms = now - r.submitMs;
-    return r.workPerStep * double( left ) - r.workPerStep * ms / s->agingMs;
+    const int left    = r.horizon > 0 ? std::max( 0, r.horizon - r.steps ) : 1000;
+    const double rate = s->busyMs > 0.0 && s->workDone > 0.0 ? s->workDone / s->busyMs : 1e6;
+    return r.workPerStep * double( left ) / rate - s->aging * ( now - r.submitMs );
 }
 
 // Queues the next slice of steps of idle running requests: all of them
@@ -2052,7 +2181,7 @@ void launch_slices( uqc_server* s ) {
     }
     if( s->policy == 1 ) std::stable_sort( idle.begin(), idle.end() );
     for( auto& pr : idle ) {
-        if( s->policy == 1 && inFlight >= s->maxStepping ) break;
+        if( s->policy == 1 && s->maxStepping > 0 && inFlight >= s->maxStepping ) break;
         uqc_request& r = s->reqs[pr.second];
         const int rc   = uqc_step_async( r.h, s->slice );
         if( rc != UQC_OK ) {
@@ -2068,6 +2197,9 @@ void launch_slices( uqc_server* s ) {
 
 int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_done ) {
     if( !s ) return UQC_ERR_ARGUMENT;
+    const double pass = s->now();
+    if( s->lastPassMs >= 0.0 && !s->running.empty() ) s->busyMs += pass - s->lastPassMs;
+    s->lastPassMs = pass;
     // running requests: collect finished slices, retire finished solves
     for( size_t k = 0; k < s->running.size(); ) {
         uqc_request& r = s->reqs[s->running[k]];
@@ -2086,6 +2218,7 @@ int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_do
             }
             else {
                 r.steps += info.steps;
+                s->workDone += r.workPerStep * double( info.steps );
                 r.iters += info.newton_iterations;
                 r.t = info.t;
                 if( !info.running ) {
@@ -2152,13 +2285,13 @@ int uqc_server_set_option( uqc_server* s, const char* key, double value ) {
         return UQC_OK;
     }
     if( k == "max_stepping" ) {
-        if( value < 1 ) return sfail( s, UQC_ERR_ARGUMENT, "max_stepping must be >= 1" );
+        if( value < 0 ) return sfail( s, UQC_ERR_ARGUMENT, "max_stepping must be >= 0" );
         s->maxStepping = int( value );
         return UQC_OK;
     }
-    if( k == "aging_ms" ) {
-        if( !( value > 0 ) ) return sfail( s, UQC_ERR_ARGUMENT, "aging_ms must be > 0" );
-        s->agingMs = value;
+    if( k == "aging" ) {
+        if( !( value >= 0 ) ) return sfail( s, UQC_ERR_ARGUMENT, "aging must be >= 0" );
+        s->aging = value;
         return UQC_OK;
     }
     return sfail( s, UQC_ERR_ARGUMENT, "unknown server option '" + k + "'" );
@@ -2382,6 +2515,7 @@ extern "C" int uqc_closure_solve_device_noalloc( uqc_solver* h, int n, double* d
         KParams P      = make_params( h );
         P.wt           = tWt;
         P.nCells       = n;
+        P.nWork        = n;
         P.phi          = tPhi;
         P.phiWf        = tPhiWf;
         P.lam          = d_lambda;

@@ -41,7 +41,7 @@ class Server:
 
     def set_option(self, key: str, value: float):
         """Scheduling options of uqc_server_set_option: "policy" (0 round robin,
-        1 shortest remaining work first), "max_stepping", "aging_ms"."""
+        1 shortest remaining time first), "max_stepping" (0: no limit), "aging"."""
         self._check(self.lib.uqc_server_set_option(self.h, key.encode(), float(value)))
 
     def close(self):

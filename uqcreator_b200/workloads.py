@@ -12,6 +12,12 @@ a [uqc] table that the reference ignores and this package reads:
   precision   "fp64" (plain form) or "mixed" (tensor-core Hessian)
   newton      "reference", "guarded" or "safe" Newton (see euler2d)
   steps       stop after this many time steps (0: run to tEnd only)
+  refinementIndicator   "moments" (the code's sum of |u(0, i)|, default) or
+              "energy" (the paper's S_l) for the level rule
+  refinementBounds      [lower, upper] of the level rule (default [0.004, 0.02])
+  retardationLevels / retardationResiduals   the highest refinement level
+              allowed, raised to retardationLevels[k] once the residual has
+              fallen below retardationResiduals[k-1] (one fewer residuals)
 
 Problems and their ic parameters:
   Burgers1D       [uL, uR, x0, x1]          ramp of code/src/burgers.cpp:48-68
@@ -55,13 +61,13 @@ mesh_params = [{mesh_params}]
 precision = "{precision}"
 newton = "{newton}"
 steps = {steps}
-"""
+{uqc_extra}"""
 
 
 def make_toml(*, name, problem, closure, dim, ncells=0, a=0.0, b=1.0, sigmas, cfl, tend, degrees,
               nquad, ic, bounds=(3.0, 12.0), mesh="uniform1d", mesh_params=(0, 0, 0.0, 0),
               maxit=1000, eps=1e-10, degtype="totalDegree", precision="fp64", gamma=None,
-              newton="reference", steps=0, mesh_extra="") -> str:
+              newton="reference", steps=0, mesh_extra="", uqc_extra="") -> str:
     degrees = list(degrees)
     quads = [nquad] * len(degrees)
     extra = f"gamma = {gamma!r}\n" if gamma is not None else ""
@@ -73,7 +79,7 @@ def make_toml(*, name, problem, closure, dim, ncells=0, a=0.0, b=1.0, sigmas, cf
         maxit=int(maxit), eps=repr(float(eps)), ic=",".join(repr(float(v)) for v in ic),
         bounds=",".join(repr(float(v)) for v in bounds), mesh=mesh,
         mesh_params=",".join(repr(v) if isinstance(v, float) else str(v) for v in mesh_params),
-        precision=precision, newton=newton, steps=int(steps), mesh_extra=mesh_extra)
+        precision=precision, newton=newton, steps=int(steps), mesh_extra=mesh_extra, uqc_extra=uqc_extra)
 
 
 def burgers1d(ncells=500, tend=0.11, degree=4, nquad=20, eps=1e-10, x0=0.5, **kw) -> str:
