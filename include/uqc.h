@@ -118,6 +118,12 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *                    cell, several cells per CTA), 64 (two warps per cell,
  *                    up to four cells per CTA) or 256 (a CTA per cell);
  *                    0 = automatic.
+ *   "closure_tiny"   systems of at most 6 duals per cell (states x moments)
+ *                    on at most 64 nodes: -1 (default) / 1: the Newton of
+ *                    each cell runs in registers on one warp (sums over nodes
+ *                    by butterfly reduction, every lane solving the small
+ *                    system itself), in both precisions (FP64 arithmetic);
+ *                    0: the general closure kernel.
  *   "closure_tables_smem"  1: the closure kernels stage the basis tables in
  *                    shared memory; 0: they read them through the L1 cache
  *                    (more cells per SM); -1 = automatic.

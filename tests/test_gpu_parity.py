@@ -188,3 +188,29 @@ def test_closure_on_a_subset_with_its_own_tolerance():
     from uqcreator_b200._lib import lib, ptr
     assert lib().uqc_moments_mean_var(s.h, ptr(mv)) == 0
     np.testing.assert_array_equal(mv, s.mean_var())
+
+
+@pytest.mark.parametrize("toml,steps", [
+    (W.burgers1d(ncells=800, degree=5, nquad=24, tend=0.05), 40),           # 6 duals per cell
+    (W.shallow_water1d(ncells=600, max_degree=2, nquad=12), 40),             # 2 states x 1-3 moments, 2 levels
+    (W.burgers1d(ncells=300, degree=3, nquad=8, tend=0.05, newton="guarded"), 30),
+])
+def test_register_newton_matches_oracle_and_general_kernel(toml, steps):
+    """Systems of at most 6 duals on at most 64 nodes take the register Newton
+    (option closure_tiny, on by default there); it meets the FP64 bound against
+    the oracle and agrees with the general closure kernel."""
+    s, o = _pair(toml)
+    gk = Solver(toml)
+    gk.set_option("closure_tiny", 0)
+    gk.init_state()
+    a, b, c = s.step(steps), o.step(steps), gk.step(steps)
+    assert a["failed_cells"] == 0 and b["failures"] == 0 and c["failed_cells"] == 0
+    assert a["newton_iterations"] > 0
+    area = o.geometry()["area"]
+    err = rel_l1(s.mean_var(), o.mean_var(), area)
+    assert np.all(err <= TOL_MV), err
+    us, _, vs = s.download_state()
+    ug, _, vg = gk.download_state()
+    np.testing.assert_array_equal(vs, o.get_state()[2])
+    np.testing.assert_array_equal(vs, vg)
+    np.testing.assert_allclose(us, ug, rtol=1e-9, atol=1e-11)

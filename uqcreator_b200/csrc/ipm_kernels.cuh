@@ -548,6 +548,245 @@ out:
     return rc;
 }
 
+// Closure of a cell with at most TINY_N duals (n = NS nTj) and at most 64
+// nodes on one warp, all in registers: lane l holds nodes l and l + 32, sums
+// over nodes are butterfly reductions (every lane ends with the full sums),
+// and every lane factors and solves the n x n system itself, so an iteration
+// has no shared-memory round trip and no warp barrier. The iteration is
+// newton_cell's SolveClosure path (closure.cpp:133-193: Newton direction by
+// posv, step halving while the gradient norm grows, convergence on ||g|| <
+// eps), with the finiteness guard of newtonMode 1 and the One-Shot step of
+// maxIter == 1; SolveClosureSafe (newtonMode 2) runs newton_cell. On return
+// w.lam holds the duals and, for a converged cell, w.uk holds U at them
+// (state-major), as newton_cell leaves them.
+constexpr int TINY_N = 6;
+template <int NS> __device__ __forceinline__ constexpr int du_index( int m, int l ) {
+    // DU's packed order of the state pair (m, l), m <= l: rows m' < m first
+    int p = 0;
+    for( int a = 0; a < m; ++a ) p += NS - a;
+    return p + ( l - m );
+}
+template <int CL>
+__device__ int newton_cell_tiny( const KParams& P, const double* phi, const double* phiWf, CellWs& w, int nTj, int& iters, int& lsTrials ) {
+    constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP, TN = TINY_N, TT = TINY_N / NS, TH = TINY_N * ( TINY_N + 1 ) / 2;
+    const int lane = threadIdx.x & 31;
+    const int n    = NS * nTj;
+    const bool guard = P.newtonMode != 0;
+    iters    = 0;
+    lsTrials = 0;
+    // the lane's nodes: basis values and weights (phiWf(k, i) = phi(k, i) wt_k
+    // exactly: wt_k = w_k / 2^dimXi)
+    double ph[2][TT], wk[2];
+    bool valid[2];
+    (void)phiWf;
+#pragma unroll
+    for( int q = 0; q < 2; ++q ) {
+        const int k = lane + 32 * q;
+        valid[q]    = k < P.nQ;
+        wk[q]       = valid[q] ? P.wt[k] : 0.0;
+#pragma unroll
+        for( int i = 0; i < TT; ++i ) ph[q][i] = valid[q] && i < nTj ? phi[size_t( k ) * P.ld + i] : 0.0;
+    }
+    double lam[TN], uh[TN], g[TN], d[TN], lamN[TN], gN[TN];
+#pragma unroll
+    for( int r = 0; r < TN; ++r ) {
+        const int s = r / TT, i = r - s * TT;    // compact index r = s TT + i (TT columns per state)
+        const bool on = i < nTj;
+        lam[r] = on ? w.lam[s * P.nT + i] : 0.0;
+        uh[r]  = on ? w.uh[s * P.nT + i] : 0.0;
+        g[r] = d[r] = lamN[r] = gN[r] = 0.0;
+    }
+    // Lambda and U at the lane's nodes for the duals x; gradient into gout; returns ||g||
+    double LamA[2][NS], UA[2][NS];    // at the accepted duals
+    double LamT[2][NS], UT[2][NS];    // at the last trial
+    auto gradient_at = [&]( const double( &x )[TN], double( &Lam )[2][NS], double( &U )[2][NS], double( &gout )[TN] ) {
+        double acc[TN];
+#pragma unroll
+        for( int r = 0; r < TN; ++r ) acc[r] = 0.0;
+#pragma unroll
+        for( int q = 0; q < 2; ++q ) {
+#pragma unroll
+            for( int st = 0; st < NS; ++st ) {
+                double a = 0.0;
+#pragma unroll
+                for( int i = 0; i < TT; ++i )
+                    if( i < nTj ) a = fma( x[st * TT + i], ph[q][i], a );
+                Lam[q][st] = a;
+            }
+            if( valid[q] ) Closure<CL>::U( Lam[q], U[q], true, P.phys );
+            else {
+#pragma unroll
+                for( int st = 0; st < NS; ++st ) U[q][st] = 0.0;
+            }
+#pragma unroll
+            for( int r = 0; r < TN; ++r ) {
+                const int st = r / TT, i = r - st * TT;
+                acc[r] = fma( U[q][st], ph[q][i] * wk[q], acc[r] );
+            }
+        }
+        double sq = 0.0;
+#pragma unroll
+        for( int r = 0; r < TN; ++r ) {
+            double v = acc[r];
+#pragma unroll
+            for( int o = 16; o > 0; o >>= 1 ) v += __shfl_xor_sync( 0xffffffffu, v, o );
+            const int i = r - ( r / TT ) * TT;
+            gout[r]     = i < nTj ? v - uh[r] : 0.0;
+            sq          = fma( gout[r], gout[r], sq );
+        }
+        return sqrt( sq );
+    };
+    // Newton direction d = H^-1 g at the accepted duals (LamA); false: not positive definite
+    auto direction = [&]() {
+        double h[TH];
+#pragma unroll
+        for( int e = 0; e < TH; ++e ) h[e] = 0.0;
+#pragma unroll
+        for( int q = 0; q < 2; ++q ) {
+            double y[NP];
+            if( valid[q] ) Closure<CL>::DU( LamA[q], y, P.phys );
+            else {
+#pragma unroll
+                for( int e = 0; e < NP; ++e ) y[e] = 0.0;
+            }
+#pragma unroll
+            for( int a = 0; a < TN; ++a ) {
+                const int sa = a / TT, ia = a - sa * TT;
+#pragma unroll
+                for( int b = 0; b <= a; ++b ) {
+                    const int sb = b / TT, ib = b - sb * TT;
+                    const double du = y[du_index<NS>( sb < sa ? sb : sa, sb < sa ? sa : sb )];
+                    h[a * ( a + 1 ) / 2 + b] = fma( ph[q][ia] * ph[q][ib] * wk[q], du, h[a * ( a + 1 ) / 2 + b] );
+                }
+            }
+        }
+#pragma unroll
+        for( int e = 0; e < TH; ++e ) {
+#pragma unroll
+            for( int o = 16; o > 0; o >>= 1 ) h[e] += __shfl_xor_sync( 0xffffffffu, h[e], o );
+        }
+        // Cholesky H = L L^T in place (rows and columns of the unused states'
+        // padding are skipped), then L y = g, L^T d = y
+        bool pd = true;
+#pragma unroll
+        for( int j = 0; j < TN; ++j ) {
+            if( j - ( j / TT ) * TT >= nTj ) continue;
+            double dj = h[j * ( j + 1 ) / 2 + j];
+#pragma unroll
+            for( int k = 0; k < j; ++k )
+                if( k - ( k / TT ) * TT < nTj ) dj -= h[j * ( j + 1 ) / 2 + k] * h[j * ( j + 1 ) / 2 + k];
+            pd = pd && dj > 0.0;
+            const double ljj = sqrt( dj );
+            h[j * ( j + 1 ) / 2 + j] = ljj;
+#pragma unroll
+            for( int i = j + 1; i < TN; ++i ) {
+                if( i - ( i / TT ) * TT >= nTj ) continue;
+                double v = h[i * ( i + 1 ) / 2 + j];
+#pragma unroll
+                for( int k = 0; k < j; ++k )
+                    if( k - ( k / TT ) * TT < nTj ) v -= h[i * ( i + 1 ) / 2 + k] * h[j * ( j + 1 ) / 2 + k];
+                h[i * ( i + 1 ) / 2 + j] = v / ljj;
+            }
+        }
+        double y[TN];
+#pragma unroll
+        for( int i = 0; i < TN; ++i ) {
+            double v = g[i];
+#pragma unroll
+            for( int k = 0; k < i; ++k )
+                if( k - ( k / TT ) * TT < nTj ) v -= h[i * ( i + 1 ) / 2 + k] * y[k];
+            y[i] = i - ( i / TT ) * TT < nTj ? v / h[i * ( i + 1 ) / 2 + i] : 0.0;
+        }
+#pragma unroll
+        for( int i = TN - 1; i >= 0; --i ) {
+            double v = y[i];
+#pragma unroll
+            for( int k = i + 1; k < TN; ++k )
+                if( k - ( k / TT ) * TT < nTj ) v -= h[k * ( k + 1 ) / 2 + i] * d[k];
+            d[i] = i - ( i / TT ) * TT < nTj ? v / h[i * ( i + 1 ) / 2 + i] : 0.0;
+        }
+        return pd;
+    };
+    auto trial = [&]( double step ) {
+#pragma unroll
+        for( int r = 0; r < TN; ++r ) lamN[r] = lam[r] + -step * d[r];
+        return gradient_at( lamN, LamT, UT, gN );
+    };
+    auto accept = [&]() {
+#pragma unroll
+        for( int r = 0; r < TN; ++r ) {
+            lam[r] = lamN[r];
+            g[r]   = gN[r];
+        }
+#pragma unroll
+        for( int q = 0; q < 2; ++q )
+#pragma unroll
+            for( int st = 0; st < NS; ++st ) {
+                LamA[q][st] = LamT[q][st];
+                UA[q][st]   = UT[q][st];
+            }
+    };
+    int rc    = UQC_CELL_MAX_ITER;
+    double gn = gradient_at( lam, LamA, UA, g );
+    double gnN = 0.0;
+    if( gn < P.eps ) {
+        rc = UQC_CELL_CONVERGED;
+        goto out;
+    }
+    for( int l = 0; l < P.maxIter; ++l ) {
+        if( l != 0 ) gn = gnN;
+        if( !direction() ) {
+            rc = UQC_CELL_NOT_PD;
+            goto out;
+        }
+        ++iters;
+        if( P.maxIter == 1 ) {
+            // One-Shot IPM: lam -= H^-1 g, no line search (closure.cpp:151-154)
+            trial( 1.0 );
+            accept();
+            rc = UQC_CELL_CONVERGED;
+            goto out;
+        }
+        double stepSize = 1.0;
+        gnN             = trial( stepSize );
+        int refine      = 0;
+        while( gn < gnN || ( guard && !isfinite( gnN ) ) ) {
+            stepSize *= 0.5;
+            ++lsTrials;
+            gnN = trial( stepSize );
+            if( gnN < P.eps ) {
+                accept();
+                rc = UQC_CELL_CONVERGED;
+                goto out;
+            }
+            if( ++refine > 1000 ) {
+                rc = UQC_CELL_LINE_SEARCH;
+                goto out;
+            }
+        }
+        accept();
+        if( gnN < P.eps ) {
+            rc = UQC_CELL_CONVERGED;
+            goto out;
+        }
+    }
+out:
+#pragma unroll
+    for( int r = 0; r < TN; ++r ) {
+        const int st = r / TT, i = r - st * TT;
+        if( i < nTj && lane == r ) w.lam[st * P.nT + i] = lam[r];
+    }
+    if( rc == UQC_CELL_CONVERGED ) {
+#pragma unroll
+        for( int q = 0; q < 2; ++q )
+            if( valid[q] )
+#pragma unroll
+                for( int st = 0; st < NS; ++st ) w.uk[st * P.nQ + lane + 32 * q] = UA[q][st];
+    }
+    __syncwarp();
+    return rc;
+}
+
 // Mixed form, step mode: inexact (chord) Newton with a reused FP32 factor.
 // Same loop as newton_cell's SolveClosure path (FP64 gradient, line search,
 // convergence test), but the direction H0^-1 g comes from the factor the cell
@@ -786,7 +1025,9 @@ template <int GROUP> constexpr int closure_max_block() { return GROUP <= 64 ? 25
 // (FP32 factor not positive definite, line search or iteration limit) are
 // appended to P.fallbackList, with their last accepted duals written back,
 // for a pass of the FP64 form; they get no status or epilogue here.
-template <int CL, int GROUP, class HT>
+// TINY (GROUP 32, HT double): every cell's Newton runs in registers
+// (newton_cell_tiny; n <= TINY_N duals, <= 64 nodes, not SolveClosureSafe).
+template <int CL, int GROUP, class HT, bool TINY = false>
 __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KParams P, int mode ) {
     constexpr int NS = Closure<CL>::NS, NP = Closure<CL>::NP;
     constexpr bool MIXED = sizeof( HT ) == 4;
@@ -859,7 +1100,10 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
         else
         {
             PT_BEGIN( tn );
-            if constexpr( MIXED ) {
+            if constexpr( TINY ) {
+                rc = newton_cell_tiny<CL>( P, phi, phiWf, w, nTj, iters, ls );
+            }
+            else if constexpr( MIXED ) {
                 if( mode == 1 && P.factorStore && P.newtonMode != 2 && P.maxIter > 1 ) {
                     // reuse the cell's stored FP32 factor when it was formed for this level
                     const int nH    = int( ( hess_doubles( NS * nTj ) + 1 ) & ~size_t( 1 ) );    // floats of the tiles
@@ -1399,14 +1643,23 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         isLast        = done == gridDim.x - 1;
     }
     __syncthreads();
-    if( isLast && threadIdx.x == 0 ) {
+    double total = 0.0;
+    if( isLast && threadIdx.x < 32 ) {
         __threadfence();
-        double s = 0.0;
-        for( unsigned b = 0; b < gridDim.x; ++b ) s += ( (volatile double*)P.blockPartial )[b];
+        // the CTA partials in CTA order: the warp loads 32 at a time, lane 0
+        // adds them in sequence from the shuffles
+        for( unsigned b0 = 0; b0 < gridDim.x; b0 += 32 ) {
+            const unsigned b = b0 + threadIdx.x;
+            const double v   = b < gridDim.x ? ( (volatile double*)P.blockPartial )[b] : 0.0;
+            const unsigned m = min( 32u, gridDim.x - b0 );
+            for( unsigned j = 0; j < m; ++j ) total += __shfl_sync( 0xffffffffu, v, int( j ) );
+        }
+    }
+    if( isLast && threadIdx.x == 0 ) {
         Control* C    = P.ctl;
         C->nActive[C->steps & 1] = 0;    // this step's lists are consumed (before steps advances)
         C->nCheck[C->steps & 1]  = 0;
-        C->residual   = s;
+        C->residual   = total;
         C->dt         = dt;
         C->t          = C->t + dt;
         C->steps      = C->steps + 1;
@@ -1416,7 +1669,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         // retardation: raise the level cap as the residual falls below the thresholds
         if( P.nRet > 0 ) {
             int k = C->retIndex;
-            while( k < P.nRet && s < P.retRes[k] ) ++k;
+            while( k < P.nRet && total < P.retRes[k] ) ++k;
             C->retIndex = k;
             C->levelCap = P.retLev[k];
         }

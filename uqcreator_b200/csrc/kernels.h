@@ -21,7 +21,8 @@ enum KernelId {
     KERNEL_INVERT        = 11,   // k_invert with the Hessian on CUDA cores
     KERNEL_INVERT_SWEEP  = 12,   // k_invert_sweep (from k_hess_tc's values, n <= 84)
     KERNEL_UPDATE_WALL   = 13,   // k_update for meshes with wall cells (2-D Euler)
-    KERNEL_UPDATE_PLAIN_WALL = 14
+    KERNEL_UPDATE_PLAIN_WALL = 14,
+    KERNEL_CLOSURE_TINY      = 15    // k_closure with the register Newton of tiny systems
 };
 
 // nullptr when there is no such variant

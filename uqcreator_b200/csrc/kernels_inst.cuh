@@ -14,6 +14,7 @@ template <int CL> void* kernel_of( int group, int which ) {
             if( group == 64 ) return (void*)&k_closure<CL, 64, double>;
             if( group == 256 ) return (void*)&k_closure<CL, 256, double>;
             return nullptr;
+        case KERNEL_CLOSURE_TINY: return (void*)&k_closure<CL, 32, double, true>;
         case KERNEL_CLOSURE_MIXED:
             if( group == 32 ) return (void*)&k_closure<CL, 32, float>;
             if( group == 64 ) return (void*)&k_closure<CL, 64, float>;

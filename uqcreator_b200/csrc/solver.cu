@@ -42,6 +42,9 @@ struct uqc_solver {
     bool deviceReady        = false;
     int nS = 1, ld = 1, group = 32, numSMs = 148;
     int closureGroup = 32, closureGroupOverride = 0;    // threads per cell in k_closure (32, 64 or 256)
+    int tinyOpt = -1;                  // option closure_tiny: -1 automatic, 0 off, 1 on where it applies
+    bool closureTiny = false;          // planned: the register Newton of tiny systems (k_closure TINY)
+    int tinyGrid     = 0;
     size_t ldc = 1;
     // device buffers
     double *d_phi = nullptr, *d_phiWf = nullptr, *d_xi = nullptr;
@@ -556,6 +559,14 @@ void plan_launches( uqc_solver* h ) {
     int occ = 0;
     CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kc, h->closureBlock, h->closureSmem ) );
     h->closureGrid = std::max( 1, occ ) * h->numSMs;
+    // tiny systems (n <= TINY_N duals, <= 64 nodes): the register Newton, a warp per cell
+    h->closureTiny = h->tinyOpt != 0 && h->closureGroup == 32 && n <= size_t( TINY_N ) && nQ <= 64;
+    if( h->closureTiny ) {
+        void* kt = pick( cl, 32, KERNEL_CLOSURE_TINY );
+        allow_dynamic_smem( kt );
+        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kt, h->closureBlock, h->closureSmem ) );
+        h->tinyGrid = std::max( 1, occ ) * h->numSMs;
+    }
     // update kernel: a warp per cell; phiWf + one node-flux buffer per warp
     {
         const size_t uTables = h->tablesInSmem ? ( ( size_t( nQ ) * h->ld + 4 + 3 ) & ~size_t( 3 ) ) * sizeof( double ) : 0;
@@ -768,6 +779,15 @@ void release( uqc_solver* h ) {
 // an empty list returns at once). The work counters and the fallback list
 // length must be zero on entry (k_update resets them after every step).
 void launch_closure( uqc_solver* h, KParams& P, int mode ) {
+    if( h->closureTiny && h->cfg.newtonMode != 2 ) {
+        // tiny systems: the FP64 register Newton in both precisions (the mixed
+        // form's FP32 Hessian saves nothing at this size)
+        KParams Q      = P;
+        Q.tablesInSmem = h->closureTablesInSmem;
+        void* args[]   = {&Q, &mode};
+        launch( h, pick( h->cfg.closure, 32, KERNEL_CLOSURE_TINY ), h->tinyGrid, h->closureBlock, h->closureSmem, args );
+        return;
+    }
     if( mode == 1 && P.gStore ) {
         // the mixed form in rounds: k_chord, then per round the Hessians of
         // the listed cells (tensor cores or CUDA cores) and their inverses,
@@ -1085,6 +1105,16 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
         int v = int( value );
         if( v != 0 && v != 32 && v != 64 && v != 256 ) return fail( h, UQC_ERR_ARGUMENT, "closure_group must be 0, 32, 64 or 256" );
         h->closureGroupOverride = v;
+        if( h->deviceReady ) return guarded( h, [&] {
+                plan_launches( h );
+                return UQC_OK;
+            } );
+        return UQC_OK;
+    }
+    if( k == "closure_tiny" ) {
+        int v = int( value );
+        if( v < -1 || v > 1 ) return fail( h, UQC_ERR_ARGUMENT, "closure_tiny must be -1, 0 or 1" );
+        h->tinyOpt = v;
         if( h->deviceReady ) return guarded( h, [&] {
                 plan_launches( h );
                 return UQC_OK;
