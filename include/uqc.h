@@ -106,6 +106,47 @@ typedef struct uqc_step_info {
 int uqc_create_from_file( const char* toml_path, void* cuda_stream, uqc_solver** out, char* err, int err_len );
 /* Same, from TOML text in memory; files it names are relative to the working directory. */
 int uqc_create_from_string( const char* toml_text, void* cuda_stream, uqc_solver** out, char* err, int err_len );
+/* The same settings as a struct, for callers without a TOML file: each field
+ * is the key of the reference's input file named beside it (Settings::Init,
+ * settings.cpp:22-323) or of the [uqc] table. Strings may be NULL where the
+ * key is optional; uqc_config_defaults fills the reference's defaults. The
+ * handle is the one uqc_create_from_string makes from the equivalent file. */
+typedef struct uqc_config {
+    const char* problem;        /* [general] problem: "Burgers1D", "Euler2D", "ShallowWater1D" */
+    const char* restart_file;   /* [general] restartFile (NULL: none) */
+    int import_dual_state;      /* [general] importDualState */
+    int mesh_dimension;         /* [mesh] dimension: 1 or 2 */
+    int n_cells;                /* [mesh] numberOfCells (1-D) */
+    double a, b;                /* [mesh] a, b (1-D interval) */
+    const char* su2_file;       /* [mesh] SU2MeshFile (format "SU2"; NULL: no SU2 mesh) */
+    int n_su2_bc;               /* [mesh] SU2BC: markers and types ("dirichlet", "noslip", "swwall") */
+    const char* const* su2_bc_marker;
+    const char* const* su2_bc_type;
+    int dim_xi;                 /* [problem] distribution: dim_xi Legendre dimensions ... */
+    double sigma[4];            /* ... with these widths */
+    double cfl;                 /* [problem] CFL */
+    double t_end;               /* [problem] tEnd */
+    double min_residual;        /* [problem] residual (negative: not set) */
+    double gamma;               /* [problem] gamma (Euler; 0: default 1.4) */
+    const char* closure;        /* [moment_system] closure: "BoundedBarrier", "Euler2D", "ShallowWater" */
+    int max_degree;             /* [moment_system] moments = [["maxDegree"|"totalDegree"], [degrees]] */
+    int n_levels;               /* refinement levels: degree[0..n_levels-1] */
+    int degree[16];
+    int quad_points[16];        /* [moment_system] quadPoints = [["tensorizedGrid"], [n per level]] */
+    int max_iterations;         /* [moment_system] maxIterations */
+    double epsilon;             /* [moment_system] epsilon */
+    int n_ic;                   /* [uqc] ic */
+    double ic[8];
+    double bounds[2];           /* [uqc] bounds (bounded barrier) */
+    int nx, ny;                 /* [uqc] mesh = "tri_jitter", mesh_params = [nx, ny, jitter, seed] (nx = 0: not used) */
+    double jitter;
+    unsigned long long seed;
+    int precision;              /* [uqc] precision: uqc_precision */
+    int newton_mode;            /* [uqc] newton: 0 reference, 1 guarded, 2 safe */
+    int steps;                  /* [uqc] steps (0: to tEnd) */
+} uqc_config;
+void uqc_config_defaults( uqc_config* cfg );
+int uqc_create_from_config( const uqc_config* cfg, void* cuda_stream, uqc_solver** out, char* err, int err_len );
 void uqc_destroy( uqc_solver* h );                        /* ~MomentSolver (momentsolver.cpp:32-35) */
 const char* uqc_last_error( const uqc_solver* h );
 int uqc_get_info( const uqc_solver* h, uqc_info* out );

@@ -400,6 +400,8 @@ static void set_err( char* err, int errlen, const std::string& m ) {
     }
 }
 
+static int full_solve_files( uqcref* h, const char* prefix, double* meanVar, char* err, int errlen, bool gpu );
+
 extern "C" {
 
 // Builds settings (the reference's own Settings parser, settings.cpp:22-323),
@@ -751,6 +753,21 @@ int uqcref_full_solve( uqcref* h, double* meanVar, double* lambda15, char* err, 
 // the file sink's pattern "%Y-%m-%d %H:%M:%S.%f | %v" (restated here: main.cpp
 // is not compiled into the harness).
 int uqcref_full_solve_export( uqcref* h, const char* prefix, double* meanVar, char* err, int errlen ) {
+    return full_solve_files( h, prefix, meanVar, err, errlen, false );
+}
+
+// The same with GpuMomentSolver (oracle/ref/gpumomentsolver.cpp, linked into
+// the GPU variant of the harness only) in place of MomentSolver.
+int uqcref_full_solve_gpu( uqcref* h, const char* prefix, double* meanVar, char* err, int errlen ) {
+    return full_solve_files( h, prefix, meanVar, err, errlen, true );
+}
+
+}    // extern "C"
+
+// GpuMomentSolver(settings, mesh, problem).Solve(), defined by the GPU variant.
+extern "C" __attribute__( ( weak ) ) int uqcref_gpu_moment_solver_run( Settings*, Mesh*, Problem*, char*, int );
+
+static int full_solve_files( uqcref* h, const char* prefix, double* meanVar, char* err, int errlen, bool gpu ) {
     try {
         auto momentLog = spdlog::get( "moments" );
         auto dualLog   = spdlog::get( "duals" );
@@ -758,7 +775,13 @@ int uqcref_full_solve_export( uqcref* h, const char* prefix, double* meanVar, ch
         momentLog->lines.clear();
         dualLog->lines.clear();
         h->mesh->exported.clear();
-        {
+        if( gpu ) {
+            if( !uqcref_gpu_moment_solver_run ) throw uqc_ref_error( "this harness variant has no GpuMomentSolver" );
+            char e[512] = {0};
+            if( uqcref_gpu_moment_solver_run( h->settings.get(), h->mesh.get(), h->problem.get(), e, int( sizeof e ) ) != 0 )
+                throw uqc_ref_error( e );
+        }
+        else {
             MomentSolver solver( h->settings.get(), h->mesh.get(), h->problem.get() );
             solver.Solve();
         }
@@ -793,5 +816,3 @@ int uqcref_full_solve_export( uqcref* h, const char* prefix, double* meanVar, ch
         return -1;
     }
 }
-
-}    // extern "C"

@@ -63,6 +63,8 @@ def _lib(variant: str = "exact") -> C.CDLL:
     lib.uqcref_full_solve.argtypes = [C.c_void_p, _dp, _dp, C.c_char_p, C.c_int]
     lib.uqcref_full_solve_export.restype = C.c_int
     lib.uqcref_full_solve_export.argtypes = [C.c_void_p, C.c_char_p, _dp, C.c_char_p, C.c_int]
+    lib.uqcref_full_solve_gpu.restype = C.c_int
+    lib.uqcref_full_solve_gpu.argtypes = [C.c_void_p, C.c_char_p, _dp, C.c_char_p, C.c_int]
     _LIBS[variant] = lib
     return lib
 
@@ -183,6 +185,17 @@ class RefSolver:
         rc = self.lib.uqcref_full_solve_export(self.h, os.fsencode(prefix), _p(mv), err, 512)
         if rc != 0:
             raise RuntimeError("reference Solve: " + err.value.decode())
+        return mv.reshape(self.n_cells, 2 * self.n_states)
+
+    def full_solve_gpu(self, prefix):
+        """As full_solve_export with GpuMomentSolver (the "gpu" variant only):
+        the product's time loop behind MomentSolver's constructor and Solve(),
+        writing through the reference's Mesh::Export and loggers."""
+        mv = np.zeros(self.n_cells * 2 * self.n_states)
+        err = C.create_string_buffer(512)
+        rc = self.lib.uqcref_full_solve_gpu(self.h, os.fsencode(prefix), _p(mv), err, 512)
+        if rc != 0:
+            raise RuntimeError("GpuMomentSolver: " + err.value.decode())
         return mv.reshape(self.n_cells, 2 * self.n_states)
 
     def full_solve(self):

@@ -32,6 +32,7 @@ EXPORTS = [
     "uqc_server_request", "uqc_server_release", "uqc_server_request_error", "uqc_export_state", "uqc_write_vtk",
     "uqc_debug_mixed_inverse", "uqc_server_set_option", "uqc_solve_closure_cells", "uqc_moments_mean_var",
     "uqc_partition", "uqc_get_shard", "uqc_shard_buffers", "uqc_halo_pack", "uqc_step_phase",
+    "uqc_config_defaults", "uqc_create_from_config",
 ]
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
 NOALLOC_MAX_CELLS = 65536
@@ -48,6 +49,20 @@ class Info(C.Structure):
                 ("n_levels", C.c_int), ("dim_xi", C.c_int), ("n_faces", C.c_int), ("mesh_dim", C.c_int),
                 ("n_total_level", C.c_int * 16), ("precision", C.c_int), ("newton_mode", C.c_int),
                 ("t", C.c_double), ("steps", C.c_longlong), ("mixed_form", C.c_int), ("mixed_rounds", C.c_int)]
+
+
+class Config(C.Structure):
+    """uqc_config (include/uqc.h): the input file's keys as a struct."""
+    _fields_ = [("problem", C.c_char_p), ("restart_file", C.c_char_p), ("import_dual_state", C.c_int),
+                ("mesh_dimension", C.c_int), ("n_cells", C.c_int), ("a", C.c_double), ("b", C.c_double),
+                ("su2_file", C.c_char_p), ("n_su2_bc", C.c_int), ("su2_bc_marker", C.POINTER(C.c_char_p)),
+                ("su2_bc_type", C.POINTER(C.c_char_p)), ("dim_xi", C.c_int), ("sigma", C.c_double * 4),
+                ("cfl", C.c_double), ("t_end", C.c_double), ("min_residual", C.c_double), ("gamma", C.c_double),
+                ("closure", C.c_char_p), ("max_degree", C.c_int), ("n_levels", C.c_int), ("degree", C.c_int * 16),
+                ("quad_points", C.c_int * 16), ("max_iterations", C.c_int), ("epsilon", C.c_double), ("n_ic", C.c_int),
+                ("ic", C.c_double * 8), ("bounds", C.c_double * 2), ("nx", C.c_int), ("ny", C.c_int),
+                ("jitter", C.c_double), ("seed", C.c_ulonglong), ("precision", C.c_int), ("newton_mode", C.c_int),
+                ("steps", C.c_int)]
 
 
 class ShardInfo(C.Structure):
@@ -137,6 +152,8 @@ def lib() -> C.CDLL:
         "uqc_server_set_option": ([_vp, C.c_char_p, C.c_double], C.c_int),
         "uqc_solve_closure_cells": ([_vp, _up, C.c_int, C.c_double, C.c_int, C.POINTER(StepInfo)], C.c_int),
         "uqc_moments_mean_var": ([_vp, _dp], C.c_int),
+        "uqc_config_defaults": ([C.POINTER(Config)], None),
+        "uqc_create_from_config": ([C.POINTER(Config), _vp, C.POINTER(_vp), C.c_char_p, C.c_int], C.c_int),
         "uqc_partition": ([_vp, C.c_int, C.c_int], C.c_int),
         "uqc_get_shard": ([_vp, C.POINTER(ShardInfo), _ip, _ip, _ip, _ip, _ip], C.c_int),
         "uqc_shard_buffers": ([_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)], C.c_int),

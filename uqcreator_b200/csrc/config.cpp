@@ -6,6 +6,9 @@
 #include <sstream>
 
 #include "host.h"
+#include "uqc.h"
+
+#include <cstdio>
 
 namespace uqc {
 namespace {
@@ -314,6 +317,71 @@ Config parse_config( const std::string& text ) {
     if( c.closure == CL_EULER2D && c.meshDim != 2 ) throw ConfigError( "Euler2D needs a 2-D mesh" );
     if( c.closure != CL_EULER2D && c.meshDim != 1 ) throw ConfigError( c.problemName + " needs a 1-D mesh" );
     return c;
+}
+
+namespace {
+std::string toml_str( const char* v ) {
+    std::string out = "\"";
+    for( const char* p = v; *p; ++p ) {
+        if( *p == '"' || *p == '\\' ) out += '\\';
+        out += *p;
+    }
+    return out + "\"";
+}
+std::string toml_num( double v ) {
+    char b[40];
+    std::snprintf( b, sizeof b, "%.17g", v );
+    std::string s = b;
+    if( s.find_first_of( ".eEn" ) == std::string::npos ) s += ".0";    // a float, not an integer
+    return s;
+}
+}    // namespace
+
+std::string config_struct_to_toml( const void* p ) {
+    const uqc_config& c = *static_cast<const uqc_config*>( p );
+    if( !c.problem || !c.closure ) throw ConfigError( "uqc_config: problem and closure are required" );
+    if( c.n_levels < 1 || c.n_levels > 16 ) throw ConfigError( "uqc_config: n_levels must be 1..16" );
+    if( c.dim_xi < 1 || c.dim_xi > 3 ) throw ConfigError( "uqc_config: dim_xi must be 1..3" );
+    if( c.n_ic < 0 || c.n_ic > 8 ) throw ConfigError( "uqc_config: n_ic must be 0..8" );
+    std::string t;
+    t += "[general]\nproblem = " + toml_str( c.problem ) + "\n";
+    if( c.restart_file ) {
+        t += "restartFile = " + toml_str( c.restart_file ) + "\n";
+        t += std::string( "importDualState = " ) + ( c.import_dual_state ? "true" : "false" ) + "\n";
+    }
+    t += "\n[mesh]\ndimension = " + std::to_string( c.mesh_dimension ) + "\n";
+    if( c.mesh_dimension == 1 ) t += "numberOfCells = " + std::to_string( c.n_cells ) + "\na = " + toml_num( c.a ) + "\nb = " + toml_num( c.b ) + "\n";
+    if( c.su2_file ) {
+        t += "format = \"SU2\"\nSU2MeshFile = " + toml_str( c.su2_file ) + "\nSU2BC = [";
+        for( int i = 0; i < c.n_su2_bc; ++i ) {
+            if( !c.su2_bc_marker || !c.su2_bc_type || !c.su2_bc_marker[i] || !c.su2_bc_type[i] ) throw ConfigError( "uqc_config: SU2 marker or type missing" );
+            t += std::string( i ? ", " : "" ) + "[" + toml_str( c.su2_bc_marker[i] ) + ", " + toml_str( c.su2_bc_type[i] ) + "]";
+        }
+        t += "]\n";
+    }
+    t += "\n[problem]\ntimestepping = \"explicitEuler\"\ndistribution = [[";
+    for( int l = 0; l < c.dim_xi; ++l ) t += std::string( l ? ", " : "" ) + "\"Legendre\"";
+    t += "], [";
+    for( int l = 0; l < c.dim_xi; ++l ) t += std::string( l ? ", " : "" ) + toml_num( c.sigma[l] );
+    t += "]]\nCFL = " + toml_num( c.cfl ) + "\ntEnd = " + toml_num( c.t_end ) + "\n";
+    if( c.min_residual >= 0.0 ) t += "residual = " + toml_num( c.min_residual ) + "\n";
+    if( c.gamma > 0.0 ) t += "gamma = " + toml_num( c.gamma ) + "\n";
+    t += "\n[moment_system]\nclosure = " + toml_str( c.closure ) + "\nmoments = [[" + std::string( c.max_degree ? "\"maxDegree\"" : "\"totalDegree\"" ) + "], [";
+    for( int l = 0; l < c.n_levels; ++l ) t += std::string( l ? ", " : "" ) + std::to_string( c.degree[l] );
+    t += "]]\nquadPoints = [[\"tensorizedGrid\"], [";
+    for( int l = 0; l < c.n_levels; ++l ) t += std::string( l ? ", " : "" ) + std::to_string( c.quad_points[l] );
+    t += "]]\nmaxIterations = " + std::to_string( c.max_iterations ) + "\nepsilon = " + toml_num( c.epsilon ) + "\n";
+    t += "\n[uqc]\nic = [";
+    for( int i = 0; i < c.n_ic; ++i ) t += std::string( i ? ", " : "" ) + toml_num( c.ic[i] );
+    t += "]\nbounds = [" + toml_num( c.bounds[0] ) + ", " + toml_num( c.bounds[1] ) + "]\n";
+    if( c.nx > 0 )
+        t += "mesh = \"tri_jitter\"\nmesh_params = [" + std::to_string( c.nx ) + ", " + std::to_string( c.ny ) + ", " + toml_num( c.jitter ) + ", " +
+             std::to_string( c.seed ) + "]\n";
+    t += std::string( "precision = " ) + ( c.precision == 1 ? "\"mixed\"" : "\"fp64\"" ) + "\n";
+    if( c.newton_mode < 0 || c.newton_mode > 2 ) throw ConfigError( "uqc_config: newton_mode must be 0, 1 or 2" );
+    static const char* modes[] = {"reference", "guarded", "safe"};
+    t += std::string( "newton = \"" ) + modes[c.newton_mode] + "\"\nsteps = " + std::to_string( c.steps ) + "\n";
+    return t;
 }
 
 }    // namespace uqc

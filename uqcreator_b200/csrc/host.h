@@ -64,6 +64,9 @@ struct Config {
 
 Config parse_config( const std::string& tomlText );
 
+// The input file equivalent to a uqc_config struct (include/uqc.h).
+std::string config_struct_to_toml( const void* uqcConfig );
+
 // Basis and quadrature: tensor Gauss-Legendre grid and scaled Legendre basis
 // tables phiTilde / phiTildeWf of Closure::Closure (closure.cpp:16-84).
 struct Tables {

@@ -1025,6 +1025,35 @@ int uqc_create_from_string( const char* toml_text, void* cuda_stream, uqc_solver
     return create_impl( toml_text, ".", cuda_stream, out, err, err_len );
 }
 
+void uqc_config_defaults( uqc_config* c ) {
+    if( !c ) return;
+    std::memset( c, 0, sizeof( *c ) );
+    c->mesh_dimension = 1;
+    c->dim_xi         = 1;
+    c->min_residual   = -1.0;
+    c->n_levels       = 1;
+    c->max_iterations = 1000;    // settings.cpp: maxIterations default
+    c->epsilon        = 5e-5;    // settings.cpp: epsilon default
+    c->bounds[0]      = 3.0;
+    c->bounds[1]      = 12.0;
+}
+
+int uqc_create_from_config( const uqc_config* cfg, void* cuda_stream, uqc_solver** out, char* err, int err_len ) {
+    if( !cfg || !out ) return UQC_ERR_ARGUMENT;
+    *out = nullptr;
+    std::string text;
+    try {
+        text = config_struct_to_toml( cfg );
+    } catch( const std::exception& e ) {
+        if( err && err_len > 0 ) {
+            std::strncpy( err, e.what(), size_t( err_len - 1 ) );
+            err[err_len - 1] = 0;
+        }
+        return UQC_ERR_CONFIG;
+    }
+    return create_impl( text.c_str(), ".", cuda_stream, out, err, err_len );
+}
+
 int uqc_create_from_file( const char* toml_path, void* cuda_stream, uqc_solver** out, char* err, int err_len ) {
     if( !toml_path || !out ) return UQC_ERR_ARGUMENT;
     std::ifstream f( toml_path );

@@ -87,6 +87,27 @@ class Solver:
         self.n_levels, self.dim_xi, self.n_faces = info.n_levels, info.dim_xi, info.n_faces
         self.n_total_levels = list(info.n_total_level)[: info.n_levels]
 
+    @classmethod
+    def from_config(cls, cfg, stream=None) -> "Solver":
+        """A solver from a uqc_config struct (uqcreator_b200._lib.Config) instead
+        of an input file (uqc_create_from_config)."""
+        self = cls.__new__(cls)
+        self.settings = None
+        self.lib = L.lib()
+        h = C.c_void_p()
+        err = C.create_string_buffer(1024)
+        s = None if stream is None else C.c_void_p(int(stream))
+        rc = self.lib.uqc_create_from_config(C.byref(cfg), s, C.byref(h), err, 1024)
+        if rc != 0:
+            raise UqcError(rc, err.value.decode())
+        self.h = h
+        info = Info()
+        check(h, self.lib.uqc_get_info(h, C.byref(info)))
+        self.n_cells, self.n_states, self.n_total, self.n_quad = info.n_cells, info.n_states, info.n_total, info.n_quad
+        self.n_levels, self.dim_xi, self.n_faces = info.n_levels, info.dim_xi, info.n_faces
+        self.n_total_levels = list(info.n_total_level)[: info.n_levels]
+        return self
+
     def form(self):
         """Precision in use and how UQC_MIXED steps run the closure (uqc_info:
         mixed_form 0 single kernel, 1 rounds with the CUDA-core Hessian, 2 with
