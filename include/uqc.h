@@ -159,6 +159,10 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *                    cell, several cells per CTA), 64 (two warps per cell,
  *                    up to four cells per CTA) or 256 (a CTA per cell);
  *                    0 = automatic.
+ *   "update_warps", "check_warps", "chord_warps"  warps (cells) per CTA of
+ *                    the update kernel (default 8), the convergence-check
+ *                    kernel (default 16) and the mixed form's chord kernel
+ *                    (default 16), each capped by shared memory; 0 = default.
  *   "closure_tiny"   systems of at most 6 duals per cell (states x moments)
  *                    on at most 64 nodes: -1 (default) / 1: the Newton of
  *                    each cell runs in registers on one warp (sums over nodes

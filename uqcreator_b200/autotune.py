@@ -1,21 +1,26 @@
-"""Autotuner of the closure's launch shapes and schedule.
+"""Autotuner of the time step's launch shapes and schedules.
 
-FP64 form: the closure kernel can run a cell on one warp, two warps (several
-cells per CTA, named barriers) or a whole CTA, and can stage the basis tables
-in shared memory or read them through L1 (which leaves room for more cells per
-SM). Mixed form in rounds (2-D Euler): the chord schedule decides how often a
-cell's held inverse is re-formed (re-factor after a step with the held
-inverse that reduced ||g|| by less than 1/theta; more re-factorisations mean
-fewer, dearer iterations) and how many re-factorisation rounds a step runs
-before the FP64 form takes the remaining cells.
+What it chooses, per configuration shape:
+- closure (FP64 form): a cell on one warp, two warps (several cells per CTA,
+  named barriers) or a whole CTA, with the basis tables staged in shared memory
+  or read through L1 (which leaves room for more cells per SM);
+- chord schedule (mixed form in rounds, 2-D Euler): theta, the contraction
+  below which a cell's held inverse is re-formed (more re-factorisations mean
+  fewer, dearer iterations), and the re-factorisation rounds per step before
+  the FP64 form takes the remaining cells;
+- CTA sizes: cells (warps) per CTA of the chord kernel, the convergence-check
+  kernel and the update kernel (occupancy against shared memory and
+  registers, and the grain of the work stealing).
 
 Which is fastest depends on the moments per cell, the node count, the
-precision and the state. `autotune(solver)` times every candidate on a few
-time steps of the solver's own state (after untimed warm-up steps, so held
-inverses are in their steady state), restores the state, applies the fastest
-through uqc_set_option and returns the timings. Results are cached per
-configuration shape (states, moments, nodes, levels, uncertain dimensions,
-precision, mixed form) in a JSON file, so a shape is tuned once per machine.
+precision and the state. `autotune(solver)` times the candidates on a few time
+steps of the solver's own state (after untimed warm-up steps, so held inverses
+are in their steady state) by coordinate descent: the groups above in turn,
+each candidate with the best of the groups before it applied. It restores the
+state, applies the best options through uqc_set_option and returns the
+timings. Results are cached per configuration shape (states, moments, nodes,
+levels, uncertain dimensions, precision, mixed form) in a JSON file, so a shape
+is tuned once per machine.
 
     s = Solver(toml); s.init_state(); s.step(3)     # tune on a representative state
     best = autotune(s)
@@ -29,7 +34,7 @@ from pathlib import Path
 
 from ._lib import UqcError, Info, lib, check
 
-__all__ = ["autotune", "candidates", "DEFAULT_CACHE"]
+__all__ = ["autotune", "candidates", "groups", "DEFAULT_CACHE"]
 
 DEFAULT_CACHE = Path(os.environ.get("UQC_AUTOTUNE_CACHE", Path.home() / ".cache" / "uqcreator_b200" / "autotune.json"))
 
@@ -39,7 +44,7 @@ ROUNDS = (2, 3)
 
 
 def candidates(n_per_cell: int, mixed_form: int = 0):
-    """Options worth timing: launch shapes of the FP64 closure kernel for
+    """Options of the first group: launch shapes of the FP64 closure kernel for
     n = states x moments duals per cell, or (mixed form in rounds) the chord
     schedule: theta x re-factorisation rounds."""
     if mixed_form >= 1:
@@ -48,17 +53,19 @@ def candidates(n_per_cell: int, mixed_form: int = 0):
     return [{"closure_group": g, "closure_tables_smem": t} for g in groups for t in (1, 0)]
 
 
-def _key(solver, precision, mixed_form):
-    return (f"s{solver.n_states}_t{solver.n_total}_q{solver.n_quad}_l{solver.n_levels}_d{solver.dim_xi}_p{precision}"
-            f"_m{mixed_form if precision else 0}")
-
-
-def _parse(name):
-    out = {}
-    for kv in name.split(","):
-        k, v = kv.split("=")
-        out[k] = float(v) if "." in v else int(v)
+def groups(n_per_cell: int, mixed_form: int = 0):
+    """The option groups of the coordinate descent, in order: (name, candidates)."""
+    out = [("closure" if mixed_form == 0 else "schedule", candidates(n_per_cell, mixed_form))]
+    if mixed_form >= 1:
+        out.append(("chord_cta", [{"chord_warps": w} for w in (8, 12, 16)]))
+    out.append(("check_cta", [{"check_warps": w} for w in (8, 16)]))
+    out.append(("update_cta", [{"update_warps": w} for w in (4, 8, 16)]))
     return out
+
+
+def _key(solver, precision, mixed_form):
+    return (f"v2_s{solver.n_states}_t{solver.n_total}_q{solver.n_quad}_l{solver.n_levels}_d{solver.dim_xi}_p{precision}"
+            f"_m{mixed_form if precision else 0}")
 
 
 def autotune(solver, steps: int = 2, repeats: int = 2, cache: Path | None = DEFAULT_CACHE, verbose: bool = False,
@@ -85,31 +92,41 @@ def autotune(solver, steps: int = 2, repeats: int = 2, cache: Path | None = DEFA
     u0, l0, v0 = solver.download_state()
     t0 = info.t
     timings = {}
-    for opts in candidates(solver.n_states * solver.n_total, mixed_form):
-        name = ",".join(f"{k}={v}" for k, v in opts.items())
-        try:
-            for k, v in opts.items():
-                solver.set_option(k, v)
-            best_ms = None
-            for _ in range(repeats):
-                solver.upload_state(u0, l0, v0, t=t0)
-                if warmup:
-                    solver.step(warmup)
-                solver.step(steps)
-                ms = solver.last_timing()[2] / steps
-                best_ms = ms if best_ms is None or ms < best_ms else best_ms
-            timings[name] = best_ms
-        except UqcError as e:    # a shape that does not fit this configuration
-            timings[name] = None
+    best = {}
+
+    def time_options(opts):
+        for k, v in opts.items():
+            solver.set_option(k, v)
+        best_ms = None
+        for _ in range(repeats):
+            solver.upload_state(u0, l0, v0, t=t0)
+            if warmup:
+                solver.step(warmup)
+            solver.step(steps)
+            ms = solver.last_timing()[2] / steps
+            best_ms = ms if best_ms is None or ms < best_ms else best_ms
+        return best_ms
+
+    for gname, cands in groups(solver.n_states * solver.n_total, mixed_form):
+        group_best, group_ms = None, None
+        for opts in cands:
+            name = ",".join(f"{k}={v}" for k, v in opts.items())
+            try:
+                ms = time_options(opts)
+            except UqcError as e:    # a shape that does not fit this configuration
+                ms = None
+                if verbose:
+                    print("autotune: skip", name, e)
+            timings[name] = ms
             if verbose:
-                print("autotune: skip", name, e)
-        if verbose:
-            print("autotune:", name, timings[name])
-    valid = {k: v for k, v in timings.items() if v is not None}
-    if not valid:
-        raise UqcError(-2, "no launch shape fits this configuration")
-    best_name = min(valid, key=valid.get)
-    best = _parse(best_name)
+                print("autotune:", gname, name, ms)
+            if ms is not None and (group_ms is None or ms < group_ms):
+                group_best, group_ms = opts, ms
+        if group_best is None:
+            raise UqcError(-2, f"no {gname} option fits this configuration")
+        best.update(group_best)
+        for k, v in group_best.items():
+            solver.set_option(k, v)
     for k, v in best.items():
         solver.set_option(k, v)
     solver.upload_state(u0, l0, v0, t=t0)

@@ -43,6 +43,8 @@ struct uqc_solver {
     int nS = 1, ld = 1, group = 32, numSMs = 148;
     int closureGroup = 32, closureGroupOverride = 0;    // threads per cell in k_closure (32, 64 or 256)
     int tinyOpt = -1;                  // option closure_tiny: -1 automatic, 0 off, 1 on where it applies
+    int updateWarpsOpt = 0, checkWarpsOpt = 0, chordWarpsOpt = 0;    // options update_warps, check_warps, chord_warps (0: automatic)
+    int blockPartialCap = 0;           // doubles in d_blockPartial
     bool closureTiny = false;          // planned: the register Newton of tiny systems (k_closure TINY)
     int tinyGrid     = 0;
     size_t ldc = 1;
@@ -383,7 +385,7 @@ void plan_rounds( uqc_solver* h, int maxSmem ) {
     const size_t ws     = chord_ws_doubles( nS, nT, nQ ) * sizeof( double );
     h->chordTablesInSmem = tables <= 96 * 1024 && tables + 8 * ws <= size_t( maxSmem );
     const size_t avail   = size_t( maxSmem ) - ( h->chordTablesInSmem ? tables : 0 );
-    const int warps      = int( std::min<size_t>( 16, avail / ws ) );
+    const int warps      = int( std::min<size_t>( h->chordWarpsOpt ? h->chordWarpsOpt : 16, avail / ws ) );
     if( warps < 1 ) {
         h->v2Why = "chord workspace exceeds shared memory";
         return;
@@ -571,7 +573,7 @@ void plan_launches( uqc_solver* h ) {
     {
         const size_t uTables = h->tablesInSmem ? ( ( size_t( nQ ) * h->ld + 4 + 3 ) & ~size_t( 3 ) ) * sizeof( double ) : 0;
         const size_t perWarp = update_warp_doubles( nS, nQ ) * sizeof( double );
-        const int warps      = int( std::min<size_t>( 8, ( size_t( maxSmem ) - uTables ) / perWarp ) );
+        const int warps      = int( std::min<size_t>( h->updateWarpsOpt ? h->updateWarpsOpt : 8, ( size_t( maxSmem ) - uTables ) / perWarp ) );
         if( warps < 1 ) throw ConfigError( "update workspace exceeds shared memory" );
         h->updateBlock = 32 * warps;
         h->updateSmem  = uTables + size_t( warps ) * perWarp;
@@ -582,6 +584,13 @@ void plan_launches( uqc_solver* h ) {
         CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ku, h->updateBlock, h->updateSmem ) );
         h->updateGrid = std::max( 1, occ ) * h->numSMs;
         h->updateGrid = std::min( h->updateGrid, std::max( 1, ( h->mesh.nCells + warps - 1 ) / warps ) );
+        // one residual partial per CTA of k_update (grows with the grid; a
+        // re-plan waits for the device in cudaFree before replacing it)
+        if( h->updateGrid > h->blockPartialCap ) {
+            if( h->d_blockPartial ) cudaFree( h->d_blockPartial );
+            h->d_blockPartial  = dalloc<double>( size_t( h->updateGrid ) );
+            h->blockPartialCap = h->updateGrid;
+        }
     }
     const int ug = h->auxBlock / h->group;    // groups per CTA of the init / mean-variance kernels
     h->initSmem   = size_t( ug ) * ( size_t( nS ) * nQ + 8 ) * sizeof( double );
@@ -596,7 +605,7 @@ void plan_launches( uqc_solver* h ) {
     {
         const size_t wsc = check_ws_doubles( nS, nT, nQ ) * sizeof( double );
         const size_t av  = size_t( maxSmem ) - ( h->tablesInSmem ? tables : 0 );
-        const int warps  = int( std::min<size_t>( 16, av / wsc ) );
+        const int warps  = int( std::min<size_t>( h->checkWarpsOpt ? h->checkWarpsOpt : 16, av / wsc ) );
         if( warps < 1 ) throw ConfigError( "check workspace exceeds shared memory" );
         h->checkBlock = 32 * warps;
         h->checkSmem  = wsc * warps + ( h->tablesInSmem ? tables : 0 );
@@ -749,7 +758,6 @@ void ensure_device( uqc_solver* h ) {
     plan_launches( h );
     if( h->precision == UQC_MIXED && !h->mixedOk ) throw ConfigError( "mixed precision not available for this configuration: " + h->mixedWhy );
     if( h->precision == UQC_MIXED && h->chord ) reset_factor_store( h );
-    h->d_blockPartial = dalloc<double>( std::max( h->updateGrid, 1 ) );
     h->deviceReady = true;
     reset_control( h, 0.0 );
 }
@@ -1134,6 +1142,16 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
         int v = int( value );
         if( v != 0 && v != 32 && v != 64 && v != 256 ) return fail( h, UQC_ERR_ARGUMENT, "closure_group must be 0, 32, 64 or 256" );
         h->closureGroupOverride = v;
+        if( h->deviceReady ) return guarded( h, [&] {
+                plan_launches( h );
+                return UQC_OK;
+            } );
+        return UQC_OK;
+    }
+    if( k == "update_warps" || k == "check_warps" || k == "chord_warps" ) {
+        int v = int( value );
+        if( v < 0 || v > 16 ) return fail( h, UQC_ERR_ARGUMENT, k + " must be 0 (automatic) or 1..16" );
+        ( k == "update_warps" ? h->updateWarpsOpt : k == "check_warps" ? h->checkWarpsOpt : h->chordWarpsOpt ) = v;
         if( h->deviceReady ) return guarded( h, [&] {
                 plan_launches( h );
                 return UQC_OK;
