@@ -184,8 +184,19 @@ Config parse_config( const std::string& text ) {
         c.closure = CL_EULER2D;
     else if( cl == "ShallowWater" )
         c.closure = CL_SHALLOW_WATER;
+    else if( cl == "StochasticGalerkin" || cl == "L2Filter" || cl == "LassoFilter" ) {
+        // the linear closures take the states of the problem
+        c.closure    = c.problem == PR_BURGERS ? CL_LINEAR_BURGERS : ( c.problem == PR_EULER2D ? CL_LINEAR_EULER2D : CL_LINEAR_SW );
+        c.filterKind = cl == "StochasticGalerkin" ? FILTER_SG : ( cl == "L2Filter" ? FILTER_L2 : FILTER_LASSO );
+    }
+    else if( cl == "ExponentialFilter" )
+        // exponentialfilter.cpp:4-20 reads the filter order (never set) and the
+        // time step (set only after the closure is built, momentsolver.cpp:18-24):
+        // its factors are undefined, so there is nothing to reproduce
+        throw ConfigError( "[moment_system] 'closure' = 'ExponentialFilter': the reference's filter reads an uninitialised order and time step" );
     else
-        throw ConfigError( "[moment_system] 'closure' = '" + cl + "' is not on this hot path (BoundedBarrier, Euler2D, ShallowWater)" );
+        throw ConfigError( "[moment_system] 'closure' = '" + cl +
+                           "' is not on this hot path (BoundedBarrier, Euler2D, ShallowWater, StochasticGalerkin, L2Filter, LassoFilter, ExponentialFilter)" );
     const Value& mom = need( d, "moment_system", "moments" );
     if( mom.kind != Value::ARR || mom.items.size() != 2 ) throw ConfigError( "[moment_system] 'moments' must be [[type],[degrees]]" );
     std::string degType = str( mom.items[0].items.at( 0 ), "moments type" );
@@ -203,7 +214,7 @@ Config parse_config( const std::string& text ) {
     if( const Value* v = find( d, "moment_system", "maxIterations" ) ) c.maxIterations = int( v->num() );
     if( const Value* v = find( d, "moment_system", "epsilon" ) ) c.epsilon = v->num();
     // closure / problem consistency (the reference pairs them in Problem::Create)
-    int nS = c.closure == CL_BOUNDED_BARRIER ? 1 : ( c.closure == CL_EULER2D ? 4 : 2 );
+    int nS = closure_states( c.closure );
     int nSp = c.problem == PR_BURGERS ? 1 : ( c.problem == PR_EULER2D ? 4 : 2 );
     if( nS != nSp ) throw ConfigError( "closure '" + cl + "' does not match problem '" + c.problemName + "'" );
     // [uqc]
@@ -314,8 +325,8 @@ Config parse_config( const std::string& text ) {
     }
     else
         throw ConfigError( "[mesh] 'dimension' must be 1 or 2" );
-    if( c.closure == CL_EULER2D && c.meshDim != 2 ) throw ConfigError( "Euler2D needs a 2-D mesh" );
-    if( c.closure != CL_EULER2D && c.meshDim != 1 ) throw ConfigError( c.problemName + " needs a 1-D mesh" );
+    if( c.problem == PR_EULER2D && c.meshDim != 2 ) throw ConfigError( "Euler2D needs a 2-D mesh" );
+    if( c.problem != PR_EULER2D && c.meshDim != 1 ) throw ConfigError( c.problemName + " needs a 1-D mesh" );
     return c;
 }
 

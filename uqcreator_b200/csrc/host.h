@@ -14,7 +14,13 @@ struct ConfigError : public std::runtime_error {
     explicit ConfigError( const std::string& m ) : std::runtime_error( m ) {}
 };
 
-enum ClosureKind { CL_BOUNDED_BARRIER = 0, CL_EULER2D = 1, CL_SHALLOW_WATER = 2 };
+// Kernel closure kinds. 3-5: the linear closures (stochastic Galerkin and the
+// moment filters, Config::filterKind) with the states of Burgers, 2-D Euler and
+// shallow water.
+enum ClosureKind { CL_BOUNDED_BARRIER = 0, CL_EULER2D = 1, CL_SHALLOW_WATER = 2, CL_LINEAR_BURGERS = 3, CL_LINEAR_EULER2D = 4, CL_LINEAR_SW = 5 };
+enum FilterKind { FILTER_SG = 0, FILTER_L2 = 1, FILTER_LASSO = 2 };
+inline int closure_states( int cl ) { return ( cl == 0 || cl == 3 ) ? 1 : ( ( cl == 1 || cl == 4 ) ? 4 : 2 ); }
+inline bool closure_linear( int cl ) { return cl >= CL_LINEAR_BURGERS; }
 enum ProblemKind { PR_BURGERS = 0, PR_EULER2D = 1, PR_SHALLOW_WATER = 2 };
 
 // Everything the hot path reads from the input file. Keys and defaults follow
@@ -35,6 +41,7 @@ struct Config {
     double cfl = 0.0, tEnd = 0.0, minResidual = -1.0, gamma = 1.4;
     // [moment_system]
     ClosureKind closure = CL_BOUNDED_BARRIER;
+    int filterKind      = FILTER_SG;    // linear closures: which one (closure names of settings.cpp:176-205)
     bool maxDegree = false;
     std::vector<int> degrees;    // per refinement level
     int nQuad = 0;               // Gauss nodes per dimension (last level)

@@ -88,6 +88,12 @@ struct KParams {
     int nRet;                 // residual thresholds of the retardation schedule (0: none)
     double retRes[8];
     int retLev[9];
+    // linear closures (kinds 3-5): 0 stochastic Galerkin (factors 1 in filter),
+    // 1 L2 filter (factors in filter), 2 Lasso filter
+    int filterKind;
+    const double* filter;        // nT factors
+    const double* lassoParam;    // nT: prod_l index_l (index_l + 1)
+    const double* lassoL1;       // nT: sum_k |phiWf(k, i)|
     int nCells, nFaces, dimXi;
     int nWork;                // cells a time step works on: the first nWork (a shard's owned cells), else nCells
     double eps;
@@ -906,6 +912,29 @@ out:
 
 // ------------------------------------------------------------------ kernels
 
+// Duals of a linear closure from the moments (state-major, finest stride nT):
+// lambda(s, i) = f_i u(s, i) for stochastic Galerkin (f = 1) and the L2
+// filter (l2filter.cpp:29-35); the Lasso filter (lassofilter.cpp:36-47) scales by
+// 1 - strength_s p_i l1_i / |u(s, i)|, cut to 0 below 0 or for |u(s, i)| <
+// 1e-7, strength_s = |u(s, nT-1)| / (p_{nT-1} l1_{nT-1}), in the reference's
+// operation order. Every moment of the finest level, as the reference loops
+// over GetNTotal() whatever the cell's level.
+template <int NS, int GROUP> __device__ void linear_duals( const Grp<GROUP>& g, const KParams& P, const double* uh, double* lam ) {
+    const int nT = P.nT;
+    for( int idx = g.r; idx < NS * nT; idx += GROUP ) {
+        const int s = idx / nT, i = idx - s * nT;
+        if( P.filterKind == 2 ) {
+            const int nMax         = nT - 1;
+            const double strength  = fabs( uh[s * nT + nMax] ) / ( P.lassoParam[nMax] * P.lassoL1[nMax] );
+            double sc              = 1.0 - strength * P.lassoParam[i] * P.lassoL1[i] / fabs( uh[idx] );
+            if( sc < 0 || fabs( uh[idx] ) < 1e-7 ) sc = 0.0;
+            lam[idx] = sc * uh[idx];
+        }
+        else
+            lam[idx] = P.filter[i] * uh[idx];
+    }
+}
+
 // Refinement indicator of a cell at level lev (nTj moments) from its first
 // state's moments at(i): the sum of |u(0, i)| over the moments the level adds
 // (the last two in one uncertain dimension) of MomentSolver::ComputeRefIndicator
@@ -1100,7 +1129,12 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
         else
         {
             PT_BEGIN( tn );
-            if constexpr( TINY ) {
+            if constexpr( Closure<CL>::LINEAR ) {
+                linear_duals<NS, GROUP>( g, P, w.uh, w.lam );
+                g.sync();
+                rc = UQC_CELL_CONVERGED;
+            }
+            else if constexpr( TINY ) {
                 rc = newton_cell_tiny<CL>( P, phi, phiWf, w, nTj, iters, ls );
             }
             else if constexpr( MIXED ) {
@@ -1169,7 +1203,7 @@ __global__ void __launch_bounds__( closure_max_block<GROUP>(), 1 ) k_closure( KP
             // was at the accepted duals, so w.uk already holds U there (the
             // U(Vector&) form; the reference reconstructs with U(const Matrix&),
             // which for the Euler closure differs in the last bits only).
-            if( rc != 0 ) {
+            if( rc != 0 || Closure<CL>::LINEAR ) {
                 eval_lambda<NS, GROUP>( g, P, phi, w.lam, nTj, w.LA );
                 g.sync();
                 eval_u<CL, GROUP>( g, P, w.LA, w.uk, true );
@@ -1254,6 +1288,15 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
         __syncwarp();
         CT_END( tload, 16, g.r == 0 );
         bool converged = false;
+        if constexpr( Closure<CL>::LINEAR ) {
+            // the duals come from the moments: no test, every cell finishes here
+            if( !bad ) {
+                linear_duals<NS, 32>( g, P, uh, lam );
+                __syncwarp();
+                for( int idx = g.r; idx < int( ldc ); idx += 32 ) P.lam[cell * ldc + idx] = lam[idx];
+                converged = true;
+            }
+        }
         if( !bad ) {
             CT_BEGIN( tlu );
             // U(Lambda_k) at every node, Lambda_k in registers (closure.cpp:205-213, 234-253)
@@ -1274,6 +1317,7 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
             __syncwarp();
             CT_END( tlu, 17, g.r == 0 );
             CT_BEGIN( tgr );
+            if constexpr( !Closure<CL>::LINEAR ) {
             const double sq = gradient_sums<NS, 32>( g, P, phiWf, uk, uh, nTj, nullptr, ugs );
             const double gn = sqrt( group_sum<32>( g, sq, red ) );
             converged       = gn < P.eps;
@@ -1286,6 +1330,7 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
                 }
                 if( g.r == 0 ) gs[ldc] = gn;
             }
+            }
             CT_END( tgr, 18, g.r == 0 );
         }
         if( converged ) {
@@ -1295,7 +1340,7 @@ template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) 
             }
             __syncwarp();
             CT_BEGIN( tep );
-            const double d = cell_epilogue<CL, 32>( g, P, phiWf, uh, uk, cell, lev, nTj, red, ugs );
+            const double d = cell_epilogue<CL, 32>( g, P, phiWf, uh, uk, cell, lev, nTj, red, Closure<CL>::LINEAR ? nullptr : ugs );
             dtMin          = d < dtMin ? d : dtMin;
             CT_END( tep, 19, g.r == 0 );
         }
@@ -1465,7 +1510,7 @@ __global__ void __launch_bounds__( 256, 2 ) k_update( KParams P ) {
         bool ghost[3];
         // wall cells (Euler 2-D): faces without a neighbour see the cell's own
         // states reflected at the boundary normal (expliciteuler.cpp:24-70)
-        const bool wall = WALL && CL == 1 && bc >= 2;
+        const bool wall = WALL && NS == 4 && bc >= 2;
         double bn[2]    = {0.0, 0.0};
         if( wall ) {
             bn[0] = P.bndNormal[2 * cell];

@@ -29,5 +29,6 @@ enum KernelId {
 void* kernel_bounded_barrier( int group, int which );
 void* kernel_euler2d( int group, int which );
 void* kernel_shallow_water( int group, int which );
+void* kernel_linear( int cl, int group, int which );    // kinds 3-5
 
 }    // namespace uqc

@@ -8,21 +8,35 @@
 namespace uqc {
 
 template <int CL> void* kernel_of( int group, int which ) {
+    if constexpr( Closure<CL>::LINEAR ) {
+        // linear closures: no Newton, so no mixed, register-Newton or rounds kernels
+        if( which == KERNEL_CLOSURE_MIXED || which == KERNEL_CLOSURE_TINY || which == KERNEL_CHORD || which == KERNEL_HESS_TC ||
+            which == KERNEL_INVERT_RAW || which == KERNEL_INVERT || which == KERNEL_INVERT_SWEEP )
+            return nullptr;
+    }
     switch( which ) {
         case KERNEL_CLOSURE:
             if( group == 32 ) return (void*)&k_closure<CL, 32, double>;
             if( group == 64 ) return (void*)&k_closure<CL, 64, double>;
             if( group == 256 ) return (void*)&k_closure<CL, 256, double>;
             return nullptr;
-        case KERNEL_CLOSURE_TINY: return (void*)&k_closure<CL, 32, double, true>;
+        case KERNEL_CLOSURE_TINY:
+            if constexpr( !Closure<CL>::LINEAR ) return (void*)&k_closure<CL, 32, double, true>;
+            return nullptr;
         case KERNEL_CLOSURE_MIXED:
-            if( group == 32 ) return (void*)&k_closure<CL, 32, float>;
-            if( group == 64 ) return (void*)&k_closure<CL, 64, float>;
+            if constexpr( !Closure<CL>::LINEAR ) {
+                if( group == 32 ) return (void*)&k_closure<CL, 32, float>;
+                if( group == 64 ) return (void*)&k_closure<CL, 64, float>;
+            }
             return nullptr;
         case KERNEL_UPDATE: return (void*)&k_update<CL, true, false>;
         case KERNEL_UPDATE_PLAIN: return (void*)&k_update<CL, false, false>;
-        case KERNEL_UPDATE_WALL: return CL == 1 ? (void*)&k_update<CL, true, true> : nullptr;
-        case KERNEL_UPDATE_PLAIN_WALL: return CL == 1 ? (void*)&k_update<CL, false, true> : nullptr;
+        case KERNEL_UPDATE_WALL:
+            if constexpr( Closure<CL>::NS == 4 ) return (void*)&k_update<CL, true, true>;
+            return nullptr;
+        case KERNEL_UPDATE_PLAIN_WALL:
+            if constexpr( Closure<CL>::NS == 4 ) return (void*)&k_update<CL, false, true>;
+            return nullptr;
         case KERNEL_INIT:
             if( group == 32 ) return (void*)&k_init<CL, 32>;
             if( group == 256 ) return (void*)&k_init<CL, 256>;
@@ -45,7 +59,7 @@ template <int CL> void* kernel_of( int group, int which ) {
         case KERNEL_INVERT_RAW:
         case KERNEL_INVERT:
         case KERNEL_INVERT_SWEEP:
-            if constexpr( Closure<CL>::NS == 4 ) {    // the mixed form in rounds serves the 2-D Euler closure
+            if constexpr( CL == 1 ) {    // the mixed form in rounds serves the 2-D Euler closure
                 if( which == KERNEL_CHORD ) return (void*)&k_chord<CL>;
                 if( which == KERNEL_INVERT_SWEEP ) return (void*)&k_invert_sweep<CL>;
                 if( which == KERNEL_HESS_TC ) return (void*)&k_hess_tc<CL>;

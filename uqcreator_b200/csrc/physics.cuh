@@ -24,6 +24,7 @@ template <int CL> struct Closure;
 // U and DU of BoundedBarrier (boundedbarrier.cpp:19-31, 67-80), one state.
 template <> struct Closure<0> {
     static constexpr int NS = 1, NP = 1;
+    static constexpr bool LINEAR = false;
     __host__ __device__ static void U( const double* L, double* u, bool, const PhysParams& p ) {
         double ePos = exp( L[0] ), eNeg = 1.0 / ePos;
         if( L[0] > 0.0 )
@@ -47,6 +48,7 @@ template <> struct Closure<0> {
 // EulerClosure2D (eulerclosure2d.cpp); the class stores g = -gamma (:3).
 template <> struct Closure<1> {
     static constexpr int NS = 4, NP = 10;
+    static constexpr bool LINEAR = false;
     // The reference has two forms, U(Vector&) of :7-18 (gradient, mean/variance):
     // rho = exp(A q) (-v4)^A, and U(const Matrix&) of :27-32 (reconstruction):
     // rho = (-exp(q) v4)^A, with A = 1/(1 + g), g = -gamma. Both equal
@@ -103,6 +105,7 @@ template <> struct Closure<1> {
 // ShallowWaterClosure (shallowwaterclosure.cpp:10-42), g = 9.81.
 template <> struct Closure<2> {
     static constexpr int NS = 2, NP = 3;
+    static constexpr bool LINEAR = false;
     __host__ __device__ static void U( const double* L, double* u, bool, const PhysParams& ) {
         const double gr = 9.81;
         u[0] = ( 0.5 * ( 2 * L[0] + L[1] * L[1] ) ) / gr;
@@ -120,6 +123,32 @@ template <> struct Closure<2> {
         ds[1] = u[1] / u[0];
     }
 };
+
+// ---------------------------------------------------------------- linear closures
+// Stochastic Galerkin and the filtered forms (stochasticgalerkin.cpp:7-17,
+// l2filter.cpp:29-43, lassofilter.cpp:36-60): the
+// ansatz is the polynomial itself, U(Lambda) = Lambda, DU = identity, and the
+// duals come from the moments without a Newton solve (linear_duals in
+// ipm_kernels.cuh). Kinds 3, 4, 5 carry the states of Burgers, 2-D Euler and
+// shallow water; DS of the base class (zero) is the initial guess.
+template <int NSV> struct LinearClosure {
+    static constexpr int NS = NSV, NP = NSV * ( NSV + 1 ) / 2;
+    static constexpr bool LINEAR = true;
+    __host__ __device__ static void U( const double* L, double* u, bool, const PhysParams& ) {
+        for( int s = 0; s < NS; ++s ) u[s] = L[s];
+    }
+    __host__ __device__ static void DU( const double*, double* du, const PhysParams& ) {
+        int p = 0;
+        for( int a = 0; a < NS; ++a )
+            for( int b = a; b < NS; ++b ) du[p++] = a == b ? 1.0 : 0.0;
+    }
+    __host__ __device__ static void DS( const double*, double* ds, const PhysParams& ) {
+        for( int s = 0; s < NS; ++s ) ds[s] = 0.0;
+    }
+};
+template <> struct Closure<3> : LinearClosure<1> {};
+template <> struct Closure<4> : LinearClosure<4> {};
+template <> struct Closure<5> : LinearClosure<2> {};
 
 // packed index of the symmetric pair (a, b)
 template <int NS> __device__ __forceinline__ int pair_index( int a, int b ) {
@@ -232,5 +261,10 @@ template <> struct Problem<2> {
         y[1] = 0.0;
     }
 };
+
+// the linear closures' problems are those of the kinds with the same states
+template <> struct Problem<3> : Problem<0> {};
+template <> struct Problem<4> : Problem<1> {};
+template <> struct Problem<5> : Problem<2> {};
 
 }    // namespace uqc

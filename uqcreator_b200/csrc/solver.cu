@@ -131,6 +131,9 @@ struct uqc_solver {
     std::string cfgText;                     // the input file's text (echoed by uqc_export_state)
     std::string cfgName = "uqcreator_b200";  // the input file's path, when created from a file
     double area0 = 0.0;                      // area of the global mesh's first cell (TimeSolver's fixed dt)
+    // linear closures: the filter factors (host, device)
+    std::vector<double> filterHost, lassoParamHost, lassoL1Host;
+    double *d_filter = nullptr, *d_lassoParam = nullptr, *d_lassoL1 = nullptr;
     // spatial sharding (uqc_partition): the mesh is this rank's owned cells and halo
     bool sharded = false;
     ShardPlan shard;
@@ -170,6 +173,7 @@ template <class F> int guarded( uqc_solver* h, F&& f ) {
 }
 
 void ensure_device( uqc_solver* h );
+void build_filters( uqc_solver* h );
 
 // guarded() for entry points that touch the device
 template <class F> int guarded_dev( uqc_solver* h, F&& f ) {
@@ -197,7 +201,8 @@ template <class T> T* dupload( const std::vector<T>& v, size_t extra = 0 ) {
 // as much as testing every cell there).
 bool update_test_on( const uqc_solver* h ) {
     const bool on = h->finishInUpdateOpt == -1 ? h->tab.nLevels == 1 : h->finishInUpdateOpt != 0;
-    return h->cfg.newtonMode != 2 && on;
+    // a linear closure's duals follow the new moments: every cell goes through k_check
+    return h->cfg.newtonMode != 2 && on && !closure_linear( h->cfg.closure );
 }
 
 KParams make_params( const uqc_solver* h ) {
@@ -208,6 +213,10 @@ KParams make_params( const uqc_solver* h ) {
     P.ld      = h->ld;
     P.nLevels = h->tab.nLevels;
     for( int l = 0; l < h->tab.nLevels; ++l ) P.nTLevel[l] = h->tab.nTLevel[l];
+    P.filterKind   = h->cfg.filterKind;
+    P.filter       = h->d_filter;
+    P.lassoParam   = h->d_lassoParam;
+    P.lassoL1      = h->d_lassoL1;
     P.refIndicator = h->cfg.refIndicator;
     P.refDown      = h->cfg.refDown;
     P.refUp        = h->cfg.refUp;
@@ -288,13 +297,17 @@ void* pick( int cl, int group, int which ) {
     if( cl == 0 ) fn = kernel_bounded_barrier( group, which );
     if( cl == 1 ) fn = kernel_euler2d( group, which );
     if( cl == 2 ) fn = kernel_shallow_water( group, which );
+    if( closure_linear( cl ) ) fn = kernel_linear( cl, group, which );
     if( !fn ) throw ConfigError( "no kernel for this closure" );
     return fn;
 }
 
 void* pick_check( int cl ) { return pick( cl, 32, KERNEL_CHECK ); }
 
-int closure_np( int cl ) { return cl == 0 ? 1 : ( cl == 1 ? 10 : 3 ); }
+int closure_np( int cl ) {
+    const int ns = closure_states( cl );
+    return ns * ( ns + 1 ) / 2;
+}
 
 // Dynamic shared memory limit of a kernel: the attribute belongs to the
 // kernel function, for the whole process, so every handle sets it to the
@@ -465,6 +478,11 @@ void plan_rounds( uqc_solver* h, int maxSmem ) {
 // to 8 or 4 cells per CTA; the tables gain an FP32 copy of phi.
 void plan_mixed( uqc_solver* h, int maxSmem ) {
     const int cl = h->cfg.closure, nT = h->tab.nT, nQ = h->tab.nQ, nS = h->nS;
+    if( closure_linear( cl ) ) {
+        h->mixedOk  = false;
+        h->mixedWhy = "a linear closure (stochastic Galerkin or a filter) has no Newton system";
+        return;
+    }
     const size_t n       = size_t( nS ) * nT;
     const size_t tn      = size_t( nQ ) * h->ld + 4;
     const size_t tables  = 2 * tn * sizeof( double ) + ( tn + 1 ) / 2 * sizeof( double );
@@ -562,7 +580,7 @@ void plan_launches( uqc_solver* h ) {
     CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kc, h->closureBlock, h->closureSmem ) );
     h->closureGrid = std::max( 1, occ ) * h->numSMs;
     // tiny systems (n <= TINY_N duals, <= 64 nodes): the register Newton, a warp per cell
-    h->closureTiny = h->tinyOpt != 0 && h->closureGroup == 32 && n <= size_t( TINY_N ) && nQ <= 64;
+    h->closureTiny = h->tinyOpt != 0 && h->closureGroup == 32 && n <= size_t( TINY_N ) && nQ <= 64 && !closure_linear( cl );
     if( h->closureTiny ) {
         void* kt = pick( cl, 32, KERNEL_CLOSURE_TINY );
         allow_dynamic_smem( kt );
@@ -665,7 +683,7 @@ void build( uqc_solver* h, const std::string& text, void* stream, const std::str
     h->cfg          = parse_config( text );
     h->cfg.inputDir = inputDir;
     h->tab = build_tables( h->cfg );
-    h->nS  = h->cfg.closure == CL_BOUNDED_BARRIER ? 1 : ( h->cfg.closure == CL_EULER2D ? 4 : 2 );
+    h->nS  = closure_states( h->cfg.closure );
     h->ld  = ( h->tab.nT % 2 ) ? h->tab.nT : h->tab.nT + 1;    // odd row stride: conflict-free column reads
     h->ldc = size_t( h->nS ) * h->tab.nT;
     if( h->cfg.meshDim == 1 )
@@ -682,6 +700,7 @@ void build( uqc_solver* h, const std::string& text, void* stream, const std::str
         h->mesh = build_mesh_tri( nn, xy.data(), bnd.data(), nt, tri.data() );
     }
     h->area0     = h->mesh.area.empty() ? 0.0 : h->mesh.area[0];
+    build_filters( h );
     h->precision = h->cfg.precision;
     h->userStream = (cudaStream_t)stream;
     // host copies of the tables in the device layout (row stride ld, 8 spare
@@ -696,6 +715,44 @@ void build( uqc_solver* h, const std::string& text, void* stream, const std::str
             h->padPhi[size_t( k ) * h->ld + i]   = h->tab.phi[size_t( k ) * h->tab.nT + i];
             h->padPhiWf[size_t( k ) * h->ld + i] = h->tab.phiWf[size_t( k ) * h->tab.nT + i];
         }
+}
+
+// Factors of the linear closures as their constructors compute them, in the
+// reference's operation order: L2Filter (l2filter.cpp:3-17; the loop over the
+// states multiplies each factor in once per state), LassoFilter
+// (lassofilter.cpp:3-22: p_i = prod_l index_l (index_l + 1), l1_i = sum_k
+// |phiWf(k, i)|). index_l = digit l of i in base nMoments, the last level's
+// degree (Settings::GetNMoments, settings.cpp:226). Stochastic Galerkin: 1.
+void build_filters( uqc_solver* h ) {
+    const int nT = h->tab.nT, nQ = h->tab.nQ, d = h->tab.dimXi, nS = h->nS;
+    h->filterHost.assign( nT, 1.0 );
+    h->lassoParamHost.assign( nT, 1.0 );
+    h->lassoL1Host.assign( nT, 0.0 );
+    if( !closure_linear( h->cfg.closure ) ) return;
+    const unsigned nM = unsigned( h->cfg.degrees.back() );
+    if( nM == 0 && h->cfg.filterKind != FILTER_SG ) throw ConfigError( "the moment filters need a degree of at least 1" );
+    auto index = [&]( unsigned i, int l ) {
+        const unsigned p = unsigned( std::pow( nM, l ) );
+        return ( ( i - i % p ) / p ) % nM;
+    };
+    if( h->cfg.filterKind == FILTER_L2 ) {
+        const double lam = 0.0000015;
+        for( int s = 0; s < nS; ++s )
+            for( int i = 0; i < nT; ++i )
+                for( int l = 0; l < d; ++l ) {
+                    const unsigned ix = index( unsigned( i ), l );
+                    h->filterHost[i] *= 1.0 / ( 1.0 + lam * std::pow( ix, 2 ) * std::pow( ix + 1, 2 ) );
+                }
+    }
+    else if( h->cfg.filterKind == FILTER_LASSO ) {
+        for( int i = 0; i < nT; ++i )
+            for( int k = 0; k < nQ; ++k ) h->lassoL1Host[i] += std::fabs( h->tab.phiWf[size_t( k ) * nT + i] );
+        for( int i = 0; i < nT; ++i )
+            for( int l = 0; l < d; ++l ) {
+                const unsigned ix = index( unsigned( i ), l );
+                h->lassoParamHost[i] *= ix * ( ix + 1 );
+            }
+    }
 }
 
 // Device side of a handle, set up on first use so that configuration, tables
@@ -723,6 +780,9 @@ void ensure_device( uqc_solver* h ) {
     for( size_t i = 0; i < phi.size(); ++i ) phiF[i] = float( phi[i] );
     h->d_phiF = dupload( phiF );
     h->d_xi    = dupload( h->tab.xi );
+    h->d_filter     = dupload( h->filterHost );
+    h->d_lassoParam = dupload( h->lassoParamHost );
+    h->d_lassoL1    = dupload( h->lassoL1Host );
     h->d_wt    = dupload( h->padWt );
     const Mesh& m = h->mesh;
     std::vector<double> dx( m.nCells );
@@ -771,7 +831,8 @@ void release( uqc_solver* h ) {
                     (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
                     (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_cellDt, (void*)h->d_uRe, (void*)h->d_checkList, (void*)h->d_finFlag, (void*)h->d_phiF, (void*)h->d_fallbackList,
                     (void*)h->d_factorStore, (void*)h->d_factorLevel, (void*)h->d_gStore, (void*)h->d_v2Lists,
-                    (void*)h->d_chordIters, (void*)h->d_qTiles, (void*)h->d_sendCells} )
+                    (void*)h->d_chordIters, (void*)h->d_qTiles, (void*)h->d_sendCells, (void*)h->d_filter, (void*)h->d_lassoParam,
+                    (void*)h->d_lassoL1} )
         if( p ) cudaFree( p );
     if( h->h_ctl ) cudaFreeHost( h->h_ctl );
     for( auto& e : h->ev )
@@ -1369,6 +1430,28 @@ static void safe_closure_all( uqc_solver* h, int maxIter ) {
 // previous basis and quadrature, SolveClosureSafe, 10000 iterations); the
 // solution U(Lambda) at the new quadrature nodes from the previous basis there,
 // projected onto the new basis; the duals padded with zeros and solved again.
+// DS and U of a closure kind on the host
+static void host_closure_ds( int cl, const double* u, double* d, const PhysParams& pp ) {
+    switch( cl ) {
+        case 0: Closure<0>::DS( u, d, pp ); break;
+        case 1: Closure<1>::DS( u, d, pp ); break;
+        case 2: Closure<2>::DS( u, d, pp ); break;
+        case 3: Closure<3>::DS( u, d, pp ); break;
+        case 4: Closure<4>::DS( u, d, pp ); break;
+        default: Closure<5>::DS( u, d, pp ); break;
+    }
+}
+static void host_closure_u( int cl, const double* L, double* y, const PhysParams& pp ) {
+    switch( cl ) {
+        case 0: Closure<0>::U( L, y, false, pp ); break;
+        case 1: Closure<1>::U( L, y, false, pp ); break;
+        case 2: Closure<2>::U( L, y, false, pp ); break;
+        case 3: Closure<3>::U( L, y, false, pp ); break;
+        case 4: Closure<4>::U( L, y, false, pp ); break;
+        default: Closure<5>::U( L, y, false, pp ); break;
+    }
+}
+
 static void restart_new_order( uqc_solver* h, const std::string& base, const std::string& echo, const Config& prev ) {
     const size_t N = size_t( h->mesh.nCells );
     const int nS = h->nS, nT = h->tab.nT, nQ = h->tab.nQ;
@@ -1412,12 +1495,7 @@ static void restart_new_order( uqc_solver* h, const std::string& base, const std
             for( size_t j = 0; j < N; ++j ) {
                 double u0[4] = {0, 0, 0, 0}, d[4] = {0, 0, 0, 0};
                 for( int s = 0; s < nS; ++s ) u0[s] = u[( j * nS + s ) * nP];
-                if( h->cfg.closure == CL_BOUNDED_BARRIER )
-                    Closure<0>::DS( u0, d, pp );
-                else if( h->cfg.closure == CL_EULER2D )
-                    Closure<1>::DS( u0, d, pp );
-                else
-                    Closure<2>::DS( u0, d, pp );
+                host_closure_ds( h->cfg.closure, u0, d, pp );
                 for( int s = 0; s < nS; ++s ) lam[( j * nS + s ) * nP] = d[s];
             }
             rc = uqc_closure_solve_host( ph, int( N ), lam.data(), u.data(), nullptr, UQC_LAYOUT_STATE_MAJOR, st.data() );
@@ -1443,12 +1521,7 @@ static void restart_new_order( uqc_solver* h, const std::string& base, const std
                 for( int i = 0; i < nP; ++i ) a += lam[( j * nS + s ) * nP + i] * it.phi[size_t( k ) * nP + i];
                 L[s] = a;
             }
-            if( h->cfg.closure == CL_BOUNDED_BARRIER )
-                Closure<0>::U( L, y, false, pp );
-            else if( h->cfg.closure == CL_EULER2D )
-                Closure<1>::U( L, y, false, pp );
-            else
-                Closure<2>::U( L, y, false, pp );
+            host_closure_u( h->cfg.closure, L, y, pp );
             for( int s = 0; s < nS; ++s ) uq[size_t( s ) * nQ + k] = y[s];
         }
         for( int s = 0; s < nS; ++s ) {
@@ -1554,7 +1627,7 @@ int uqc_write_vtk( uqc_solver* h, const char* path ) {
             std::vector<int> cols;    // columns of mv (-1: zero)
         };
         std::vector<Arr> arrs;
-        const bool euler = h->cfg.closure == CL_EULER2D;
+        const bool euler = h->nS == 4;
         const char* names1[] = {"u"};
         const char* namesSW[] = {"h", "hu"};
         for( int part = 0; part < 2; ++part ) {
