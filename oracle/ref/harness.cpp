@@ -21,7 +21,9 @@
 #include "boundedbarrier.h"
 #include "burgers.h"
 #include "closure.h"
+#include "euler.h"
 #include "euler2d.h"
+#include "eulerclosure.h"
 #include "eulerclosure2d.h"
 #include "line.h"
 #include "mesh.h"
@@ -365,6 +367,7 @@ static Closure* make_closure( Settings* s, int newtonMode ) {
     switch( s->GetClosureType() ) {
         case ClosureType::C_BOUNDEDBARRIER: return new Guarded<BoundedBarrier>( s );
         case ClosureType::C_EULER_2D: return new Guarded<EulerClosure2D>( s );
+        case ClosureType::C_EULER_1D: return new Guarded<EulerClosure>( s );
         case ClosureType::C_SHALLOWWATER_1D: return new Guarded<ShallowWaterClosure>( s );
         default: return Closure::Create( s );
     }
@@ -405,7 +408,8 @@ static int full_solve_files( uqcref* h, const char* prefix, double* meanVar, cha
 extern "C" {
 
 // Builds settings (the reference's own Settings parser, settings.cpp:22-323),
-// a harness problem (kind 1 Burgers, 2 Euler2D, 3 shallow water), the mesh and
+// a harness problem (kind 1 Burgers, 2 Euler2D, 3 shallow water, 4 the reference's
+// own Euler1D), the mesh and
 // the reference's Closure (closure.cpp:16-84) and ExplicitEuler.
 // 1-D meshes come from the [mesh] table; 2-D meshes from the arrays.
 int uqcref_create( const char* toml,
@@ -434,6 +438,8 @@ int uqcref_create( const char* toml,
             h->problem.reset( new HarnessEuler2D( s, params ) );
         else if( kind == 3 )
             h->problem.reset( new HarnessShallowWater( s, params ) );
+        else if( kind == 4 )
+            h->problem.reset( new Euler( s ) );    // the reference's own 1-D Euler problem (Sod state fixed in euler.cpp:95-128)
         else
             throw uqc_ref_error( "unknown problem kind" );
         if( s->GetMeshDimension() == 1 ) {

@@ -73,7 +73,7 @@ def _p(a, t=_dp):
     return None if a is None else a.ctypes.data_as(t)
 
 
-PROBLEM_KIND = {"Burgers1D": 1, "Euler2D": 2, "ShallowWater1D": 3}
+PROBLEM_KIND = {"Burgers1D": 1, "Euler2D": 2, "ShallowWater1D": 3, "Euler1D": 4}
 NEWTON_MODE = {"reference": 0, "guarded": 1, "safe": 2}
 
 

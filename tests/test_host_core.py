@@ -28,6 +28,7 @@ CASES = {
     "euler2d_3u": (W.euler2d_3u(nx=5, ny=3), "Euler2D", EULER_IC, (3, 12)),
     "burgers1d_deg9": (W.burgers1d(ncells=40, degree=9, nquad=40), "Burgers1D", [12.0, 3.0, 0.5, 0.6], (2.5, 12.5)),
     "euler2d_deg2": (W.euler2d(nx=7, ny=5, degree=2, nquad=4, seed=3), "Euler2D", EULER_IC, (3, 12)),
+    "euler1d": (W.euler1d(ncells=40, degree=4, nquad=10), "Euler1D", [], (3, 12)),
 }
 
 

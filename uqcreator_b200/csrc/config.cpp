@@ -152,8 +152,14 @@ Config parse_config( const std::string& text ) {
         c.problem = PR_EULER2D;
     else if( c.problemName == "ShallowWater1D" )
         c.problem = PR_SHALLOW_WATER;
+    else if( c.problemName == "Euler1D" )
+        c.problem = PR_EULER1D;
+    else if( c.problemName == "ShallowWater2D" )
+        // shallowwater2d.cpp:87-90: ComputeDt is not implemented and returns 0,
+        // so the reference's time loop never advances
+        throw ConfigError( "[general] 'problem' = 'ShallowWater2D': the reference's time step for it is not implemented (always 0)" );
     else
-        throw ConfigError( "[general] 'problem' = '" + c.problemName + "' is not on this hot path (Burgers1D, Euler2D, ShallowWater1D)" );
+        throw ConfigError( "[general] 'problem' = '" + c.problemName + "' is not on this hot path (Burgers1D, Euler1D, Euler2D, ShallowWater1D)" );
     // [mesh] (settings.cpp:95-111, mesh1d.cpp:6-17)
     c.meshDim = int( need( d, "mesh", "dimension" ).num() );
     if( const Value* v = find( d, "mesh", "numberOfCells" ) ) c.nCells1d = int( v->num() );
@@ -184,9 +190,14 @@ Config parse_config( const std::string& text ) {
         c.closure = CL_EULER2D;
     else if( cl == "ShallowWater" )
         c.closure = CL_SHALLOW_WATER;
+    else if( cl == "Euler" )
+        c.closure = CL_EULER1D;
     else if( cl == "StochasticGalerkin" || cl == "L2Filter" || cl == "LassoFilter" ) {
         // the linear closures take the states of the problem
-        c.closure    = c.problem == PR_BURGERS ? CL_LINEAR_BURGERS : ( c.problem == PR_EULER2D ? CL_LINEAR_EULER2D : CL_LINEAR_SW );
+        c.closure    = c.problem == PR_BURGERS ? CL_LINEAR_BURGERS
+                       : c.problem == PR_EULER2D  ? CL_LINEAR_EULER2D
+                       : c.problem == PR_EULER1D  ? CL_LINEAR_EULER1D
+                                                  : CL_LINEAR_SW;
         c.filterKind = cl == "StochasticGalerkin" ? FILTER_SG : ( cl == "L2Filter" ? FILTER_L2 : FILTER_LASSO );
     }
     else if( cl == "ExponentialFilter" )
@@ -215,7 +226,7 @@ Config parse_config( const std::string& text ) {
     if( const Value* v = find( d, "moment_system", "epsilon" ) ) c.epsilon = v->num();
     // closure / problem consistency (the reference pairs them in Problem::Create)
     int nS = closure_states( c.closure );
-    int nSp = c.problem == PR_BURGERS ? 1 : ( c.problem == PR_EULER2D ? 4 : 2 );
+    int nSp = c.problem == PR_BURGERS ? 1 : ( c.problem == PR_EULER2D ? 4 : ( c.problem == PR_EULER1D ? 3 : 2 ) );
     if( nS != nSp ) throw ConfigError( "closure '" + cl + "' does not match problem '" + c.problemName + "'" );
     // [uqc]
     if( const Value* v = find( d, "uqc", "ic" ) )
@@ -313,7 +324,10 @@ Config parse_config( const std::string& text ) {
                 throw ConfigError( "[uqc] 'retardationResiduals' must be decreasing" );
         }
     }
-    size_t needIc = c.problem == PR_BURGERS ? 4 : ( c.problem == PR_EULER2D ? 5 : 3 );
+    // Euler1D: the reference's initial state is fixed in the problem (euler.cpp:95-128);
+    // [uqc] ic = [x0, rhoL, pL, rhoR, pR] may replace it
+    size_t needIc = c.problem == PR_BURGERS ? 4 : ( c.problem == PR_EULER2D ? 5 : ( c.problem == PR_EULER1D ? 0 : 3 ) );
+    if( c.problem == PR_EULER1D && !c.ic.empty() && c.ic.size() < 5 ) throw ConfigError( "[uqc] 'ic' needs 5 values for Euler1D (or none)" );
     if( c.ic.size() < needIc ) throw ConfigError( "[uqc] 'ic' needs " + std::to_string( needIc ) + " values for " + c.problemName );
     if( c.meshDim == 1 ) {
         if( c.nCells1d < 3 || ( std::fabs( c.a ) <= 2.2e-16 && std::fabs( c.b ) <= 2.2e-16 ) )

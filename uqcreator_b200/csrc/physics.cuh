@@ -13,6 +13,7 @@ struct PhysParams {
     double eulerA;            // Euler: 1 / (1 - gamma), the exponent of the entropy ansatz
     double cfl;
     double ic[8];
+    int nIc;                  // initial-state parameters given ([uqc] ic)
     double sigma[4];
     int dimXi;
     double dtFixed;           // shallow water: TimeSolver's dx CFL / 12
@@ -149,6 +150,49 @@ template <int NSV> struct LinearClosure {
 template <> struct Closure<3> : LinearClosure<1> {};
 template <> struct Closure<4> : LinearClosure<4> {};
 template <> struct Closure<5> : LinearClosure<2> {};
+template <> struct Closure<7> : LinearClosure<3> {};
+
+// ---------------------------------------------------------------- Euler 1-D
+// EulerClosure (eulerclosure.cpp:7-80): three states (rho, rho u, rho E), the
+// gamma of [problem] gamma. DU is packed as the entries the reference's Newton
+// reads: the Hessian block (m, l), m <= l, takes DU(l, m) (closure.cpp:255-270)
+// and posv reads the upper triangle (uplo 'U', vectorspace.cpp:152-171), so the
+// pair (m, l) holds the reference's y(l, m) (its lower triangle and diagonal,
+// with y(2, 2) as written there).
+template <> struct Closure<6> {
+    static constexpr int NS = 3, NP = 6;
+    static constexpr bool LINEAR = false;
+    __host__ __device__ static double E( const double* L, const PhysParams& p ) {
+        const double g = p.gamma;
+        return exp( ( 2.0 * L[0] * L[2] - 2.0 * L[2] * log( -L[2] ) - 2.0 * L[2] * g - L[1] * L[1] ) / ( 2.0 * L[2] * ( g - 1.0 ) ) );
+    }
+    __host__ __device__ static void U( const double* L, double* u, bool, const PhysParams& p ) {
+        u[0] = E( L, p );
+        u[1] = -( L[1] / L[2] ) * u[0];
+        u[2] = ( ( L[1] * L[1] - 2.0 * L[2] ) / ( 2.0 * ( L[2] * L[2] ) ) ) * u[0];
+    }
+    __host__ __device__ static void DU( const double* L, double* y, const PhysParams& p ) {
+        const double g = p.gamma, e = E( L, p ), l2sq = L[2] * L[2];
+        const double d1 = ( 1.0 / ( g - 1.0 ) ) * e;
+        const double d2 = -( L[1] / ( L[2] * ( g - 1.0 ) ) ) * e;
+        const double d3 = ( ( -2.0 * g + 2.0 * L[0] - 2.0 * log( -L[2] ) - 2.0 ) / ( 2.0 * ( g - 1.0 ) * L[2] ) -
+                            ( -2.0 * g * L[2] + 2.0 * L[0] * L[2] - L[1] * L[1] - 2.0 * L[2] * log( -L[2] ) ) / ( 2.0 * ( g - 1.0 ) * l2sq ) ) *
+                          e;
+        const double c = ( L[1] * L[1] - 2.0 * L[2] ) / ( 2.0 * l2sq );
+        y[0] = d1;                                                                        // (0, 0)
+        y[1] = -( L[1] / L[2] ) * d1;                                                     // y(1, 0)
+        y[2] = c * d1;                                                                    // y(2, 0)
+        y[3] = -( 1.0 / L[2] ) * e - ( L[1] / L[2] ) * d2;                                // y(1, 1)
+        y[4] = c * d2 + ( 2.0 * L[1] / ( 2.0 * l2sq ) ) * e;                              // y(2, 1)
+        y[5] = ( L[1] * L[1] / pow( L[2], -3.0 ) + pow( L[2], -2.0 ) ) * e + c * d3;    // y(2, 2)
+    }
+    __host__ __device__ static void DS( const double* u, double* ds, const PhysParams& p ) {
+        const double gamma = -p.gamma, rho = u[0], rhoU = u[1], rhoU2 = rhoU * rhoU, rhoE = u[2];
+        ds[0] = ( rhoU2 + gamma * ( 2 * rho * rhoE - rhoU2 ) ) / ( -2 * rho * rhoE + rhoU2 ) - log( pow( rho, gamma ) * ( rhoE - ( rhoU2 ) / ( 2 * rho ) ) );
+        ds[1] = -( ( 2 * rho * rhoU ) / ( -2 * rho * rhoE + rhoU2 ) );
+        ds[2] = -( rho / ( rhoE - ( rhoU2 ) / ( 2 * rho ) ) );
+    }
+};
 
 // packed index of the symmetric pair (a, b)
 template <int NS> __device__ __forceinline__ int pair_index( int a, int b ) {
@@ -266,5 +310,71 @@ template <> struct Problem<2> {
 template <> struct Problem<3> : Problem<0> {};
 template <> struct Problem<4> : Problem<1> {};
 template <> struct Problem<5> : Problem<2> {};
+
+// Euler 1-D (euler.cpp:23-128): HLL flux with the projected velocities, CFL
+// rule min over nodes of cfl dx min(|1 / (v - a)|, |1 / (v + a)|), Sod initial
+// state x0 = 0.3 + s0 xi0, left (1, 0, 1), right (0.3 + s1 xi1, 0, 0.3 + s2
+// xi2) with gamma 1.4 in the initial state (the reference's fixed values;
+// [uqc] ic = [x0, rhoL, pL, rhoR, pR] replaces them).
+template <> struct Problem<6> {
+    __device__ static void F( double gm, const double* u, double n, double* f ) {
+        const double rhoInv = 1.0 / u[0], v = u[1] * rhoInv;
+        const double p      = ( gm - 1.0 ) * ( u[2] - 0.5 * u[0] * ( v * v ) );
+        f[0]                = u[1] * n;
+        f[1]                = ( u[1] * v + p ) * n;
+        f[2]                = ( ( u[2] + p ) * v ) * n;
+    }
+    __device__ static void flux( const double* u, const double* v, const double* nu, const double* n, double nn, double* y,
+                                 const PhysParams& P ) {
+        const double gm = P.gamma;
+        double rhoInv   = 1.0 / u[0];
+        double vU       = u[1] * rhoInv;
+        double p        = ( gm - 1.0 ) * ( u[2] - 0.5 * u[0] * ( vU * vU ) );
+        double aU       = sqrt( gm * p * rhoInv );
+        rhoInv          = 1.0 / v[0];
+        double vV       = v[1] * rhoInv;
+        p               = ( gm - 1.0 ) * ( v[2] - 0.5 * v[0] * ( vV * vV ) );
+        double aV       = sqrt( gm * p * rhoInv );
+        double lmin = nu[0] * vU - aU, lmax = nu[0] * vV + aV;
+        if( lmin >= 0 )
+            F( gm, u, n[0], y );
+        else if( lmax <= 0 )
+            F( gm, v, n[0], y );
+        else {
+            // (lmax F(u) n - lmin F(v) n + lmax lmin (v - u) |n|) / (lmax - lmin), in that order
+            const double rU = 1.0 / u[0], wU = u[1] * rU, pU = ( gm - 1.0 ) * ( u[2] - 0.5 * u[0] * ( wU * wU ) );
+            const double rV = 1.0 / v[0], wV = v[1] * rV, pV = ( gm - 1.0 ) * ( v[2] - 0.5 * v[0] * ( wV * wV ) );
+            const double fu[3] = {u[1], u[1] * wU + pU, ( u[2] + pU ) * wU};
+            const double fv[3] = {v[1], v[1] * wV + pV, ( v[2] + pV ) * wV};
+            const double inv = 1.0 / ( lmax - lmin ), ll = lmax * lmin;
+            for( int i = 0; i < 3; ++i ) y[i] = inv * ( ( ( lmax * fu[i] ) * n[0] - ( lmin * fv[i] ) * n[0] ) + ( ll * ( v[i] - u[i] ) ) * nn );
+        }
+    }
+    __device__ static double dt( const double* uq, double dx, const PhysParams& P ) {
+        const double gm = P.gamma, rhoInv = 1.0 / uq[0], v = uq[1] * rhoInv;
+        const double p = ( gm - 1.0 ) * ( uq[2] - 0.5 * uq[0] * ( v * v ) ), a = sqrt( gm * p * rhoInv );
+        return ( P.cfl * dx ) * fmin( fabs( 1.0 / ( v - a ) ), fabs( 1.0 / ( v + a ) ) );
+    }
+    __device__ static void ic( const double* x, const double* xi, double* y, const PhysParams& P ) {
+        const double gic = 1.4;
+        const bool own   = P.nIc >= 5;
+        const double x0 = own ? P.ic[0] : 0.3, rhoL = own ? P.ic[1] : 1.0, pL = own ? P.ic[2] : 1.0;
+        const double rhoR = own ? P.ic[3] : 0.3;
+        double pR         = own ? P.ic[4] : 0.3;
+        if( x[0] < x0 + P.sigma[0] * xi[0] ) {
+            y[0] = rhoL;
+            y[1] = rhoL * 0.0;
+            y[2] = 0.5 * rhoL * ( 0.0 * 0.0 ) + ( pL / ( rhoL * ( gic - 1 ) ) ) * rhoL;
+        }
+        else {
+            y[0] = rhoR;
+            if( P.dimXi > 1 ) y[0] += P.sigma[1] * xi[1];
+            if( P.dimXi > 2 ) pR += P.sigma[2] * xi[2];
+            y[1] = rhoR * 0.0;
+            y[2] = 0.5 * rhoR * ( 0.0 * 0.0 ) + ( pR / ( rhoR * ( gic - 1 ) ) ) * rhoR;
+        }
+    }
+};
+template <> struct Problem<7> : Problem<6> {};
 
 }    // namespace uqc

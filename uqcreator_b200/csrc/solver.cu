@@ -237,6 +237,7 @@ KParams make_params( const uqc_solver* h ) {
     ph.eulerA      = 1.0 / ( 1.0 - h->cfg.gamma );
     ph.cfl         = h->cfg.cfl;
     for( size_t i = 0; i < h->cfg.ic.size() && i < 8; ++i ) ph.ic[i] = h->cfg.ic[i];
+    ph.nIc = int( std::min<size_t>( h->cfg.ic.size(), 8 ) );
     for( size_t i = 0; i < h->cfg.sigma.size() && i < 4; ++i ) ph.sigma[i] = h->cfg.sigma[i];
     ph.dimXi   = h->tab.dimXi;
     ph.dtFixed = h->area0 * h->cfg.cfl / 12.0;    // TimeSolver (timesolver.cpp:4-9)
@@ -297,7 +298,8 @@ void* pick( int cl, int group, int which ) {
     if( cl == 0 ) fn = kernel_bounded_barrier( group, which );
     if( cl == 1 ) fn = kernel_euler2d( group, which );
     if( cl == 2 ) fn = kernel_shallow_water( group, which );
-    if( closure_linear( cl ) ) fn = kernel_linear( cl, group, which );
+    if( closure_linear( cl ) && cl != CL_LINEAR_EULER1D ) fn = kernel_linear( cl, group, which );
+    if( cl == CL_EULER1D || cl == CL_LINEAR_EULER1D ) fn = kernel_euler1d( cl, group, which );
     if( !fn ) throw ConfigError( "no kernel for this closure" );
     return fn;
 }
@@ -1438,7 +1440,9 @@ static void host_closure_ds( int cl, const double* u, double* d, const PhysParam
         case 2: Closure<2>::DS( u, d, pp ); break;
         case 3: Closure<3>::DS( u, d, pp ); break;
         case 4: Closure<4>::DS( u, d, pp ); break;
-        default: Closure<5>::DS( u, d, pp ); break;
+        case 5: Closure<5>::DS( u, d, pp ); break;
+        case 6: Closure<6>::DS( u, d, pp ); break;
+        default: Closure<7>::DS( u, d, pp ); break;
     }
 }
 static void host_closure_u( int cl, const double* L, double* y, const PhysParams& pp ) {
@@ -1448,7 +1452,9 @@ static void host_closure_u( int cl, const double* L, double* y, const PhysParams
         case 2: Closure<2>::U( L, y, false, pp ); break;
         case 3: Closure<3>::U( L, y, false, pp ); break;
         case 4: Closure<4>::U( L, y, false, pp ); break;
-        default: Closure<5>::U( L, y, false, pp ); break;
+        case 5: Closure<5>::U( L, y, false, pp ); break;
+        case 6: Closure<6>::U( L, y, false, pp ); break;
+        default: Closure<7>::U( L, y, false, pp ); break;
     }
 }
 
@@ -1630,6 +1636,7 @@ int uqc_write_vtk( uqc_solver* h, const char* path ) {
         const bool euler = h->nS == 4;
         const char* names1[] = {"u"};
         const char* namesSW[] = {"h", "hu"};
+        const char* namesE1[] = {"rho", "rhoU", "rhoE"};
         for( int part = 0; part < 2; ++part ) {
             const std::string pre = part == 0 ? "E(" : "Var(";
             const int off         = part * nS;
@@ -1639,7 +1646,8 @@ int uqc_write_vtk( uqc_solver* h, const char* path ) {
                 arrs.push_back( {pre + "ρE)", 1, {off + 3}} );
             }
             else {
-                for( int s2 = 0; s2 < nS; ++s2 ) arrs.push_back( {pre + ( nS == 1 ? names1[0] : namesSW[s2] ) + ")", 1, {off + s2}} );
+                for( int s2 = 0; s2 < nS; ++s2 )
+                    arrs.push_back( {pre + ( nS == 1 ? names1[0] : ( nS == 3 ? namesE1[s2] : namesSW[s2] ) ) + ")", 1, {off + s2}} );
             }
         }
         const std::string file = ( std::string( path ).size() > 4 && std::string( path ).substr( std::string( path ).size() - 4 ) == ".vtk" ) ? path : std::string( path ) + ".vtk";

@@ -21,6 +21,7 @@ a [uqc] table that the reference ignores and this package reads:
 
 Problems and their ic parameters:
   Burgers1D       [uL, uR, x0, x1]          ramp of code/src/burgers.cpp:48-68
+  Euler1D         [] or [x0, rhoL, pL, rhoR, pR]   the reference's fixed Sod state (euler.cpp:95-128)
   Euler2D         [xs, rhoL, pL, rhoR, pR]  Sod-type interface at x = xs + s0 xi0
   ShallowWater1D  [xd, hL, hR]              dam break h = hL (1 + s0 xi0) | hR
 """
@@ -115,6 +116,16 @@ def shallow_water1d(ncells=1_000_000, max_degree=9, nquad=30, tend=0.05, eps=1e-
                      nquad=nquad, ic=[0.5, 1.0, 0.5], eps=eps, **kw)
 
 
+def euler1d(ncells=400, degree=4, nquad=10, tend=0.1, cfl=0.5, eps=1e-10, sigma=0.05, newton="guarded", sigmas=None,
+            **kw) -> str:
+    """1-D Euler (gamma 1.4) on [0, 1]: the reference's own Sod state (euler.cpp:95-128,
+    interface x = 0.3 + sigma xi, left (1, 0, 1), right density and pressure 0.3),
+    EulerClosure (three states), HLL flux."""
+    return make_toml(name="euler1d", problem="Euler1D", closure="Euler", dim=1, ncells=ncells, a=0.0, b=1.0,
+                     sigmas=sigmas or [sigma], cfl=cfl, tend=tend, degrees=[degree], nquad=nquad, ic=[], eps=eps, gamma=1.4,
+                     newton=newton, **kw)
+
+
 def euler2d_3u(nx=512, ny=256, degree=4, nquad=8, **kw) -> str:
     """Large 2-D Euler with 3 uncertainties, total degree 4 (35 moments x 4 states), 8^3 nodes."""
     return euler2d(nx=nx, ny=ny, degree=degree, nquad=nquad, dim_xi=3, **kw)
@@ -156,6 +167,7 @@ WORKLOADS = {
     "euler2d": euler2d,
     "sw1d": shallow_water1d,
     "euler2d_3u": euler2d_3u,
+    "euler1d": euler1d,
 }
 
 
