@@ -31,7 +31,9 @@ EULER_WEAK = [0.5, 1.0, 1.0, 0.8, 0.8]
 
 
 def _weak(toml):
-    return toml.replace("ic = [0.5, 1.0, 1.0, 0.125, 0.1]", "ic = [0.5, 1.0, 1.0, 0.8, 0.8]")
+    out = toml.replace("ic = [0.5,1.0,1.0,0.125,0.1]", "ic = [0.5,1.0,1.0,0.8,0.8]")
+    assert out != toml
+    return out
 
 
 CASES = {
@@ -62,7 +64,7 @@ def test_linear_closure_steps_match_reference(case):
     a = s.step(steps)
     b = r.step(steps)
     assert a["failed_cells"] == 0
-    assert abs(a["t"] - b["t"]) <= 1e-12 * b["t"]
+    assert abs(a["t"] - b["t"]) <= 1e-10 * b["t"]
     us, ls, vs = s.download_state()
     ur, lr, vr = r.get_state()
     assert np.isfinite(us).all() and np.isfinite(ls).all()
