@@ -1236,7 +1236,7 @@ __host__ __device__ inline size_t check_ws_doubles( int nS, int nT, int nQ ) {
 // appended to P.activeList for k_closure. Lambda is formed node by node in
 // registers and U(Lambda) stored (no nodal Lambda buffer), so up to 16 warps
 // share a CTA and the latency of this per-cell work is hidden.
-template <int CL> __global__ void __launch_bounds__( 512 ) k_check( KParams P ) {
+template <int CL> __global__ void __launch_bounds__( 512, 2 ) k_check( KParams P ) {
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
     if( !P.ctl->active ) return;
