@@ -21,7 +21,7 @@ BUILD = PKG / "_build"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_SRCS = ["config.cpp", "tables.cpp", "mesh.cpp"]
-CUDA_SRCS = ["solver.cu", "kernels_bb.cu", "kernels_euler2d.cu", "kernels_sw.cu", "kernels_linear.cu", "kernels_euler1d.cu"]
+CUDA_SRCS = ["solver.cu", "kernels_bb.cu", "kernels_euler2d.cu", "kernels_sw.cu", "kernels_linear.cu", "kernels_euler1d.cu", "kernels_logsin.cu"]
 
 
 def _sources():

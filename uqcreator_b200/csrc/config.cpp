@@ -154,6 +154,11 @@ Config parse_config( const std::string& text ) {
         c.problem = PR_SHALLOW_WATER;
     else if( c.problemName == "Euler1D" )
         c.problem = PR_EULER1D;
+    else if( c.problemName == "PNEquations2D" )
+        // momentsolver.cpp:403-411: the source of every cell is accumulated into
+        // one matrix shared by the threads of an OpenMP loop and never reset,
+        // so the reference's result depends on thread scheduling
+        throw ConfigError( "[general] 'problem' = 'PNEquations2D': the reference's source term is accumulated across cells by racing threads" );
     else if( c.problemName == "ShallowWater2D" )
         // shallowwater2d.cpp:87-90: ComputeDt is not implemented and returns 0,
         // so the reference's time loop never advances
@@ -192,6 +197,8 @@ Config parse_config( const std::string& text ) {
         c.closure = CL_SHALLOW_WATER;
     else if( cl == "Euler" )
         c.closure = CL_EULER1D;
+    else if( cl == "LogSin" )
+        c.closure = CL_LOGSIN;
     else if( cl == "StochasticGalerkin" || cl == "L2Filter" || cl == "LassoFilter" ) {
         // the linear closures take the states of the problem
         c.closure    = c.problem == PR_BURGERS ? CL_LINEAR_BURGERS
@@ -207,7 +214,7 @@ Config parse_config( const std::string& text ) {
         throw ConfigError( "[moment_system] 'closure' = 'ExponentialFilter': the reference's filter reads an uninitialised order and time step" );
     else
         throw ConfigError( "[moment_system] 'closure' = '" + cl +
-                           "' is not on this hot path (BoundedBarrier, Euler2D, ShallowWater, StochasticGalerkin, L2Filter, LassoFilter, ExponentialFilter)" );
+                           "' is not on this hot path (BoundedBarrier, LogSin, Euler, Euler2D, ShallowWater, StochasticGalerkin, L2Filter, LassoFilter)" );
     const Value& mom = need( d, "moment_system", "moments" );
     if( mom.kind != Value::ARR || mom.items.size() != 2 ) throw ConfigError( "[moment_system] 'moments' must be [[type],[degrees]]" );
     std::string degType = str( mom.items[0].items.at( 0 ), "moments type" );

@@ -17,7 +17,7 @@ struct ConfigError : public std::runtime_error {
 // Kernel closure kinds. 3-5: the linear closures (stochastic Galerkin and the
 // moment filters, Config::filterKind) with the states of Burgers, 2-D Euler and
 // shallow water; 6: the 1-D Euler entropy closure; 7: the linear closures with
-// its three states.
+// its three states; 8: LogSin (one state).
 enum ClosureKind {
     CL_BOUNDED_BARRIER = 0,
     CL_EULER2D         = 1,
@@ -26,10 +26,13 @@ enum ClosureKind {
     CL_LINEAR_EULER2D  = 4,
     CL_LINEAR_SW       = 5,
     CL_EULER1D         = 6,    // EulerClosure, three states
-    CL_LINEAR_EULER1D  = 7
+    CL_LINEAR_EULER1D  = 7,
+    CL_LOGSIN          = 8     // LogSin, one state (Burgers)
 };
 enum FilterKind { FILTER_SG = 0, FILTER_L2 = 1, FILTER_LASSO = 2 };
-inline int closure_states( int cl ) { return ( cl == 0 || cl == 3 ) ? 1 : ( ( cl == 1 || cl == 4 ) ? 4 : ( ( cl == 6 || cl == 7 ) ? 3 : 2 ) ); }
+inline int closure_states( int cl ) {
+    return ( cl == 0 || cl == 3 || cl == 8 ) ? 1 : ( ( cl == 1 || cl == 4 ) ? 4 : ( ( cl == 6 || cl == 7 ) ? 3 : 2 ) );
+}
 inline bool closure_linear( int cl ) { return ( cl >= CL_LINEAR_BURGERS && cl <= CL_LINEAR_SW ) || cl == CL_LINEAR_EULER1D; }
 enum ProblemKind { PR_BURGERS = 0, PR_EULER2D = 1, PR_SHALLOW_WATER = 2, PR_EULER1D = 3 };
 

@@ -31,5 +31,6 @@ void* kernel_euler2d( int group, int which );
 void* kernel_shallow_water( int group, int which );
 void* kernel_linear( int cl, int group, int which );    // kinds 3-5
 void* kernel_euler1d( int cl, int group, int which );   // kinds 6, 7
+void* kernel_logsin( int group, int which );            // kind 8
 
 }    // namespace uqc

@@ -152,6 +152,35 @@ template <> struct Closure<4> : LinearClosure<4> {};
 template <> struct Closure<5> : LinearClosure<2> {};
 template <> struct Closure<7> : LinearClosure<3> {};
 
+// ---------------------------------------------------------------- LogSin
+// LogSin (logsin.cpp:3-50): one state, U = ((u+ - u-) / PI) (PI / 2 + atan
+// Lambda) + u-, DU = ((u+ - u-) / PI) / (Lambda^2 + 1), with the reference's
+// PI = 3.14159265359 (mathtools.h:8) and its fixed bounds: u- = 1 - 0.1,
+// u+ = 12 + 0.1 + 0.2 with two uncertain dimensions, else u- = 3 - 0.1,
+// u+ = 12 + 0.1. DS of the base class (zero).
+template <> struct Closure<8> {
+    static constexpr int NS = 1, NP = 1;
+    static constexpr bool LINEAR = false;
+    __host__ __device__ static void bounds( const PhysParams& p, double& lo, double& hi ) {
+        const double du = 0.1;
+        lo              = p.dimXi == 2 ? 1.0 - du : 3.0 - du;
+        hi              = p.dimXi == 2 ? 12.0 + du + 0.2 : 12.0 + du;
+    }
+    __host__ __device__ static void U( const double* L, double* u, bool, const PhysParams& p ) {
+        const double pi = 3.14159265359;
+        double lo, hi;
+        bounds( p, lo, hi );
+        u[0] = ( ( hi - lo ) / pi ) * ( pi / 2 + atan( L[0] ) ) + lo;
+    }
+    __host__ __device__ static void DU( const double* L, double* du, const PhysParams& p ) {
+        const double pi = 3.14159265359;
+        double lo, hi;
+        bounds( p, lo, hi );
+        du[0] = ( ( hi - lo ) / pi ) / ( L[0] * L[0] + 1.0 );
+    }
+    __host__ __device__ static void DS( const double*, double* ds, const PhysParams& ) { ds[0] = 0.0; }
+};
+
 // ---------------------------------------------------------------- Euler 1-D
 // EulerClosure (eulerclosure.cpp:7-80): three states (rho, rho u, rho E), the
 // gamma of [problem] gamma. DU is packed as the entries the reference's Newton
@@ -376,5 +405,6 @@ template <> struct Problem<6> {
     }
 };
 template <> struct Problem<7> : Problem<6> {};
+template <> struct Problem<8> : Problem<0> {};    // LogSin with Burgers
 
 }    // namespace uqc

@@ -300,6 +300,7 @@ void* pick( int cl, int group, int which ) {
     if( cl == 2 ) fn = kernel_shallow_water( group, which );
     if( closure_linear( cl ) && cl != CL_LINEAR_EULER1D ) fn = kernel_linear( cl, group, which );
     if( cl == CL_EULER1D || cl == CL_LINEAR_EULER1D ) fn = kernel_euler1d( cl, group, which );
+    if( cl == CL_LOGSIN ) fn = kernel_logsin( group, which );
     if( !fn ) throw ConfigError( "no kernel for this closure" );
     return fn;
 }
@@ -1442,7 +1443,8 @@ static void host_closure_ds( int cl, const double* u, double* d, const PhysParam
         case 4: Closure<4>::DS( u, d, pp ); break;
         case 5: Closure<5>::DS( u, d, pp ); break;
         case 6: Closure<6>::DS( u, d, pp ); break;
-        default: Closure<7>::DS( u, d, pp ); break;
+        case 7: Closure<7>::DS( u, d, pp ); break;
+        default: Closure<8>::DS( u, d, pp ); break;
     }
 }
 static void host_closure_u( int cl, const double* L, double* y, const PhysParams& pp ) {
@@ -1454,7 +1456,8 @@ static void host_closure_u( int cl, const double* L, double* y, const PhysParams
         case 4: Closure<4>::U( L, y, false, pp ); break;
         case 5: Closure<5>::U( L, y, false, pp ); break;
         case 6: Closure<6>::U( L, y, false, pp ); break;
-        default: Closure<7>::U( L, y, false, pp ); break;
+        case 7: Closure<7>::U( L, y, false, pp ); break;
+        default: Closure<8>::U( L, y, false, pp ); break;
     }
 }
 
