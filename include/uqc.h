@@ -102,7 +102,12 @@ typedef struct uqc_step_info {
  * SU2BC = [["marker", "dirichlet" | "noslip" | "swwall"], ...];
  * Mesh2D::LoadSU2MeshFromFile, mesh2d.cpp:5-259; "neumann" and "periodic"
  * are refused with UQC_ERR_CONFIG), or the seeded "tri_jitter" mesh of the
- * [uqc] table. */
+ * [uqc] table. Problems: Burgers1D, Euler1D, Euler2D, ShallowWater1D;
+ * closures: BoundedBarrier, LogSin, Euler, Euler2D, ShallowWater and the
+ * linear StochasticGalerkin, L2Filter, LassoFilter (with any of the problems'
+ * states). ExponentialFilter, ShallowWater2D and PNEquations2D return
+ * UQC_ERR_CONFIG with the reason (the reference's code for them is undefined,
+ * unfinished or racy). */
 int uqc_create_from_file( const char* toml_path, void* cuda_stream, uqc_solver** out, char* err, int err_len );
 /* Same, from TOML text in memory; files it names are relative to the working directory. */
 int uqc_create_from_string( const char* toml_text, void* cuda_stream, uqc_solver** out, char* err, int err_len );
