@@ -117,7 +117,7 @@ int uqc_create_from_string( const char* toml_text, void* cuda_stream, uqc_solver
  * key is optional; uqc_config_defaults fills the reference's defaults. The
  * handle is the one uqc_create_from_string makes from the equivalent file. */
 typedef struct uqc_config {
-    const char* problem;        /* [general] problem: "Burgers1D", "Euler2D", "ShallowWater1D" */
+    const char* problem;        /* [general] problem: "Burgers1D", "Euler1D", "Euler2D", "ShallowWater1D" */
     const char* restart_file;   /* [general] restartFile (NULL: none) */
     int import_dual_state;      /* [general] importDualState */
     int mesh_dimension;         /* [mesh] dimension: 1 or 2 */
@@ -133,7 +133,8 @@ typedef struct uqc_config {
     double t_end;               /* [problem] tEnd */
     double min_residual;        /* [problem] residual (negative: not set) */
     double gamma;               /* [problem] gamma (Euler; 0: default 1.4) */
-    const char* closure;        /* [moment_system] closure: "BoundedBarrier", "Euler2D", "ShallowWater" */
+    const char* closure;        /* [moment_system] closure: "BoundedBarrier", "LogSin", "Euler", "Euler2D", "ShallowWater",
+                                   "StochasticGalerkin", "L2Filter", "LassoFilter" */
     int max_degree;             /* [moment_system] moments = [["maxDegree"|"totalDegree"], [degrees]] */
     int n_levels;               /* refinement levels: degree[0..n_levels-1] */
     int degree[16];
