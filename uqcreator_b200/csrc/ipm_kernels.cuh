@@ -1446,13 +1446,17 @@ __device__ __forceinline__ void finish_cell( const KParams& P, int cell, double 
 // WALL: the mesh has wall cells (ghost states at their boundary faces); the
 // instance without walls evaluates two nodes per lane at a time (independent
 // flux chains for the scheduler) with no ghost-state code.
-// CTAs per SM the register budget is cut for: 2 with three or four states, 3
-// with two, 4 with one (the small systems are latency-bound on the loads of the
-// neighbours' nodal states; more resident warps hide it)
-template <int CL> constexpr int update_min_ctas() { return Closure<CL>::NS >= 3 ? 2 : ( Closure<CL>::NS == 2 ? 3 : 4 ); }
+// CTAs per SM the register budget is cut for: 2 with three or four states, 4
+// with one or two (3 for two states with the next-step test, which would spill
+// more at 64 registers). The small systems are latency-bound on the loads of
+// the neighbours' nodal states; more resident warps hide it (measured, 1M-cell
+// shallow water: 2.33 / 1.78 / 1.61 ms at 2 / 3 / 4 CTAs per SM).
+template <int CL, bool FIN> constexpr int update_min_ctas() {
+    return Closure<CL>::NS >= 3 ? 2 : ( Closure<CL>::NS == 2 && FIN ? 3 : 4 );
+}
 
 template <int CL, bool FIN, bool WALL>
-__global__ void __launch_bounds__( 256, update_min_ctas<CL>() ) k_update( KParams P ) {
+__global__ void __launch_bounds__( 256, ( update_min_ctas<CL, FIN>() ) ) k_update( KParams P ) {
     const bool finish = FIN && P.finishInUpdate;
     constexpr int NS = Closure<CL>::NS;
     extern __shared__ __align__( 16 ) double smem[];
