@@ -599,10 +599,13 @@ void plan_launches( uqc_solver* h ) {
         h->updateBlock = 32 * warps;
         h->updateSmem  = uTables + size_t( warps ) * perWarp;
         const bool walls = h->d_bndNormal != nullptr;
-        void* ku         = pick( cl, h->group, walls ? KERNEL_UPDATE_WALL : KERNEL_UPDATE );
-        allow_dynamic_smem( ku );
-        allow_dynamic_smem( pick( cl, h->group, walls ? KERNEL_UPDATE_PLAIN_WALL : KERNEL_UPDATE_PLAIN ) );
-        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ku, h->updateBlock, h->updateSmem ) );
+        void* kf         = pick( cl, h->group, walls ? KERNEL_UPDATE_WALL : KERNEL_UPDATE );
+        void* kp         = pick( cl, h->group, walls ? KERNEL_UPDATE_PLAIN_WALL : KERNEL_UPDATE_PLAIN );
+        allow_dynamic_smem( kf );
+        allow_dynamic_smem( kp );
+        // the grid fills the SMs for the variant the steps launch (the two
+        // variants may differ in registers, so in CTAs per SM)
+        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, update_test_on( h ) ? kf : kp, h->updateBlock, h->updateSmem ) );
         h->updateGrid = std::max( 1, occ ) * h->numSMs;
         h->updateGrid = std::min( h->updateGrid, std::max( 1, ( h->mesh.nCells + warps - 1 ) / warps ) );
         // one residual partial per CTA of k_update (grows with the grid; a
@@ -1296,6 +1299,7 @@ int uqc_set_option( uqc_solver* h, const char* key, double value ) {
         h->finishInUpdateOpt = int( value );
         ++h->planGen;
         return guarded( h, [&] {
+            if( h->deviceReady ) plan_launches( h );    // the update grid follows the variant
             invalidate_lists( h );
             return UQC_OK;
         } );
