@@ -8,6 +8,9 @@ What it chooses, per configuration shape:
   below which a cell's held inverse is re-formed (more re-factorisations mean
   fewer, dearer iterations), and the re-factorisation rounds per step before
   the FP64 form takes the remaining cells;
+- where the next step's convergence test runs: in the update kernel, which
+  then lists the cells that need Newton or a level change (update_test 1), or
+  in the check kernel over every cell (0);
 - CTA sizes: cells (warps) per CTA of the chord kernel, the convergence-check
   kernel and the update kernel (occupancy against shared memory and
   registers, and the grain of the work stealing).
@@ -58,13 +61,14 @@ def groups(n_per_cell: int, mixed_form: int = 0):
     out = [("closure" if mixed_form == 0 else "schedule", candidates(n_per_cell, mixed_form))]
     if mixed_form >= 1:
         out.append(("chord_cta", [{"chord_warps": w} for w in (8, 12, 16)]))
+    out.append(("update_test", [{"update_test": v} for v in (1, 0)]))
     out.append(("check_cta", [{"check_warps": w} for w in (8, 16)]))
     out.append(("update_cta", [{"update_warps": w} for w in (4, 8, 16)]))
     return out
 
 
 def _key(solver, precision, mixed_form):
-    return (f"v2_s{solver.n_states}_t{solver.n_total}_q{solver.n_quad}_l{solver.n_levels}_d{solver.dim_xi}_p{precision}"
+    return (f"v3_s{solver.n_states}_t{solver.n_total}_q{solver.n_quad}_l{solver.n_levels}_d{solver.dim_xi}_p{precision}"
             f"_m{mixed_form if precision else 0}")
 
 
