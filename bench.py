@@ -555,6 +555,11 @@ def run_b200(args, rank, world, local):
         line["moment_rel_l1_vs_oracle_strip"] = oracle_strip_errors(forms)
     if args.serve_requests > 0:
         line["serving"] = run_serving(args, MIXED if chosen == "mixed" else FP64)
+    if not args.no_other_configs:
+        # the other configurations in the same run (GPU only; `--configs` adds the CPU samples)
+        s.close()
+        line["other_configs"] = {name: config_gpu(name, mk, st) for name, (mk, _p, _i, _b, _n, st, _s) in _configs().items()
+                                 if not name.startswith("C2")}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             cb, *_ = cpu_reference_run(0, 2, min_seconds=args.cpu_seconds)
@@ -582,41 +587,47 @@ def _configs():
     }
 
 
-def run_configs(args):
-    """One JSON line per configuration: GPU FP64 and mixed cell-steps/s from the
-    same state (C1: the whole 0.11 s solve, CUDA graphs), the mixed form's
-    moment error against the FP64 form, and the reference's own C++ (OpenMP)
-    on a sample of the configuration."""
+def config_gpu(name, mk, steps):
+    """GPU FP64 and mixed cell-steps/s of one configuration from the same state
+    (steps 0: the whole solve, CUDA graphs; else 3 warm-up steps, then `steps`
+    timed by CUDA events) and the mixed form's moment error against the FP64
+    form after them."""
     import torch
+    from uqcreator_b200 import Solver, MIXED
+    toml = mk()
+    out = {"config": name}
+    states = {}
+    for form in ("fp64", "mixed"):
+        s = Solver(toml)
+        s.init_state()
+        if form == "mixed":
+            s.set_precision(MIXED)
+        if steps == 0:    # whole solve
+            s.run(1e-3)
+            torch.cuda.synchronize(); t0 = time.perf_counter()
+            info = s.run(s.settings.GetTEnd())
+            torch.cuda.synchronize(); el = time.perf_counter() - t0
+            done = info["steps"]
+        else:
+            s.step(3)
+            s.step(steps)
+            el = sum(s.last_timing()[2:3]) / 1e3
+            done = steps
+        out[form] = {"cell_steps_per_s": s.n_cells * done / el, "ms_per_step": 1e3 * el / done, "steps": done}
+        states[form] = s.download_state()[0]
+        s.close()
+    uf, um = states["fp64"], states["mixed"]
+    out["mixed_over_fp64"] = out["mixed"]["cell_steps_per_s"] / out["fp64"]["cell_steps_per_s"]
+    out["moment_rel_l1_mixed_vs_fp64"] = float(np.abs(um - uf).sum() / np.abs(uf).sum())
+    return out
+
+
+def run_configs(args):
+    """One JSON line per configuration: config_gpu's figures and the
+    reference's own C++ (OpenMP) on a sample of the configuration."""
     from oracle import refharness
-    from uqcreator_b200 import Solver, FP64, MIXED
     for name, (mk, problem, ic, bounds, newton, steps, sample) in _configs().items():
-        toml = mk()
-        out = {"config": name}
-        states = {}
-        for form in ("fp64", "mixed"):
-            s = Solver(toml)
-            s.init_state()
-            if form == "mixed":
-                s.set_precision(MIXED)
-            if steps == 0:    # whole solve
-                s.run(1e-3)
-                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                torch.cuda.synchronize(); t0 = time.perf_counter()
-                info = s.run(s.settings.GetTEnd())
-                torch.cuda.synchronize(); el = time.perf_counter() - t0
-                done = info["steps"]
-            else:
-                s.step(3)
-                s.step(steps)
-                el = sum(s.last_timing()[2:3]) / 1e3
-                done = steps
-            out[form] = {"cell_steps_per_s": s.n_cells * done / el, "ms_per_step": 1e3 * el / done, "steps": done}
-            states[form] = s.download_state()[0]
-            s.close()
-        uf, um = states["fp64"], states["mixed"]
-        out["mixed_over_fp64"] = out["mixed"]["cell_steps_per_s"] / out["fp64"]["cell_steps_per_s"]
-        out["moment_rel_l1_mixed_vs_fp64"] = float(np.abs(um - uf).sum() / np.abs(uf).sum())
+        out = config_gpu(name, mk, steps)
         if refharness.available("omp") and not args.no_cpu_baseline:
             st = sample()
             r = refharness.RefSolver(st, problem, ic, bounds=bounds, mesh2d=__import__("uqcreator_b200").workloads.mesh_for(st),
@@ -642,6 +653,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-oracle-strip", action="store_true", help="skip the error against the oracle on the 8,000-cell strip")
     ap.add_argument("--no-autotune", action="store_true", help="time both forms in their default launch shapes")
+    ap.add_argument("--no-other-configs", action="store_true", help="skip the GPU lines of C1, C3 and C5 in the bench line")
     ap.add_argument("--serve-requests", type=int, default=120, help="requests of the serving stream (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=12.0, help="arrivals per second")
     ap.add_argument("--serve-budget-gb", type=float, default=100.0)
