@@ -4,6 +4,8 @@ What it chooses, per configuration shape:
 - closure (FP64 form): a cell on one warp, two warps (several cells per CTA,
   named barriers) or a whole CTA, with the basis tables staged in shared memory
   or read through L1 (which leaves room for more cells per SM);
+- chord schedule of the single mixed kernel: theta and whether the held FP32
+  factor is kept as its packed inverse;
 - chord schedule (mixed form in rounds, 2-D Euler): theta, the contraction
   below which a cell's held inverse is re-formed (more re-factorisations mean
   fewer, dearer iterations), and the re-factorisation rounds per step before
@@ -56,9 +58,15 @@ def candidates(n_per_cell: int, mixed_form: int = 0):
     return [{"closure_group": g, "closure_tables_smem": t} for g in groups for t in (1, 0)]
 
 
-def groups(n_per_cell: int, mixed_form: int = 0):
-    """The option groups of the coordinate descent, in order: (name, candidates)."""
+def groups(n_per_cell: int, mixed_form: int = 0, mixed: bool = False):
+    """The option groups of the coordinate descent, in order: (name, candidates).
+    mixed: the handle runs UQC_MIXED (with mixed_form 0: the single mixed kernel,
+    whose chord schedule is theta and whether the held factor is kept as its
+    inverse)."""
     out = [("closure" if mixed_form == 0 else "schedule", candidates(n_per_cell, mixed_form))]
+    if mixed and mixed_form == 0:
+        out.append(("single_schedule", [{"mixed_chord_theta": t, "mixed_chord_inverse": ci}
+                                        for t in (0.05, 0.1, 0.2, 0.35) for ci in (1, 0)]))
     if mixed_form >= 1:
         out.append(("chord_cta", [{"chord_warps": w} for w in (8, 12, 16)]))
     out.append(("update_test", [{"update_test": v} for v in (1, 0)]))
@@ -68,7 +76,7 @@ def groups(n_per_cell: int, mixed_form: int = 0):
 
 
 def _key(solver, precision, mixed_form):
-    return (f"v3_s{solver.n_states}_t{solver.n_total}_q{solver.n_quad}_l{solver.n_levels}_d{solver.dim_xi}_p{precision}"
+    return (f"v4_s{solver.n_states}_t{solver.n_total}_q{solver.n_quad}_l{solver.n_levels}_d{solver.dim_xi}_p{precision}"
             f"_m{mixed_form if precision else 0}")
 
 
@@ -111,7 +119,7 @@ def autotune(solver, steps: int = 2, repeats: int = 2, cache: Path | None = DEFA
             best_ms = ms if best_ms is None or ms < best_ms else best_ms
         return best_ms
 
-    for gname, cands in groups(solver.n_states * solver.n_total, mixed_form):
+    for gname, cands in groups(solver.n_states * solver.n_total, mixed_form, info.precision == 1):
         group_best, group_ms = None, None
         for opts in cands:
             name = ",".join(f"{k}={v}" for k, v in opts.items())

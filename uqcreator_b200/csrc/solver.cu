@@ -594,18 +594,33 @@ void plan_launches( uqc_solver* h ) {
     {
         const size_t uTables = h->tablesInSmem ? ( ( size_t( nQ ) * h->ld + 4 + 3 ) & ~size_t( 3 ) ) * sizeof( double ) : 0;
         const size_t perWarp = update_warp_doubles( nS, nQ ) * sizeof( double );
-        const int warps      = int( std::min<size_t>( h->updateWarpsOpt ? h->updateWarpsOpt : 8, ( size_t( maxSmem ) - uTables ) / perWarp ) );
+        const bool walls     = h->d_bndNormal != nullptr;
+        void* kf             = pick( cl, h->group, walls ? KERNEL_UPDATE_WALL : KERNEL_UPDATE );
+        void* kp             = pick( cl, h->group, walls ? KERNEL_UPDATE_PLAIN_WALL : KERNEL_UPDATE_PLAIN );
+        void* ku             = update_test_on( h ) ? kf : kp;    // the variant the steps launch
+        allow_dynamic_smem( kf );
+        allow_dynamic_smem( kp );
+        // warps per CTA: the option, else the count of 8, 4 or 2 that keeps the
+        // most warps resident per SM (per-warp flux buffers of many nodes fill
+        // shared memory before the registers run out; ties: the larger CTA)
+        int warps = 0, bestResident = -1;
+        for( int w : {8, 4, 2} ) {
+            if( h->updateWarpsOpt && w != 8 ) break;
+            const int cand = int( std::min<size_t>( h->updateWarpsOpt ? h->updateWarpsOpt : w, ( size_t( maxSmem ) - uTables ) / perWarp ) );
+            if( cand < 1 ) continue;
+            int o = 0;
+            CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &o, ku, 32 * cand, uTables + size_t( cand ) * perWarp ) );
+            if( o * cand > bestResident ) {
+                bestResident = o * cand;
+                warps        = cand;
+            }
+        }
         if( warps < 1 ) throw ConfigError( "update workspace exceeds shared memory" );
         h->updateBlock = 32 * warps;
         h->updateSmem  = uTables + size_t( warps ) * perWarp;
-        const bool walls = h->d_bndNormal != nullptr;
-        void* kf         = pick( cl, h->group, walls ? KERNEL_UPDATE_WALL : KERNEL_UPDATE );
-        void* kp         = pick( cl, h->group, walls ? KERNEL_UPDATE_PLAIN_WALL : KERNEL_UPDATE_PLAIN );
-        allow_dynamic_smem( kf );
-        allow_dynamic_smem( kp );
-        // the grid fills the SMs for the variant the steps launch (the two
-        // variants may differ in registers, so in CTAs per SM)
-        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, update_test_on( h ) ? kf : kp, h->updateBlock, h->updateSmem ) );
+        // the grid fills the SMs for that variant (the two variants may differ
+        // in registers, so in CTAs per SM)
+        CK( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, ku, h->updateBlock, h->updateSmem ) );
         h->updateGrid = std::max( 1, occ ) * h->numSMs;
         h->updateGrid = std::min( h->updateGrid, std::max( 1, ( h->mesh.nCells + warps - 1 ) / warps ) );
         // one residual partial per CTA of k_update (grows with the grid; a
