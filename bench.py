@@ -430,7 +430,7 @@ def run_b200_sharded(args, rank, world, local):
 
 
 def run_b200(args, rank, world, local):
-    if world > 1:
+    if world > 1 or args.sharded:
         return run_b200_sharded(args, rank, world, local)
     import torch
     from uqcreator_b200 import Solver, workloads as W, FP64, MIXED
@@ -654,6 +654,8 @@ def main():
     ap.add_argument("--no-oracle-strip", action="store_true", help="skip the error against the oracle on the 8,000-cell strip")
     ap.add_argument("--no-autotune", action="store_true", help="time both forms in their default launch shapes")
     ap.add_argument("--no-other-configs", action="store_true", help="skip the GPU lines of C1, C3 and C5 in the bench line")
+    ap.add_argument("--sharded", action="store_true",
+                    help="N = 1: run the sharded path (one shard, a one-rank NCCL group) that N > 1 runs")
     ap.add_argument("--serve-requests", type=int, default=120, help="requests of the serving stream (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=12.0, help="arrivals per second")
     ap.add_argument("--serve-budget-gb", type=float, default=100.0)
@@ -665,6 +667,15 @@ def main():
     ap.add_argument("--configs", action="store_true", help="one line per configuration (C1, C2, C3, C5) instead of the bench line")
     args = ap.parse_args()
     rank, world, local = dist_init()
+    one_rank_group = False
+    if args.sharded and world == 1 and args.impl == "b200":
+        import socket
+        import torch.distributed as dist
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+        dist.init_process_group("cpu:gloo,cuda:nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+        one_rank_group = True
     if args.serving_only:
         if rank == 0:
             import torch
@@ -678,7 +689,7 @@ def main():
         run_reference(args, rank, world)
     else:
         run_b200(args, rank, world, local)
-    if world > 1:
+    if world > 1 or one_rank_group:
         import torch.distributed as dist
         dist.destroy_process_group()
 
