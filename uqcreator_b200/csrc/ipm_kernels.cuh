@@ -300,12 +300,48 @@ __device__ void eval_u( const Grp<GROUP>& g, const KParams& P, const double* L, 
 // sum_(s,i) (m - uh)^2 of this thread. Warp groups: a thread per basis
 // function i, its NS sums as independent chains sharing each table value (one
 // table load per NS FMAs, one chain of nQ per sum, in node order as
-// node_dot's single chain); CTA groups: a thread per (s, i) with node_dot.
+// node_dot's single chain; a single warp with nTj <= 16 also splits the nodes
+// over lane groups); CTA groups: a thread per (s, i) with node_dot.
 // gout (compact stride nTj) and ms (stride nT) may be null.
 template <int NS, int GROUP>
 __device__ __forceinline__ double gradient_sums( const Grp<GROUP>& g, const KParams& P, const double* phiWf, const double* uk, const double* uh,
                                                  int nTj, double* gout, double* ms ) {
     double sq = 0.0;
+    if constexpr( GROUP == 32 ) {
+        if( nTj <= 16 ) {
+            // few basis functions: the warp splits the nodes as well, lane =
+            // i + w part (w = nTj rounded up to a power of two), each part
+            // summing the nodes k = part (mod 32 / w), then a butterfly over
+            // the parts (a fixed order, so the sums are reproducible)
+            int w = 1;
+            while( w < nTj ) w <<= 1;
+            const int i = g.r & ( w - 1 ), part = g.r / w, parts = 32 / w;
+            double a[NS];
+#pragma unroll
+            for( int st = 0; st < NS; ++st ) a[st] = 0.0;
+            if( i < nTj ) {
+                const double* t = phiWf + size_t( part ) * P.ld + i;
+                for( int k = part; k < P.nQ; k += parts, t += size_t( parts ) * P.ld ) {
+                    const double wk = *t;
+#pragma unroll
+                    for( int st = 0; st < NS; ++st ) a[st] = fma( uk[st * P.nQ + k], wk, a[st] );
+                }
+            }
+#pragma unroll
+            for( int st = 0; st < NS; ++st )
+                for( int o = w; o < 32; o <<= 1 ) a[st] += __shfl_xor_sync( 0xffffffffu, a[st], o );
+            if( part == 0 && i < nTj ) {
+#pragma unroll
+                for( int st = 0; st < NS; ++st ) {
+                    if( ms ) ms[st * P.nT + i] = a[st];
+                    const double d = a[st] - uh[st * P.nT + i];
+                    if( gout ) gout[st * nTj + i] = d;
+                    sq += d * d;
+                }
+            }
+            return sq;
+        }
+    }
     if constexpr( GROUP <= 64 ) {
         for( int i = g.r; i < nTj; i += GROUP ) {
             double a[NS];
