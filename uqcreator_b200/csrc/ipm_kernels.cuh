@@ -1436,8 +1436,11 @@ __device__ __forceinline__ void project_lane( const double* Gs, const double* t,
     }
 }
 
-// doubles per warp of k_update's shared memory: the nodal flux sums and 16 of face data
-__host__ __device__ inline size_t update_warp_doubles( int nS, int nQ ) { return ( ( size_t( nS ) * nQ + 3 ) & ~size_t( 3 ) ) + 16; }
+// doubles per warp of k_update's shared memory: the nodal flux sums, 16 of
+// face data, and the face fluxes of the nodes after the last full 64-node block
+__host__ __device__ inline size_t update_warp_doubles( int nS, int nQ, int nFaces ) {
+    return ( ( size_t( nS ) * nQ + 3 ) & ~size_t( 3 ) ) + 16 + ( ( size_t( nFaces ) * ( nQ & 63 ) * nS + 3 ) & ~size_t( 3 ) );
+}
 
 // Warp-buffered append to a device list (warp-uniform call): lane `cnt` keeps
 // the entry; 32 entries take one atomicAdd on the list length.
@@ -1511,7 +1514,7 @@ __global__ void __launch_bounds__( 256, ( update_min_ctas<CL, FIN>() ) ) k_updat
     }
     // per warp: the summed nodal fluxes (NS x nQ, node-major), then the cell's
     // face data: unit normal (2), scaled normal (2) and length of each face
-    double* Gs       = base + size_t( warp ) * update_warp_doubles( NS, P.nQ );
+    double* Gs       = base + size_t( warp ) * update_warp_doubles( NS, P.nQ, P.nFaces );
     double* fd       = Gs + ( ( size_t( NS ) * P.nQ + 3 ) & ~size_t( 3 ) );
     const double dt  = __longlong_as_double( (long long)P.ctl->dtBits );
     const size_t ldc = size_t( NS ) * P.nT;
@@ -1563,6 +1566,8 @@ __global__ void __launch_bounds__( 256, ( update_min_ctas<CL, FIN>() ) ) k_updat
         }
 #pragma unroll
         for( int f = 0; f < 3; ++f ) {
+            ghost[f] = false;
+            ub[f]    = ua;
             if( f < P.nFaces ) {
                 const int nb = P.nbr[cell * P.nFaces + f];
                 ghost[f]     = wall && nb == P.nCells;
@@ -1609,10 +1614,11 @@ __global__ void __launch_bounds__( 256, ( update_min_ctas<CL, FIN>() ) ) k_updat
             }
         }
         else {
-            // nodes k and k + 32 together; a lane without a second node repeats its first
-            for( int k0 = lane; k0 < P.nQ; k0 += 64 ) {
-                const bool two = k0 + 32 < P.nQ;
-                const int k1   = two ? k0 + 32 : k0;
+            // nodes k and k + 32 together over the full 64-node blocks
+            const int kPair = P.nQ & ~63;
+            for( int k0 = lane; k0 < kPair; k0 += 64 ) {
+                const bool two = true;
+                const int k1   = k0 + 32;
                 double a0[NS], a1[NS], g0[NS], g1[NS];
 #pragma unroll
                 for( int s = 0; s < NS; ++s ) {
@@ -1643,6 +1649,51 @@ __global__ void __launch_bounds__( 256, ( update_min_ctas<CL, FIN>() ) ) k_updat
                 if( two ) {
 #pragma unroll
                     for( int s = 0; s < NS; ++s ) Gs[k1 * NS + s] = g1[s];
+                }
+            }
+            // the remaining R = nQ mod 64 nodes: a slot per (face, node), two
+            // slots per lane at a time (a lane without a second slot repeats its
+            // first), so that no lane idles for a whole face; the fluxes go to
+            // the scratch, then each node's are summed in face order as above
+            const int R = P.nQ - kPair;
+            if( R > 0 ) {
+                double* Yt  = fd + 16;
+                const int S = P.nFaces * R;
+                for( int j0 = lane; j0 < S; j0 += 64 ) {
+                    const bool two = j0 + 32 < S;
+                    const int j1   = two ? j0 + 32 : j0;
+                    const int f0 = j0 / R, k0 = kPair + j0 - f0 * R;
+                    const int f1 = j1 / R, k1 = kPair + j1 - f1 * R;
+                    const double* n0 = f0 == 0 ? ub[0] : ( f0 == 1 ? ub[1] : ub[2] );
+                    const double* n1 = f1 == 0 ? ub[0] : ( f1 == 1 ? ub[1] : ub[2] );
+                    double a0[NS], a1[NS], b0[NS], b1[NS], y0[NS], y1[NS];
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) {
+                        a0[s] = ua[s * P.nQ + k0];
+                        a1[s] = ua[s * P.nQ + k1];
+                        b0[s] = n0[s * P.nQ + k0];
+                        b1[s] = n1[s * P.nQ + k1];
+                    }
+                    Problem<CL>::flux( a0, b0, fd + 5 * f0, fd + 5 * f0 + 2, fd[5 * f0 + 4], y0, P.phys );
+                    Problem<CL>::flux( a1, b1, fd + 5 * f1, fd + 5 * f1 + 2, fd[5 * f1 + 4], y1, P.phys );
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) Yt[j0 * NS + s] = y0[s];
+                    if( two ) {
+#pragma unroll
+                        for( int s = 0; s < NS; ++s ) Yt[j1 * NS + s] = y1[s];
+                    }
+                }
+                __syncwarp();
+                for( int t = lane; t < R; t += 32 ) {
+                    double gsum[NS];
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) gsum[s] = 0.0;
+                    for( int f = 0; f < P.nFaces; ++f ) {
+#pragma unroll
+                        for( int s = 0; s < NS; ++s ) gsum[s] += Yt[( f * R + t ) * NS + s];
+                    }
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) Gs[( kPair + t ) * NS + s] = gsum[s];
                 }
             }
         }

@@ -593,7 +593,7 @@ void plan_launches( uqc_solver* h ) {
     // update kernel: a warp per cell; phiWf + one node-flux buffer per warp
     {
         const size_t uTables = h->tablesInSmem ? ( ( size_t( nQ ) * h->ld + 4 + 3 ) & ~size_t( 3 ) ) * sizeof( double ) : 0;
-        const size_t perWarp = update_warp_doubles( nS, nQ ) * sizeof( double );
+        const size_t perWarp = update_warp_doubles( nS, nQ, h->mesh.nFaces ) * sizeof( double );
         const bool walls     = h->d_bndNormal != nullptr;
         void* kf             = pick( cl, h->group, walls ? KERNEL_UPDATE_WALL : KERNEL_UPDATE );
         void* kp             = pick( cl, h->group, walls ? KERNEL_UPDATE_PLAIN_WALL : KERNEL_UPDATE_PLAIN );
