@@ -1409,14 +1409,22 @@ template <int CL> __device__ __forceinline__ void wall_ghost( const double* a, c
 }
 
 // rhs(s, i) = sum_k Gs(s, k) phiWf(k, i) for one i (t = phiWf + i), the NS
-// states as independent chains sharing each table value.
+// states as independent chains sharing each table value; SPLIT: over the nodes
+// k = k0, k0 + dk, ... only (a separate instance: the contiguous loop's
+// constant strides keep its addressing cheap).
 // Gs is node-major (Gs[k NS + s]), so a node's NS values come in 16-byte
 // shared-memory loads.
-template <int NS>
-__device__ __forceinline__ void project_lane( const double* Gs, const double* t, int ld, int nQ, double* r ) {
+template <int NS, bool SPLIT = false>
+__device__ __forceinline__ void project_lane( const double* Gs, const double* t, int ld, int nQ, double* r, int k0 = 0, int dk = 1 ) {
 #pragma unroll
     for( int s = 0; s < NS; ++s ) r[s] = 0.0;
-    for( int k = 0; k < nQ; ++k, t += ld ) {
+    if constexpr( !SPLIT ) {
+        k0 = 0;
+        dk = 1;
+    }
+    t += size_t( k0 ) * ld;
+    const size_t tStep = size_t( dk ) * ld;
+    for( int k = k0; k < nQ; k += dk, t += tStep ) {
         const double w = *t;
         double g[NS];
         if constexpr( NS % 2 == 0 ) {
@@ -1485,6 +1493,10 @@ __device__ __forceinline__ void finish_cell( const KParams& P, int cell, double 
 // WALL: the mesh has wall cells (ghost states at their boundary faces); the
 // instance without walls evaluates two nodes per lane at a time (independent
 // flux chains for the scheduler) with no ghost-state code.
+// SPLIT: a level's last block of m <= 16 basis functions also splits the nodes
+// over lane groups in the projection (an instance of its own: the second copy
+// of the projection loop measured 1.7 % slower on 2-D Euler with 21 functions,
+// which never takes it; 10 % faster on 35 functions and 512 nodes).
 // CTAs per SM the register budget is cut for: 2 with three or four states, 4
 // with one or two (3 for two states with the next-step test, which would spill
 // more at 64 registers). The small systems are latency-bound on the loads of
@@ -1494,7 +1506,7 @@ template <int CL, bool FIN> constexpr int update_min_ctas() {
     return Closure<CL>::NS >= 3 ? 2 : ( Closure<CL>::NS == 2 && FIN ? 3 : 4 );
 }
 
-template <int CL, bool FIN, bool WALL>
+template <int CL, bool FIN, bool WALL, bool SPLIT>
 __global__ void __launch_bounds__( 256, ( update_min_ctas<CL, FIN>() ) ) k_update( KParams P ) {
     const bool finish = FIN && P.finishInUpdate;
     constexpr int NS = Closure<CL>::NS;
@@ -1703,14 +1715,7 @@ __global__ void __launch_bounds__( 256, ( update_min_ctas<CL, FIN>() ) ) k_updat
         const double c = dt / P.area[cell];
         double sq      = 0.0;
         double v0a = 0.0, v0b = 0.0;    // u_new(0, lane) and u_new(0, lane + 32), for the level rule
-        for( int i = lane; i < nTj; i += 32 ) {    // beyond the level u stays zero (epilogue)
-            // the re-projected moments first: their loads overlap the
-            // projection (uRe and u may alias, so a load after a store to u
-            // could not be moved ahead of it)
-            double old[NS], r[NS];
-#pragma unroll
-            for( int s = 0; s < NS; ++s ) old[s] = P.uRe[cell * ldc + s * P.nT + i];
-            project_lane<NS>( Gs, phiWf + i, P.ld, P.nQ, r );
+        auto apply     = [&]( int i, const double* old, const double* r ) {
 #pragma unroll
             for( int s = 0; s < NS; ++s ) {
                 const double v   = old[s] - r[s] * c;
@@ -1720,6 +1725,47 @@ __global__ void __launch_bounds__( 256, ( update_min_ctas<CL, FIN>() ) ) k_updat
                 if( s == 0 && i < 32 ) v0a = v;
                 if( s == 0 && i >= 32 && i < 64 ) v0b = v;
                 if( s == 0 && i == 0 ) res += fabs( v - P.uOld0[cell] ) * P.area[cell];
+            }
+        };
+        if constexpr( !SPLIT ) {
+            for( int i = lane; i < nTj; i += 32 ) {    // beyond the level u stays zero (epilogue)
+                // the re-projected moments first: their loads overlap the
+                // projection (uRe and u may alias, so a load after a store to u
+                // could not be moved ahead of it)
+                double old[NS], r[NS];
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) old[s] = P.uRe[cell * ldc + s * P.nT + i];
+                project_lane<NS>( Gs, phiWf + i, P.ld, P.nQ, r );
+                apply( i, old, r );
+            }
+        }
+        else {
+            // blocks of 32 functions; a block of m <= 16 (the last) splits the
+            // nodes over 32 / w lane groups too (w = m rounded up to a power
+            // of two), each group summing the nodes k = part (mod 32 / w),
+            // then a butterfly over the groups
+            for( int i0 = 0; i0 < nTj; i0 += 32 ) {
+                const int m = min( 32, nTj - i0 );
+                int w       = 1;
+                while( w < m ) w <<= 1;
+                const int part = lane / w, i = i0 + ( lane & ( w - 1 ) );
+                const bool in  = i < i0 + m;
+                double old[NS], r[NS];
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) {
+                    old[s] = ( in && part == 0 ) ? P.uRe[cell * ldc + s * P.nT + i] : 0.0;
+                    r[s]   = 0.0;
+                }
+                if( in ) {
+                    if( w == 32 )
+                        project_lane<NS>( Gs, phiWf + i, P.ld, P.nQ, r );
+                    else
+                        project_lane<NS, true>( Gs, phiWf + i, P.ld, P.nQ, r, part, 32 / w );
+                }
+#pragma unroll
+                for( int s = 0; s < NS; ++s )
+                    for( int o = w; o < 32; o <<= 1 ) r[s] += __shfl_xor_sync( 0xffffffffu, r[s], o );
+                if( in && part == 0 ) apply( i, old, r );
             }
         }
         if( finish ) {

@@ -22,7 +22,9 @@ enum KernelId {
     KERNEL_INVERT_SWEEP  = 12,   // k_invert_sweep (from k_hess_tc's values, n <= 84)
     KERNEL_UPDATE_WALL   = 13,   // k_update for meshes with wall cells (2-D Euler)
     KERNEL_UPDATE_PLAIN_WALL = 14,
-    KERNEL_CLOSURE_TINY      = 15    // k_closure with the register Newton of tiny systems
+    KERNEL_CLOSURE_TINY      = 15,   // k_closure with the register Newton of tiny systems
+    KERNEL_UPDATE_SPLIT      = 16,   // k_update (with / without the test) whose projection splits
+    KERNEL_UPDATE_PLAIN_SPLIT = 17   // the nodes of a small last block of basis functions
 };
 
 // nullptr when there is no such variant

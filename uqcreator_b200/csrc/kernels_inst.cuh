@@ -29,13 +29,15 @@ template <int CL> void* kernel_of( int group, int which ) {
                 if( group == 64 ) return (void*)&k_closure<CL, 64, float>;
             }
             return nullptr;
-        case KERNEL_UPDATE: return (void*)&k_update<CL, true, false>;
-        case KERNEL_UPDATE_PLAIN: return (void*)&k_update<CL, false, false>;
+        case KERNEL_UPDATE: return (void*)&k_update<CL, true, false, false>;
+        case KERNEL_UPDATE_PLAIN: return (void*)&k_update<CL, false, false, false>;
+        case KERNEL_UPDATE_SPLIT: return (void*)&k_update<CL, true, false, true>;
+        case KERNEL_UPDATE_PLAIN_SPLIT: return (void*)&k_update<CL, false, false, true>;
         case KERNEL_UPDATE_WALL:
-            if constexpr( Closure<CL>::NS == 4 ) return (void*)&k_update<CL, true, true>;
+            if constexpr( Closure<CL>::NS == 4 ) return (void*)&k_update<CL, true, true, false>;
             return nullptr;
         case KERNEL_UPDATE_PLAIN_WALL:
-            if constexpr( Closure<CL>::NS == 4 ) return (void*)&k_update<CL, false, true>;
+            if constexpr( Closure<CL>::NS == 4 ) return (void*)&k_update<CL, false, true, false>;
             return nullptr;
         case KERNEL_INIT:
             if( group == 32 ) return (void*)&k_init<CL, 32>;

@@ -205,6 +205,17 @@ bool update_test_on( const uqc_solver* h ) {
     return h->cfg.newtonMode != 2 && on && !closure_linear( h->cfg.closure );
 }
 
+// The update kernel instance: with or without the next step's test (fin),
+// for meshes with walls, or (no walls) with the node-split projection when a
+// level's last block of 32 basis functions holds 1-16 of them.
+int update_kernel_id( const uqc_solver* h, bool fin ) {
+    if( h->d_bndNormal != nullptr ) return fin ? KERNEL_UPDATE_WALL : KERNEL_UPDATE_PLAIN_WALL;
+    bool split = false;
+    for( int n : h->tab.nTLevel ) split = split || ( n % 32 >= 1 && n % 32 <= 16 );
+    if( split ) return fin ? KERNEL_UPDATE_SPLIT : KERNEL_UPDATE_PLAIN_SPLIT;
+    return fin ? KERNEL_UPDATE : KERNEL_UPDATE_PLAIN;
+}
+
 KParams make_params( const uqc_solver* h ) {
     KParams P{};
     P.nS      = h->nS;
@@ -594,9 +605,8 @@ void plan_launches( uqc_solver* h ) {
     {
         const size_t uTables = h->tablesInSmem ? ( ( size_t( nQ ) * h->ld + 4 + 3 ) & ~size_t( 3 ) ) * sizeof( double ) : 0;
         const size_t perWarp = update_warp_doubles( nS, nQ, h->mesh.nFaces ) * sizeof( double );
-        const bool walls     = h->d_bndNormal != nullptr;
-        void* kf             = pick( cl, h->group, walls ? KERNEL_UPDATE_WALL : KERNEL_UPDATE );
-        void* kp             = pick( cl, h->group, walls ? KERNEL_UPDATE_PLAIN_WALL : KERNEL_UPDATE_PLAIN );
+        void* kf             = pick( cl, h->group, update_kernel_id( h, true ) );
+        void* kp             = pick( cl, h->group, update_kernel_id( h, false ) );
         void* ku             = update_test_on( h ) ? kf : kp;    // the variant the steps launch
         allow_dynamic_smem( kf );
         allow_dynamic_smem( kp );
@@ -968,10 +978,8 @@ void enqueue_update( uqc_solver* h, KParams P ) {
     step_lists( h, P );
     P.finishInUpdate = update_test_on( h );
     void* args[]     = {&P};
-    const bool walls = h->d_bndNormal != nullptr;
-    const int which  = walls ? ( P.finishInUpdate ? KERNEL_UPDATE_WALL : KERNEL_UPDATE_PLAIN_WALL )
-                             : ( P.finishInUpdate ? KERNEL_UPDATE : KERNEL_UPDATE_PLAIN );
-    launch( h, pick( h->cfg.closure, h->group, which ), h->updateGrid, h->updateBlock, h->updateSmem, args );
+    launch( h, pick( h->cfg.closure, h->group, update_kernel_id( h, P.finishInUpdate != 0 ) ), h->updateGrid, h->updateBlock, h->updateSmem,
+            args );
 }
 
 void enqueue_step( uqc_solver* h, KParams& P ) {
