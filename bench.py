@@ -13,7 +13,9 @@ A step is one explicit time step of the hot path (closure for every cell,
 nodal reconstruction, kinetic flux, update). `value` is cell-steps/s of the
 chosen form with the state resident in HBM; `e2e` is the same metric through
 the C ABI with the state uploaded from and downloaded to pinned host memory
-every step. The plain FP64 form is timed in the same run (`fp64`), from the same
+every step (uqc_step_host: one call per step, the copies in chunks beside the
+convergence check and the duals' download beside the update; every step starts
+cold, with no held factors or lists, as after any state upload). The plain FP64 form is timed in the same run (`fp64`), from the same
 state, and the chosen form's moments are compared with it after the K steps.
 
 `serving`: p50/p99 request latency and aggregate cell-steps/s of the request
@@ -504,10 +506,9 @@ def run_b200(args, rank, world, local):
     ev0.record(stream)
     tcur = warm["t"]
     for _ in range(e2e_steps):
-        s.upload_state(hu, hl, hv, t=tcur)
-        inf = s.step(1)
+        # one C-ABI call per step: host state in, host state out (uqc_step_host)
+        inf = s.step_host(hu, hl, hv, t=tcur, out=(hu, hl, hv))[3]
         tcur = inf["t"]
-        s.download_state(out=(hu, hl, hv))
     ev1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(max(ev0.elapsed_time(ev1), 1e3 * (time.perf_counter() - t0)), world)

@@ -266,6 +266,20 @@ int uqc_cell_status( uqc_solver* h, int* status, int* iterations );
 int uqc_step( uqc_solver* h, int n_steps, uqc_step_info* info );
 /* MomentSolver::Solve's time loop to the configured tEnd (or t_end > 0). */
 int uqc_run( uqc_solver* h, double t_end, uqc_step_info* info );
+/* One time step from caller-owned HOST state to host state (the call a
+ * GpuMomentSolver adapter that keeps the reference's _u / _lambda on the host
+ * makes per step, momentsolver.cpp:79-152): the same result as
+ * uqc_upload_state(u_in, lambda_in, level_in, UQC_LAYOUT_STATE_MAJOR, t),
+ * uqc_step(h, 1, info) and uqc_download_state(u_out, lambda_out, level_out,
+ * UQC_LAYOUT_STATE_MAJOR), with the copies beside the kernels: moments and
+ * duals go up in chunks of cells, each chunk's convergence check starting as
+ * its chunk lands; the duals come back while the update runs, the moments and
+ * levels after it. Pinned host memory lets the copies run asynchronously.
+ * level_in NULL keeps the resident levels, level_out NULL skips them; the out
+ * arrays may be the in arrays. uqc_last_timing: [0] from the first copy to the
+ * end of the closure phase, [1] the update. */
+int uqc_step_host( uqc_solver* h, const double* u_in, const double* lambda_in, const unsigned* level_in, double t, double* u_out,
+                   double* lambda_out, unsigned* level_out, uqc_step_info* info );
 /* Mean and variance per cell and state (MomentSolver::WriteMeanAndVar,
  * momentsolver.cpp:302-328): out[j * 2 nS + s] = E, out[j * 2 nS + nS + s] = Var. */
 int uqc_mean_var( uqc_solver* h, double* out );

@@ -32,7 +32,7 @@ EXPORTS = [
     "uqc_server_request", "uqc_server_release", "uqc_server_request_error", "uqc_export_state", "uqc_write_vtk",
     "uqc_debug_mixed_inverse", "uqc_server_set_option", "uqc_solve_closure_cells", "uqc_moments_mean_var",
     "uqc_partition", "uqc_get_shard", "uqc_shard_buffers", "uqc_halo_pack", "uqc_step_phase",
-    "uqc_config_defaults", "uqc_create_from_config",
+    "uqc_config_defaults", "uqc_create_from_config", "uqc_step_host",
 ]
 REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed"}
 NOALLOC_MAX_CELLS = 65536
@@ -125,6 +125,7 @@ def lib() -> C.CDLL:
         "uqc_cell_status": ([_vp, _ip, _ip], C.c_int),
         "uqc_step": ([_vp, C.c_int, C.POINTER(StepInfo)], C.c_int),
         "uqc_run": ([_vp, C.c_double, C.POINTER(StepInfo)], C.c_int),
+        "uqc_step_host": ([_vp, _dp, _dp, _up, C.c_double, _dp, _dp, _up, C.POINTER(StepInfo)], C.c_int),
         "uqc_mean_var": ([_vp, _dp], C.c_int),
         "uqc_closure_solve_host": ([_vp, C.c_int, _dp, _dp, _up, C.c_int, _ip], C.c_int),
         "uqc_closure_solve_device": ([_vp, C.c_int, _vp, _vp, _vp, _vp], C.c_int),

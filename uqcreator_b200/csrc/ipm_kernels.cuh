@@ -96,6 +96,7 @@ struct KParams {
     const double* lassoL1;       // nT: sum_k |phiWf(k, i)|
     int nCells, nFaces, dimXi;
     int nWork;                // cells a time step works on: the first nWork (a shard's owned cells), else nCells
+    int cellBase;             // k_check without a list: cells cellBase .. cellBase + nWork - 1 (0 but for uqc_step_host's chunks)
     double eps;
     int maxIter, newtonMode;
     PhysParams phys;
@@ -1308,7 +1309,7 @@ template <int CL> __global__ void __launch_bounds__( 512, 2 ) k_check( KParams P
     double* red      = uk + size_t( NS ) * P.nQ;
     double dtMin     = 1e300;
     for( int item = blockIdx.x * nWarps + warp; item < nItems; item += gridDim.x * nWarps ) {
-        const int cell = listMode ? P.checkList[size_t( par ) * P.nCells + item] : item;
+        const int cell = listMode ? P.checkList[size_t( par ) * P.nCells + item] : P.cellBase + item;
         if( !listMode && P.finFlag && g.r == 0 ) P.finFlag[cell] = 0;
         CT_BEGIN( tcell );
         CT_BEGIN( tload );

@@ -118,6 +118,8 @@ struct uqc_solver {
     bool asyncPending     = false;
     int asyncStepsBefore  = 0;
     std::vector<cudaEvent_t> stepEvents;
+    cudaStream_t copyStream = nullptr;       // uqc_step_host: the copies beside the kernels
+    std::vector<cudaEvent_t> hostEvents;     // uqc_step_host: chunk arrivals and phase ends
     float lastMs[3] = {0, 0, 0};
     // CUDA graphs of n whole time steps (uqc_run, uqc_step_async), rebuilt
     // when anything the kernels' arguments hold changes (planGen)
@@ -871,6 +873,9 @@ void release( uqc_solver* h ) {
     if( h->asyncEv ) cudaEventDestroy( h->asyncEv );
     for( auto& e : h->stepEvents )
         if( e ) cudaEventDestroy( e );
+    for( auto& e : h->hostEvents )
+        if( e ) cudaEventDestroy( e );
+    if( h->copyStream ) cudaStreamDestroy( h->copyStream );
     if( h->ownStream && h->stream ) cudaStreamDestroy( h->stream );
 }
 
@@ -1965,6 +1970,90 @@ int uqc_step( uqc_solver* h, int n_steps, uqc_step_info* info ) {
             h->lastMs[1] += b;
             h->lastMs[2] += a + b;
         }
+        return failed ? fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( failed ) + " cells did not converge" ) : UQC_OK;
+    } );
+}
+
+int uqc_step_host( uqc_solver* h, const double* u_in, const double* lambda_in, const unsigned* level_in, double t, double* u_out,
+                   double* lambda_out, unsigned* level_out, uqc_step_info* info ) {
+    if( !h || !u_in || !lambda_in || !u_out || !lambda_out ) return UQC_ERR_ARGUMENT;
+    if( h->sharded ) return fail( h, UQC_ERR_STATE, "a sharded handle steps through uqc_step_phase" );
+    return guarded_dev( h, [&] {
+        const int N = h->mesh.nCells;
+        if( level_in )
+            for( int j = 0; j < N; ++j )
+                if( level_in[j] >= unsigned( h->tab.nLevels ) ) throw std::invalid_argument( "refinement level out of range" );
+        constexpr int CHUNKS = 8;
+        if( !h->copyStream ) CK( cudaStreamCreateWithFlags( &h->copyStream, cudaStreamNonBlocking ) );
+        if( h->hostEvents.empty() ) {
+            h->hostEvents.resize( CHUNKS + 4 );
+            for( auto& e : h->hostEvents ) CK( cudaEventCreate( &e ) );
+        }
+        cudaEvent_t* ev = h->hostEvents.data();    // [0, CHUNKS): chunk c landed; then start, closure end, update end, copies done
+        // the state the upload replaces (as uqc_upload_state): levels, no
+        // held factors, a fresh control block (synchronous, so the earlier
+        // work on the stream is done before the copies start)
+        if( level_in )
+            CK( cudaMemcpyAsync( h->d_level, level_in, size_t( N ) * sizeof( unsigned ), cudaMemcpyHostToDevice, h->stream ) );
+        else if( !h->stateReady ) {
+            std::vector<unsigned> lv( N, unsigned( h->tab.nLevels - 1 ) );
+            CK( cudaMemcpyAsync( h->d_level, lv.data(), size_t( N ) * sizeof( unsigned ), cudaMemcpyHostToDevice, h->stream ) );
+        }
+        if( h->d_factorLevel ) reset_factor_store( h );
+        reset_control( h, t );
+        h->stateReady = true;
+        h->launches   = 0;
+        const int stepsBefore = h->h_ctl->steps;
+        KParams P             = make_params( h );
+        step_lists( h, P );
+        // moments and duals in chunks of cells on the copy stream; each
+        // chunk's convergence check waits for its chunk only
+        const size_t ldc = h->ldc;
+        CK( cudaEventRecord( ev[CHUNKS], h->stream ) );
+        for( int c = 0; c < CHUNKS; ++c ) {
+            const size_t c0 = size_t( N ) * c / CHUNKS, c1 = size_t( N ) * ( c + 1 ) / CHUNKS;
+            if( c1 > c0 ) {
+                CK( cudaMemcpyAsync( h->d_u + c0 * ldc, u_in + c0 * ldc, ( c1 - c0 ) * ldc * sizeof( double ), cudaMemcpyHostToDevice, h->copyStream ) );
+                CK( cudaMemcpyAsync( h->d_lam + c0 * ldc, lambda_in + c0 * ldc, ( c1 - c0 ) * ldc * sizeof( double ), cudaMemcpyHostToDevice,
+                                     h->copyStream ) );
+            }
+            CK( cudaEventRecord( ev[c], h->copyStream ) );
+        }
+        if( h->cfg.newtonMode != 2 ) {
+            for( int c = 0; c < CHUNKS; ++c ) {
+                const int c0 = int( size_t( N ) * c / CHUNKS ), c1 = int( size_t( N ) * ( c + 1 ) / CHUNKS );
+                CK( cudaStreamWaitEvent( h->stream, ev[c], 0 ) );
+                if( c1 == c0 ) continue;
+                KParams Q    = P;
+                Q.cellBase   = c0;
+                Q.nWork      = c1 - c0;
+                void* args[] = {&Q};
+                launch( h, pick_check( h->cfg.closure ), h->checkGrid, h->checkBlock, h->checkSmem, args );
+            }
+        }
+        else
+            CK( cudaStreamWaitEvent( h->stream, ev[CHUNKS - 1], 0 ) );
+        launch_closure( h, P, 1 );
+        CK( cudaEventRecord( ev[CHUNKS + 1], h->stream ) );
+        // the duals are final: they come back while the update runs
+        CK( cudaStreamWaitEvent( h->copyStream, ev[CHUNKS + 1], 0 ) );
+        CK( cudaMemcpyAsync( lambda_out, h->d_lam, size_t( N ) * ldc * sizeof( double ), cudaMemcpyDeviceToHost, h->copyStream ) );
+        enqueue_update( h, P );
+        CK( cudaEventRecord( ev[CHUNKS + 2], h->stream ) );
+        CK( cudaStreamWaitEvent( h->copyStream, ev[CHUNKS + 2], 0 ) );
+        CK( cudaMemcpyAsync( u_out, h->d_u, size_t( N ) * ldc * sizeof( double ), cudaMemcpyDeviceToHost, h->copyStream ) );
+        if( level_out ) CK( cudaMemcpyAsync( level_out, h->d_level, size_t( N ) * sizeof( unsigned ), cudaMemcpyDeviceToHost, h->copyStream ) );
+        CK( cudaEventRecord( ev[CHUNKS + 3], h->copyStream ) );
+        CK( cudaStreamWaitEvent( h->stream, ev[CHUNKS + 3], 0 ) );    // later work on the stream sees the copies done
+        CK( cudaGetLastError() );
+        CK( cudaStreamSynchronize( h->copyStream ) );
+        int failed = fill_info( h, info, stepsBefore );
+        float a = 0.f, b = 0.f;
+        CK( cudaEventElapsedTime( &a, ev[CHUNKS], ev[CHUNKS + 1] ) );
+        CK( cudaEventElapsedTime( &b, ev[CHUNKS + 1], ev[CHUNKS + 2] ) );
+        h->lastMs[0] = a;    // closure phase, from the start of the first copy
+        h->lastMs[1] = b;
+        h->lastMs[2] = a + b;
         return failed ? fail( h, UQC_ERR_NOT_CONVERGED, std::to_string( failed ) + " cells did not converge" ) : UQC_OK;
     } );
 }

@@ -225,6 +225,29 @@ class Solver:
             check(self.h, rc)
         return info.as_dict()
 
+    def step_host(self, u, lam, level=None, t=0.0, out=None, raise_on_failure=True):
+        """One step from host state to host state (uqc_step_host): upload, step
+        and download with the copies beside the kernels. u, lam: (n_cells,
+        n_states, n_total) float64, C-contiguous (pinned memory for overlap);
+        out = (u, lam, level) arrays to fill (may be the inputs), else new ones.
+        Returns (u, lam, level, info)."""
+        shape = (self.n_cells, self.n_states, self.n_total)
+        for a in (u, lam):
+            assert a.shape == shape and a.dtype == np.float64 and a.flags.c_contiguous
+        lev = None if level is None else np.ascontiguousarray(level, dtype=np.uint32)
+        if out is None:
+            out = (np.empty(shape), np.empty(shape), np.empty(self.n_cells, dtype=np.uint32))
+        uo, lo, vo = out
+        for a in (uo, lo):
+            assert a.shape == shape and a.dtype == np.float64 and a.flags.c_contiguous
+        assert vo is None or (vo.dtype == np.uint32 and vo.shape == (self.n_cells,))
+        info = StepInfo()
+        rc = self.lib.uqc_step_host(self.h, ptr(u), ptr(lam), ptr(lev, L._up), float(t), ptr(uo), ptr(lo), ptr(vo, L._up),
+                                    C.byref(info))
+        if rc != 0 and (raise_on_failure or rc != -4):
+            check(self.h, rc)
+        return uo, lo, vo, info.as_dict()
+
     def step_async(self, n_steps=1):
         """Enqueues n_steps steps and returns at once (uqc_step_async)."""
         check(self.h, self.lib.uqc_step_async(self.h, n_steps))
