@@ -272,9 +272,10 @@ int uqc_run( uqc_solver* h, double t_end, uqc_step_info* info );
  * uqc_upload_state(u_in, lambda_in, level_in, UQC_LAYOUT_STATE_MAJOR, t),
  * uqc_step(h, 1, info) and uqc_download_state(u_out, lambda_out, level_out,
  * UQC_LAYOUT_STATE_MAJOR), with the copies beside the kernels: moments and
- * duals go up in chunks of cells, each chunk's convergence check starting as
- * its chunk lands; the duals come back while the update runs, the moments and
- * levels after it. Pinned host memory lets the copies run asynchronously.
+ * duals go up in chunks of cells, each chunk's closure (check and Newton)
+ * starting as its chunk lands and its duals going down as it ends, beside the
+ * later chunks' uploads; the moments and levels come down after the update.
+ * Pinned host memory lets the copies run asynchronously.
  * level_in NULL keeps the resident levels, level_out NULL skips them; the out
  * arrays may be the in arrays. uqc_last_timing: [0] from the first copy to the
  * end of the closure phase, [1] the update. */

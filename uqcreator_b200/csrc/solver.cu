@@ -118,7 +118,8 @@ struct uqc_solver {
     bool asyncPending     = false;
     int asyncStepsBefore  = 0;
     std::vector<cudaEvent_t> stepEvents;
-    cudaStream_t copyStream = nullptr;       // uqc_step_host: the copies beside the kernels
+    cudaStream_t copyStream = nullptr;       // uqc_step_host: the uploads beside the kernels
+    cudaStream_t copyStreamOut = nullptr;    // ... and the downloads (the other copy direction)
     std::vector<cudaEvent_t> hostEvents;     // uqc_step_host: chunk arrivals and phase ends
     float lastMs[3] = {0, 0, 0};
     // CUDA graphs of n whole time steps (uqc_run, uqc_step_async), rebuilt
@@ -876,6 +877,7 @@ void release( uqc_solver* h ) {
     for( auto& e : h->hostEvents )
         if( e ) cudaEventDestroy( e );
     if( h->copyStream ) cudaStreamDestroy( h->copyStream );
+    if( h->copyStreamOut ) cudaStreamDestroy( h->copyStreamOut );
     if( h->ownStream && h->stream ) cudaStreamDestroy( h->stream );
 }
 
@@ -1985,11 +1987,16 @@ int uqc_step_host( uqc_solver* h, const double* u_in, const double* lambda_in, c
                 if( level_in[j] >= unsigned( h->tab.nLevels ) ) throw std::invalid_argument( "refinement level out of range" );
         constexpr int CHUNKS = 8;
         if( !h->copyStream ) CK( cudaStreamCreateWithFlags( &h->copyStream, cudaStreamNonBlocking ) );
+        if( !h->copyStreamOut ) CK( cudaStreamCreateWithFlags( &h->copyStreamOut, cudaStreamNonBlocking ) );
         if( h->hostEvents.empty() ) {
-            h->hostEvents.resize( CHUNKS + 4 );
+            h->hostEvents.resize( 2 * CHUNKS + 4 );
             for( auto& e : h->hostEvents ) CK( cudaEventCreate( &e ) );
         }
-        cudaEvent_t* ev = h->hostEvents.data();    // [0, CHUNKS): chunk c landed; then start, closure end, update end, copies done
+        // [0, CHUNKS): chunk c landed; [CHUNKS, 2 CHUNKS): chunk c's closure
+        // done; then start, closure phase end, update end, copies done
+        cudaEvent_t* landed = h->hostEvents.data();
+        cudaEvent_t* solved = landed + CHUNKS;
+        cudaEvent_t* ev     = solved + CHUNKS;
         // the state the upload replaces (as uqc_upload_state): levels, no
         // held factors, a fresh control block (synchronous, so the earlier
         // work on the stream is done before the copies start)
@@ -2004,53 +2011,75 @@ int uqc_step_host( uqc_solver* h, const double* u_in, const double* lambda_in, c
         h->stateReady = true;
         h->launches   = 0;
         const int stepsBefore = h->h_ctl->steps;
+        const int par         = h->h_ctl->steps & 1;    // the running step's active list
         KParams P             = make_params( h );
         step_lists( h, P );
-        // moments and duals in chunks of cells on the copy stream; each
-        // chunk's convergence check waits for its chunk only
         const size_t ldc = h->ldc;
-        CK( cudaEventRecord( ev[CHUNKS], h->stream ) );
+        auto lo          = [&]( int c ) { return size_t( N ) * c / CHUNKS; };
+        CK( cudaEventRecord( ev[0], h->stream ) );
+        // moments and duals in chunks of cells on the upload stream
         for( int c = 0; c < CHUNKS; ++c ) {
-            const size_t c0 = size_t( N ) * c / CHUNKS, c1 = size_t( N ) * ( c + 1 ) / CHUNKS;
+            const size_t c0 = lo( c ), c1 = lo( c + 1 );
             if( c1 > c0 ) {
                 CK( cudaMemcpyAsync( h->d_u + c0 * ldc, u_in + c0 * ldc, ( c1 - c0 ) * ldc * sizeof( double ), cudaMemcpyHostToDevice, h->copyStream ) );
                 CK( cudaMemcpyAsync( h->d_lam + c0 * ldc, lambda_in + c0 * ldc, ( c1 - c0 ) * ldc * sizeof( double ), cudaMemcpyHostToDevice,
                                      h->copyStream ) );
             }
-            CK( cudaEventRecord( ev[c], h->copyStream ) );
+            CK( cudaEventRecord( landed[c], h->copyStream ) );
         }
+        // the closure half of the step chunk by chunk as each lands: the
+        // check of the chunk's cells, the Newton of those it lists (the work
+        // counters and the list start again from zero for each chunk), then
+        // the chunk's final duals go down on the download stream, beside the
+        // later chunks' uploads. A cell's closure reads and writes only its
+        // own state, so the chunks give the cells the unchunked results.
+        auto download_duals = [&]( size_t c0, size_t c1, cudaEvent_t after ) {
+            CK( cudaEventRecord( after, h->stream ) );
+            CK( cudaStreamWaitEvent( h->copyStreamOut, after, 0 ) );
+            if( c1 > c0 )
+                CK( cudaMemcpyAsync( lambda_out + c0 * ldc, h->d_lam + c0 * ldc, ( c1 - c0 ) * ldc * sizeof( double ), cudaMemcpyDeviceToHost,
+                                     h->copyStreamOut ) );
+        };
         if( h->cfg.newtonMode != 2 ) {
             for( int c = 0; c < CHUNKS; ++c ) {
-                const int c0 = int( size_t( N ) * c / CHUNKS ), c1 = int( size_t( N ) * ( c + 1 ) / CHUNKS );
-                CK( cudaStreamWaitEvent( h->stream, ev[c], 0 ) );
-                if( c1 == c0 ) continue;
-                KParams Q    = P;
-                Q.cellBase   = c0;
-                Q.nWork      = c1 - c0;
-                void* args[] = {&Q};
-                launch( h, pick_check( h->cfg.closure ), h->checkGrid, h->checkBlock, h->checkSmem, args );
+                const size_t c0 = lo( c ), c1 = lo( c + 1 );
+                CK( cudaStreamWaitEvent( h->stream, landed[c], 0 ) );
+                if( c1 > c0 ) {
+                    if( c > 0 ) {
+                        reset_work( h );
+                        CK( cudaMemsetAsync( &h->d_ctl->nActive[par], 0, sizeof( unsigned ), h->stream ) );
+                        CK( cudaMemsetAsync( &h->d_ctl->v2Work[0], 0, sizeof( h->d_ctl->v2Work ) + sizeof( h->d_ctl->v2Count ), h->stream ) );
+                    }
+                    KParams Q    = P;
+                    Q.cellBase   = int( c0 );
+                    Q.nWork      = int( c1 - c0 );
+                    void* args[] = {&Q};
+                    launch( h, pick_check( h->cfg.closure ), h->checkGrid, h->checkBlock, h->checkSmem, args );
+                    launch_closure( h, P, 1 );
+                }
+                download_duals( c0, c1, solved[c] );
             }
         }
-        else
-            CK( cudaStreamWaitEvent( h->stream, ev[CHUNKS - 1], 0 ) );
-        launch_closure( h, P, 1 );
-        CK( cudaEventRecord( ev[CHUNKS + 1], h->stream ) );
-        // the duals are final: they come back while the update runs
-        CK( cudaStreamWaitEvent( h->copyStream, ev[CHUNKS + 1], 0 ) );
-        CK( cudaMemcpyAsync( lambda_out, h->d_lam, size_t( N ) * ldc * sizeof( double ), cudaMemcpyDeviceToHost, h->copyStream ) );
+        else {
+            // safe mode: every cell takes Newton steps (no check), all at once
+            CK( cudaStreamWaitEvent( h->stream, landed[CHUNKS - 1], 0 ) );
+            launch_closure( h, P, 1 );
+            download_duals( 0, size_t( N ), solved[0] );
+        }
+        CK( cudaEventRecord( ev[1], h->stream ) );
         enqueue_update( h, P );
-        CK( cudaEventRecord( ev[CHUNKS + 2], h->stream ) );
-        CK( cudaStreamWaitEvent( h->copyStream, ev[CHUNKS + 2], 0 ) );
-        CK( cudaMemcpyAsync( u_out, h->d_u, size_t( N ) * ldc * sizeof( double ), cudaMemcpyDeviceToHost, h->copyStream ) );
-        if( level_out ) CK( cudaMemcpyAsync( level_out, h->d_level, size_t( N ) * sizeof( unsigned ), cudaMemcpyDeviceToHost, h->copyStream ) );
-        CK( cudaEventRecord( ev[CHUNKS + 3], h->copyStream ) );
-        CK( cudaStreamWaitEvent( h->stream, ev[CHUNKS + 3], 0 ) );    // later work on the stream sees the copies done
+        CK( cudaEventRecord( ev[2], h->stream ) );
+        CK( cudaStreamWaitEvent( h->copyStreamOut, ev[2], 0 ) );
+        CK( cudaMemcpyAsync( u_out, h->d_u, size_t( N ) * ldc * sizeof( double ), cudaMemcpyDeviceToHost, h->copyStreamOut ) );
+        if( level_out ) CK( cudaMemcpyAsync( level_out, h->d_level, size_t( N ) * sizeof( unsigned ), cudaMemcpyDeviceToHost, h->copyStreamOut ) );
+        CK( cudaEventRecord( ev[3], h->copyStreamOut ) );
+        CK( cudaStreamWaitEvent( h->stream, ev[3], 0 ) );    // later work on the stream sees the copies done
         CK( cudaGetLastError() );
-        CK( cudaStreamSynchronize( h->copyStream ) );
+        CK( cudaStreamSynchronize( h->copyStreamOut ) );
         int failed = fill_info( h, info, stepsBefore );
         float a = 0.f, b = 0.f;
-        CK( cudaEventElapsedTime( &a, ev[CHUNKS], ev[CHUNKS + 1] ) );
-        CK( cudaEventElapsedTime( &b, ev[CHUNKS + 1], ev[CHUNKS + 2] ) );
+        CK( cudaEventElapsedTime( &a, ev[0], ev[1] ) );
+        CK( cudaEventElapsedTime( &b, ev[1], ev[2] ) );
         h->lastMs[0] = a;    // closure phase, from the start of the first copy
         h->lastMs[1] = b;
         h->lastMs[2] = a + b;
