@@ -274,7 +274,9 @@ int uqc_run( uqc_solver* h, double t_end, uqc_step_info* info );
  * UQC_LAYOUT_STATE_MAJOR), with the copies beside the kernels: moments and
  * duals go up in chunks of cells, each chunk's closure (check and Newton)
  * starting as its chunk lands and its duals going down as it ends, beside the
- * later chunks' uploads; the moments and levels come down after the update.
+ * later chunks' uploads; the update runs in chunks too, each chunk's moments
+ * going down as it ends. Moments, duals, levels, t and dt are those of the
+ * three calls bit for bit; the residual sums the same terms in another order.
  * Pinned host memory lets the copies run asynchronously.
  * level_in NULL keeps the resident levels, level_out NULL skips them; the out
  * arrays may be the in arrays. uqc_last_timing: [0] from the first copy to the

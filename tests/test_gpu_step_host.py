@@ -2,9 +2,10 @@
 the kernels) against uqc_upload_state + uqc_step + uqc_download_state on the
 same state (needs a B200).
 
-The chunked convergence check and the overlapped copies change nothing a
-cell computes, so the two paths agree bit for bit: moments, duals, levels,
-time, time step and residual. Cases: 2-D Euler (FP64 and the mixed form),
+The chunked closure and update and the overlapped copies change nothing a
+cell computes, so the two paths agree bit for bit in moments, duals, levels,
+time and time step; the residual sums the same terms in another order
+(relative 1e-12). Cases: 2-D Euler (FP64 and the mixed form),
 1-D Burgers (register Newton), adaptive shallow water (levels), and the
 output written over the input arrays.
 """
@@ -54,8 +55,9 @@ def test_step_host_matches_upload_step_download(case):
         np.testing.assert_array_equal(ub, ua)
         np.testing.assert_array_equal(lb, la)
         np.testing.assert_array_equal(vb, va)
-        for key in ("t", "dt", "residual", "newton_iterations", "active_cells", "failed_cells"):
+        for key in ("t", "dt", "newton_iterations", "active_cells", "failed_cells"):
             assert b[key] == a[key], (key, a[key], b[key])
+        assert b["residual"] == pytest.approx(a["residual"], rel=1e-12, abs=1e-300)
         # in place: the outputs over the inputs
         uc, lc, vc, c = s.step_host(hu, hl, hv, t=t0, out=(hu, hl, hv))
         assert uc is hu

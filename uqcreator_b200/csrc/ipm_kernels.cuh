@@ -117,7 +117,8 @@ struct KParams {
     unsigned* level;
     const unsigned* nTotalCell;  // closure-only calls: moments per cell (else from level)
     int *status, *iters;
-    double* blockPartial;     // one per CTA of k_update
+    double* blockPartial;     // one per CTA of k_update (and launch, for a chunked update)
+    int updChunk, updChunks;  // k_update over cells cellBase .. cellBase + nWork - 1 as launch updChunk of updChunks (else 0 of 1)
     int* activeList;          // step mode: cells that need Newton (filled by k_check / k_update), or null
     unsigned* activeCount;
     int listParity;           // step mode: two lists of nCells, the running step's is (ctl->steps & 1)
@@ -1543,7 +1544,7 @@ __global__ void __launch_bounds__( 256, ( update_min_ctas<CL, FIN>() ) ) k_updat
         ccount = P.checkCount + ( ( P.ctl->steps + 1 ) & 1 );
     }
     WarpListBuf nbuf, cbuf;    // next step's active list and check list
-    for( int cell = blockIdx.x * nWarps + warp; cell < P.nWork; cell += gridDim.x * nWarps ) {
+    for( int cell = P.cellBase + blockIdx.x * nWarps + warp; cell < P.cellBase + P.nWork; cell += gridDim.x * nWarps ) {
         const int bc = P.boundary[cell];
         if( finish && lane == 0 && P.finFlag[cell] ) {
             // finished by the previous update: this step's closure status
@@ -1825,21 +1826,24 @@ __global__ void __launch_bounds__( 256, ( update_min_ctas<CL, FIN>() ) ) k_updat
     if( threadIdx.x == 0 ) {
         double s = 0.0;
         for( int w = 0; w < int( blockDim.x >> 5 ); ++w ) s += blockRes[w];
-        P.blockPartial[blockIdx.x] = s;
+        P.blockPartial[size_t( P.updChunk ) * gridDim.x + blockIdx.x] = s;
         __threadfence();
         unsigned done = atomicAdd( &P.ctl->doneBlocks, 1u );
-        isLast        = done == gridDim.x - 1;
+        // the launches of a chunked update run one after another on the
+        // stream: the last CTA of the last launch finishes the step
+        isLast = done == gridDim.x * unsigned( P.updChunks ) - 1;
     }
     __syncthreads();
     double total = 0.0;
     if( isLast && threadIdx.x < 32 ) {
         __threadfence();
-        // the CTA partials in CTA order: the warp loads 32 at a time, lane 0
-        // adds them in sequence from the shuffles
-        for( unsigned b0 = 0; b0 < gridDim.x; b0 += 32 ) {
+        // the CTA partials in launch and CTA order: the warp loads 32 at a
+        // time, lane 0 adds them in sequence from the shuffles
+        const unsigned nb = gridDim.x * unsigned( P.updChunks );
+        for( unsigned b0 = 0; b0 < nb; b0 += 32 ) {
             const unsigned b = b0 + threadIdx.x;
-            const double v   = b < gridDim.x ? ( (volatile double*)P.blockPartial )[b] : 0.0;
-            const unsigned m = min( 32u, gridDim.x - b0 );
+            const double v   = b < nb ? ( (volatile double*)P.blockPartial )[b] : 0.0;
+            const unsigned m = min( 32u, nb - b0 );
             for( unsigned j = 0; j < m; ++j ) total += __shfl_sync( 0xffffffffu, v, int( j ) );
         }
     }

@@ -45,6 +45,8 @@ struct uqc_solver {
     int tinyOpt = -1;                  // option closure_tiny: -1 automatic, 0 off, 1 on where it applies
     int updateWarpsOpt = 0, checkWarpsOpt = 0, chordWarpsOpt = 0;    // options update_warps, check_warps, chord_warps (0: automatic)
     int blockPartialCap = 0;           // doubles in d_blockPartial
+    double* d_chunkPartial = nullptr;  // uqc_step_host's chunked update: a partial per CTA and launch
+    int chunkPartialCap    = 0;
     bool closureTiny = false;          // planned: the register Newton of tiny systems (k_closure TINY)
     int tinyGrid     = 0;
     size_t ldc = 1;
@@ -282,6 +284,8 @@ KParams make_params( const uqc_solver* h ) {
     P.status       = h->d_status;
     P.iters        = h->d_iters;
     P.blockPartial  = h->d_blockPartial;
+    P.updChunk      = 0;
+    P.updChunks     = 1;
     P.ctl           = h->d_ctl;
     P.workCounter   = h->d_ctl ? &h->d_ctl->workCounter : nullptr;
     P.fallbackList  = h->d_fallbackList;
@@ -861,7 +865,7 @@ void release( uqc_solver* h ) {
     h->graphs.clear();
     for( void* p : {(void*)h->d_phi, (void*)h->d_phiWf, (void*)h->d_xi, (void*)h->d_wt, (void*)h->d_area, (void*)h->d_dx, (void*)h->d_center,
                     (void*)h->d_unitN, (void*)h->d_scaledN, (void*)h->d_nbr, (void*)h->d_boundary, (void*)h->d_u, (void*)h->d_lam,
-                    (void*)h->d_bndNormal, (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_level, (void*)h->d_status,
+                    (void*)h->d_bndNormal, (void*)h->d_uQ, (void*)h->d_uOld0, (void*)h->d_blockPartial, (void*)h->d_chunkPartial, (void*)h->d_level, (void*)h->d_status,
                     (void*)h->d_iters, (void*)h->d_ctl, (void*)h->d_xLam, (void*)h->d_xU, (void*)h->d_xNt, (void*)h->d_xStatus,
                     (void*)h->d_xIters, (void*)h->d_activeList, (void*)h->d_cellDt, (void*)h->d_uRe, (void*)h->d_checkList, (void*)h->d_finFlag, (void*)h->d_phiF, (void*)h->d_fallbackList,
                     (void*)h->d_factorStore, (void*)h->d_factorLevel, (void*)h->d_gStore, (void*)h->d_v2Lists,
@@ -2067,10 +2071,40 @@ int uqc_step_host( uqc_solver* h, const double* u_in, const double* lambda_in, c
             download_duals( 0, size_t( N ), solved[0] );
         }
         CK( cudaEventRecord( ev[1], h->stream ) );
-        enqueue_update( h, P );
+        // the update in chunks of cells too, each chunk's moments going down
+        // as its launch ends (the residual sums the launches' CTA partials in
+        // order: the same terms as one launch, in another order)
+        const int need = h->updateGrid * CHUNKS;
+        if( need > h->chunkPartialCap ) {
+            if( h->d_chunkPartial ) {
+                CK( cudaStreamSynchronize( h->stream ) );
+                cudaFree( h->d_chunkPartial );
+            }
+            h->d_chunkPartial  = dalloc<double>( size_t( need ) );
+            h->chunkPartialCap = need;
+        }
+        {
+            KParams U = P;
+            step_lists( h, U );
+            U.finishInUpdate = update_test_on( h );
+            U.blockPartial   = h->d_chunkPartial;
+            U.updChunks      = CHUNKS;
+            void* ku         = pick( h->cfg.closure, h->group, update_kernel_id( h, U.finishInUpdate != 0 ) );
+            for( int c = 0; c < CHUNKS; ++c ) {
+                const size_t c0 = lo( c ), c1 = lo( c + 1 );
+                U.cellBase   = int( c0 );
+                U.nWork      = int( c1 - c0 );
+                U.updChunk   = c;
+                void* args[] = {&U};
+                launch( h, ku, h->updateGrid, h->updateBlock, h->updateSmem, args );
+                CK( cudaEventRecord( solved[c], h->stream ) );
+                CK( cudaStreamWaitEvent( h->copyStreamOut, solved[c], 0 ) );
+                if( c1 > c0 )
+                    CK( cudaMemcpyAsync( u_out + c0 * ldc, h->d_u + c0 * ldc, ( c1 - c0 ) * ldc * sizeof( double ), cudaMemcpyDeviceToHost,
+                                         h->copyStreamOut ) );
+            }
+        }
         CK( cudaEventRecord( ev[2], h->stream ) );
-        CK( cudaStreamWaitEvent( h->copyStreamOut, ev[2], 0 ) );
-        CK( cudaMemcpyAsync( u_out, h->d_u, size_t( N ) * ldc * sizeof( double ), cudaMemcpyDeviceToHost, h->copyStreamOut ) );
         if( level_out ) CK( cudaMemcpyAsync( level_out, h->d_level, size_t( N ) * sizeof( unsigned ), cudaMemcpyDeviceToHost, h->copyStreamOut ) );
         CK( cudaEventRecord( ev[3], h->copyStreamOut ) );
         CK( cudaStreamWaitEvent( h->stream, ev[3], 0 ) );    // later work on the stream sees the copies done
