@@ -801,7 +801,13 @@ __host__ __device__ inline size_t sweep_raw_floats( int pairs, int NP ) { return
 // a pivot-row buffer: 32 SWEEP_CW columns (those beyond the matrix hold
 // zeros) and the pivot itself at index 32 SWEEP_CW
 constexpr int SWEEP_PR = 32 * SWEEP_CW + 4;
-__host__ __device__ inline size_t sweep_ws_floats( int pairs, int NP ) { return sweep_raw_floats( pairs, NP ) + 2 * SWEEP_PR + 8; }
+// a pivot-column buffer: the same values by row group, SWEEP_PG floats per
+// group (SWEEP_RG rounded up to 4), so that a warp reads its rows' column
+// values in 16-byte loads
+constexpr int SWEEP_PG = ( SWEEP_RG + 3 ) & ~3, SWEEP_PC = 4 * SWEEP_PG;
+__host__ __device__ inline size_t sweep_ws_floats( int pairs, int NP ) {
+    return sweep_raw_floats( pairs, NP ) + 2 * SWEEP_PR + 2 * SWEEP_PC + 8;
+}
 
 // H^-1 of the cells of re-factor list `round` from the raw values k_hess_tc
 // left in their store slots, by the sweep operator (Gauss-Jordan on a
@@ -824,7 +830,8 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_invert_sweep( KP
     const int nT = P.nT, n = NS * nT, pairs = nT * ( nT + 1 ) / 2;
     float* raw  = fsm + size_t( cg ) * sweep_ws_floats( pairs, NP );
     float* prow = raw + sweep_raw_floats( pairs, NP );    // two pivot-row buffers of SWEEP_PR floats
-    int* misc   = reinterpret_cast<int*>( prow + 2 * SWEEP_PR );    // [0] item, [1] not positive definite
+    float* pcol = prow + 2 * SWEEP_PR;                     // two pivot-column buffers of SWEEP_PC floats
+    int* misc   = reinterpret_cast<int*>( pcol + 2 * SWEEP_PC );    // [0] item, [1] not positive definite
     const int bar = 1 + cg, tid = threadIdx.x & 127;
     auto sync = [&]() { asm volatile( "bar.sync %0, 128;" ::"r"( bar ) : "memory" ); };
     const int* list = refactor_list( P, round );
@@ -872,10 +879,12 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_invert_sweep( KP
                 const int k = RG * gg + rr;
                 if( k >= n ) break;
                 float* pr = prow + ( k & 1 ) * SWEEP_PR;
+                float* pc = pcol + ( k & 1 ) * SWEEP_PC;
                 const int kl = k & 31, kq = k >> 5;
                 if( g == gg ) {
                     // the pivot row; at the pivot p - 1 (so that pr[k] / p = 1 - 1/p,
-                    // the factor that turns column k into a_ik / p), p itself at the end
+                    // the factor that turns column k into a_ik / p), p itself at the end;
+                    // the same values by row group in the column buffer
 #pragma unroll
                     for( int q = 0; q < CW; ++q ) {
                         float v = a[rr][q];
@@ -883,7 +892,10 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_invert_sweep( KP
                             pr[32 * CW] = v;
                             v -= 1.f;
                         }
-                        pr[lane + 32 * q] = v;
+                        const int c       = lane + 32 * q;
+                        pr[c]             = v;
+                        const int cg2     = c / RG;
+                        if( cg2 < 4 ) pc[cg2 * SWEEP_PG + ( c - cg2 * RG )] = v;
                     }
                 }
                 sync();
@@ -894,11 +906,21 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_invert_sweep( KP
                 float sv[CW];
 #pragma unroll
                 for( int q = 0; q < CW; ++q ) sv[q] = pr[lane + 32 * q] * pinv;
+                // a_ik of this warp's rows (column k = row k), 16 bytes at a time
+                float f[SWEEP_PG];
+                const float4* pc4 = reinterpret_cast<const float4*>( pc + g * SWEEP_PG );
+#pragma unroll
+                for( int v4 = 0; v4 < SWEEP_PG / 4; ++v4 ) {
+                    const float4 x = pc4[v4];
+                    f[4 * v4]      = x.x;
+                    f[4 * v4 + 1]  = x.y;
+                    f[4 * v4 + 2]  = x.z;
+                    f[4 * v4 + 3]  = x.w;
+                }
 #pragma unroll
                 for( int rr2 = 0; rr2 < RG; ++rr2 ) {
-                    const float f = pr[RG * g + rr2];    // a_ik (column k = row k)
 #pragma unroll
-                    for( int q = 0; q < CW; ++q ) a[rr2][q] = fmaf( -f, sv[q], a[rr2][q] );
+                    for( int q = 0; q < CW; ++q ) a[rr2][q] = fmaf( -f[rr2], sv[q], a[rr2][q] );
                 }
                 if( g == gg ) {    // the pivot row: a_kj / p, and -1/p at the pivot
 #pragma unroll
