@@ -499,12 +499,13 @@ def run_b200(args, rank, world, local):
     hv = torch.empty(v0.shape, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     hu[...] = u0; hl[...] = l0; hv[...] = v0
     e2e_steps = max(1, min(args.steps, 10))
+    # one untimed call first: its streams, events and buffers are made on first use
+    tcur = s.step_host(hu, hl, hv, t=warm["t"], out=(hu, hl, hv))[3]["t"]
     torch.cuda.synchronize()
     barrier(world)
     t0 = time.perf_counter()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    tcur = warm["t"]
     for _ in range(e2e_steps):
         # one C-ABI call per step: host state in, host state out (uqc_step_host)
         inf = s.step_host(hu, hl, hv, t=tcur, out=(hu, hl, hv))[3]
