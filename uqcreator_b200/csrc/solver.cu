@@ -122,6 +122,7 @@ struct uqc_solver {
     std::vector<cudaEvent_t> stepEvents;
     cudaStream_t copyStream = nullptr;       // uqc_step_host: the uploads beside the kernels
     cudaStream_t copyStreamOut = nullptr;    // ... and the downloads (the other copy direction)
+    cudaStream_t checkStream   = nullptr;    // ... and its chunks' convergence checks
     std::vector<cudaEvent_t> hostEvents;     // uqc_step_host: chunk arrivals and phase ends
     float lastMs[3] = {0, 0, 0};
     // CUDA graphs of n whole time steps (uqc_run, uqc_step_async), rebuilt
@@ -882,6 +883,7 @@ void release( uqc_solver* h ) {
         if( e ) cudaEventDestroy( e );
     if( h->copyStream ) cudaStreamDestroy( h->copyStream );
     if( h->copyStreamOut ) cudaStreamDestroy( h->copyStreamOut );
+    if( h->checkStream ) cudaStreamDestroy( h->checkStream );
     if( h->ownStream && h->stream ) cudaStreamDestroy( h->stream );
 }
 
@@ -1992,15 +1994,17 @@ int uqc_step_host( uqc_solver* h, const double* u_in, const double* lambda_in, c
         constexpr int CHUNKS = 8;
         if( !h->copyStream ) CK( cudaStreamCreateWithFlags( &h->copyStream, cudaStreamNonBlocking ) );
         if( !h->copyStreamOut ) CK( cudaStreamCreateWithFlags( &h->copyStreamOut, cudaStreamNonBlocking ) );
+        if( !h->checkStream ) CK( cudaStreamCreateWithFlags( &h->checkStream, cudaStreamNonBlocking ) );
         if( h->hostEvents.empty() ) {
-            h->hostEvents.resize( 2 * CHUNKS + 4 );
+            h->hostEvents.resize( 3 * CHUNKS + 4 );
             for( auto& e : h->hostEvents ) CK( cudaEventCreate( &e ) );
         }
-        // [0, CHUNKS): chunk c landed; [CHUNKS, 2 CHUNKS): chunk c's closure
-        // done; then start, closure phase end, update end, copies done
-        cudaEvent_t* landed = h->hostEvents.data();
-        cudaEvent_t* solved = landed + CHUNKS;
-        cudaEvent_t* ev     = solved + CHUNKS;
+        // per chunk c: landed, closure done (later: update done), checked;
+        // then start, closure phase end, update end, copies done
+        cudaEvent_t* landed  = h->hostEvents.data();
+        cudaEvent_t* solved  = landed + CHUNKS;
+        cudaEvent_t* checked = solved + CHUNKS;
+        cudaEvent_t* ev      = checked + CHUNKS;
         // the state the upload replaces (as uqc_upload_state): levels, no
         // held factors, a fresh control block (synchronous, so the earlier
         // work on the stream is done before the copies start)
@@ -2045,24 +2049,43 @@ int uqc_step_host( uqc_solver* h, const double* u_in, const double* lambda_in, c
                                      h->copyStreamOut ) );
         };
         if( h->cfg.newtonMode != 2 ) {
+            // the checks on a stream of their own, so that chunk c + 1's check
+            // fills the SMs that chunk c's Newton leaves idle in its tail; the
+            // chunks alternate between the two active lists (the next step's
+            // list is not in use before the update), and a check waits until
+            // the Newton two chunks back has consumed its list
             for( int c = 0; c < CHUNKS; ++c ) {
                 const size_t c0 = lo( c ), c1 = lo( c + 1 );
-                CK( cudaStreamWaitEvent( h->stream, landed[c], 0 ) );
+                const int lp    = c & 1;
+                KParams Q       = P;
+                Q.activeList    = h->d_activeList + size_t( lp ) * N;
+                Q.activeCount   = &h->d_ctl->nActive[lp];
+                Q.listParity    = 0;
+                CK( cudaStreamWaitEvent( h->checkStream, landed[c], 0 ) );
+                if( c >= 2 ) CK( cudaStreamWaitEvent( h->checkStream, solved[c - 2], 0 ) );
+                if( c1 > c0 ) {
+                    if( c >= 2 ) CK( cudaMemsetAsync( &h->d_ctl->nActive[lp], 0, sizeof( unsigned ), h->checkStream ) );
+                    KParams K    = Q;
+                    K.cellBase   = int( c0 );
+                    K.nWork      = int( c1 - c0 );
+                    void* args[] = {&K};
+                    CK( cudaLaunchKernel( pick_check( h->cfg.closure ), dim3( h->checkGrid ), dim3( h->checkBlock ), args, h->checkSmem,
+                                          h->checkStream ) );
+                    ++h->launches;
+                }
+                CK( cudaEventRecord( checked[c], h->checkStream ) );
+                CK( cudaStreamWaitEvent( h->stream, checked[c], 0 ) );
                 if( c1 > c0 ) {
                     if( c > 0 ) {
                         reset_work( h );
-                        CK( cudaMemsetAsync( &h->d_ctl->nActive[par], 0, sizeof( unsigned ), h->stream ) );
                         CK( cudaMemsetAsync( &h->d_ctl->v2Work[0], 0, sizeof( h->d_ctl->v2Work ) + sizeof( h->d_ctl->v2Count ), h->stream ) );
                     }
-                    KParams Q    = P;
-                    Q.cellBase   = int( c0 );
-                    Q.nWork      = int( c1 - c0 );
-                    void* args[] = {&Q};
-                    launch( h, pick_check( h->cfg.closure ), h->checkGrid, h->checkBlock, h->checkSmem, args );
-                    launch_closure( h, P, 1 );
+                    launch_closure( h, Q, 1 );
                 }
                 download_duals( c0, c1, solved[c] );
             }
+            // the next step's list (k_update's, with its convergence test) starts empty
+            CK( cudaMemsetAsync( &h->d_ctl->nActive[( par + 1 ) & 1], 0, sizeof( unsigned ), h->stream ) );
         }
         else {
             // safe mode: every cell takes Newton steps (no check), all at once
