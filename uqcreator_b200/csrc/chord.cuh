@@ -162,6 +162,60 @@ template <int NS> __device__ __forceinline__ void load_node( const double* a, in
     }
 }
 
+// The trial gradient for nTj <= 64 / PARTS basis functions: the warp's lanes
+// take (part, i) slots in two rounds (slot j = part nTj + i, round j / 32,
+// lane j mod 32), each summing the nodes k = part (mod PARTS), so that no lane
+// idles over all nodes; lane i then gathers its PARTS partial sums by
+// shuffles and adds them in part order. Outputs as chord_gradient's.
+template <int NS, int PARTS>
+__device__ __forceinline__ double chord_gradient_split( const KParams& P, const double* phiWf, const double* uk, const double* uh, int nTj,
+                                                        double* gout, double* ms, int lane ) {
+    const int slots = PARTS * nTj;
+    double v[2][NS];
+#pragma unroll
+    for( int r = 0; r < 2; ++r ) {
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) v[r][s] = 0.0;
+        const int j = lane + 32 * r;
+        if( j < slots ) {
+            const int p = j / nTj, i = j - p * nTj;
+            const double* t = phiWf + size_t( p ) * P.ld + i;
+            const int tStep = PARTS * P.ld;
+            for( int k = p; k < P.nQ; k += PARTS, t += tStep ) {
+                const double w = *t;
+                double x[NS];
+                load_node<NS>( uk, k, x );
+#pragma unroll
+                for( int s = 0; s < NS; ++s ) v[r][s] = fma( x[s], w, v[r][s] );
+            }
+        }
+    }
+    double m[NS];
+#pragma unroll
+    for( int p = 0; p < PARTS; ++p ) {
+        const int j = p * nTj + lane, src = j & 31;
+        const bool second = j >= 32;
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) {
+            const double a0 = __shfl_sync( 0xffffffffu, v[0][s], src );
+            const double a1 = __shfl_sync( 0xffffffffu, v[1][s], src );
+            const double x  = second ? a1 : a0;
+            m[s]            = p == 0 ? x : m[s] + x;
+        }
+    }
+    double sq = 0.0;
+    if( lane < nTj ) {
+#pragma unroll
+        for( int s = 0; s < NS; ++s ) {
+            const double d       = m[s] - uh[s * P.nT + lane];
+            ms[s * P.nT + lane]  = m[s];
+            gout[s * nTj + lane] = d;
+            sq += d * d;
+        }
+    }
+    return sq;
+}
+
 // Trial gradient of the chord kernel (closure.cpp:234-253): lane i sums
 // m(s, i) = sum_k uk(s, k) phiWf(k, i) over even and odd nodes as separate
 // chains (half the dependent FMA chain of one sum), uk node-major;
@@ -318,7 +372,9 @@ template <int CL> __global__ void __launch_bounds__( 512, 1 ) k_chord( KParams P
                 }
             }
             __syncwarp();
-            const double sq = chord_gradient<NS>( P, phiWf, w.uk, w.uh, nTj, w.gN, w.m, lane );
+            const double sq = nTj <= 16 ? chord_gradient_split<NS, 4>( P, phiWf, w.uk, w.uh, nTj, w.gN, w.m, lane )
+                              : nTj <= 21 ? chord_gradient_split<NS, 3>( P, phiWf, w.uk, w.uh, nTj, w.gN, w.m, lane )
+                                          : chord_gradient<NS>( P, phiWf, w.uk, w.uh, nTj, w.gN, w.m, lane );
             return sqrt( group_sum<32>( g, sq, w.red ) );
         };
         if( bad ) {
