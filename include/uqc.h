@@ -198,6 +198,8 @@ int uqc_set_newton( uqc_solver* h, int max_iterations, double epsilon, int newto
  *                    level, 0 with several.
  *   "graphs"         1 (default): uqc_run and uqc_step_async launch cached
  *                    CUDA graphs of whole time steps; 0: direct launches.
+ *   "host_chunks"    uqc_step_host: chunks of cells the copies and kernels
+ *                    of a step are split into (1-32, default 6).
  *   "mixed_max_iterations"  UQC_MIXED: Newton iterations of the FP32 pass
  *                    after which a cell continues in the FP64 form (>= 2;
  *                    0 = the configured maxIterations).

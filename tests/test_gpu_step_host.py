@@ -83,3 +83,25 @@ def test_step_host_first_state_and_levels_kept():
     np.testing.assert_array_equal(lb, la)
     np.testing.assert_array_equal(vb, va)
     assert info["steps"] == 1
+
+
+@pytest.mark.parametrize("chunks", [1, 3, 13, 32])
+def test_step_host_chunk_counts(chunks):
+    """Any chunk count (option host_chunks, here more chunks than some meshes
+    have cells per chunk) gives the three calls' result."""
+    toml = W.euler2d(nx=12, ny=5)
+    s = Solver(toml)
+    s.set_precision(MIXED)
+    s.init_state()
+    s.step(2)
+    u0, l0, v0 = s.download_state()
+    t0 = s.step(0)["t"]
+    s.upload_state(u0, l0, v0, t=t0)
+    a = s.step(1)
+    ua, la, va = s.download_state()
+    s.set_option("host_chunks", chunks)
+    ub, lb, vb, b = s.step_host(_pinned(u0), _pinned(l0), _pinned(v0), t=t0)
+    np.testing.assert_array_equal(ub, ua)
+    np.testing.assert_array_equal(lb, la)
+    np.testing.assert_array_equal(vb, va)
+    assert b["t"] == a["t"] and b["dt"] == a["dt"]
