@@ -1993,6 +1993,7 @@ int uqc_step_host( uqc_solver* h, const double* u_in, const double* lambda_in, c
                    double* lambda_out, unsigned* level_out, uqc_step_info* info ) {
     if( !h || !u_in || !lambda_in || !u_out || !lambda_out ) return UQC_ERR_ARGUMENT;
     if( h->sharded ) return fail( h, UQC_ERR_STATE, "a sharded handle steps through uqc_step_phase" );
+    if( h->asyncPending ) return fail( h, UQC_ERR_STATE, "a uqc_step_async is in flight" );
     return guarded_dev( h, [&] {
         const int N = h->mesh.nCells;
         if( level_in )
