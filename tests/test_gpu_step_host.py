@@ -105,3 +105,22 @@ def test_step_host_chunk_counts(chunks):
     np.testing.assert_array_equal(lb, la)
     np.testing.assert_array_equal(vb, va)
     assert b["t"] == a["t"] and b["dt"] == a["dt"]
+
+
+def test_step_host_refused_while_async_steps_run():
+    """A uqc_step_async batch in flight owns the control block: uqc_step_host
+    is refused until the batch has been queried to completion."""
+    from uqcreator_b200._lib import UqcError
+    toml = W.euler2d(nx=12, ny=5)
+    s = Solver(toml)
+    s.init_state()
+    u0, l0, v0 = s.download_state()
+    s.step_async(2)
+    with pytest.raises(UqcError):
+        s.step_host(_pinned(u0), _pinned(l0), _pinned(v0), t=0.0)
+    import time
+    deadline = time.monotonic() + 60.0
+    while s.step_query() is None:
+        assert time.monotonic() < deadline
+        time.sleep(0.001)
+    s.step_host(_pinned(u0), _pinned(l0), _pinned(v0), t=0.0)
