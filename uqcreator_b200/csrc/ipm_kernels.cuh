@@ -1316,9 +1316,16 @@ template <int CL> __global__ void __launch_bounds__( 512, 2 ) k_check( KParams P
         CT_BEGIN( tload );
         const int lev = int( P.level[cell] ), nTj = P.nTLevel[lev];
         bool bad = false;
+        // the duals node-major (lam[i NS + s]: a basis function's NS duals in
+        // 16-byte loads for the nodal sums), state-major for the linear closures
         for( int idx = g.r; idx < int( ldc ); idx += 32 ) {
             double a = P.lam[cell * ldc + idx], b = P.u[cell * ldc + idx];
-            lam[idx] = a;
+            if constexpr( Closure<CL>::LINEAR )
+                lam[idx] = a;
+            else {
+                const int s = idx / P.nT, i = idx - s * P.nT;
+                lam[i * NS + s] = a;
+            }
             uh[idx]  = b;
             bad      = bad || !isfinite( a ) || !isfinite( b );
         }
@@ -1345,8 +1352,25 @@ template <int CL> __global__ void __launch_bounds__( 512, 2 ) k_check( KParams P
                 for( int s = 0; s < NS; ++s ) Lk[s] = 0.0;
                 for( int i = 0; i < nTj; ++i ) {
                     const double r = row[i];
+                    double li[NS];
+                    if constexpr( Closure<CL>::LINEAR ) {
 #pragma unroll
-                    for( int s = 0; s < NS; ++s ) Lk[s] = fma( lam[s * P.nT + i], r, Lk[s] );
+                        for( int s = 0; s < NS; ++s ) li[s] = lam[s * P.nT + i];
+                    }
+                    else if constexpr( NS % 2 == 0 ) {
+#pragma unroll
+                        for( int s = 0; s < NS; s += 2 ) {
+                            const double2 t = *reinterpret_cast<const double2*>( lam + i * NS + s );
+                            li[s]           = t.x;
+                            li[s + 1]       = t.y;
+                        }
+                    }
+                    else {
+#pragma unroll
+                        for( int s = 0; s < NS; ++s ) li[s] = lam[i * NS + s];
+                    }
+#pragma unroll
+                    for( int s = 0; s < NS; ++s ) Lk[s] = fma( li[s], r, Lk[s] );
                 }
                 Closure<CL>::U( Lk, y, true, P.phys );
 #pragma unroll
