@@ -300,16 +300,32 @@ def run_serving(args, precision):
                  policy=args.serve_policy, max_stepping=args.serve_max_stepping)
     if args.serve_policy == 1:
         srv.set_option("aging", args.serve_aging)
+    import threading
+    ids, failures = [], []
+
+    def front_end():
+        # requests arrive on a thread of their own (their solvers are built
+        # there), the main thread runs the scheduling passes
+        try:
+            for arr, kind, toml in stream:
+                wait = arr - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(wait)
+                ids.append((srv.submit(toml, precision), kind))
+        except Exception as e:    # reported after the loop
+            failures.append(e)
+
     t0 = time.perf_counter()
-    i, ids = 0, []
+    th = threading.Thread(target=front_end, daemon=True)
+    th.start()
     while True:
-        now = time.perf_counter() - t0
-        while i < len(stream) and stream[i][0] <= now:
-            ids.append((srv.submit(stream[i][2], precision), stream[i][1]))
-            i += 1
+        alive = th.is_alive()
         q, r, _ = srv.progress()
-        if i == len(stream) and q == 0 and r == 0:
+        if not alive and q == 0 and r == 0:
             break
+    th.join()
+    if failures:
+        raise failures[0]
     el = time.perf_counter() - t0
     res = [srv.result(k, mean_var=False) for k, _ in ids]
     srv.close()

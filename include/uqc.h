@@ -447,7 +447,11 @@ typedef struct uqc_request_info {
 int uqc_server_create( unsigned long long device_budget_bytes, int max_active, int steps_per_slice, uqc_server** out );
 void uqc_server_destroy( uqc_server* s );
 const char* uqc_server_last_error( const uqc_server* s );
-/* precision: uqc_precision of the request. */
+/* precision: uqc_precision of the request. May be called from another thread
+ * than uqc_server_progress (a request front end): the request's solver is
+ * built (mesh, tables; host work only) before the server's lock is taken, so
+ * the scheduling loop does not wait for it. The other server calls take the
+ * same lock; uqc_server_destroy must not race with any of them. */
 int uqc_server_submit( uqc_server* s, const char* toml_text, int precision, long long* id );
 /* One scheduling pass; counts after it (any pointer may be NULL). */
 int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_done );

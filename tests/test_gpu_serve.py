@@ -68,6 +68,37 @@ def test_server_results_same_alone_and_in_mix():
     srv.close()
 
 
+def test_server_submissions_from_another_thread():
+    """A front-end thread submits while the main thread runs the scheduling
+    passes: every request finishes with its result alone, bit for bit."""
+    import threading
+    reqs = _requests()
+    alone = [_alone(t)[0] for t in reqs]
+    srv = Server(budget_bytes=8 << 30, max_active=3, steps_per_slice=2)
+    ids = [None] * len(reqs)
+
+    def front_end():
+        for k, t in enumerate(reqs):
+            ids[k] = srv.submit(t)
+            time.sleep(0.002)
+
+    th = threading.Thread(target=front_end)
+    th.start()
+    deadline = time.monotonic() + 120.0
+    while True:
+        alive = th.is_alive()
+        q, r, _ = srv.progress()
+        if not alive and q == 0 and r == 0:
+            break
+        assert time.monotonic() < deadline
+    th.join()
+    for rid, ref in zip(ids, alone):
+        res = srv.result(rid)
+        assert res["state"] == "done" and res["status"] == 0, res
+        np.testing.assert_array_equal(res["mean_var"], ref)
+    srv.close()
+
+
 def test_server_mixed_precision_request_within_tolerance():
     toml = W.euler2d(nx=16, ny=8, degree=3, nquad=6, tend=0.01)
     ref, _ = _alone(toml)

@@ -6,8 +6,8 @@ The chunked closure and update and the overlapped copies change nothing a
 cell computes, so the two paths agree bit for bit in moments, duals, levels,
 time and time step; the residual sums the same terms in another order
 (relative 1e-12). Cases: 2-D Euler (FP64 and the mixed form),
-1-D Burgers (register Newton), adaptive shallow water (levels), and the
-output written over the input arrays.
+1-D Burgers (register Newton), adaptive shallow water (levels; both forms),
+1-D Euler, and the output written over the input arrays.
 """
 import numpy as np
 import pytest
@@ -21,6 +21,8 @@ CASES = {
     "euler2d_mixed": (lambda: W.euler2d(nx=40, ny=16), True),
     "burgers1d": (lambda: W.burgers1d(ncells=300), False),
     "sw_levels": (lambda: W.shallow_water1d(ncells=3000), False),
+    "sw_levels_mixed": (lambda: W.shallow_water1d(ncells=3000), True),
+    "euler1d": (lambda: W.euler1d(ncells=400), False),
 }
 
 

@@ -2459,6 +2459,10 @@ struct uqc_server {
     int done = 0;
     std::chrono::steady_clock::time_point t0;
     std::string err;
+    // submissions may come from another thread than progress(): the server's
+    // state is changed under this lock (a submission takes it only to enqueue,
+    // after building its solver)
+    mutable std::recursive_mutex mu;
     double now() const { return std::chrono::duration<double, std::milli>( std::chrono::steady_clock::now() - t0 ).count(); }
 };
 
@@ -2510,6 +2514,7 @@ int uqc_server_submit( uqc_server* s, const char* toml_text, int precision, long
     uqc_request r;
     char err[512] = {0};
     int rc = uqc_create_from_string( toml_text, nullptr, &r.h, err, sizeof( err ) );    // host side only
+    std::lock_guard<std::recursive_mutex> lock( s->mu );
     if( rc != UQC_OK ) return sfail( s, rc, err );
     r.id        = s->nextId++;
     r.precision = precision;
@@ -2569,6 +2574,7 @@ void launch_slices( uqc_server* s ) {
 
 int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_done ) {
     if( !s ) return UQC_ERR_ARGUMENT;
+    std::lock_guard<std::recursive_mutex> lock( s->mu );
     const double pass = s->now();
     if( s->lastPassMs >= 0.0 && !s->running.empty() ) s->busyMs += pass - s->lastPassMs;
     s->lastPassMs = pass;
@@ -2650,6 +2656,7 @@ int uqc_server_progress( uqc_server* s, int* n_queued, int* n_running, int* n_do
 
 int uqc_server_set_option( uqc_server* s, const char* key, double value ) {
     if( !s || !key ) return UQC_ERR_ARGUMENT;
+    std::lock_guard<std::recursive_mutex> lock( s->mu );
     const std::string k = key;
     if( k == "policy" ) {
         if( value != 0.0 && value != 1.0 ) return sfail( s, UQC_ERR_ARGUMENT, "policy must be 0 or 1" );
@@ -2671,6 +2678,7 @@ int uqc_server_set_option( uqc_server* s, const char* key, double value ) {
 
 int uqc_server_request( const uqc_server* s, long long id, uqc_request_info* info, double* mean_var ) {
     if( !s || !info ) return UQC_ERR_ARGUMENT;
+    std::lock_guard<std::recursive_mutex> lock( s->mu );
     auto it = s->reqs.find( id );
     if( it == s->reqs.end() ) return UQC_ERR_ARGUMENT;
     const uqc_request& r    = it->second;
@@ -2692,12 +2700,14 @@ int uqc_server_request( const uqc_server* s, long long id, uqc_request_info* inf
 
 const char* uqc_server_request_error( const uqc_server* s, long long id ) {
     if( !s ) return "null server";
+    std::lock_guard<std::recursive_mutex> lock( s->mu );
     auto it = s->reqs.find( id );
     return it == s->reqs.end() ? "unknown request" : it->second.err.c_str();
 }
 
 int uqc_server_release( uqc_server* s, long long id ) {
     if( !s ) return UQC_ERR_ARGUMENT;
+    std::lock_guard<std::recursive_mutex> lock( s->mu );
     auto it = s->reqs.find( id );
     if( it == s->reqs.end() || ( it->second.state != UQC_REQ_DONE && it->second.state != UQC_REQ_FAILED ) )
         return sfail( s, UQC_ERR_STATE, "request " + std::to_string( id ) + " is not finished" );
